@@ -1,0 +1,210 @@
+/* segpu: B200-native semi-Lagrangian advection and spectral-element
+ * Helmholtz/Poisson solves for SE (davelee2804/SE).
+ *
+ * C-ABI drop-in for SE's per-timestep hot path. Every object mirrors a
+ * reference class; the comment above each entry point names the reference
+ * interface it replaces (paths inside the SE checkout).
+ *
+ * Conventions
+ *  - Every call returns an int status: SE_OK (0) or a negative SE_ERR_* code;
+ *    se_last_error() gives a one-line message for the calling thread.
+ *  - Host arrays are in the reference layout: a field of ndofs components on
+ *    a mesh with nVertsTotal vertices is double[nVertsTotal][ndofs],
+ *    row-major, vertex index = j*nVerts[0] + i (x fastest), periodic duplicate
+ *    vertices stored (src/base/Field.cpp:17-35, src/base/Mesh.cpp:59-72).
+ *  - Device state (field values, solver vectors) lives in GPU memory owned by
+ *    the library; work is queued on the stream set by se_set_stream
+ *    (default: the legacy default stream). Calls that return host results
+ *    synchronise that stream.
+ *  - Objects are not thread-safe; use one object per thread or serialise.
+ *  - There is no CPU fallback: without a usable CUDA device every call that
+ *    needs one fails with SE_ERR_CUDA.
+ */
+#ifndef SEGPU_H
+#define SEGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SE_OK 0
+#define SE_ERR_ARG (-1)          /* invalid argument or handle */
+#define SE_ERR_OOM (-2)          /* device or host allocation failed */
+#define SE_ERR_CUDA (-3)         /* CUDA runtime error, or no CUDA device */
+#define SE_ERR_UNSUPPORTED (-4)  /* configuration the reference supports but this build does not */
+#define SE_ERR_NOT_CONVERGED (-5) /* solver stopped without converging; see se_solve_stats.reason */
+#define SE_ERR_TIMEOUT (-6)      /* a bounded device-side wait gave up */
+#define SE_ERR_DOMAIN (-7)       /* a departure point left the mesh after the periodic wrap */
+
+/* PETSc-compatible converged reasons reported in se_solve_stats.reason. */
+#define SE_KSP_CONVERGED_RTOL 2
+#define SE_KSP_CONVERGED_ATOL 3
+#define SE_KSP_DIVERGED_ITS (-3)
+#define SE_KSP_DIVERGED_DTOL (-4)
+#define SE_KSP_DIVERGED_INDEFINITE_PC (-8)
+#define SE_KSP_DIVERGED_NANORINF (-9)
+#define SE_KSP_DIVERGED_INDEFINITE_MAT (-10)
+
+typedef struct se_mesh se_mesh;
+typedef struct se_bcs se_bcs;
+typedef struct se_field se_field;
+typedef struct se_advector se_advector;
+typedef struct se_linsys se_linsys; /* a HelmholtzEqn or a PoissonEqn */
+
+/* Last error message of the calling thread ("" if none). */
+const char* se_last_error(void);
+/* Library version string. */
+const char* se_version(void);
+/* Stream for all subsequent device work of the calling process
+ * (a cudaStream_t passed as void*; NULL = legacy default stream). */
+int se_set_stream(void* stream);
+/* Block until all queued device work of the library is done. */
+int se_synchronize(void);
+
+/* ------------------------------------------------------------------ Mesh --
+ * Replaces Mesh::Mesh(name, nEls, "legendre", N, min, max, periodic)
+ * (src/base/Mesh.h:6, src/base/Mesh.cpp:17-84). Only the GLL ("legendre")
+ * element exists here; 2 <= N <= 12. */
+int se_mesh_create(const int nEls[2], int N, const double min[2], const double max[2],
+                   const int periodic[2], se_mesh** out);
+int se_mesh_destroy(se_mesh* mesh);
+/* nVerts[2], nVertsTotal (Mesh members, src/base/Mesh.h:11-13). */
+int se_mesh_sizes(const se_mesh* mesh, int nVerts[2], int* nVertsTotal);
+/* Mesh::verts as double[nVertsTotal][2] (src/base/Mesh.cpp:62-72). */
+int se_mesh_verts(const se_mesh* mesh, double* verts);
+/* GLL tables: abcissa[N+1], weights[N+1], dCij[(N+1)^2]
+ * (src/base/Legendre.cpp:28-95). Any pointer may be NULL. */
+int se_mesh_gll(const se_mesh* mesh, double* abcissa, double* weights, double* dCij);
+/* Mesh::GlobalToLocal at npts host points (src/base/Mesh.cpp:109-176),
+ * evaluated on the GPU: element index and local coordinates. */
+int se_mesh_global_to_local(const se_mesh* mesh, const double* pts, int npts, int* el,
+                            double* lcoord);
+
+/* ------------------------------------------------------------------- BCs --
+ * Replaces BCs::BCs(bottom, top, left, right, mesh, 0) for a scalar field
+ * (src/base/BCs.h:3, src/base/BCs.cpp:36-195). */
+int se_bcs_create(se_mesh* mesh, int bottom, int top, int left, int right, se_bcs** out);
+int se_bcs_destroy(se_bcs* bcs);
+/* Number of vector unknowns (nVertsTotal - size[0]). */
+int se_bcs_vec_size(const se_bcs* bcs, int* n);
+/* fieldToVecMap[nVertsTotal], vecToFieldMap[vec_size] (BCs members). */
+int se_bcs_maps(const se_bcs* bcs, int* field_to_vec, int* vec_to_field);
+
+/* ----------------------------------------------------------------- Field --
+ * Replaces Field(name, mesh, nDofs, bcs) with its public double** vals
+ * (src/base/Field.h:7-11). Values live on the GPU; upload/download move the
+ * whole [nVertsTotal][ndofs] array. 1 <= ndofs <= 2. bcs may be NULL. */
+int se_field_create(se_mesh* mesh, int ndofs, se_bcs* bcs, se_field** out);
+int se_field_destroy(se_field* field);
+int se_field_upload(se_field* field, const double* vals);
+int se_field_download(const se_field* field, double* vals);
+/* Device pointer to the values (double[nVertsTotal][ndofs]). */
+int se_field_device_ptr(se_field* field, double** dptr);
+/* Field::Copy (src/base/Field.cpp:49-55), device to device. */
+int se_field_copy(se_field* dst, const se_field* src);
+/* Field::PeriodicUpdate (src/base/Field.cpp:232-252). */
+int se_field_periodic_update(se_field* field);
+/* Field::Integrate(dof, average) (src/base/Field.cpp:181-200). */
+int se_field_integrate(const se_field* field, int dof, int average, double* out);
+/* Field::InterpGlobal at npts host points (src/base/Field.cpp:70-76);
+ * out is double[npts][ndofs]. */
+int se_field_interp_global(const se_field* field, const double* pts, int npts, double* out);
+
+/* -------------------------------------------------------------- Advector --
+ * Replaces Advector(field, velocity) (first order) and
+ * Advector(field, velocity, fieldMinusOne, velMinusOne) (second order),
+ * Advect(dt) and the public fieldSL (src/base/Advector.h:3-15,
+ * src/base/Advector.cpp:54-274). velocity fields have ndofs = 2 and share the
+ * field's mesh. N >= 3 (the reference's bicubic path for N < 3 is not built).
+ * The advector keeps pointers to the fields; they must outlive it. */
+int se_advector_create(se_field* field, se_field* velocity, se_field* field_prev,
+                       se_field* vel_prev, se_advector** out);
+int se_advector_destroy(se_advector* adv);
+/* Advector::Advect(dt): writes fieldSL. */
+int se_advect(se_advector* adv, double dt);
+/* The advector's fieldSL (owned by the advector). */
+int se_advector_field_sl(se_advector* adv, se_field** field_sl);
+/* Departure data of the last se_advect: element index of every vertex's
+ * departure point (second order: x1 then x2), as Mesh::GetEl assigns them.
+ * el has nVertsTotal (first order) or 2*nVertsTotal (second order) entries;
+ * xy (nullable) gets the coordinates. Enables recording on the first call. */
+int se_advector_departures(se_advector* adv, int* el, double* xy);
+
+/* ----------------------------------------------------------- linear solve --
+ * Solver options: SE's KSP options database entries
+ * (-<prefix>ksp_type cg -<prefix>pc_type jacobi -<prefix>ksp_rtol ...). */
+#define SE_NORM_PRECONDITIONED 0
+#define SE_NORM_UNPRECONDITIONED 1
+#define SE_NORM_NATURAL 2
+#define SE_MODE_REFERENCE 0 /* the reference's Laplacian with detJac forced to 1 (src/base/Operator.cpp:72) */
+#define SE_MODE_EXACT 1     /* the Laplacian with its true Jacobian */
+#define SE_PREC_FP64 0      /* every operation in FP64: the drop-in */
+#define SE_PREC_MIXED 1     /* FP32 inner CG, FP64 iterative refinement */
+typedef struct {
+  double rtol;    /* default 1e-5 (PETSc) */
+  double atol;    /* default 1e-50 */
+  double dtol;    /* default 1e5 */
+  int max_it;     /* default 10000 */
+  int norm_type;  /* SE_NORM_*, default preconditioned */
+  int mode;       /* SE_MODE_*, default SE_MODE_REFERENCE */
+  int precision;  /* SE_PREC_*, default SE_PREC_FP64 */
+  int inner_max_it; /* mixed: inner CG iteration cap per refinement step (default 2000) */
+  double inner_rtol; /* mixed: inner CG relative tolerance (default 1e-6) */
+} se_solver_opts;
+
+typedef struct {
+  int reason;     /* SE_KSP_* */
+  int its;        /* CG iterations (mixed: inner iterations summed) */
+  int outer_its;  /* mixed: refinement steps; FP64: 0 */
+  double rnorm;   /* final residual norm in the chosen norm */
+  double rnorm0;  /* initial residual norm in the chosen norm */
+} se_solve_stats;
+
+int se_solver_opts_default(se_solver_opts* opts);
+/* Parse a PETSc-style options string for one prefix, e.g.
+ * "-helm_ksp_rtol 1e-10 -helm_ksp_max_it 500", into opts. Unknown options
+ * and other prefixes are ignored; a ksp_type other than cg or a pc_type
+ * other than jacobi returns SE_ERR_UNSUPPORTED. */
+int se_solver_opts_parse(se_solver_opts* opts, const char* prefix, const char* options);
+
+/* Replaces HelmholtzEqn(sol, rhs, c, nu, dt, svvCutoff)
+ * (src/linsys/HelmholtzEqn.h:3, src/linsys/HelmholtzEqn.cpp:43-104):
+ * A = c*Mass + nu*dt*Laplacian on sol's mesh and boundary conditions.
+ * rhs may be NULL (right-hand side = Dirichlet lifting only).
+ * svvCutoff must be 0 (spectral vanishing viscosity is not built). */
+int se_helmholtz_create(se_field* sol, se_field* rhs, double c, double nu, double dt,
+                        int svvCutoff, const se_solver_opts* opts, se_linsys** out);
+/* Replaces PoissonEqn(sol, rhs, c) (src/linsys/PoissonEqn.cpp:30-80):
+ * A = c*Laplacian. */
+int se_poisson_create(se_field* sol, se_field* rhs, double c, const se_solver_opts* opts,
+                      se_linsys** out);
+int se_linsys_destroy(se_linsys* ls);
+int se_linsys_set_opts(se_linsys* ls, const se_solver_opts* opts);
+/* HelmholtzEqn::Assemble / PoissonEqn::Assemble
+ * (src/linsys/HelmholtzEqn.cpp:113-125): captures the Dirichlet lifting
+ * from the current boundary values of sol. Called by the first solve if not
+ * called before. */
+int se_linsys_assemble(se_linsys* ls);
+/* HelmholtzEqn::Solve(name, removeNullSpace) / PoissonEqn::Solve
+ * (src/linsys/HelmholtzEqn.cpp:127-158, src/linsys/PoissonEqn.cpp:102-134):
+ * f = Mass*rhs + lifting, CG + Jacobi with zero initial guess, solution
+ * copied into sol's unknowns and periodic copies. stats may be NULL.
+ * Returns SE_ERR_NOT_CONVERGED if the reason is negative. */
+int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats);
+/* y = A x on vector unknowns (device pointers, vec_size entries each). */
+int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev);
+/* The Jacobi diagonal of A (device pointer, vec_size entries). */
+int se_linsys_diagonal(se_linsys* ls, double* d_dev);
+int se_linsys_vec_size(const se_linsys* ls, int* n);
+
+/* ------------------------------------------------------------ utilities -- */
+/* CalcTimeStep(velocity, courantNo) (src/base/Utils.cpp:23-40). */
+int se_calc_time_step(const se_field* velocity, double courant, double* dt);
+/* FieldError(numeric, analytic, dof, normalise) (src/base/Utils.cpp:232-254). */
+int se_field_error(const se_field* numeric, const se_field* analytic, int dof, int normalise,
+                   double* err);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SEGPU_H */

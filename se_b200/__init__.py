@@ -1,0 +1,13 @@
+"""se_b200 -- B200-native semi-Lagrangian advection and spectral-element
+Helmholtz/Poisson solves for SE (davelee2804/SE).
+
+The product is ``libsegpu.so`` (C-ABI declared in ``include/segpu.h``),
+built in-tree by :mod:`se_b200.build`. :mod:`se_b200.segpu` mirrors the
+reference's classes (Mesh, BCs, Field, Advector, HelmholtzEqn, PoissonEqn)
+over that C-ABI.
+"""
+from .segpu import (BCs, Advector, CalcTimeStep, Field, FieldError, HelmholtzEqn, Mesh,  # noqa: F401
+                    PoissonEqn, SEError, load_library, set_stream, solver_opts, synchronize)
+
+__all__ = ["Mesh", "BCs", "Field", "Advector", "HelmholtzEqn", "PoissonEqn", "CalcTimeStep",
+           "FieldError", "SEError", "load_library", "set_stream", "synchronize", "solver_opts"]

@@ -1,0 +1,1012 @@
+// Host side of the segpu C-ABI (include/segpu.h): object lifetimes, the
+// mesh/GLL/boundary tables, device memory and kernel launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/segpu.h"
+#include "common.cuh"
+
+using namespace seg;
+
+// ------------------------------------------------------------- errors -----
+namespace {
+thread_local std::string g_err;
+cudaStream_t g_stream = nullptr;
+std::mutex g_scratch_mu;
+double* g_scratch = nullptr;  // reductions: partials + results
+constexpr int kScratch = 8192;
+unsigned* g_err_word = nullptr;  // device error bits of SL kernels
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(SE_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+#define CK(call)                                     \
+  do {                                               \
+    cudaError_t e_ = (call);                         \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+int ensure_globals() {
+  if (g_scratch) return SE_OK;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return fail(SE_ERR_CUDA, "no CUDA device available");
+  CK(cudaMalloc(&g_scratch, sizeof(double) * (kScratch + 8)));
+  CK(cudaMalloc(&g_err_word, sizeof(unsigned)));
+  CK(cudaMemset(g_err_word, 0, sizeof(unsigned)));
+  return SE_OK;
+}
+
+template <class T>
+int dalloc(T** p, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(e == cudaErrorMemoryAllocation ? SE_ERR_OOM : SE_ERR_CUDA, "cudaMalloc(%zu): %s",
+                n * sizeof(T), cudaGetErrorString(e));
+  }
+  return SE_OK;
+}
+template <class T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// ------------------------------------------------------------ GLL tables --
+// GLL nodes, weights and the cardinal-derivative matrix computed by the same
+// procedure as the reference's Legendre element (src/base/Legendre.cpp:15-95,
+// src/base/Jacobi.cpp:34-89, src/base/Element.cpp:54-106): the Legendre
+// polynomial P_N as monomial coefficients from the three-term recurrence,
+// evaluated by pow() over terms of matching parity, interior nodes by Newton
+// on P_N' from the left in steps of 1e-3, then mirrored and sorted. Keeping the
+// procedure keeps the nodes, and so the mesh vertex coordinates, identical to
+// the reference's bit for bit.
+struct Poly {
+  int n;
+  double c[SE_MAXN + 3];
+};
+void poly_next(Poly& out, int n, const Poly& m1, const Poly& m2) {
+  out.n = n;
+  std::fill(out.c, out.c + SE_MAXN + 3, 0.0);
+  const double a = 0.0;
+  double c1 = 2 * n * (2 * a + n) * (2 * a + 2 * n - 2);
+  double c2 = (2 * a + 2 * n - 1) * (2 * a + 2 * n) * (2 * a + 2 * n - 2);
+  double c3 = 2 * (a + n - 1) * (a + n - 1) * (2 * a + 2 * n);
+  c2 /= c1;
+  c3 /= c1;
+  for (int i = 0; i <= m1.n; i++) out.c[i + 1] += c2 * m1.c[i];
+  for (int i = 0; i <= m2.n; i++) out.c[i] -= c3 * m2.c[i];
+}
+double peval(const Poly& p, double x) {
+  double s = 0.0;
+  for (int i = p.n; i >= 0; i -= 2) s += p.c[i] * std::pow(x, i);
+  return s;
+}
+double pderiv(const Poly& p, double x) {
+  double s = 0.0;
+  for (int i = p.n; i >= 1; i -= 2) s += p.c[i] * i * std::pow(x, i - 1);
+  return s;
+}
+double pderiv2(const Poly& p, double x) {
+  double s = 0.0;
+  for (int i = p.n; i >= 2; i -= 2) s += p.c[i] * i * (i - 1) * std::pow(x, i - 2);
+  return s;
+}
+
+struct Gll {
+  int N;
+  double x[SE_MAXN1], w[SE_MAXN1], dC[SE_MAXN1 * SE_MAXN1], lambda[SE_MAXN1];
+  double Kh[SE_MAXN1 * SE_MAXN1];
+};
+void gll_build(int N, Gll& g) {
+  g.N = N;
+  Poly P[SE_MAXN + 3];
+  P[0].n = 0;
+  std::fill(P[0].c, P[0].c + SE_MAXN + 3, 0.0);
+  P[0].c[0] = 1.0;
+  P[1].n = 1;
+  std::fill(P[1].c, P[1].c + SE_MAXN + 3, 0.0);
+  P[1].c[1] = 1.0;
+  for (int i = 2; i <= N + 1; i++) poly_next(P[i], i, P[i - 1], P[i - 2]);
+  const Poly& PN = P[N];
+  double* x = g.x;
+  x[0] = -1.0;
+  const double step = 1.0e-3;
+  const int half = ((N + 1) % 2 == 1) ? N / 2 : (N + 1) / 2;
+  for (int i = 1; i < half; i++) {
+    double x0 = x[i - 1];
+    bool again;
+    do {
+      x0 += step;
+      double r = x0, rp;
+      for (int it = 0; it < 100000; it++) {
+        rp = r;
+        r = rp - pderiv(PN, rp) / pderiv2(PN, rp);
+        if (std::fabs(r - rp) < 1.0e-12) break;
+      }
+      x[i] = r;
+      again = r > 0.0 - step;
+      for (int k = 0; k < i && !again; k++)
+        if (std::fabs(x[k] - r) < 1.0e-6) again = true;
+    } while (again);
+    x[N - i] = -x[i];
+  }
+  x[N] = 1.0;
+  if ((N + 1) % 2 == 1) x[(N + 1) / 2] = 0.0;
+  // ascending selection sort (ties keep the first occurrence)
+  {
+    double tmp[SE_MAXN1];
+    bool done[SE_MAXN1] = {false};
+    int mi = 0;
+    for (int i = 0; i <= N; i++) {
+      double mv = 1.0e+99;
+      for (int j = 0; j <= N; j++)
+        if (!done[j] && x[j] < mv) {
+          mv = x[j];
+          mi = j;
+        }
+      tmp[i] = mv;
+      done[mi] = true;
+    }
+    std::copy(tmp, tmp + N + 1, x);
+  }
+  g.w[0] = 2.0 / ((N + 1) * N);
+  for (int i = 1; i < N; i++) g.w[i] = 2.0 / ((N + 1) * N * peval(PN, x[i]) * peval(PN, x[i]));
+  g.w[N] = 2.0 / ((N + 1) * N);
+  Poly PP;
+  poly_next(PP, N, P[N - 1], P[N - 2]);
+  for (int i = 0; i <= N; i++)
+    for (int j = 0; j <= N; j++) {
+      double v;
+      if (i == j && i == 0)
+        v = -0.25 * N * (N + 1);
+      else if (i == j && i == N)
+        v = +0.25 * N * (N + 1);
+      else if (i == j)
+        v = 0.0;
+      else
+        v = peval(PP, x[i]) / (peval(PP, x[j]) * (x[i] - x[j]));
+      g.dC[i * (N + 1) + j] = v;
+    }
+  // Lagrange product weights and the 1-D stiffness Kh = D^T diag(w) D, in
+  // extended precision from the double tables.
+  for (int j = 0; j <= N; j++) {
+    long double p = 1.0L;
+    for (int k = 0; k <= N; k++)
+      if (k != j) p *= (long double)x[j] - (long double)x[k];
+    g.lambda[j] = (double)(1.0L / p);
+  }
+  for (int a = 0; a <= N; a++)
+    for (int b = 0; b <= N; b++) {
+      long double s = 0.0L;
+      for (int q = 0; q <= N; q++)
+        s += (long double)g.w[q] * (long double)g.dC[q * (N + 1) + a] *
+             (long double)g.dC[q * (N + 1) + b];
+      g.Kh[a * (N + 1) + b] = (double)s;
+    }
+}
+}  // namespace
+
+// ------------------------------------------------------------- objects ----
+struct se_mesh {
+  Gll gll;
+  MeshDev dev;
+  int nVertsTotal;
+};
+struct se_bcs {
+  se_mesh* mesh;
+  int bottom, top, left, right;  // after the periodic adjustments
+  Dir d[2];                      // unknown ranges (operator fields filled later)
+  int vec_size;
+};
+struct se_field {
+  se_mesh* mesh;
+  int ndofs;
+  se_bcs* bcs;
+  double* vals;  // device [nVertsTotal][ndofs]
+};
+struct se_advector {
+  se_field *field, *vel, *field_prev, *vel_prev;
+  se_field* sl;
+  int* dep_el;
+  double* dep_xy;
+  bool record;
+};
+struct se_linsys {
+  se_field *sol, *rhs;
+  bool poisson;
+  double c, nu, dt;
+  se_solver_opts opts;
+  se_bcs* own_bcs;  // when sol has no BCs: natural boundaries, all vertices unknown
+  OpDev op;
+  int n;
+  bool assembled;
+  double *f, *lift, *x, *r, *z, *p0, *p1, *w;
+  // single-solve CG schedule
+  CgSolve* d_solve;
+  CgTile* d_tiles;
+  int* d_block_begin;
+  double* d_partials;
+  unsigned* d_bar;  // [0] arrivals, [1] generation
+  int* d_active;
+  unsigned* d_err;
+  int grid, nseg, seg_begin, seg_end;
+};
+
+namespace {
+// Unknown range along one direction (the rectangle the reference's BCs maps
+// select: src/base/BCs.cpp:36-195).
+Dir make_dir(const MeshDev& m, int d, bool lo_bc, bool hi_bc) {
+  Dir r;
+  r.nE = m.nEls[d];
+  r.N = m.N;
+  r.nV = m.nVerts[d];
+  r.periodic = m.periodic[d];
+  r.lo = lo_bc ? 1 : 0;
+  r.hi = (r.periodic || hi_bc) ? r.nV - 1 : r.nV;
+  return r;
+}
+
+void fill_op(se_linsys* ls) {
+  const se_mesh* me = ls->sol->mesh;
+  const MeshDev& m = me->dev;
+  const se_bcs* b = ls->sol->bcs ? ls->sol->bcs : ls->own_bcs;
+  OpDev& op = ls->op;
+  std::memset(&op, 0, sizeof(op));
+  op.d[0] = b->d[0];
+  op.d[1] = b->d[1];
+  op.G[0] = op.d[0].hi - op.d[0].lo;
+  op.G[1] = op.d[1].hi - op.d[1].lo;
+  const double hx = m.dx[0], hy = m.dx[1];
+  const double s = ls->poisson ? ls->c : ls->nu * ls->dt;
+  const double cm = ls->poisson ? 0.0 : ls->c;
+  op.alpha = cm * (0.5 * hx) * (0.5 * hy);
+  if (ls->opts.mode == SE_MODE_EXACT) {
+    op.beta[0] = s * (hy / hx);
+    op.beta[1] = s * (hx / hy);
+  } else {
+    // the reference's Laplacian drops detJ (src/base/Operator.cpp:72)
+    op.beta[0] = s * (2.0 / hx) * (2.0 / hx);
+    op.beta[1] = s * (2.0 / hy) * (2.0 / hy);
+  }
+  const int n = m.N + 1;
+  for (int a = 0; a < n * n; a++) op.Kh[a] = me->gll.Kh[a];
+  for (int a = 0; a < n; a++) op.w[a] = me->gll.w[a];
+}
+
+// Static schedule for one cooperative launch over several solves: tiles of
+// kCgTileX x kCgTileY unknowns, grouped solve by solve, split into `grid`
+// contiguous chunks; a segment is the run of one solve's tiles inside one
+// chunk, so each solve's segments are contiguous.
+struct Schedule {
+  std::vector<CgTile> tiles;
+  std::vector<int> block_begin;
+  std::vector<int> seg_begin, seg_end;  // per solve
+  int nseg = 0;
+};
+Schedule make_schedule(const std::vector<const OpDev*>& ops, int max_grid) {
+  Schedule S;
+  for (size_t s = 0; s < ops.size(); s++) {
+    const OpDev& op = *ops[s];
+    for (int y = 0; y < op.G[1]; y += kCgTileY)
+      for (int x = 0; x < op.G[0]; x += kCgTileX) S.tiles.push_back({(int)s, x, y, 0});
+  }
+  const int nt = (int)S.tiles.size();
+  int grid = std::max(1, std::min(max_grid, nt));
+  S.block_begin.resize(grid + 1);
+  for (int b = 0; b <= grid; b++) S.block_begin[b] = (int)((long)nt * b / grid);
+  S.seg_begin.assign(ops.size(), -1);
+  S.seg_end.assign(ops.size(), -1);
+  int seg = -1;
+  for (int b = 0; b < grid; b++) {
+    int last = -1;
+    for (int t = S.block_begin[b]; t < S.block_begin[b + 1]; t++) {
+      if (S.tiles[t].solve != last) {
+        ++seg;
+        last = S.tiles[t].solve;
+        if (S.seg_begin[last] < 0) S.seg_begin[last] = seg;
+        S.seg_end[last] = seg + 1;
+      }
+      S.tiles[t].seg = seg;
+    }
+  }
+  S.nseg = seg + 1;
+  return S;
+}
+
+
+}  // namespace
+
+namespace {
+CgSolve make_solve(const se_linsys* ls, const double* b, double* x, double rtol, double atol,
+                   double dtol, int max_it, int remove_null) {
+  CgSolve cs;
+  std::memset(&cs, 0, sizeof(cs));
+  cs.op = ls->op;
+  cs.b = b;
+  cs.x = x;
+  cs.r = ls->r;
+  cs.z = ls->z;
+  cs.p0 = ls->p0;
+  cs.p1 = ls->p1;
+  cs.w = ls->w;
+  cs.rtol = rtol;
+  cs.atol = atol;
+  cs.dtol = dtol;
+  cs.max_it = max_it;
+  cs.norm_type = ls->opts.norm_type;
+  cs.remove_null = remove_null;
+  cs.n = ls->n;
+  cs.seg_begin = ls->seg_begin;
+  cs.seg_end = ls->seg_end;
+  return cs;
+}
+
+void linsys_free(se_linsys* ls) {
+  dfree(ls->f);
+  dfree(ls->lift);
+  dfree(ls->x);
+  dfree(ls->r);
+  dfree(ls->z);
+  dfree(ls->p0);
+  dfree(ls->p1);
+  dfree(ls->w);
+  dfree(ls->d_solve);
+  dfree(ls->d_tiles);
+  dfree(ls->d_block_begin);
+  dfree(ls->d_partials);
+  dfree(ls->d_bar);
+  dfree(ls->d_active);
+  dfree(ls->d_err);
+  delete ls->own_bcs;
+  delete ls;
+}
+
+int linsys_alloc(se_linsys* ls) {
+  const int n = ls->n;
+  int rc;
+  if ((rc = dalloc(&ls->f, n)) || (rc = dalloc(&ls->lift, n)) || (rc = dalloc(&ls->x, n)) ||
+      (rc = dalloc(&ls->r, n)) || (rc = dalloc(&ls->z, n)) || (rc = dalloc(&ls->p0, n)) ||
+      (rc = dalloc(&ls->p1, n)) || (rc = dalloc(&ls->w, n)))
+    return rc;
+  CK(cudaMemset(ls->lift, 0, sizeof(double) * n));
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  const int maxg = cg_max_grid(dev);
+  if (maxg <= 0) return fail(SE_ERR_CUDA, "cannot size the cooperative CG launch");
+  Schedule S = make_schedule({&ls->op}, maxg);
+  ls->grid = (int)S.block_begin.size() - 1;
+  ls->nseg = S.nseg;
+  ls->seg_begin = S.seg_begin[0];
+  ls->seg_end = S.seg_end[0];
+  if ((rc = dalloc(&ls->d_solve, 1)) || (rc = dalloc(&ls->d_tiles, S.tiles.size())) ||
+      (rc = dalloc(&ls->d_block_begin, S.block_begin.size())) ||
+      (rc = dalloc(&ls->d_partials, (size_t)S.nseg * 4)) || (rc = dalloc(&ls->d_bar, 2)) ||
+      (rc = dalloc(&ls->d_active, 1)) || (rc = dalloc(&ls->d_err, 1)))
+    return rc;
+  CK(cudaMemcpy(ls->d_tiles, S.tiles.data(), sizeof(CgTile) * S.tiles.size(),
+                cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(ls->d_block_begin, S.block_begin.data(), sizeof(int) * S.block_begin.size(),
+                cudaMemcpyHostToDevice));
+  CK(cudaMemset(ls->d_bar, 0, 2 * sizeof(unsigned)));
+  CK(cudaMemset(ls->d_err, 0, sizeof(unsigned)));
+  return SE_OK;
+}
+
+// Run the persistent CG for A x = b on this system's schedule; fills stats.
+int run_cg(se_linsys* ls, const double* b, double* x, double rtol, double atol, double dtol,
+           int max_it, int remove_null, CgSolve* out_state) {
+  CgSolve cs = make_solve(ls, b, x, rtol, atol, dtol, max_it, remove_null);
+  cudaStream_t s = g_stream;
+  CK(cudaMemcpyAsync(ls->d_solve, &cs, sizeof(cs), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(ls->d_bar, 0, sizeof(unsigned), s));  // arrivals; generation keeps counting
+  CK(cudaMemsetAsync(ls->d_err, 0, sizeof(unsigned), s));
+  CgBatch B;
+  B.solves = ls->d_solve;
+  B.nsolves = 1;
+  B.tiles = ls->d_tiles;
+  B.block_tile_begin = ls->d_block_begin;
+  B.partials = ls->d_partials;
+  B.nseg = ls->nseg;
+  B.bar_count = ls->d_bar;
+  B.bar_gen = ls->d_bar + 1;
+  B.n_active = ls->d_active;
+  B.err = ls->d_err;
+  CK(launch_cg(B, ls->grid, s));
+  unsigned err = 0;
+  CK(cudaMemcpyAsync(out_state, ls->d_solve, sizeof(CgSolve), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&err, ls->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (err & KERR_BARRIER_TIMEOUT) return fail(SE_ERR_TIMEOUT, "CG grid barrier timed out");
+  return SE_OK;
+}
+
+int check_field(const se_field* f) {
+  if (!f || !f->mesh || !f->vals) return fail(SE_ERR_ARG, "null field");
+  return SE_OK;
+}
+}  // namespace
+
+// =========================================================== C-ABI ========
+extern "C" {
+
+const char* se_last_error(void) { return g_err.c_str(); }
+const char* se_version(void) { return "segpu 0.1 (sm_100a)"; }
+
+int se_set_stream(void* stream) {
+  g_stream = (cudaStream_t)stream;
+  return SE_OK;
+}
+int se_synchronize(void) {
+  CK(cudaStreamSynchronize(g_stream));
+  return SE_OK;
+}
+
+// ---------------------------------------------------------------- mesh ----
+int se_mesh_create(const int nEls[2], int N, const double min[2], const double max[2],
+                   const int periodic[2], se_mesh** out) {
+  if (!out || !nEls || !min || !max || !periodic) return fail(SE_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (N < 2 || N > SE_MAXN)
+    return fail(SE_ERR_UNSUPPORTED, "polynomial order %d outside [2, %d]", N, SE_MAXN);
+  if (nEls[0] < 1 || nEls[1] < 1) return fail(SE_ERR_ARG, "element counts must be positive");
+  if (!(max[0] > min[0]) || !(max[1] > min[1])) return fail(SE_ERR_ARG, "empty domain");
+  long nv = (long)(nEls[0] * (long)N + 1) * (nEls[1] * (long)N + 1);
+  if (nv > (1L << 30)) return fail(SE_ERR_UNSUPPORTED, "mesh too large");
+  se_mesh* m = new se_mesh();
+  gll_build(N, m->gll);
+  MeshDev& d = m->dev;
+  std::memset(&d, 0, sizeof(d));
+  d.N = N;
+  for (int k = 0; k < 2; k++) {
+    d.nEls[k] = nEls[k];
+    d.nVerts[k] = nEls[k] * N + 1;
+    d.periodic[k] = periodic[k] != 0;
+    d.min[k] = min[k];
+    d.max[k] = max[k];
+    d.dx[k] = (d.max[k] - d.min[k]) / d.nEls[k];
+    d.two_over_dx[k] = 2.0 / d.dx[k];
+    d.span[k] = d.max[k] - d.min[k];
+    d.nspan[k] = d.min[k] - d.max[k];
+  }
+  for (int i = 0; i <= N; i++) {
+    d.abcissa[i] = m->gll.x[i];
+    d.lambda[i] = m->gll.lambda[i];
+    d.w[i] = m->gll.w[i];
+  }
+  for (int i = 0; i < (N + 1) * (N + 1); i++) d.dC[i] = m->gll.dC[i];
+  m->nVertsTotal = d.nVerts[0] * d.nVerts[1];
+  *out = m;
+  return SE_OK;
+}
+int se_mesh_destroy(se_mesh* mesh) {
+  delete mesh;
+  return SE_OK;
+}
+int se_mesh_sizes(const se_mesh* mesh, int nVerts[2], int* nVertsTotal) {
+  if (!mesh) return fail(SE_ERR_ARG, "null mesh");
+  if (nVerts) {
+    nVerts[0] = mesh->dev.nVerts[0];
+    nVerts[1] = mesh->dev.nVerts[1];
+  }
+  if (nVertsTotal) *nVertsTotal = mesh->nVertsTotal;
+  return SE_OK;
+}
+int se_mesh_verts(const se_mesh* mesh, double* verts) {
+  if (!mesh || !verts) return fail(SE_ERR_ARG, "null argument");
+  const MeshDev& d = mesh->dev;
+  for (int v = 0; v < mesh->nVertsTotal; v++) {
+    int t[2] = {v % d.nVerts[0], v / d.nVerts[0]};
+    for (int k = 0; k < 2; k++) {
+      int e = t[k] / d.N;
+      double l = d.abcissa[t[k] % d.N];
+      verts[2 * v + k] = d.min[k] + e * d.dx[k] + ((l + 1.0) / 2.0) * d.dx[k];
+    }
+  }
+  return SE_OK;
+}
+int se_mesh_gll(const se_mesh* mesh, double* abcissa, double* weights, double* dCij) {
+  if (!mesh) return fail(SE_ERR_ARG, "null mesh");
+  const int n = mesh->dev.N + 1;
+  if (abcissa) std::memcpy(abcissa, mesh->gll.x, sizeof(double) * n);
+  if (weights) std::memcpy(weights, mesh->gll.w, sizeof(double) * n);
+  if (dCij) std::memcpy(dCij, mesh->gll.dC, sizeof(double) * n * n);
+  return SE_OK;
+}
+int se_mesh_global_to_local(const se_mesh* mesh, const double* pts, int npts, int* el,
+                            double* lcoord) {
+  if (!mesh || npts < 0 || (npts && (!pts || !el || !lcoord)))
+    return fail(SE_ERR_ARG, "bad argument");
+  if (npts == 0) return SE_OK;
+  double *dp = nullptr, *dl = nullptr;
+  int* de = nullptr;
+  int rc;
+  if ((rc = dalloc(&dp, 2 * (size_t)npts)) || (rc = dalloc(&dl, 2 * (size_t)npts)) ||
+      (rc = dalloc(&de, npts))) {
+    dfree(dp);
+    dfree(dl);
+    dfree(de);
+    return rc;
+  }
+  cudaStream_t s = g_stream;
+  cudaError_t e = cudaMemcpyAsync(dp, pts, sizeof(double) * 2 * npts, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = launch_global_to_local(mesh->dev, dp, npts, de, dl, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(el, de, sizeof(int) * npts, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(lcoord, dl, sizeof(double) * 2 * npts, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  dfree(dp);
+  dfree(dl);
+  dfree(de);
+  if (e != cudaSuccess) return cuda_fail(e, "global_to_local");
+  return SE_OK;
+}
+
+// ----------------------------------------------------------------- bcs ----
+int se_bcs_create(se_mesh* mesh, int bottom, int top, int left, int right, se_bcs** out) {
+  if (!mesh || !out) return fail(SE_ERR_ARG, "null argument");
+  *out = nullptr;
+  const MeshDev& m = mesh->dev;
+  bool b = bottom != 0, t = top != 0, l = left != 0, r = right != 0;
+  // src/base/BCs.cpp:51-58: periodic and wall conditions exclude each other
+  if ((b || t) && m.periodic[1])
+    return fail(SE_ERR_ARG, "both periodic and non-periodic conditions in y");
+  if ((l || r) && m.periodic[0])
+    return fail(SE_ERR_ARG, "both periodic and non-periodic conditions in x");
+  // src/base/BCs.cpp:113-194: the reference builds maps for no/full
+  // periodicity and for periodicity in x only.
+  if (m.periodic[1] && !m.periodic[0])
+    return fail(SE_ERR_UNSUPPORTED, "periodic in y only is not built by the reference");
+  if (m.periodic[0] && !m.periodic[1] && b && !t)
+    return fail(SE_ERR_UNSUPPORTED, "periodic x with a bottom wall only (reference: bc error)");
+  se_bcs* bc = new se_bcs();
+  bc->mesh = mesh;
+  bc->bottom = b;
+  bc->top = t || m.periodic[1];
+  bc->left = l;
+  bc->right = r || m.periodic[0];
+  bc->d[0] = make_dir(m, 0, l, r);
+  bc->d[1] = make_dir(m, 1, b, t);
+  bc->vec_size = (bc->d[0].hi - bc->d[0].lo) * (bc->d[1].hi - bc->d[1].lo);
+  *out = bc;
+  return SE_OK;
+}
+int se_bcs_destroy(se_bcs* bcs) {
+  delete bcs;
+  return SE_OK;
+}
+int se_bcs_vec_size(const se_bcs* bcs, int* n) {
+  if (!bcs || !n) return fail(SE_ERR_ARG, "null argument");
+  *n = bcs->vec_size;
+  return SE_OK;
+}
+int se_bcs_maps(const se_bcs* bcs, int* field_to_vec, int* vec_to_field) {
+  if (!bcs) return fail(SE_ERR_ARG, "null bcs");
+  const MeshDev& m = bcs->mesh->dev;
+  const Dir &dx = bcs->d[0], &dy = bcs->d[1];
+  const int G0 = dx.hi - dx.lo, nvx = m.nVerts[0], nvy = m.nVerts[1];
+  for (int j = 0; j < nvy; j++)
+    for (int i = 0; i < nvx; i++) {
+      int gi = (dx.periodic && i == nvx - 1) ? 0 : i;
+      int gj = (dy.periodic && j == nvy - 1) ? 0 : j;
+      bool in = gi >= dx.lo && gi < dx.hi && gj >= dy.lo && gj < dy.hi;
+      int v = in ? (gj - dy.lo) * G0 + (gi - dx.lo) : -1;
+      if (field_to_vec) field_to_vec[j * nvx + i] = v;
+      if (vec_to_field && in && gi == i && gj == j) vec_to_field[v] = j * nvx + i;
+    }
+  return SE_OK;
+}
+
+// --------------------------------------------------------------- field ----
+int se_field_create(se_mesh* mesh, int ndofs, se_bcs* bcs, se_field** out) {
+  if (!mesh || !out) return fail(SE_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (ndofs < 1 || ndofs > 2) return fail(SE_ERR_UNSUPPORTED, "ndofs %d not in [1, 2]", ndofs);
+  if (bcs && bcs->mesh != mesh) return fail(SE_ERR_ARG, "bcs built on another mesh");
+  if (int rc = ensure_globals()) return rc;
+  se_field* f = new se_field();
+  f->mesh = mesh;
+  f->ndofs = ndofs;
+  f->bcs = bcs;
+  int rc = dalloc(&f->vals, (size_t)mesh->nVertsTotal * ndofs);
+  if (rc) {
+    delete f;
+    return rc;
+  }
+  cudaError_t e = cudaMemsetAsync(f->vals, 0, sizeof(double) * mesh->nVertsTotal * ndofs, g_stream);
+  if (e != cudaSuccess) {
+    dfree(f->vals);
+    delete f;
+    return cuda_fail(e, "cudaMemset");
+  }
+  *out = f;
+  return SE_OK;
+}
+int se_field_destroy(se_field* field) {
+  if (!field) return SE_OK;
+  dfree(field->vals);
+  delete field;
+  return SE_OK;
+}
+int se_field_upload(se_field* field, const double* vals) {
+  if (int rc = check_field(field)) return rc;
+  if (!vals) return fail(SE_ERR_ARG, "null host array");
+  CK(cudaMemcpyAsync(field->vals, vals, sizeof(double) * field->mesh->nVertsTotal * field->ndofs,
+                     cudaMemcpyHostToDevice, g_stream));
+  return SE_OK;
+}
+int se_field_download(const se_field* field, double* vals) {
+  if (int rc = check_field(field)) return rc;
+  if (!vals) return fail(SE_ERR_ARG, "null host array");
+  CK(cudaMemcpyAsync(vals, field->vals, sizeof(double) * field->mesh->nVertsTotal * field->ndofs,
+                     cudaMemcpyDeviceToHost, g_stream));
+  CK(cudaStreamSynchronize(g_stream));
+  return SE_OK;
+}
+int se_field_device_ptr(se_field* field, double** dptr) {
+  if (int rc = check_field(field)) return rc;
+  if (!dptr) return fail(SE_ERR_ARG, "null argument");
+  *dptr = field->vals;
+  return SE_OK;
+}
+int se_field_copy(se_field* dst, const se_field* src) {
+  if (int rc = check_field(dst)) return rc;
+  if (int rc = check_field(src)) return rc;
+  if (dst->mesh->nVertsTotal != src->mesh->nVertsTotal || dst->ndofs != src->ndofs)
+    return fail(SE_ERR_ARG, "field shapes differ");
+  CK(cudaMemcpyAsync(dst->vals, src->vals, sizeof(double) * dst->mesh->nVertsTotal * dst->ndofs,
+                     cudaMemcpyDeviceToDevice, g_stream));
+  return SE_OK;
+}
+int se_field_periodic_update(se_field* field) {
+  if (int rc = check_field(field)) return rc;
+  CK(launch_periodic_update(field->mesh->dev, field->ndofs, field->vals, g_stream));
+  return SE_OK;
+}
+int se_field_integrate(const se_field* field, int dof, int average, double* out) {
+  if (int rc = check_field(field)) return rc;
+  if (!out || dof < 0 || dof >= field->ndofs) return fail(SE_ERR_ARG, "bad argument");
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  CK(launch_quadrature(field->mesh->dev, field->ndofs, dof, field->vals, nullptr, g_scratch,
+                       kScratch, g_scratch + kScratch, g_stream));
+  double r[2];
+  CK(cudaMemcpyAsync(r, g_scratch + kScratch, sizeof(r), cudaMemcpyDeviceToHost, g_stream));
+  CK(cudaStreamSynchronize(g_stream));
+  const MeshDev& m = field->mesh->dev;
+  *out = average ? r[0] / ((m.max[0] - m.min[0]) * (m.max[1] - m.min[1])) : r[0];
+  return SE_OK;
+}
+int se_field_interp_global(const se_field* field, const double* pts, int npts, double* out) {
+  if (int rc = check_field(field)) return rc;
+  if (npts < 0 || (npts && (!pts || !out))) return fail(SE_ERR_ARG, "bad argument");
+  if (npts == 0) return SE_OK;
+  double *dp = nullptr, *dout = nullptr;
+  int rc;
+  if ((rc = dalloc(&dp, 2 * (size_t)npts)) || (rc = dalloc(&dout, (size_t)npts * field->ndofs))) {
+    dfree(dp);
+    dfree(dout);
+    return rc;
+  }
+  cudaStream_t s = g_stream;
+  cudaError_t e = cudaMemcpyAsync(dp, pts, sizeof(double) * 2 * npts, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = launch_interp_global(field->mesh->dev, field->ndofs, field->vals, dp, npts, dout, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, dout, sizeof(double) * npts * field->ndofs, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  dfree(dp);
+  dfree(dout);
+  if (e != cudaSuccess) return cuda_fail(e, "interp_global");
+  return SE_OK;
+}
+
+// ------------------------------------------------------------ advector ----
+int se_advector_create(se_field* field, se_field* velocity, se_field* field_prev,
+                       se_field* vel_prev, se_advector** out) {
+  if (!out) return fail(SE_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (int rc = check_field(field)) return rc;
+  if (int rc = check_field(velocity)) return rc;
+  if (velocity->ndofs != 2) return fail(SE_ERR_ARG, "velocity needs 2 components");
+  if (velocity->mesh != field->mesh) return fail(SE_ERR_ARG, "velocity on another mesh");
+  if ((field_prev == nullptr) != (vel_prev == nullptr))
+    return fail(SE_ERR_ARG, "second order needs both previous fields");
+  if (field_prev) {
+    if (int rc = check_field(field_prev)) return rc;
+    if (int rc = check_field(vel_prev)) return rc;
+    if (field_prev->mesh != field->mesh || vel_prev->mesh != field->mesh ||
+        field_prev->ndofs != field->ndofs || vel_prev->ndofs != 2)
+      return fail(SE_ERR_ARG, "previous fields do not match");
+  }
+  if (field->mesh->dev.N < 3)
+    return fail(SE_ERR_UNSUPPORTED, "N < 3 uses the reference's bicubic path, not built");
+  se_advector* a = new se_advector();
+  a->field = field;
+  a->vel = velocity;
+  a->field_prev = field_prev;
+  a->vel_prev = vel_prev;
+  int rc = se_field_create(field->mesh, field->ndofs, field->bcs, &a->sl);
+  if (rc) {
+    delete a;
+    return rc;
+  }
+  // fieldSL starts as a copy of the field (src/base/Advector.cpp:64-65)
+  if ((rc = se_field_copy(a->sl, field))) {
+    se_field_destroy(a->sl);
+    delete a;
+    return rc;
+  }
+  *out = a;
+  return SE_OK;
+}
+int se_advector_destroy(se_advector* adv) {
+  if (!adv) return SE_OK;
+  se_field_destroy(adv->sl);
+  dfree(adv->dep_el);
+  dfree(adv->dep_xy);
+  delete adv;
+  return SE_OK;
+}
+int se_advect(se_advector* adv, double dt) {
+  if (!adv) return fail(SE_ERR_ARG, "null advector");
+  const se_mesh* me = adv->field->mesh;
+  CK(cudaMemsetAsync(g_err_word, 0, sizeof(unsigned), g_stream));
+  CK(launch_sl(me->dev, adv->field->ndofs, adv->field->vals, adv->vel->vals,
+               adv->field_prev ? adv->field_prev->vals : nullptr,
+               adv->vel_prev ? adv->vel_prev->vals : nullptr, dt, adv->sl->vals,
+               adv->record ? adv->dep_el : nullptr, adv->record ? adv->dep_xy : nullptr,
+               g_err_word, g_stream));
+  return SE_OK;
+}
+int se_advector_field_sl(se_advector* adv, se_field** field_sl) {
+  if (!adv || !field_sl) return fail(SE_ERR_ARG, "null argument");
+  *field_sl = adv->sl;
+  return SE_OK;
+}
+int se_advector_departures(se_advector* adv, int* el, double* xy) {
+  if (!adv) return fail(SE_ERR_ARG, "null advector");
+  const int nv = adv->field->mesh->nVertsTotal;
+  const int k = adv->field_prev ? 2 : 1;
+  if (!adv->record) {
+    int rc;
+    if ((rc = dalloc(&adv->dep_el, (size_t)k * nv)) || (rc = dalloc(&adv->dep_xy, (size_t)2 * k * nv)))
+      return rc;
+    adv->record = true;
+    return fail(SE_ERR_ARG, "departure recording enabled; call se_advect first");
+  }
+  if (el) CK(cudaMemcpyAsync(el, adv->dep_el, sizeof(int) * k * nv, cudaMemcpyDeviceToHost, g_stream));
+  if (xy)
+    CK(cudaMemcpyAsync(xy, adv->dep_xy, sizeof(double) * 2 * k * nv, cudaMemcpyDeviceToHost,
+                       g_stream));
+  CK(cudaStreamSynchronize(g_stream));
+  unsigned err = 0;
+  CK(cudaMemcpy(&err, g_err_word, sizeof(err), cudaMemcpyDeviceToHost));
+  if (err & KERR_DOMAIN) return fail(SE_ERR_DOMAIN, "a departure point left the mesh");
+  return SE_OK;
+}
+
+// -------------------------------------------------------------- linsys ----
+int se_solver_opts_default(se_solver_opts* o) {
+  if (!o) return fail(SE_ERR_ARG, "null options");
+  o->rtol = 1e-5;
+  o->atol = 1e-50;
+  o->dtol = 1e5;
+  o->max_it = 10000;
+  o->norm_type = SE_NORM_PRECONDITIONED;
+  o->mode = SE_MODE_REFERENCE;
+  o->precision = SE_PREC_FP64;
+  o->inner_max_it = 2000;
+  o->inner_rtol = 1e-6;
+  return SE_OK;
+}
+
+int se_solver_opts_parse(se_solver_opts* o, const char* prefix, const char* options) {
+  if (!o || !options) return fail(SE_ERR_ARG, "null argument");
+  std::string pre = std::string("-") + (prefix ? prefix : "");
+  std::vector<std::string> tok;
+  {
+    std::string cur;
+    for (const char* p = options;; p++) {
+      if (*p == 0 || *p == ' ' || *p == '\t' || *p == '\n') {
+        if (!cur.empty()) tok.push_back(cur);
+        cur.clear();
+        if (*p == 0) break;
+      } else {
+        cur.push_back(*p);
+      }
+    }
+  }
+  for (size_t i = 0; i < tok.size(); i++) {
+    const std::string& t = tok[i];
+    if (t.compare(0, pre.size(), pre) != 0) continue;
+    std::string key = t.substr(pre.size());
+    std::string val = (i + 1 < tok.size() && tok[i + 1][0] != '-') ? tok[i + 1] : "";
+    if (!val.empty()) i++;
+    char* end = nullptr;
+    if (key == "ksp_type") {
+      if (val != "cg") return fail(SE_ERR_UNSUPPORTED, "ksp_type %s (only cg)", val.c_str());
+    } else if (key == "pc_type") {
+      if (val != "jacobi") return fail(SE_ERR_UNSUPPORTED, "pc_type %s (only jacobi)", val.c_str());
+    } else if (key == "ksp_rtol") {
+      o->rtol = std::strtod(val.c_str(), &end);
+    } else if (key == "ksp_atol") {
+      o->atol = std::strtod(val.c_str(), &end);
+    } else if (key == "ksp_divtol") {
+      o->dtol = std::strtod(val.c_str(), &end);
+    } else if (key == "ksp_max_it") {
+      o->max_it = (int)std::strtol(val.c_str(), &end, 10);
+    } else if (key == "ksp_norm_type") {
+      if (val == "preconditioned") o->norm_type = SE_NORM_PRECONDITIONED;
+      else if (val == "unpreconditioned") o->norm_type = SE_NORM_UNPRECONDITIONED;
+      else if (val == "natural") o->norm_type = SE_NORM_NATURAL;
+      else return fail(SE_ERR_UNSUPPORTED, "ksp_norm_type %s", val.c_str());
+    }
+  }
+  return SE_OK;
+}
+
+namespace {
+int linsys_create(se_field* sol, se_field* rhs, bool poisson, double c, double nu, double dt,
+                  const se_solver_opts* opts, se_linsys** out) {
+  if (!out) return fail(SE_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (int rc = check_field(sol)) return rc;
+  if (sol->ndofs != 1) return fail(SE_ERR_UNSUPPORTED, "only scalar solution fields");
+  if (rhs) {
+    if (int rc = check_field(rhs)) return rc;
+    if (rhs->mesh != sol->mesh || rhs->ndofs != 1) return fail(SE_ERR_ARG, "rhs does not match sol");
+  }
+  const MeshDev& m = sol->mesh->dev;
+  for (int k = 0; k < 2; k++)
+    if (m.periodic[k] && m.nEls[k] < 2)
+      return fail(SE_ERR_UNSUPPORTED, "a periodic direction needs at least 2 elements");
+  se_linsys* ls = new se_linsys();
+  std::memset((void*)ls, 0, sizeof(*ls));
+  ls->sol = sol;
+  ls->rhs = rhs;
+  ls->poisson = poisson;
+  ls->c = c;
+  ls->nu = nu;
+  ls->dt = dt;
+  if (opts) ls->opts = *opts; else se_solver_opts_default(&ls->opts);
+  if (!sol->bcs) {
+    int rc = se_bcs_create(sol->mesh, 0, 0, 0, 0, &ls->own_bcs);
+    if (rc) {
+      delete ls;
+      return rc;
+    }
+  }
+  fill_op(ls);
+  ls->n = ls->op.G[0] * ls->op.G[1];
+  int rc = linsys_alloc(ls);
+  if (rc) {
+    linsys_free(ls);
+    return rc;
+  }
+  *out = ls;
+  return SE_OK;
+}
+}  // namespace
+
+int se_helmholtz_create(se_field* sol, se_field* rhs, double c, double nu, double dt,
+                        int svvCutoff, const se_solver_opts* opts, se_linsys** out) {
+  if (svvCutoff != 0) return fail(SE_ERR_UNSUPPORTED, "spectral vanishing viscosity not built");
+  return linsys_create(sol, rhs, false, c, nu, dt, opts, out);
+}
+int se_poisson_create(se_field* sol, se_field* rhs, double c, const se_solver_opts* opts,
+                      se_linsys** out) {
+  return linsys_create(sol, rhs, true, c, 0.0, 0.0, opts, out);
+}
+int se_linsys_destroy(se_linsys* ls) {
+  if (ls) linsys_free(ls);
+  return SE_OK;
+}
+int se_linsys_set_opts(se_linsys* ls, const se_solver_opts* opts) {
+  if (!ls || !opts) return fail(SE_ERR_ARG, "null argument");
+  int old_mode = ls->opts.mode;
+  ls->opts = *opts;
+  if (opts->mode != old_mode) {
+    fill_op(ls);
+    ls->assembled = false;
+  }
+  return SE_OK;
+}
+int se_linsys_assemble(se_linsys* ls) {
+  if (!ls) return fail(SE_ERR_ARG, "null system");
+  CK(launch_lift(ls->op, ls->sol->mesh->dev, ls->sol->vals, ls->lift, g_stream));
+  ls->assembled = true;
+  return SE_OK;
+}
+int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats) {
+  if (!ls) return fail(SE_ERR_ARG, "null system");
+  if (!ls->assembled)
+    if (int rc = se_linsys_assemble(ls)) return rc;
+  const MeshDev& m = ls->sol->mesh->dev;
+  CK(launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, g_stream));
+  CgSolve st;
+  int rc = run_cg(ls, ls->f, ls->x, ls->opts.rtol, ls->opts.atol, ls->opts.dtol, ls->opts.max_it,
+                  remove_null_space, &st);
+  if (rc) return rc;
+  CK(launch_update_field(ls->op, m, ls->x, ls->sol->vals, g_stream));
+  if (stats) {
+    stats->reason = st.reason;
+    stats->its = st.its;
+    stats->outer_its = 0;
+    stats->rnorm = st.dp;
+    stats->rnorm0 = st.rnorm0;
+  }
+  if (st.reason < 0) return fail(SE_ERR_NOT_CONVERGED, "KSP diverged, reason %d after %d its",
+                                 st.reason, st.its);
+  return SE_OK;
+}
+int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev) {
+  if (!ls || !x_dev || !y_dev) return fail(SE_ERR_ARG, "null argument");
+  CK(launch_op_apply(ls->op, x_dev, y_dev, g_stream));
+  return SE_OK;
+}
+int se_linsys_diagonal(se_linsys* ls, double* d_dev) {
+  if (!ls || !d_dev) return fail(SE_ERR_ARG, "null argument");
+  CK(launch_op_diag(ls->op, d_dev, g_stream));
+  return SE_OK;
+}
+int se_linsys_vec_size(const se_linsys* ls, int* n) {
+  if (!ls || !n) return fail(SE_ERR_ARG, "null argument");
+  *n = ls->n;
+  return SE_OK;
+}
+
+// ----------------------------------------------------------- utilities ----
+int se_calc_time_step(const se_field* velocity, double courant, double* dt) {
+  if (int rc = check_field(velocity)) return rc;
+  if (velocity->ndofs != 2 || !dt) return fail(SE_ERR_ARG, "bad argument");
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  CK(launch_max_speed_sq(velocity->mesh->nVertsTotal, velocity->vals, g_scratch, kScratch,
+                         g_scratch + kScratch, g_stream));
+  double mx = 0.0;
+  CK(cudaMemcpyAsync(&mx, g_scratch + kScratch, sizeof(double), cudaMemcpyDeviceToHost, g_stream));
+  CK(cudaStreamSynchronize(g_stream));
+  const MeshDev& m = velocity->mesh->dev;
+  double minSep = m.dx[0] < m.dx[1] ? m.dx[0] : m.dx[1];
+  *dt = courant * minSep / std::sqrt(mx);
+  return SE_OK;
+}
+int se_field_error(const se_field* numeric, const se_field* analytic, int dof, int normalise,
+                   double* err) {
+  if (int rc = check_field(numeric)) return rc;
+  if (int rc = check_field(analytic)) return rc;
+  if (!err || dof < 0 || dof >= numeric->ndofs || numeric->mesh != analytic->mesh ||
+      numeric->ndofs != analytic->ndofs)
+    return fail(SE_ERR_ARG, "bad argument");
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  CK(launch_quadrature(numeric->mesh->dev, numeric->ndofs, dof, numeric->vals, analytic->vals,
+                       g_scratch, kScratch, g_scratch + kScratch, g_stream));
+  double r[2];
+  CK(cudaMemcpyAsync(r, g_scratch + kScratch, sizeof(r), cudaMemcpyDeviceToHost, g_stream));
+  CK(cudaStreamSynchronize(g_stream));
+  *err = normalise ? std::sqrt(r[0] / r[1]) : std::sqrt(r[0]);
+  return SE_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,153 @@
+// Internal declarations shared by the segpu CUDA sources (not installed).
+//
+// Device data layout
+//  - Field values: double[nVertsTotal][ndofs] in the reference's vertex
+//    order (x fastest, periodic duplicates stored), so that host uploads and
+//    downloads are single copies and the SL gathers read an element's
+//    (N+1)^2 block as N+1 contiguous rows of N+1 values.
+//  - Solver vectors ("unknowns"): the reference's vector ordering, which on
+//    SE's regular Cartesian meshes is always a row-major rectangle of the
+//    vertex grid: rows [lo_y, hi_y), columns [lo_x, hi_x). Dirichlet and
+//    periodic-duplicate vertices are not unknowns.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#define SE_MAXN 12
+#define SE_MAXN1 (SE_MAXN + 1)
+
+namespace seg {
+
+// Everything a kernel needs to know about one mesh (passed by value; lives
+// in the kernel parameter bank).
+struct MeshDev {
+  int N;
+  int nEls[2];
+  int nVerts[2];
+  int periodic[2];
+  double min[2], max[2], dx[2];
+  double two_over_dx[2];  // 2.0/dx, rounded as the reference rounds it
+  double span[2];         // max - min
+  double nspan[2];        // min - max
+  double abcissa[SE_MAXN1];
+  double lambda[SE_MAXN1];  // 1 / prod_{k != j} (x_j - x_k): Lagrange product weights
+  double w[SE_MAXN1];       // GLL weights
+  double dC[SE_MAXN1 * SE_MAXN1];  // cardinal derivative matrix, row = point
+};
+
+// One direction of the tensor-product operator on the unknown grid.
+struct Dir {
+  int nE, N, nV;
+  int periodic;
+  int lo, hi;  // unknown vertex range [lo, hi)
+};
+
+// A = alpha (W x W) + beta[0] (Kx x W) + beta[1] (W x Ky): the assembled
+// c*Mass + s*Laplacian of SE on a uniform Cartesian GLL mesh, with Kh the
+// 1-D reference-element stiffness and W the assembled 1-D GLL weights.
+struct OpDev {
+  Dir d[2];
+  int G[2];  // unknowns per direction
+  double alpha;
+  double beta[2];
+  double Kh[SE_MAXN1 * SE_MAXN1];
+  double w[SE_MAXN1];
+};
+
+// Device-side error bits (a single unsigned word per library instance).
+enum : unsigned {
+  KERR_DOMAIN = 1u,            // departure point outside the mesh after the wrap
+  KERR_BARRIER_TIMEOUT = 2u,   // a grid barrier wait gave up
+  KERR_BAD_CONFIG = 4u,
+};
+
+// ---- exact-rounding arithmetic: the reference's coordinate operations, one
+// IEEE operation at a time, never contracted into FMAs.
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
+
+// ---------------------------------------------------------------------------
+// Host launch wrappers (defined in sl.cu / linsys.cu). All take the stream.
+
+// SL advection. field: [Nv][ndofs]; vel/vel_prev: [Nv][2]; out: [Nv][ndofs].
+// field_prev == nullptr selects the first-order scheme. dep_el/dep_xy are
+// optional recordings of the departure elements/points (all vertices).
+cudaError_t launch_sl(const MeshDev& m, int ndofs, const double* field, const double* vel,
+                      const double* field_prev, const double* vel_prev, double dt,
+                      double* out, int* dep_el, double* dep_xy, unsigned* err,
+                      cudaStream_t s);
+// Mesh::GlobalToLocal at points (device arrays).
+cudaError_t launch_global_to_local(const MeshDev& m, const double* pts, int npts, int* el,
+                                   double* lc, cudaStream_t s);
+// Field::InterpGlobal at points (device arrays).
+cudaError_t launch_interp_global(const MeshDev& m, int ndofs, const double* vals,
+                                 const double* pts, int npts, double* out, cudaStream_t s);
+// Field::PeriodicUpdate.
+cudaError_t launch_periodic_update(const MeshDev& m, int ndofs, double* vals, cudaStream_t s);
+// Quadrature sums over all elements: sum detJ*w*a (Integrate) or, with
+// b != nullptr, sums of detJ*w*(a-b)^2 and detJ*w*b^2 (FieldError).
+// Results land in out2[0..1] (device), deterministic order.
+cudaError_t launch_quadrature(const MeshDev& m, int ndofs, int dof, const double* a,
+                              const double* b, double* scratch, int nscratch, double* out2,
+                              cudaStream_t s);
+// Max over vertices of |v|^2 (CalcTimeStep), deterministic.
+cudaError_t launch_max_speed_sq(int nv, const double* vel, double* scratch, int nscratch,
+                                double* out, cudaStream_t s);
+
+// Linear-system pieces.
+cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, cudaStream_t s);
+cudaError_t launch_op_diag(const OpDev& op, double* d, cudaStream_t s);
+// f = Mass*rhs over the unknowns (FieldRHS + Vector::Assemble), plus lift.
+cudaError_t launch_rhs_assemble(const OpDev& op, const MeshDev& m, const double* rhs_vals,
+                                const double* lift, double* f, cudaStream_t s);
+// lift = -A[unknowns, Dirichlet] * sol_vals[Dirichlet].
+cudaError_t launch_lift(const OpDev& op, const MeshDev& m, const double* sol_vals, double* lift,
+                        cudaStream_t s);
+// sol_vals[unknown vertices and their periodic copies] = x.
+cudaError_t launch_update_field(const OpDev& op, const MeshDev& m, const double* x,
+                                double* sol_vals, cudaStream_t s);
+
+// Persistent CG over a batch of solves.
+struct CgSolve {
+  OpDev op;
+  const double* b;  // right-hand side (unknowns)
+  double *x, *r, *z, *p0, *p1, *w;
+  double rtol, atol, dtol;
+  int max_it;
+  int norm_type;
+  int remove_null;
+  int n;  // unknowns
+  // segment range of this solve in the partial-sum table
+  int seg_begin, seg_end;
+  // state (written by the kernel)
+  double beta, betaold, dpi, dpiold, rnorm0, ttol, dp, bcoef, a, zmean;
+  int its, reason, done, pbuf;
+};
+struct CgTile {
+  int solve;
+  int x0, y0;  // first unknown column/row of the tile
+  int seg;     // partial-sum segment this tile accumulates into
+};
+struct CgBatch {
+  CgSolve* solves;  // device array
+  int nsolves;
+  const CgTile* tiles;  // device array, grouped by block (contiguous chunks)
+  const int* block_tile_begin;  // [grid+1]
+  double* partials;  // [nseg][4]
+  int nseg;
+  unsigned* bar_count;
+  unsigned* bar_gen;
+  int* n_active;
+  unsigned* err;
+};
+constexpr int kCgTileX = 32;
+constexpr int kCgTileY = 8;
+constexpr int kCgThreads = kCgTileX * kCgTileY;
+// Blocks of kCgThreads that can be co-resident on this device.
+int cg_max_grid(int device);
+cudaError_t launch_cg(const CgBatch& batch, int grid, cudaStream_t s);
+
+}  // namespace seg

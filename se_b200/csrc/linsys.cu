@@ -1,0 +1,577 @@
+// Matrix-free Helmholtz/Poisson operator and a persistent, deterministic
+// Jacobi-preconditioned CG for sm_100a.
+//
+// Operator. SE assembles A = c*Mass + s*Laplacian element by element into a
+// PETSc AIJ matrix (src/base/Matrix.cpp:63-149, src/base/Operator.cpp:63-84,
+// 157-177). On SE's meshes every element is the same axis-aligned rectangle
+// (src/base/Mesh.cpp:17-84) and the GLL mass matrix is diagonal, so the
+// assembled operator is a sum of Kronecker products of 1-D assembled
+// operators:
+//     A = alpha (W (x) W) + beta_x (Kx (x) W) + beta_y (W (x) Ky)
+// with Kx/Ky the assembled 1-D reference stiffness (Kh = D^T diag(w) D) and
+// W the assembled 1-D GLL weights. Applying it is a sum-factorised
+// contraction along rows and along columns of the unknown grid: at most
+// 2N+1 taps per direction, 16 bytes of HBM traffic per unknown in FP64.
+// The gather-scatter (direct stiffness summation) is implicit: every output
+// unknown sums its own row of the assembled 1-D operators in a fixed order,
+// so the result is deterministic and needs no atomics.
+//
+// CG. One cooperative launch runs all iterations of a batch of solves.
+// Tiles of 32x8 unknowns are statically assigned in contiguous chunks to the
+// resident blocks; every dot product is reduced in a fixed order
+// (warp shuffles, then block, then segment by segment in the last block to
+// reach the grid barrier), so repeated solves are bit-for-bit identical.
+// Two grid barriers per iteration (three with a constant null space).
+// The iteration is PETSc's KSPCG with PCJACOBI (zero initial guess,
+// preconditioned/unpreconditioned/natural norm, RTOL/ATOL/DTOL tests and
+// the sign checks for an indefinite matrix or preconditioner), as SE runs
+// it from src/linsys/HelmholtzEqn.cpp:141-150.
+#include "common.cuh"
+
+namespace seg {
+namespace {
+
+// Fold a vertex index onto its periodic partner.
+__device__ __forceinline__ int fold(const Dir& d, int g) {
+  return (d.periodic && g == d.nV - 1) ? 0 : g;
+}
+__device__ __forceinline__ bool unknown(const Dir& d, int g) { return g >= d.lo && g < d.hi; }
+
+// Assembled 1-D GLL weight of vertex g.
+__device__ __forceinline__ double wsum(const OpDev& op, const Dir& d, int g) {
+  int e = g / d.N, a = g - e * d.N;
+  double s = 0.0;
+  if (e < d.nE) s += op.w[a];
+  if (a == 0 && (e > 0 || d.periodic)) s += op.w[d.N];
+  return s;
+}
+// Assembled 1-D stiffness diagonal of vertex g.
+__device__ __forceinline__ double kdiag(const OpDev& op, const Dir& d, int g) {
+  const int n = d.N + 1;
+  int e = g / d.N, a = g - e * d.N;
+  double s = 0.0;
+  if (e < d.nE) s += op.Kh[a * n + a];
+  if (a == 0 && (e > 0 || d.periodic)) s += op.Kh[d.N * n + d.N];
+  return s;
+}
+// Row g of the assembled 1-D stiffness applied to val(vertex): the row of
+// element e = g/N at local a, plus the last row of element e-1 when g is the
+// element's left end. Dirichlet vertices contribute only when the caller's
+// val() returns them.
+template <class F>
+__device__ __forceinline__ double krow(const OpDev& op, const Dir& d, int g, const F& val) {
+  const int N = d.N, n = N + 1;
+  int e = g / N, a = g - e * N;
+  double s = 0.0;
+  if (e < d.nE) {
+    const double* k = op.Kh + a * n;
+    const int g0 = e * N;
+    for (int b = 0; b < n; b++) s = fma(k[b], val(fold(d, g0 + b)), s);
+  }
+  if (a == 0 && (e > 0 || d.periodic)) {
+    const double* k = op.Kh + N * n;
+    const int g0 = (e > 0 ? e - 1 : d.nE - 1) * N;
+    for (int b = 0; b < n; b++) s = fma(k[b], val(fold(d, g0 + b)), s);
+  }
+  return s;
+}
+
+__device__ __forceinline__ double diag_at(const OpDev& op, int gx, int gy) {
+  const double wx = wsum(op, op.d[0], gx), wy = wsum(op, op.d[1], gy);
+  return op.alpha * wx * wy + op.beta[0] * kdiag(op, op.d[0], gx) * wy +
+         op.beta[1] * wx * kdiag(op, op.d[1], gy);
+}
+
+// y(gx, gy) = (A x) for unknown vertex (gx, gy), x given by xv(ux, uy) on
+// unknown coordinates.
+template <class X>
+__device__ __forceinline__ double apply_at(const OpDev& op, int gx, int gy, const X& xv) {
+  const Dir &dx = op.d[0], &dy = op.d[1];
+  const double wx = wsum(op, dx, gx), wy = wsum(op, dy, gy);
+  const int ux = gx - dx.lo, uy = gy - dy.lo;
+  double self = xv(ux, uy);
+  double kx = krow(op, dx, gx, [&](int g) { return unknown(dx, g) ? xv(g - dx.lo, uy) : 0.0; });
+  double ky = krow(op, dy, gy, [&](int g) { return unknown(dy, g) ? xv(ux, g - dy.lo) : 0.0; });
+  return op.alpha * wx * wy * self + op.beta[0] * wy * kx + op.beta[1] * wx * ky;
+}
+
+__global__ void __launch_bounds__(256) op_apply_kernel(const OpDev op, const double* __restrict__ x,
+                                                       double* __restrict__ y) {
+  const int ux = blockIdx.x * blockDim.x + threadIdx.x;
+  const int uy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ux >= op.G[0] || uy >= op.G[1]) return;
+  const int G0 = op.G[0];
+  auto xv = [&](int a, int b) { return __ldg(x + (size_t)b * G0 + a); };
+  y[(size_t)uy * G0 + ux] = apply_at(op, ux + op.d[0].lo, uy + op.d[1].lo, xv);
+}
+
+__global__ void op_diag_kernel(const OpDev op, double* __restrict__ d) {
+  const int ux = blockIdx.x * blockDim.x + threadIdx.x;
+  const int uy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ux >= op.G[0] || uy >= op.G[1]) return;
+  d[(size_t)uy * op.G[0] + ux] = diag_at(op, ux + op.d[0].lo, uy + op.d[1].lo);
+}
+
+// FieldRHS (src/base/RHSOp.cpp:31-50) assembled by Vector::Assemble
+// (src/base/Vector.cpp:89-121): each element contributes detJ*w_i*w_j*f at
+// its own vertex, so unknown (gx, gy) sums detJ*w*w*f over the vertices that
+// map to it (itself, and the periodic duplicates that fold onto it).
+__device__ __forceinline__ int contribs(const Dir& d, int g, int* v, int* side) {
+  // returns vertices that fold onto g and whether each is an element's left
+  // end (0), an interior node (1) or an element's right end (2)
+  int e = g / d.N, a = g - e * d.N, k = 0;
+  if (a != 0) {
+    v[k] = g;
+    side[k++] = 1;
+    return k;
+  }
+  if (e < d.nE) {
+    v[k] = g;
+    side[k++] = 0;
+  }
+  if (e > 0) {
+    v[k] = g;
+    side[k++] = 2;
+  } else if (d.periodic) {
+    v[k] = d.nV - 1;
+    side[k++] = 2;
+  }
+  return k;
+}
+__global__ void rhs_assemble_kernel(const OpDev op, const MeshDev m, const double* __restrict__ rhs,
+                                    const double* __restrict__ lift, double* __restrict__ f) {
+  const int ux = blockIdx.x * blockDim.x + threadIdx.x;
+  const int uy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ux >= op.G[0] || uy >= op.G[1]) return;
+  const Dir &dx = op.d[0], &dy = op.d[1];
+  const int gx = ux + dx.lo, gy = uy + dy.lo;
+  int vx[2], sx[2], vy[2], sy[2];
+  int nx = contribs(dx, gx, vx, sx), ny = contribs(dy, gy, vy, sy);
+  const double detj = (0.5 * m.dx[0]) * (0.5 * m.dx[1]);
+  const int nvx = m.nVerts[0];
+  double s = 0.0;
+  for (int b = 0; b < ny; b++) {
+    double wy = sy[b] == 1 ? op.w[gy - (gy / dy.N) * dy.N] : (sy[b] == 0 ? op.w[0] : op.w[dy.N]);
+    for (int a = 0; a < nx; a++) {
+      double wx = sx[a] == 1 ? op.w[gx - (gx / dx.N) * dx.N] : (sx[a] == 0 ? op.w[0] : op.w[dx.N]);
+      if (rhs) s += detj * (wx * wy) * rhs[(size_t)vy[b] * nvx + vx[a]];
+    }
+  }
+  const size_t k = (size_t)uy * op.G[0] + ux;
+  f[k] = s + (lift ? lift[k] : 0.0);
+}
+
+// Matrix::Assemble's Dirichlet lifting (src/base/Matrix.cpp:117-140):
+// lift = -sum over Dirichlet columns of A[row, col] * u_D(col).
+__global__ void lift_kernel(const OpDev op, const MeshDev m, const double* __restrict__ sol,
+                            double* __restrict__ lift) {
+  const int ux = blockIdx.x * blockDim.x + threadIdx.x;
+  const int uy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ux >= op.G[0] || uy >= op.G[1]) return;
+  const Dir &dx = op.d[0], &dy = op.d[1];
+  const int gx = ux + dx.lo, gy = uy + dy.lo;
+  const int nvx = m.nVerts[0];
+  const double wx = wsum(op, dx, gx), wy = wsum(op, dy, gy);
+  double kx = krow(op, dx, gx, [&](int g) { return unknown(dx, g) ? 0.0 : sol[(size_t)gy * nvx + g]; });
+  double ky = krow(op, dy, gy, [&](int g) { return unknown(dy, g) ? 0.0 : sol[(size_t)g * nvx + gx]; });
+  lift[(size_t)uy * op.G[0] + ux] = -(op.beta[0] * wy * kx + op.beta[1] * wx * ky);
+}
+
+// Vector::UpdateField (src/base/Vector.cpp:40-61) with the periodic copies.
+__global__ void update_field_kernel(const OpDev op, const MeshDev m, const double* __restrict__ x,
+                                    double* __restrict__ sol) {
+  const int ux = blockIdx.x * blockDim.x + threadIdx.x;
+  const int uy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ux >= op.G[0] || uy >= op.G[1]) return;
+  const int gx = ux + op.d[0].lo, gy = uy + op.d[1].lo;
+  const int nvx = m.nVerts[0], nvy = m.nVerts[1];
+  const double v = x[(size_t)uy * op.G[0] + ux];
+  sol[(size_t)gy * nvx + gx] = v;
+  const bool cx = op.d[0].periodic && gx == 0, cy = op.d[1].periodic && gy == 0;
+  if (cx) sol[(size_t)gy * nvx + nvx - 1] = v;
+  if (cy) sol[(size_t)(nvy - 1) * nvx + gx] = v;
+  if (cx && cy) sol[(size_t)nvy * nvx - 1] = v;
+}
+
+// ------------------------------------------------------------ grid barrier --
+__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid-wide barrier for a cooperative launch. The last block to arrive runs
+// last_fn (with the whole block) before releasing the others. Waits are
+// bounded: after ~2^26 polls a block records KERR_BARRIER_TIMEOUT and goes
+// on; callers check the error word after every barrier and return.
+constexpr long kBarrierPolls = 1L << 26;
+template <class F>
+__device__ __forceinline__ void grid_barrier(const CgBatch& B, F&& last_fn) {
+  __shared__ unsigned s_last, s_gen;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned gen = ld_acquire(B.bar_gen);
+    __threadfence();
+    unsigned arrived = atomicAdd(B.bar_count, 1u) + 1u;
+    s_last = arrived == gridDim.x;
+    s_gen = gen;
+  }
+  __syncthreads();
+  if (s_last) {
+    __threadfence();
+    last_fn();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      atomicExch(B.bar_count, 0u);
+      __threadfence();
+      st_release(B.bar_gen, s_gen + 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    long polls = 0;
+    while (ld_acquire(B.bar_gen) == s_gen) {
+      if (++polls > kBarrierPolls) {
+        atomicOr(B.err, KERR_BARRIER_TIMEOUT);
+        break;
+      }
+      if (polls > 256) __nanosleep(64);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// Fixed-order block reduction of 4 sums into lane 0 of warp 0.
+__device__ __forceinline__ void block_sum4(double v[4]) {
+  __shared__ double sm[kCgThreads / 32][4];
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0)
+#pragma unroll
+    for (int q = 0; q < 4; q++) sm[w][q] = v[q];
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      v[q] = l < kCgThreads / 32 ? sm[l][q] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    }
+  }
+  __syncthreads();
+}
+
+// Sum of partial slot q over a solve's segments, fixed order; result valid in
+// every lane of warp 0.
+__device__ __forceinline__ double seg_sum(const CgBatch& B, const CgSolve& S, int q) {
+  const int l = threadIdx.x & 31;
+  double s = 0.0;
+  for (int k = S.seg_begin + l; k < S.seg_end; k += 32) s += B.partials[(size_t)k * 4 + q];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+enum { PH_INIT = 0, PH_NULL, PH_APPLY, PH_UPDATE };
+
+// One pass over this block's tiles. Accumulates per-segment partial sums.
+template <int PH>
+__device__ void cg_pass(const CgBatch& B, int t0, int t1) {
+  const int tx = threadIdx.x & (kCgTileX - 1), ty = threadIdx.x / kCgTileX;
+  int cur_seg = -1;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int t = t0; t < t1; t++) {
+    const CgTile T = B.tiles[t];
+    const CgSolve& S = B.solves[T.solve];
+    if (T.seg != cur_seg) {
+      if (cur_seg >= 0) {
+        block_sum4(acc);
+        if (threadIdx.x == 0)
+#pragma unroll
+          for (int q = 0; q < 4; q++) B.partials[(size_t)cur_seg * 4 + q] = acc[q];
+      }
+      cur_seg = T.seg;
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[q] = 0.0;
+    }
+    if (S.done) continue;
+    const int ux = T.x0 + tx, uy = T.y0 + ty;
+    if (ux >= S.op.G[0] || uy >= S.op.G[1]) continue;
+    const int G0 = S.op.G[0];
+    const size_t k = (size_t)uy * G0 + ux;
+    const int gx = ux + S.op.d[0].lo, gy = uy + S.op.d[1].lo;
+    if (PH == PH_INIT) {
+      // r = b (x = 0), z = D^{-1} r
+      double r = S.b[k];
+      double z = r / diag_at(S.op, gx, gy);
+      S.x[k] = 0.0;
+      S.r[k] = r;
+      S.z[k] = z;
+      acc[0] += z * z;
+      acc[1] += z * r;
+      acc[2] += r * r;
+      acc[3] += z;
+    } else if (PH == PH_NULL) {
+      // z -= mean(z)
+      double z = S.z[k] - S.zmean;
+      double r = S.r[k];
+      S.z[k] = z;
+      acc[0] += z * z;
+      acc[1] += z * r;
+      acc[2] += r * r;
+    } else if (PH == PH_APPLY) {
+      // p = z + bcoef p_old (p = z on the first iteration); w = A p. The
+      // current p is (pbuf ? p1 : p0); the new one goes to the other buffer.
+      const double* z = S.z;
+      const double* po = S.pbuf ? S.p1 : S.p0;
+      double* pn = S.pbuf ? S.p0 : S.p1;
+      const double bc = S.its == 0 ? 0.0 : S.bcoef;
+      // z and p are rewritten by this kernel between passes: plain coherent
+      // loads, never the read-only (non-coherent) path.
+      auto pv = [&](int a, int b) {
+        const size_t q = (size_t)b * G0 + a;
+        return S.its == 0 ? z[q] : fma(bc, po[q], z[q]);
+      };
+      const double p = pv(ux, uy);
+      const double w = apply_at(S.op, gx, gy, pv);
+      pn[k] = p;
+      S.w[k] = w;
+      acc[0] += p * w;
+    } else {
+      // x += a p; r -= a w; z = D^{-1} r (p is the buffer the apply wrote;
+      // the barrier after the apply flipped pbuf to point at it)
+      const double* pn = S.pbuf ? S.p1 : S.p0;
+      const double a = S.a;
+      double p = pn[k], w = S.w[k];
+      double x = S.x[k] + a * p;
+      double r = S.r[k] - a * w;
+      double z = r / diag_at(S.op, gx, gy);
+      S.x[k] = x;
+      S.r[k] = r;
+      S.z[k] = z;
+      acc[0] += z * z;
+      acc[1] += z * r;
+      acc[2] += r * r;
+      acc[3] += z;
+    }
+  }
+  if (cur_seg >= 0) {
+    block_sum4(acc);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q < 4; q++) B.partials[(size_t)cur_seg * 4 + q] = acc[q];
+  }
+}
+
+// Residual norm in the chosen norm from the partials of the last pass.
+__device__ __forceinline__ double cg_norm(const CgSolve& S, double zz, double zr, double rr) {
+  if (S.norm_type == 0) return sqrt(zz);
+  if (S.norm_type == 1) return sqrt(rr);
+  return sqrt(fabs(zr));
+}
+
+// Convergence test of KSPConvergedDefault; sets reason/done. n = iteration.
+__device__ __forceinline__ void cg_converged(CgSolve& S, int n, double dp) {
+  if (!(dp == dp) || isinf(dp)) {
+    S.reason = -9;
+    S.done = 1;
+    return;
+  }
+  if (n == 0) {
+    S.rnorm0 = dp;
+    S.ttol = fmax(S.rtol * dp, S.atol);
+  }
+  if (dp <= S.ttol) {
+    S.reason = dp < S.atol ? 3 : 2;
+    S.done = 1;
+  } else if (n > 0 && dp >= S.dtol * S.rnorm0) {
+    S.reason = -4;
+    S.done = 1;
+  }
+}
+
+__global__ void __launch_bounds__(kCgThreads) cg_kernel(const CgBatch B) {
+  const int t0 = B.block_tile_begin[blockIdx.x], t1 = B.block_tile_begin[blockIdx.x + 1];
+  const bool any_null = [&] {
+    for (int s = 0; s < B.nsolves; s++)
+      if (B.solves[s].remove_null) return true;
+    return false;
+  }();
+
+  // ---- r = b, z = D^{-1} r; norms; beta = z.r
+  cg_pass<PH_INIT>(B, t0, t1);
+  grid_barrier(B, [&] {
+    if (threadIdx.x >= 32) return;
+    for (int s = 0; s < B.nsolves; s++) {
+      CgSolve& S = B.solves[s];
+      const double zsum = seg_sum(B, S, 3);
+      if (threadIdx.x == 0) S.zmean = S.remove_null ? zsum / S.n : 0.0;
+    }
+  });
+  if (*B.err) return;
+  if (any_null) {
+    cg_pass<PH_NULL>(B, t0, t1);
+    grid_barrier(B, [] {});
+    if (*B.err) return;
+  }
+  grid_barrier(B, [&] {
+    if (threadIdx.x >= 32) return;
+    int active = 0;
+    for (int s = 0; s < B.nsolves; s++) {
+      CgSolve& S = B.solves[s];
+      const double zz = seg_sum(B, S, 0), zr = seg_sum(B, S, 1), rr = seg_sum(B, S, 2);
+      if (threadIdx.x == 0) {
+        S.its = 0;
+        S.reason = 0;
+        S.done = 0;
+        S.pbuf = 0;
+        S.dpi = 0.0;
+        S.betaold = 0.0;
+        const double dp = cg_norm(S, zz, zr, rr);
+        S.dp = dp;
+        cg_converged(S, 0, dp);
+        S.beta = zr;
+        if (!S.done && S.max_it <= 0) {
+          S.reason = -3;
+          S.done = 1;
+        }
+        if (!S.done && S.beta == 0.0) {
+          S.reason = 3;
+          S.done = 1;
+        }
+        active += !S.done;
+      }
+    }
+    if (threadIdx.x == 0) *B.n_active = active;
+  });
+  if (*B.err) return;
+
+  while (*(volatile int*)B.n_active > 0) {
+    // ---- p = z + (beta/betaold) p; w = A p; dpi = p.w
+    cg_pass<PH_APPLY>(B, t0, t1);
+    grid_barrier(B, [&] {
+      if (threadIdx.x >= 32) return;
+      for (int s = 0; s < B.nsolves; s++) {
+        CgSolve& S = B.solves[s];
+        if (S.done) continue;
+        const double dpi = seg_sum(B, S, 0);
+        if (threadIdx.x == 0) {
+          const double dpiold = S.dpi;
+          S.dpiold = dpiold;
+          S.dpi = dpi;
+          S.betaold = S.beta;
+          S.pbuf ^= 1;  // the apply wrote the other buffer
+          if (dpi == 0.0 || (S.its > 0 && dpi * dpiold <= 0.0)) {
+            S.reason = -10;
+            S.done = 1;
+          } else {
+            S.a = S.beta / dpi;
+          }
+        }
+      }
+    });
+    if (*B.err) return;
+    // ---- x += a p, r -= a w, z = D^{-1} r; norms
+    cg_pass<PH_UPDATE>(B, t0, t1);
+    if (any_null) {
+      grid_barrier(B, [&] {
+        if (threadIdx.x >= 32) return;
+        for (int s = 0; s < B.nsolves; s++) {
+          CgSolve& S = B.solves[s];
+          const double zsum = seg_sum(B, S, 3);
+          if (threadIdx.x == 0) S.zmean = S.remove_null ? zsum / S.n : 0.0;
+        }
+      });
+      if (*B.err) return;
+      cg_pass<PH_NULL>(B, t0, t1);
+    }
+    grid_barrier(B, [&] {
+      if (threadIdx.x >= 32) return;
+      int active = 0;
+      for (int s = 0; s < B.nsolves; s++) {
+        CgSolve& S = B.solves[s];
+        if (S.done) continue;
+        const double zz = seg_sum(B, S, 0), zr = seg_sum(B, S, 1), rr = seg_sum(B, S, 2);
+        if (threadIdx.x == 0) {
+          S.its += 1;
+          const double dp = cg_norm(S, zz, zr, rr);
+          S.dp = dp;
+          cg_converged(S, S.its, dp);
+          if (!S.done) {
+            const double beta = zr;
+            if (beta == 0.0) {
+              S.reason = 3;
+              S.done = 1;
+            } else if (beta * S.betaold < 0.0) {
+              S.reason = -8;
+              S.done = 1;
+            } else if (S.its >= S.max_it) {
+              S.reason = -3;
+              S.done = 1;
+            } else {
+              S.beta = beta;
+              S.bcoef = beta / S.betaold;
+            }
+          }
+          active += !S.done;
+        }
+      }
+      if (threadIdx.x == 0) *B.n_active = active;
+    });
+    if (*B.err) return;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, cudaStream_t s) {
+  dim3 block(32, 8), grid((op.G[0] + 31) / 32, (op.G[1] + 7) / 8);
+  op_apply_kernel<<<grid, block, 0, s>>>(op, x, y);
+  return cudaGetLastError();
+}
+cudaError_t launch_op_diag(const OpDev& op, double* d, cudaStream_t s) {
+  dim3 block(32, 8), grid((op.G[0] + 31) / 32, (op.G[1] + 7) / 8);
+  op_diag_kernel<<<grid, block, 0, s>>>(op, d);
+  return cudaGetLastError();
+}
+cudaError_t launch_rhs_assemble(const OpDev& op, const MeshDev& m, const double* rhs_vals,
+                                const double* lift, double* f, cudaStream_t s) {
+  dim3 block(32, 8), grid((op.G[0] + 31) / 32, (op.G[1] + 7) / 8);
+  rhs_assemble_kernel<<<grid, block, 0, s>>>(op, m, rhs_vals, lift, f);
+  return cudaGetLastError();
+}
+cudaError_t launch_lift(const OpDev& op, const MeshDev& m, const double* sol_vals, double* lift,
+                        cudaStream_t s) {
+  dim3 block(32, 8), grid((op.G[0] + 31) / 32, (op.G[1] + 7) / 8);
+  lift_kernel<<<grid, block, 0, s>>>(op, m, sol_vals, lift);
+  return cudaGetLastError();
+}
+cudaError_t launch_update_field(const OpDev& op, const MeshDev& m, const double* x,
+                                double* sol_vals, cudaStream_t s) {
+  dim3 block(32, 8), grid((op.G[0] + 31) / 32, (op.G[1] + 7) / 8);
+  update_field_kernel<<<grid, block, 0, s>>>(op, m, x, sol_vals);
+  return cudaGetLastError();
+}
+
+int cg_max_grid(int device) {
+  int sms = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_kernel, kCgThreads, 0) !=
+      cudaSuccess)
+    return 0;
+  return sms * per_sm;
+}
+
+cudaError_t launch_cg(const CgBatch& batch, int grid, cudaStream_t s) {
+  void* args[] = {const_cast<CgBatch*>(&batch)};
+  return cudaLaunchCooperativeKernel((const void*)cg_kernel, dim3(grid), dim3(kCgThreads), args,
+                                     0, s);
+}
+
+}  // namespace seg

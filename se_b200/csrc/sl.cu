@@ -1,0 +1,540 @@
+// Semi-Lagrangian advection on GLL quadrilateral meshes, sm_100a.
+//
+// One thread per owned vertex (periodic duplicates are written by their
+// partner thread, which is what Field::PeriodicUpdate leaves in the
+// reference). Each thread integrates the backward trajectory and gathers the
+// (N+1)^2 element block of the field at every stage.
+//
+// Reference: src/base/Advector.cpp:150-274 (PeriodicUpdate, IntegrateRK2,
+// FirstOrder, SecondOrder, ExtrapolateVelocities), src/base/Mesh.cpp:109-176
+// (GetEl, GlobalToLocal), src/base/Legendre.cpp:145-169 and :293-305
+// (ShapeFuncsAtCoord, IsRoot), src/base/Field.cpp:57-76 (InterpLocal/Global).
+//
+// Parity: coordinates (vertex positions, departure points, element search,
+// local coordinates, wrap) use the reference's exact IEEE operation order, so
+// that for equal velocities the departure element is bit-identical. The
+// cardinal functions use the Lagrange product form with prefix/suffix
+// products (no divisions) instead of the reference's P_N' formula; both
+// evaluate the same polynomial and agree to a few ulps.
+#include "common.cuh"
+
+namespace seg {
+namespace {
+
+// ------------------------------------------------------- mesh geometry ----
+// Mesh::Mesh vertex coordinate along direction d (src/base/Mesh.cpp:66-71).
+__device__ __forceinline__ double vertex_coord(const MeshDev& m, int d, int t) {
+  int e = t / m.N;
+  double l = m.abcissa[t - e * m.N];
+  return xadd(xadd(m.min[d], xmul((double)e, m.dx[d])),
+              xmul(xdiv(xadd(l, 1.0), 2.0), m.dx[d]));
+}
+
+// Mesh::GetEl along one direction (src/base/Mesh.cpp:109-136). Out-of-mesh
+// points (possible only when a trajectory crosses more than one period) are
+// clamped to the nearest element and flagged.
+__device__ __forceinline__ int get_topo(const MeshDev& m, int d, double c, unsigned* err) {
+  double t = xsub(c, m.max[d]);
+  if (t >= -1.0e-12 && t <= 1.0e-12) return m.nEls[d] - 1;
+  double out = xdiv(xsub(c, m.min[d]), m.dx[d]);
+  double integer = trunc(out);
+  double frac = out - integer;  // exact
+  int topo = (int)integer;
+  if (topo > 0 && frac >= -1.0e-12 && frac <= 1.0e-12) topo--;
+  if (topo < 0 || topo >= m.nEls[d] || !(out == out)) {
+    if (err) atomicOr(err, KERR_DOMAIN);
+    topo = topo < 0 || !(out == out) ? 0 : m.nEls[d] - 1;
+  }
+  return topo;
+}
+
+// Mesh::GlobalToLocal along one direction (src/base/Mesh.cpp:163-176).
+__device__ __forceinline__ double local_coord(const MeshDev& m, int d, double c, int topo) {
+  double l = xsub(xmul(xsub(xsub(c, m.min[d]), xmul((double)topo, m.dx[d])), m.two_over_dx[d]),
+                  1.0);
+  if (l < -1.0) l = -1.0;
+  if (l > +1.0) l = +1.0;
+  return l;
+}
+
+// Legendre::IsRoot (src/base/Legendre.cpp:293-305): index of the first GLL
+// node within 1e-8, or -1.
+template <int N>
+__device__ __forceinline__ int snap_node(const MeshDev& m, double l) {
+  int s = -1;
+#pragma unroll
+  for (int k = N; k >= 0; k--)
+    if (fabs(l - m.abcissa[k]) < 1.0e-8) s = k;
+  return s;
+}
+
+// GLL cardinal functions at a non-node coordinate: N_j(l) = lambda_j *
+// prod_{k != j} (l - x_k), from prefix and suffix products.
+template <int N>
+__device__ __forceinline__ void cardinal(const MeshDev& m, double l, double* c) {
+  double d[N + 1];
+#pragma unroll
+  for (int k = 0; k <= N; k++) d[k] = l - m.abcissa[k];
+  double pre = 1.0;
+#pragma unroll
+  for (int k = 0; k <= N; k++) {
+    c[k] = pre;
+    pre *= d[k];
+  }
+  double suf = 1.0;
+#pragma unroll
+  for (int k = N; k >= 0; k--) {
+    c[k] *= suf * m.lambda[k];
+    suf *= d[k];
+  }
+}
+
+// Advector::PeriodicUpdate (src/base/Advector.cpp:150-162).
+__device__ __forceinline__ double wrap(const MeshDev& m, int d, double c) {
+  if (c < m.min[d]) c = m.periodic[d] ? xadd(m.span[d], c) : m.min[d];
+  if (c > m.max[d]) c = m.periodic[d] ? xadd(m.nspan[d], c) : m.max[d];
+  return c;
+}
+
+// ----------------------------------------------------------- value types ----
+struct V1 {
+  double a;
+};
+struct V2 {
+  double a, b;
+};
+__device__ __forceinline__ V1 vzero(V1) { return {0.0}; }
+__device__ __forceinline__ V2 vzero(V2) { return {0.0, 0.0}; }
+__device__ __forceinline__ V1 vfma(double s, V1 v, V1 acc) { return {fma(s, v.a, acc.a)}; }
+__device__ __forceinline__ V2 vfma(double s, V2 v, V2 acc) {
+  return {fma(s, v.a, acc.a), fma(s, v.b, acc.b)};
+}
+
+// Sources: the nodal value of a field at vertex k.
+struct Scalar {
+  typedef V1 T;
+  const double* __restrict__ p;
+  __device__ __forceinline__ T operator()(int k) const { return {__ldg(p + k)}; }
+};
+struct Vec2 {
+  typedef V2 T;
+  const double2* __restrict__ p;
+  __device__ __forceinline__ T operator()(int k) const {
+    double2 v = __ldg(p + k);
+    return {v.x, v.y};
+  }
+};
+// c0*v + c1*vm with the reference's rounding (Advector::ExtrapolateVelocities,
+// src/base/Advector.cpp:367-377): each product rounded, then the sum.
+struct Vec2Mix {
+  typedef V2 T;
+  const double2* __restrict__ v;
+  const double2* __restrict__ vm;
+  double c0, c1;
+  __device__ __forceinline__ T operator()(int k) const {
+    double2 a = __ldg(v + k), b = __ldg(vm + k);
+    return {xadd(xmul(c0, a.x), xmul(c1, b.x)), xadd(xmul(c0, a.y), xmul(c1, b.y))};
+  }
+};
+
+// Field::InterpGlobal (src/base/Field.cpp:70-76) at global point (gx, gy).
+// Snapped directions reduce to a row, a column or a single vertex; the
+// reference sums the same products plus exact zeros.
+template <int N, class Src>
+__device__ __forceinline__ typename Src::T interp(const MeshDev& m, const Src& src, double gx,
+                                                  double gy, int* el_out, unsigned* err) {
+  typedef typename Src::T T;
+  int tx = get_topo(m, 0, gx, err), ty = get_topo(m, 1, gy, err);
+  if (el_out) *el_out = ty * m.nEls[0] + tx;
+  double lx = local_coord(m, 0, gx, tx), ly = local_coord(m, 1, gy, ty);
+  int sx = snap_node<N>(m, lx), sy = snap_node<N>(m, ly);
+  const int nvx = m.nVerts[0];
+  const int base = ty * N * nvx + tx * N;
+  if (sx >= 0 && sy >= 0) return src(base + sy * nvx + sx);
+  double cx[N + 1], cy[N + 1];
+  T acc = vzero(T());
+  if (sy >= 0) {
+    cardinal<N>(m, lx, cx);
+    const int row = base + sy * nvx;
+#pragma unroll
+    for (int i = 0; i <= N; i++) acc = vfma(cx[i], src(row + i), acc);
+    return acc;
+  }
+  cardinal<N>(m, ly, cy);
+  if (sx >= 0) {
+#pragma unroll
+    for (int j = 0; j <= N; j++) acc = vfma(cy[j], src(base + j * nvx + sx), acc);
+    return acc;
+  }
+  cardinal<N>(m, lx, cx);
+#pragma unroll
+  for (int j = 0; j <= N; j++) {
+    T r = vzero(T());
+    const int row = base + j * nvx;
+#pragma unroll
+    for (int i = 0; i <= N; i++) r = vfma(cx[i], src(row + i), r);
+    acc = vfma(cy[j], r, acc);
+  }
+  return acc;
+}
+
+template <class T>
+__device__ __forceinline__ void store(double* out, int node, T v);
+template <>
+__device__ __forceinline__ void store<V1>(double* out, int node, V1 v) {
+  out[node] = v.a;
+}
+template <>
+__device__ __forceinline__ void store<V2>(double* out, int node, V2 v) {
+  reinterpret_cast<double2*>(out)[node] = make_double2(v.a, v.b);
+}
+
+// Write the value of owned vertex (i, j) and of its periodic copies.
+template <class T>
+__device__ __forceinline__ void store_with_copies(const MeshDev& m, double* out, int i, int j,
+                                                  T v) {
+  const int nvx = m.nVerts[0], nvy = m.nVerts[1];
+  store<T>(out, j * nvx + i, v);
+  if (m.periodic[0] && i == 0) store<T>(out, j * nvx + nvx - 1, v);
+  if (m.periodic[1] && j == 0) store<T>(out, (nvy - 1) * nvx + i, v);
+  if (m.periodic[0] && m.periodic[1] && i == 0 && j == 0) store<T>(out, nvy * nvx - 1, v);
+}
+
+// Advector::FirstOrder with IntegrateRK2 (src/base/Advector.cpp:164-229).
+template <int N, class FSrc>
+__global__ void __launch_bounds__(256) sl_first_kernel(const MeshDev m, FSrc field,
+                                                       const double2* __restrict__ vel,
+                                                       double dt, double half_dt,
+                                                       double* __restrict__ out,
+                                                       int* __restrict__ dep_el,
+                                                       double2* __restrict__ dep_xy,
+                                                       unsigned* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nvx = m.nVerts[0], nvy = m.nVerts[1];
+  const bool owner = i < nvx - m.periodic[0] && j < nvy - m.periodic[1];
+  if (i >= nvx || j >= nvy || (!owner && !dep_el)) return;
+  Vec2 v{vel};
+  const double ox = vertex_coord(m, 0, i), oy = vertex_coord(m, 1, j);
+  V2 u = interp<N>(m, v, ox, oy, nullptr, err);
+  double xh = wrap(m, 0, xsub(ox, xmul(half_dt, u.a)));
+  double yh = wrap(m, 1, xsub(oy, xmul(half_dt, u.b)));
+  u = interp<N>(m, v, xh, yh, nullptr, err);
+  const double xd = wrap(m, 0, xsub(ox, xmul(dt, u.a)));
+  const double yd = wrap(m, 1, xsub(oy, xmul(dt, u.b)));
+  int el;
+  typename FSrc::T val = interp<N>(m, field, xd, yd, &el, err);
+  if (dep_el) {
+    dep_el[j * nvx + i] = el;
+    if (dep_xy) dep_xy[j * nvx + i] = make_double2(xd, yd);
+  }
+  if (owner) store_with_copies(m, out, i, j, val);
+}
+
+// Advector::SecondOrder (src/base/Advector.cpp:231-274) with the
+// extrapolated velocities formed on the fly at each gathered vertex.
+template <int N, class FSrc>
+__global__ void __launch_bounds__(256) sl_second_kernel(const MeshDev m, FSrc field,
+                                                        FSrc field_prev,
+                                                        const double2* __restrict__ vel,
+                                                        const double2* __restrict__ vel_prev,
+                                                        double dt, double half_dt,
+                                                        double* __restrict__ out,
+                                                        int* __restrict__ dep_el,
+                                                        double2* __restrict__ dep_xy,
+                                                        unsigned* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nvx = m.nVerts[0], nvy = m.nVerts[1];
+  const bool owner = i < nvx - m.periodic[0] && j < nvy - m.periodic[1];
+  if (i >= nvx || j >= nvy || (!owner && !dep_el)) return;
+  const Vec2Mix plus_one{vel, vel_prev, 2.0, -1.0};
+  const Vec2Mix plus_half{vel, vel_prev, 1.5, -0.5};
+  const Vec2Mix minus_half{vel, vel_prev, 0.5, 0.5};
+  const Vec2 v{vel};
+  const double ox = vertex_coord(m, 0, i), oy = vertex_coord(m, 1, j);
+  V2 u = interp<N>(m, plus_one, ox, oy, nullptr, err);
+  double xh = wrap(m, 0, xsub(ox, xmul(half_dt, u.a)));
+  double yh = wrap(m, 1, xsub(oy, xmul(half_dt, u.b)));
+  u = interp<N>(m, plus_half, xh, yh, nullptr, err);
+  const double x1 = wrap(m, 0, xsub(ox, xmul(dt, u.a)));
+  const double y1 = wrap(m, 1, xsub(oy, xmul(dt, u.b)));
+  u = interp<N>(m, v, x1, y1, nullptr, err);
+  xh = wrap(m, 0, xsub(x1, xmul(half_dt, u.a)));
+  yh = wrap(m, 1, xsub(y1, xmul(half_dt, u.b)));
+  u = interp<N>(m, minus_half, xh, yh, nullptr, err);
+  const double x2 = wrap(m, 0, xsub(x1, xmul(dt, u.a)));
+  const double y2 = wrap(m, 1, xsub(y1, xmul(dt, u.b)));
+  int el1, el2;
+  typename FSrc::T p1 = interp<N>(m, field, x1, y1, &el1, err);
+  typename FSrc::T p2 = interp<N>(m, field_prev, x2, y2, &el2, err);
+  if (dep_el) {
+    const int nv = nvx * nvy;
+    dep_el[j * nvx + i] = el1;
+    dep_el[nv + j * nvx + i] = el2;
+    if (dep_xy) {
+      dep_xy[j * nvx + i] = make_double2(x1, y1);
+      dep_xy[nv + j * nvx + i] = make_double2(x2, y2);
+    }
+  }
+  if (owner) {
+    // fieldSL = 2 psi(x1) - 0.5 psiPrev(x2) (src/base/Advector.cpp:266-268)
+    typename FSrc::T r;
+    double* rp = reinterpret_cast<double*>(&r);
+    const double* a = reinterpret_cast<const double*>(&p1);
+    const double* b = reinterpret_cast<const double*>(&p2);
+#pragma unroll
+    for (int d = 0; d < (int)(sizeof(r) / sizeof(double)); d++)
+      rp[d] = xsub(xmul(2.0, a[d]), xmul(0.5, b[d]));
+    store_with_copies(m, out, i, j, r);
+  }
+}
+
+template <int N>
+cudaError_t launch_sl_n(const MeshDev& m, int ndofs, const double* field, const double* vel,
+                        const double* field_prev, const double* vel_prev, double dt, double* out,
+                        int* dep_el, double* dep_xy, unsigned* err, cudaStream_t s) {
+  dim3 block(32, 8);
+  dim3 grid((m.nVerts[0] + 31) / 32, (m.nVerts[1] + 7) / 8);
+  const double half_dt = 0.5 * dt;
+  const double2* v = reinterpret_cast<const double2*>(vel);
+  const double2* vm = reinterpret_cast<const double2*>(vel_prev);
+  double2* dxy = reinterpret_cast<double2*>(dep_xy);
+  if (!field_prev) {
+    if (ndofs == 1)
+      sl_first_kernel<N, Scalar><<<grid, block, 0, s>>>(m, Scalar{field}, v, dt, half_dt, out,
+                                                         dep_el, dxy, err);
+    else
+      sl_first_kernel<N, Vec2><<<grid, block, 0, s>>>(
+          m, Vec2{reinterpret_cast<const double2*>(field)}, v, dt, half_dt, out, dep_el, dxy,
+          err);
+  } else {
+    if (ndofs == 1)
+      sl_second_kernel<N, Scalar><<<grid, block, 0, s>>>(m, Scalar{field}, Scalar{field_prev},
+                                                          v, vm, dt, half_dt, out, dep_el, dxy,
+                                                          err);
+    else
+      sl_second_kernel<N, Vec2><<<grid, block, 0, s>>>(
+          m, Vec2{reinterpret_cast<const double2*>(field)},
+          Vec2{reinterpret_cast<const double2*>(field_prev)}, v, vm, dt, half_dt, out, dep_el,
+          dxy, err);
+  }
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------ point queries (tests) ----
+__global__ void global_to_local_kernel(const MeshDev m, const double2* __restrict__ pts,
+                                       int npts, int* el, double2* lc) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npts) return;
+  double2 p = pts[k];
+  int tx = get_topo(m, 0, p.x, nullptr), ty = get_topo(m, 1, p.y, nullptr);
+  el[k] = ty * m.nEls[0] + tx;
+  lc[k] = make_double2(local_coord(m, 0, p.x, tx), local_coord(m, 1, p.y, ty));
+}
+
+template <int N>
+__global__ void interp_points_kernel(const MeshDev m, int ndofs, const double* __restrict__ vals,
+                                     const double2* __restrict__ pts, int npts, double* out) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= npts) return;
+  double2 p = pts[k];
+  if (ndofs == 1) {
+    V1 r = interp<N>(m, Scalar{vals}, p.x, p.y, nullptr, nullptr);
+    out[k] = r.a;
+  } else {
+    V2 r = interp<N>(m, Vec2{reinterpret_cast<const double2*>(vals)}, p.x, p.y, nullptr, nullptr);
+    out[2 * k] = r.a;
+    out[2 * k + 1] = r.b;
+  }
+}
+
+__global__ void periodic_update_kernel(const MeshDev m, int ndofs, double* vals) {
+  const int nvx = m.nVerts[0], nvy = m.nVerts[1];
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  // rows: copy column 0 -> nvx-1; then columns: row 0 -> nvy-1 (incl. corner)
+  if (m.periodic[0] && k < nvy)
+    for (int d = 0; d < ndofs; d++)
+      vals[(size_t)(k * nvx + nvx - 1) * ndofs + d] = vals[(size_t)(k * nvx) * ndofs + d];
+}
+__global__ void periodic_update_rows_kernel(const MeshDev m, int ndofs, double* vals) {
+  const int nvx = m.nVerts[0], nvy = m.nVerts[1];
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m.periodic[1] && k < nvx)
+    for (int d = 0; d < ndofs; d++)
+      vals[(size_t)((nvy - 1) * nvx + k) * ndofs + d] = vals[(size_t)k * ndofs + d];
+}
+
+// Fixed-order block reduction of two sums; deterministic.
+template <int B>
+__device__ __forceinline__ void block_sum2(double& a, double& b) {
+  __shared__ double sa[B / 32], sb[B / 32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    sa[w] = a;
+    sb[w] = b;
+  }
+  __syncthreads();
+  if (w == 0) {
+    a = l < B / 32 ? sa[l] : 0.0;
+    b = l < B / 32 ? sb[l] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+  }
+}
+
+// Element quadrature sums with the affine Jacobian (hx/2)(hy/2): one block
+// per group of elements, partials summed in a second pass in fixed order.
+__global__ void __launch_bounds__(256) quadrature_kernel(const MeshDev m, int ndofs, int dof,
+                                                         const double* __restrict__ a,
+                                                         const double* __restrict__ b,
+                                                         double* partial) {
+  const int n = m.N + 1, nn = n * n;
+  const int nel = m.nEls[0] * m.nEls[1];
+  const double detj = (0.5 * m.dx[0]) * (0.5 * m.dx[1]);
+  double s0 = 0.0, s1 = 0.0;
+  for (long q = (long)blockIdx.x * blockDim.x + threadIdx.x; q < (long)nel * nn;
+       q += (long)gridDim.x * blockDim.x) {
+    int el = (int)(q / nn), pt = (int)(q - (long)el * nn);
+    int px = pt % n, py = pt / n;
+    int ex = el % m.nEls[0], ey = el / m.nEls[0];
+    int node = (ey * m.N + py) * m.nVerts[0] + ex * m.N + px;
+    double wq = detj * (m.w[px] * m.w[py]);
+    double va = a[(size_t)node * ndofs + dof];
+    if (b) {
+      double vb = b[(size_t)node * ndofs + dof];
+      s0 += wq * (va - vb) * (va - vb);
+      s1 += wq * vb * vb;
+    } else {
+      s0 += wq * va;
+    }
+  }
+  block_sum2<256>(s0, s1);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = s0;
+    partial[2 * blockIdx.x + 1] = s1;
+  }
+}
+__global__ void __launch_bounds__(256) sum_partials_kernel(const double* partial, int np,
+                                                           double* out2) {
+  double s0 = 0.0, s1 = 0.0;
+  for (int k = threadIdx.x; k < np; k += blockDim.x) {
+    s0 += partial[2 * k];
+    s1 += partial[2 * k + 1];
+  }
+  block_sum2<256>(s0, s1);
+  if (threadIdx.x == 0) {
+    out2[0] = s0;
+    out2[1] = s1;
+  }
+}
+__global__ void __launch_bounds__(256) max_speed_kernel(int nv, const double2* __restrict__ vel,
+                                                        double* partial) {
+  double mx = 0.0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nv; k += gridDim.x * blockDim.x) {
+    double2 v = vel[k];
+    double s = v.x * v.x + v.y * v.y;
+    mx = fmax(mx, s);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  __shared__ double sm[8];
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < 8; w++) mx = fmax(mx, sm[w]);
+    partial[blockIdx.x] = mx;
+  }
+}
+__global__ void max_partials_kernel(const double* partial, int np, double* out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double mx = 0.0;
+    for (int k = 0; k < np; k++) mx = fmax(mx, partial[k]);
+    *out = mx;
+  }
+}
+
+}  // namespace
+
+// Dispatch a runtime polynomial order onto the compile-time one (NN).
+#define SE_DISPATCH_N(N, ...)                     \
+  switch (N) {                                    \
+    case 2: { constexpr int NN = 2; __VA_ARGS__; }   \
+    case 3: { constexpr int NN = 3; __VA_ARGS__; }   \
+    case 4: { constexpr int NN = 4; __VA_ARGS__; }   \
+    case 5: { constexpr int NN = 5; __VA_ARGS__; }   \
+    case 6: { constexpr int NN = 6; __VA_ARGS__; }   \
+    case 7: { constexpr int NN = 7; __VA_ARGS__; }   \
+    case 8: { constexpr int NN = 8; __VA_ARGS__; }   \
+    case 9: { constexpr int NN = 9; __VA_ARGS__; }   \
+    case 10: { constexpr int NN = 10; __VA_ARGS__; } \
+    case 11: { constexpr int NN = 11; __VA_ARGS__; } \
+    case 12: { constexpr int NN = 12; __VA_ARGS__; } \
+    default: return cudaErrorInvalidValue;        \
+  }
+
+cudaError_t launch_sl(const MeshDev& m, int ndofs, const double* field, const double* vel,
+                      const double* field_prev, const double* vel_prev, double dt, double* out,
+                      int* dep_el, double* dep_xy, unsigned* err, cudaStream_t s) {
+  if (m.N < 3) return cudaErrorInvalidValue;
+  SE_DISPATCH_N(m.N, return launch_sl_n<NN>(m, ndofs, field, vel, field_prev, vel_prev, dt, out,
+                                            dep_el, dep_xy, err, s));
+}
+
+cudaError_t launch_global_to_local(const MeshDev& m, const double* pts, int npts, int* el,
+                                   double* lc, cudaStream_t s) {
+  if (npts <= 0) return cudaSuccess;
+  global_to_local_kernel<<<(npts + 255) / 256, 256, 0, s>>>(
+      m, reinterpret_cast<const double2*>(pts), npts, el, reinterpret_cast<double2*>(lc));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_interp_global(const MeshDev& m, int ndofs, const double* vals,
+                                 const double* pts, int npts, double* out, cudaStream_t s) {
+  if (npts <= 0) return cudaSuccess;
+  SE_DISPATCH_N(m.N, {
+    interp_points_kernel<NN><<<(npts + 127) / 128, 128, 0, s>>>(
+        m, ndofs, vals, reinterpret_cast<const double2*>(pts), npts, out);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t launch_periodic_update(const MeshDev& m, int ndofs, double* vals, cudaStream_t s) {
+  if (m.periodic[0])
+    periodic_update_kernel<<<(m.nVerts[1] + 255) / 256, 256, 0, s>>>(m, ndofs, vals);
+  if (m.periodic[1])
+    periodic_update_rows_kernel<<<(m.nVerts[0] + 255) / 256, 256, 0, s>>>(m, ndofs, vals);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_quadrature(const MeshDev& m, int ndofs, int dof, const double* a,
+                              const double* b, double* scratch, int nscratch, double* out2,
+                              cudaStream_t s) {
+  long work = (long)m.nEls[0] * m.nEls[1] * (m.N + 1) * (m.N + 1);
+  int blocks = (int)((work + 255) / 256);
+  if (blocks > nscratch / 2) blocks = nscratch / 2;
+  if (blocks < 1) return cudaErrorInvalidValue;
+  quadrature_kernel<<<blocks, 256, 0, s>>>(m, ndofs, dof, a, b, scratch);
+  sum_partials_kernel<<<1, 256, 0, s>>>(scratch, blocks, out2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_max_speed_sq(int nv, const double* vel, double* scratch, int nscratch,
+                                double* out, cudaStream_t s) {
+  int blocks = (nv + 255) / 256;
+  if (blocks > nscratch) blocks = nscratch;
+  if (blocks < 1) return cudaErrorInvalidValue;
+  max_speed_kernel<<<blocks, 256, 0, s>>>(nv, reinterpret_cast<const double2*>(vel), scratch);
+  max_partials_kernel<<<1, 32, 0, s>>>(scratch, blocks, out);
+  return cudaGetLastError();
+}
+
+}  // namespace seg

@@ -1,0 +1,461 @@
+"""Python mirror of SE's hot-path classes over the segpu C-ABI.
+
+The classes keep the reference's names, constructor arguments and methods,
+so code written against SE's ``src/base`` / ``src/linsys`` reads the same:
+
+=====================  =================================================
+reference (C++)        here
+=====================  =================================================
+``Mesh``               :class:`Mesh`   (src/base/Mesh.h:4-37)
+``BCs``                :class:`BCs`    (src/base/BCs.h:1-22)
+``Field``              :class:`Field`  (src/base/Field.h:5-31)
+``Advector``           :class:`Advector` (src/base/Advector.h:1-28)
+``HelmholtzEqn``       :class:`HelmholtzEqn` (src/linsys/HelmholtzEqn.h:1-22)
+``PoissonEqn``         :class:`PoissonEqn` (src/linsys/PoissonEqn.h:1-19)
+``CalcTimeStep``       :func:`CalcTimeStep` (src/base/Utils.cpp:23-40)
+``FieldError``         :func:`FieldError` (src/base/Utils.cpp:232-254)
+=====================  =================================================
+
+Everything runs on the GPU through ``libsegpu.so``; a missing library or a
+missing CUDA device raises :class:`SEError` -- there is no CPU fallback.
+Where the reference calls ``exit(1)`` on a configuration error, this layer
+raises :class:`SEError` with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsegpu.so")
+
+SE_OK = 0
+SE_ERR_ARG = -1
+SE_ERR_OOM = -2
+SE_ERR_CUDA = -3
+SE_ERR_UNSUPPORTED = -4
+SE_ERR_NOT_CONVERGED = -5
+SE_ERR_TIMEOUT = -6
+SE_ERR_DOMAIN = -7
+
+NORM_PRECONDITIONED, NORM_UNPRECONDITIONED, NORM_NATURAL = 0, 1, 2
+MODE_REFERENCE, MODE_EXACT = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+
+KSP_REASONS = {2: "CONVERGED_RTOL", 3: "CONVERGED_ATOL", -3: "DIVERGED_ITS",
+               -4: "DIVERGED_DTOL", -8: "DIVERGED_INDEFINITE_PC",
+               -9: "DIVERGED_NANORINF", -10: "DIVERGED_INDEFINITE_MAT"}
+
+
+class SEError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"segpu error {code}: {msg}")
+        self.code = code
+
+
+class SolverOpts(ctypes.Structure):
+    _fields_ = [("rtol", ctypes.c_double), ("atol", ctypes.c_double),
+                ("dtol", ctypes.c_double), ("max_it", ctypes.c_int),
+                ("norm_type", ctypes.c_int), ("mode", ctypes.c_int),
+                ("precision", ctypes.c_int), ("inner_max_it", ctypes.c_int),
+                ("inner_rtol", ctypes.c_double)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("reason", ctypes.c_int), ("its", ctypes.c_int), ("outer_its", ctypes.c_int),
+                ("rnorm", ctypes.c_double), ("rnorm0", ctypes.c_double)]
+
+    def as_dict(self):
+        return {"reason": self.reason, "its": self.its, "outer_its": self.outer_its,
+                "rnorm": self.rnorm, "rnorm0": self.rnorm0}
+
+
+_lib = None
+_vp = ctypes.c_void_p
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+# name -> argtypes for every entry point declared in include/segpu.h
+SIGNATURES = {
+    "se_last_error": [], "se_version": [], "se_set_stream": [_vp], "se_synchronize": [],
+    "se_mesh_create": [_I, ctypes.c_int, _D, _D, _I, ctypes.POINTER(_vp)],
+    "se_mesh_destroy": [_vp], "se_mesh_sizes": [_vp, _I, _I], "se_mesh_verts": [_vp, _D],
+    "se_mesh_gll": [_vp, _D, _D, _D],
+    "se_mesh_global_to_local": [_vp, _D, ctypes.c_int, _I, _D],
+    "se_bcs_create": [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                      ctypes.POINTER(_vp)],
+    "se_bcs_destroy": [_vp], "se_bcs_vec_size": [_vp, _I], "se_bcs_maps": [_vp, _I, _I],
+    "se_field_create": [_vp, ctypes.c_int, _vp, ctypes.POINTER(_vp)],
+    "se_field_destroy": [_vp], "se_field_upload": [_vp, _D], "se_field_download": [_vp, _D],
+    "se_field_device_ptr": [_vp, ctypes.POINTER(_vp)], "se_field_copy": [_vp, _vp],
+    "se_field_periodic_update": [_vp],
+    "se_field_integrate": [_vp, ctypes.c_int, ctypes.c_int, _D],
+    "se_field_interp_global": [_vp, _D, ctypes.c_int, _D],
+    "se_advector_create": [_vp, _vp, _vp, _vp, ctypes.POINTER(_vp)],
+    "se_advector_destroy": [_vp], "se_advect": [_vp, ctypes.c_double],
+    "se_advector_field_sl": [_vp, ctypes.POINTER(_vp)],
+    "se_advector_departures": [_vp, _I, _D],
+    "se_solver_opts_default": [ctypes.POINTER(SolverOpts)],
+    "se_solver_opts_parse": [ctypes.POINTER(SolverOpts), ctypes.c_char_p, ctypes.c_char_p],
+    "se_helmholtz_create": [_vp, _vp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                            ctypes.c_int, ctypes.POINTER(SolverOpts), ctypes.POINTER(_vp)],
+    "se_poisson_create": [_vp, _vp, ctypes.c_double, ctypes.POINTER(SolverOpts),
+                          ctypes.POINTER(_vp)],
+    "se_linsys_destroy": [_vp], "se_linsys_set_opts": [_vp, ctypes.POINTER(SolverOpts)],
+    "se_linsys_assemble": [_vp],
+    "se_linsys_solve": [_vp, ctypes.c_int, ctypes.POINTER(SolveStats)],
+    "se_linsys_apply": [_vp, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
+    "se_linsys_vec_size": [_vp, _I],
+    "se_calc_time_step": [_vp, ctypes.c_double, _D],
+    "se_field_error": [_vp, _vp, ctypes.c_int, ctypes.c_int, _D],
+}
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libsegpu.so (raises if it is missing: the GPU path has no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise SEError(SE_ERR_CUDA, f"{path} is missing: run `python -m se_b200.build`")
+    L = ctypes.CDLL(path)
+    for name, args in SIGNATURES.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = ctypes.c_char_p if name in ("se_last_error", "se_version") else ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != SE_OK:
+        msg = _lib.se_last_error().decode()
+        raise SEError(rc, msg)
+
+
+def _pd(a):
+    return a.ctypes.data_as(_D)
+
+
+def _pi(a):
+    return a.ctypes.data_as(_I)
+
+
+def set_stream(stream_ptr: int | None):
+    """Queue library work on a cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream)."""
+    _check(load_library().se_set_stream(_vp(stream_ptr or 0)))
+
+
+def synchronize():
+    _check(load_library().se_synchronize())
+
+
+class Mesh:
+    """Mesh(name, nEls, "legendre", N, min, max, periodic) (src/base/Mesh.h:6)."""
+
+    def __init__(self, name, nEls, elType, N, min, max, periodic):
+        if elType != "legendre":
+            raise SEError(SE_ERR_UNSUPPORTED, f"element type {elType!r}: only 'legendre' is built")
+        L = load_library()
+        self.name = name
+        self.N = int(N)
+        self.nEls = [int(nEls[0]), int(nEls[1])]
+        self.min = [float(min[0]), float(min[1])]
+        self.max = [float(max[0]), float(max[1])]
+        self.periodic = [bool(periodic[0]), bool(periodic[1])]
+        ne = (ctypes.c_int * 2)(*self.nEls)
+        mn = (ctypes.c_double * 2)(*self.min)
+        mx = (ctypes.c_double * 2)(*self.max)
+        pe = (ctypes.c_int * 2)(*[int(p) for p in self.periodic])
+        h = _vp()
+        _check(L.se_mesh_create(ne, self.N, mn, mx, pe, ctypes.byref(h)))
+        self._h = h
+        nv = (ctypes.c_int * 2)()
+        nt = ctypes.c_int()
+        _check(L.se_mesh_sizes(h, nv, ctypes.byref(nt)))
+        self.nVerts = [nv[0], nv[1]]
+        self.nVertsTotal = nt.value
+        self.nElsTotal = self.nEls[0] * self.nEls[1]
+        self.dx = [(self.max[k] - self.min[k]) / self.nEls[k] for k in range(2)]
+
+    @property
+    def verts(self):
+        v = np.zeros((self.nVertsTotal, 2))
+        _check(_lib.se_mesh_verts(self._h, _pd(v)))
+        return v
+
+    def gll(self):
+        n = self.N + 1
+        a, w, d = np.zeros(n), np.zeros(n), np.zeros(n * n)
+        _check(_lib.se_mesh_gll(self._h, _pd(a), _pd(w), _pd(d)))
+        return a, w, d.reshape(n, n)
+
+    def GlobalToLocal(self, pts):
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 2)
+        el = np.zeros(len(pts), dtype=np.int32)
+        lc = np.zeros_like(pts)
+        _check(_lib.se_mesh_global_to_local(self._h, _pd(pts), len(pts), _pi(el), _pd(lc)))
+        return el, lc
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.se_mesh_destroy(self._h)
+            self._h = None
+
+
+class BCs:
+    """BCs(bottom, top, left, right, mesh, 0) for a scalar field (src/base/BCs.h:3)."""
+
+    def __init__(self, bcBottom, bcTop, bcLeft, bcRight, mesh: Mesh, vecOffset=0):
+        if vecOffset != 0:
+            raise SEError(SE_ERR_UNSUPPORTED, "vecOffset != 0 (block systems) is not built")
+        h = _vp()
+        _check(load_library().se_bcs_create(mesh._h, int(bcBottom), int(bcTop), int(bcLeft),
+                                            int(bcRight), ctypes.byref(h)))
+        self._h, self.mesh = h, mesh
+        n = ctypes.c_int()
+        _check(_lib.se_bcs_vec_size(h, ctypes.byref(n)))
+        self.vecSize = n.value
+
+    def maps(self):
+        f2v = np.zeros(self.mesh.nVertsTotal, dtype=np.int32)
+        v2f = np.zeros(self.vecSize, dtype=np.int32)
+        _check(_lib.se_bcs_maps(self._h, _pi(f2v), _pi(v2f)))
+        return f2v, v2f
+
+    @property
+    def fieldToVecMap(self):
+        return self.maps()[0]
+
+    @property
+    def vecToFieldMap(self):
+        return self.maps()[1]
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.se_bcs_destroy(self._h)
+            self._h = None
+
+
+class Field:
+    """Field(name, mesh, nDofs, bcs) (src/base/Field.h:7). ``vals`` reads or
+    writes the whole [nVertsTotal][nDofs] array on the GPU."""
+
+    def __init__(self, name, mesh: Mesh, nDofs, bcs: BCs | None, _handle=None, _owner=None):
+        self.name, self.mesh, self.nDofs, self.bcs = name, mesh, int(nDofs), bcs
+        self._owner = _owner
+        if _handle is not None:
+            self._h, self._borrowed = _handle, True
+            return
+        h = _vp()
+        _check(load_library().se_field_create(mesh._h, self.nDofs, bcs._h if bcs else None,
+                                              ctypes.byref(h)))
+        self._h, self._borrowed = h, False
+
+    def _shape(self):
+        n = self.mesh.nVertsTotal
+        return (n,) if self.nDofs == 1 else (n, self.nDofs)
+
+    @property
+    def vals(self) -> np.ndarray:
+        out = np.zeros(self._shape())
+        _check(_lib.se_field_download(self._h, _pd(out)))
+        return out
+
+    @vals.setter
+    def vals(self, v):
+        a = np.ascontiguousarray(np.broadcast_to(np.asarray(v, dtype=np.float64), self._shape()))
+        _check(_lib.se_field_upload(self._h, _pd(a)))
+
+    def device_ptr(self) -> int:
+        p = _vp()
+        _check(_lib.se_field_device_ptr(self._h, ctypes.byref(p)))
+        return p.value
+
+    def Copy(self, field: "Field"):
+        _check(_lib.se_field_copy(self._h, field._h))
+
+    def PeriodicUpdate(self):
+        _check(_lib.se_field_periodic_update(self._h))
+
+    def Integrate(self, dof=0, average=False):
+        out = ctypes.c_double()
+        _check(_lib.se_field_integrate(self._h, dof, int(average), ctypes.byref(out)))
+        return out.value
+
+    def InterpGlobal(self, pts):
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 2)
+        out = np.zeros((len(pts), self.nDofs))
+        _check(_lib.se_field_interp_global(self._h, _pd(pts), len(pts), _pd(out)))
+        return out
+
+    def SetICFunc(self, dof, func):
+        """Field::SetICFunc (src/base/Field.cpp:226-230) with a vectorised func(x, y)."""
+        X = self.mesh.verts
+        v = self.vals
+        vals = func(X[:, 0], X[:, 1])
+        if self.nDofs == 1:
+            v = np.asarray(vals, dtype=np.float64) + 0 * v
+        else:
+            v[:, dof] = vals
+        self.vals = v
+
+    def __del__(self):
+        if getattr(self, "_h", None) and not self._borrowed and _lib is not None:
+            _lib.se_field_destroy(self._h)
+            self._h = None
+
+
+class Advector:
+    """Advector(field, velocity[, fieldMinusOne, velMinusOne]) (src/base/Advector.h:3-4)."""
+
+    def __init__(self, field: Field, velocity: Field, fieldMinusOne: Field | None = None,
+                 velMinusOne: Field | None = None):
+        h = _vp()
+        _check(load_library().se_advector_create(
+            field._h, velocity._h, fieldMinusOne._h if fieldMinusOne else None,
+            velMinusOne._h if velMinusOne else None, ctypes.byref(h)))
+        self._h = h
+        self.field, self.velocity = field, velocity
+        self.fieldMinusOne, self.velMinusOne = fieldMinusOne, velMinusOne
+        self.secondOrder = fieldMinusOne is not None
+        sl = _vp()
+        _check(_lib.se_advector_field_sl(h, ctypes.byref(sl)))
+        self.fieldSL = Field(f"{field.name}-SL", field.mesh, field.nDofs, field.bcs,
+                             _handle=sl, _owner=self)
+
+    def Advect(self, dt):
+        _check(_lib.se_advect(self._h, float(dt)))
+
+    def record_departures(self):
+        """Enable recording of departure elements/points for the next Advect."""
+        rc = _lib.se_advector_departures(self._h, None, None)
+        if rc not in (SE_OK, SE_ERR_ARG):
+            _check(rc)
+
+    def departures(self):
+        """(elements, points) of the last Advect; second order stacks x1 then x2."""
+        k = 2 if self.secondOrder else 1
+        n = self.field.mesh.nVertsTotal
+        el = np.zeros(k * n, dtype=np.int32)
+        xy = np.zeros((k * n, 2))
+        _check(_lib.se_advector_departures(self._h, _pi(el), _pd(xy)))
+        return el, xy
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.se_advector_destroy(self._h)
+            self._h = None
+
+
+def solver_opts(prefix: str = "", options: str = "", **kw) -> SolverOpts:
+    """Default solver options, a PETSc-style options string for one prefix,
+    then keyword overrides (rtol, atol, dtol, max_it, norm_type, mode, precision)."""
+    o = SolverOpts()
+    _check(load_library().se_solver_opts_default(ctypes.byref(o)))
+    if options:
+        _check(_lib.se_solver_opts_parse(ctypes.byref(o), prefix.encode(), options.encode()))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class _LinSys:
+    _h = None
+
+    def Assemble(self):
+        _check(_lib.se_linsys_assemble(self._h))
+
+    def set_opts(self, opts: SolverOpts):
+        self.opts = opts
+        _check(_lib.se_linsys_set_opts(self._h, ctypes.byref(opts)))
+
+    def _solve(self, removeNullSpace: bool, raise_on_diverge: bool):
+        st = SolveStats()
+        rc = _lib.se_linsys_solve(self._h, int(bool(removeNullSpace)), ctypes.byref(st))
+        if rc == SE_ERR_NOT_CONVERGED and not raise_on_diverge:
+            rc = SE_OK
+        _check(rc)
+        self.stats = st.as_dict()
+        return self.stats
+
+    @property
+    def vecSize(self):
+        n = ctypes.c_int()
+        _check(_lib.se_linsys_vec_size(self._h, ctypes.byref(n)))
+        return n.value
+
+    def apply(self, x_ptr: int, y_ptr: int):
+        """y = A x on device pointers of vecSize doubles."""
+        _check(_lib.se_linsys_apply(self._h, _vp(x_ptr), _vp(y_ptr)))
+
+    def diagonal(self, d_ptr: int):
+        _check(_lib.se_linsys_diagonal(self._h, _vp(d_ptr)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.se_linsys_destroy(self._h)
+            self._h = None
+
+
+class HelmholtzEqn(_LinSys):
+    """HelmholtzEqn(solField, rhsField, c, nu, dt, svvCutoff)
+    (src/linsys/HelmholtzEqn.h:3): A = c*Mass + nu*dt*Laplacian."""
+
+    def __init__(self, solField: Field, rhsField: Field | None, c, nu, dt, svvCutoff=0,
+                 opts: SolverOpts | None = None):
+        self.solField, self.rhsField = solField, rhsField
+        self.c, self.nu, self.dt = float(c), float(nu), float(dt)
+        self.opts = opts or solver_opts()
+        h = _vp()
+        _check(load_library().se_helmholtz_create(
+            solField._h, rhsField._h if rhsField else None, self.c, self.nu, self.dt,
+            int(svvCutoff), ctypes.byref(self.opts), ctypes.byref(h)))
+        self._h = h
+
+    def Solve(self, name: str = "helm_", removeNullSpace: bool = False, options: str = "",
+              raise_on_diverge: bool = False):
+        """HelmholtzEqn::Solve(name, removeNullSpace); ``options`` is the PETSc
+        options string consulted under prefix ``name``."""
+        if options:
+            o = SolverOpts.from_buffer_copy(self.opts)
+            _check(_lib.se_solver_opts_parse(ctypes.byref(o), name.encode(), options.encode()))
+            self.set_opts(o)
+        return self._solve(removeNullSpace, raise_on_diverge)
+
+
+class PoissonEqn(_LinSys):
+    """PoissonEqn(solField, rhsField, c) (src/linsys/PoissonEqn.h:3): A = c*Laplacian."""
+
+    def __init__(self, solField: Field, rhsField: Field | None, c, opts: SolverOpts | None = None):
+        self.solField, self.rhsField, self.c = solField, rhsField, float(c)
+        self.opts = opts or solver_opts()
+        h = _vp()
+        _check(load_library().se_poisson_create(solField._h, rhsField._h if rhsField else None,
+                                                self.c, ctypes.byref(self.opts),
+                                                ctypes.byref(h)))
+        self._h = h
+
+    def Solve(self, removeNullSpace: bool = False, options: str = "",
+              raise_on_diverge: bool = False):
+        """PoissonEqn::Solve(removeNullSpace) with the options prefix "poisson_"."""
+        if options:
+            o = SolverOpts.from_buffer_copy(self.opts)
+            _check(_lib.se_solver_opts_parse(ctypes.byref(o), b"poisson_", options.encode()))
+            self.set_opts(o)
+        return self._solve(removeNullSpace, raise_on_diverge)
+
+
+def CalcTimeStep(velocity: Field, courantNo: float) -> float:
+    out = ctypes.c_double()
+    _check(load_library().se_calc_time_step(velocity._h, float(courantNo), ctypes.byref(out)))
+    return out.value
+
+
+def FieldError(numeric: Field, analytic: Field, dof: int = 0, normalise: bool = True) -> float:
+    out = ctypes.c_double()
+    _check(load_library().se_field_error(numeric._h, analytic._h, dof, int(normalise),
+                                         ctypes.byref(out)))
+    return out.value
