@@ -158,6 +158,7 @@ typedef struct {
   int outer_its;  /* mixed: refinement steps; FP64: 0 */
   double rnorm;   /* final residual norm in the chosen norm */
   double rnorm0;  /* initial residual norm in the chosen norm */
+  double kernel_ms; /* device time of the CG launch(es), CUDA events */
 } se_solve_stats;
 
 int se_solver_opts_default(se_solver_opts* opts);

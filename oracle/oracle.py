@@ -67,6 +67,7 @@ def lib():
         L.or_mesh_create.restype = _vp
         L.or_mesh_create.argtypes = [_int, _int, _int, _dbl, _dbl, _dbl, _dbl, _int, _int]
         L.or_mesh_destroy.argtypes = [_vp]
+        L.or_mesh_set_accurate.argtypes = [_vp, _int]
         L.or_mesh_nverts.argtypes = [_vp]
         L.or_mesh_verts.argtypes = [_vp, _D]
         L.or_gll.argtypes = [_int, _D, _D, _D, _D]
@@ -147,7 +148,7 @@ class Mesh:
     by the reference's own ``Mesh`` class (``use_ref=True``)."""
 
     def __init__(self, nx, ny, N, lo=(0.0, 0.0), hi=(1.0, 1.0), periodic=(True, True),
-                 use_ref=False):
+                 use_ref=False, accurate=False):
         self.nx, self.ny, self.N = nx, ny, N
         self.lo, self.hi, self.periodic = tuple(lo), tuple(hi), tuple(bool(p) for p in periodic)
         self.use_ref = use_ref
@@ -156,6 +157,9 @@ class Mesh:
         self.h = create(nx, ny, N, lo[0], lo[1], hi[0], hi[1], int(periodic[0]), int(periodic[1]))
         if not self.h:
             raise ValueError("mesh rejected")
+        if accurate:
+            assert not use_ref, "the reference has only its own formula"
+            self.L.or_mesh_set_accurate(self.h, 1)
         self.nvx, self.nvy = nx * N + 1, ny * N + 1
         self.nv = self.nvx * self.nvy
 

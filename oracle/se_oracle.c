@@ -57,6 +57,7 @@ struct or_mesh {
   double dC[(MAXN + 1) * (MAXN + 1)];
   double Pc[MAXN + 2]; /* monomial coefficients of P_N */
   double* verts;       /* [nVertsTotal][2] */
+  int accurate;        /* 1: cardinal functions in extended precision */
 };
 
 /* ---------------------------------------------------------------- Jacobi --
@@ -305,12 +306,54 @@ void or_shape_funcs_at(const or_mesh* m, const double* coords, int npts, double*
   for (int k = 0; k < npts; k++) shape_funcs_at(m, coords + 2 * k, Ni + (size_t)k * m->nn);
 }
 
+/* Extended-precision variant of the interpolation, a test switch that is
+ * not part of the reference: the same element search, local coordinates and
+ * 1e-8 node snap, but the cardinal functions as Lagrange products and the
+ * sum in long double. The reference's own formula evaluates P_N'(x) as a
+ * monomial sum, which cancels near the GLL nodes (relative error up to
+ * ~1e-16 * C / |x - x_k|, i.e. ~1e-8 at the snap radius); this variant is
+ * accurate to rounding and measures how close a faster evaluation is to
+ * the reference's mathematics. */
+static void interp_accurate(const or_mesh* m, int ndofs, const double* vals, int el,
+                            const double* l, double* val) {
+  int N = m->N, snap[2];
+  long double c[2][MAXN + 1];
+  for (int d = 0; d < 2; d++) {
+    if (is_root(m, l[d], &snap[d])) {
+      for (int j = 0; j <= N; j++) c[d][j] = (j == snap[d]) ? 1.0L : 0.0L;
+    } else {
+      for (int j = 0; j <= N; j++) {
+        long double p = 1.0L;
+        for (int k = 0; k <= N; k++)
+          if (k != j)
+            p *= ((long double)l[d] - (long double)m->abcissa[k]) /
+                 ((long double)m->abcissa[j] - (long double)m->abcissa[k]);
+        c[d][j] = p;
+      }
+    }
+  }
+  int nodes[(MAXN + 1) * (MAXN + 1)];
+  el_nodes(m, el, nodes);
+  for (int d = 0; d < ndofs; d++) {
+    long double s = 0.0L;
+    for (int k = 0; k < m->nn; k++)
+      s += c[0][k % (N + 1)] * c[1][k / (N + 1)] * (long double)vals[(size_t)nodes[k] * ndofs + d];
+    val[d] = (double)s;
+  }
+}
+
+void or_mesh_set_accurate(or_mesh* m, int on) { m->accurate = on != 0; }
+
 /* src/base/Field.cpp:57-76 */
 static void interp_global(const or_mesh* m, int ndofs, const double* vals,
                           const double* g, double* val) {
   double l[2], Ni[(MAXN + 1) * (MAXN + 1)];
   int nodes[(MAXN + 1) * (MAXN + 1)];
   int el = global_to_local(m, g, l);
+  if (m->accurate) {
+    interp_accurate(m, ndofs, vals, el, l, val);
+    return;
+  }
   shape_funcs_at(m, l, Ni);
   el_nodes(m, el, nodes);
   for (int d = 0; d < ndofs; d++) val[d] = 0.0;

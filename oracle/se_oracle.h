@@ -30,6 +30,9 @@ void or_gll(int N, double* abcissa, double* weights, double* dCij, double* Pj);
 or_mesh* or_mesh_create(int nx, int ny, int N, double x0, double y0, double x1,
                         double y1, int perx, int pery);
 void or_mesh_destroy(or_mesh* m);
+/* Test switch, not part of the reference: interpolate with extended-precision
+ * Lagrange-product cardinal functions (same search, coordinates and snap). */
+void or_mesh_set_accurate(or_mesh* m, int on);
 int or_mesh_nverts(const or_mesh* m);
 void or_mesh_verts(const or_mesh* m, double* out);
 void or_global_to_local(const or_mesh* m, const double* pts, int npts, int* el,

@@ -7,7 +7,9 @@ reference's classes (Mesh, BCs, Field, Advector, HelmholtzEqn, PoissonEqn)
 over that C-ABI.
 """
 from .segpu import (BCs, Advector, CalcTimeStep, Field, FieldError, HelmholtzEqn, Mesh,  # noqa: F401
-                    PoissonEqn, SEError, load_library, set_stream, solver_opts, synchronize)
+                    PoissonEqn, SEError, load_library, set_stream, solver_opts, synchronize,
+                    MODE_EXACT, MODE_REFERENCE, PREC_FP64, PREC_MIXED, NORM_NATURAL,
+                    NORM_PRECONDITIONED, NORM_UNPRECONDITIONED)
 
 __all__ = ["Mesh", "BCs", "Field", "Advector", "HelmholtzEqn", "PoissonEqn", "CalcTimeStep",
            "FieldError", "SEError", "load_library", "set_stream", "synchronize", "solver_opts"]

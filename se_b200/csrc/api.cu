@@ -252,6 +252,7 @@ struct se_linsys {
   int* d_active;
   unsigned* d_err;
   int grid, nseg, seg_begin, seg_end;
+  cudaEvent_t ev[2];
 };
 
 namespace {
@@ -379,6 +380,8 @@ void linsys_free(se_linsys* ls) {
   dfree(ls->d_bar);
   dfree(ls->d_active);
   dfree(ls->d_err);
+  if (ls->ev[0]) cudaEventDestroy(ls->ev[0]);
+  if (ls->ev[1]) cudaEventDestroy(ls->ev[1]);
   delete ls->own_bcs;
   delete ls;
 }
@@ -393,8 +396,17 @@ int linsys_alloc(se_linsys* ls) {
   CK(cudaMemset(ls->lift, 0, sizeof(double) * n));
   int dev = 0;
   CK(cudaGetDevice(&dev));
-  const int maxg = cg_max_grid(dev);
+  int maxg = cg_max_grid(dev, ls->op.d[0].N);
   if (maxg <= 0) return fail(SE_ERR_CUDA, "cannot size the cooperative CG launch");
+  {
+    // Blocks per SM for the persistent CG: fewer blocks mean fewer barrier
+    // arrivals and partial sums per iteration; the default of 2 was the best
+    // of 1..4 on the 64x64, p=8 solve. SE_CG_BLOCKS_PER_SM overrides it.
+    int sms = 1, per = 2;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (const char* e = std::getenv("SE_CG_BLOCKS_PER_SM")) per = std::max(1, std::atoi(e));
+    maxg = std::min(maxg, sms * per);
+  }
   Schedule S = make_schedule({&ls->op}, maxg);
   ls->grid = (int)S.block_begin.size() - 1;
   ls->nseg = S.nseg;
@@ -416,7 +428,7 @@ int linsys_alloc(se_linsys* ls) {
 
 // Run the persistent CG for A x = b on this system's schedule; fills stats.
 int run_cg(se_linsys* ls, const double* b, double* x, double rtol, double atol, double dtol,
-           int max_it, int remove_null, CgSolve* out_state) {
+           int max_it, int remove_null, CgSolve* out_state, float* kernel_ms) {
   CgSolve cs = make_solve(ls, b, x, rtol, atol, dtol, max_it, remove_null);
   cudaStream_t s = g_stream;
   CK(cudaMemcpyAsync(ls->d_solve, &cs, sizeof(cs), cudaMemcpyHostToDevice, s));
@@ -433,11 +445,18 @@ int run_cg(se_linsys* ls, const double* b, double* x, double rtol, double atol, 
   B.bar_gen = ls->d_bar + 1;
   B.n_active = ls->d_active;
   B.err = ls->d_err;
-  CK(launch_cg(B, ls->grid, s));
+  if (!ls->ev[0]) {
+    CK(cudaEventCreate(&ls->ev[0]));
+    CK(cudaEventCreate(&ls->ev[1]));
+  }
+  CK(cudaEventRecord(ls->ev[0], s));
+  CK(launch_cg(B, ls->grid, ls->op.d[0].N, s));
+  CK(cudaEventRecord(ls->ev[1], s));
   unsigned err = 0;
   CK(cudaMemcpyAsync(out_state, ls->d_solve, sizeof(CgSolve), cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&err, ls->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  if (kernel_ms) CK(cudaEventElapsedTime(kernel_ms, ls->ev[0], ls->ev[1]));
   if (err & KERR_BARRIER_TIMEOUT) return fail(SE_ERR_TIMEOUT, "CG grid barrier timed out");
   return SE_OK;
 }
@@ -946,8 +965,9 @@ int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats)
   const MeshDev& m = ls->sol->mesh->dev;
   CK(launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, g_stream));
   CgSolve st;
+  float kms = 0.f;
   int rc = run_cg(ls, ls->f, ls->x, ls->opts.rtol, ls->opts.atol, ls->opts.dtol, ls->opts.max_it,
-                  remove_null_space, &st);
+                  remove_null_space, &st, &kms);
   if (rc) return rc;
   CK(launch_update_field(ls->op, m, ls->x, ls->sol->vals, g_stream));
   if (stats) {
@@ -956,6 +976,7 @@ int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats)
     stats->outer_its = 0;
     stats->rnorm = st.dp;
     stats->rnorm0 = st.rnorm0;
+    stats->kernel_ms = kms;
   }
   if (st.reason < 0) return fail(SE_ERR_NOT_CONVERGED, "KSP diverged, reason %d after %d its",
                                  st.reason, st.its);

@@ -144,10 +144,12 @@ struct CgBatch {
   unsigned* err;
 };
 constexpr int kCgTileX = 32;
-constexpr int kCgTileY = 8;
+constexpr int kCgTileY = 16;
 constexpr int kCgThreads = kCgTileX * kCgTileY;
+// Shared memory of one CG block for polynomial orders up to maxN.
+size_t cg_smem_bytes(int maxN);
 // Blocks of kCgThreads that can be co-resident on this device.
-int cg_max_grid(int device);
-cudaError_t launch_cg(const CgBatch& batch, int grid, cudaStream_t s);
+int cg_max_grid(int device, int maxN);
+cudaError_t launch_cg(const CgBatch& batch, int grid, int maxN, cudaStream_t s);
 
 }  // namespace seg

@@ -95,14 +95,94 @@ __device__ __forceinline__ double apply_at(const OpDev& op, int gx, int gy, cons
   return op.alpha * wx * wy * self + op.beta[0] * wy * kx + op.beta[1] * wx * ky;
 }
 
-__global__ void __launch_bounds__(256) op_apply_kernel(const OpDev op, const double* __restrict__ x,
-                                                       double* __restrict__ y) {
-  const int ux = blockIdx.x * blockDim.x + threadIdx.x;
-  const int uy = blockIdx.y * blockDim.y + threadIdx.y;
-  if (ux >= op.G[0] || uy >= op.G[1]) return;
+// ------------------------------------------------ shared-memory tiles ----
+// A tile of kCgTileX x kCgTileY unknowns plus a halo of N vertices on every
+// side, in unwrapped vertex coordinates: the halo of a periodic boundary
+// vertex holds the wrapped-around vertices, and halo entries that are not
+// unknowns (Dirichlet, outside a non-periodic mesh) hold 0. Loading it is one
+// batch of independent coalesced loads; the stencil taps then read shared
+// memory instead of chaining one L2 round trip per tap.
+__device__ __forceinline__ int tile_w(int N) { return kCgTileX + 2 * N; }
+__device__ __forceinline__ int tile_h(int N) { return kCgTileY + 2 * N; }
+
+// Unknown index along one direction of unwrapped vertex g, or -1.
+__device__ __forceinline__ int unknown_of(const Dir& d, int g) {
+  if (d.periodic) {
+    const int L = d.nV - 1;
+    g %= L;
+    if (g < 0) g += L;
+  } else if (g < 0 || g >= d.nV) {
+    return -1;
+  }
+  return (g >= d.lo && g < d.hi) ? g - d.lo : -1;
+}
+
+// Row of the assembled 1-D stiffness at (unwrapped) vertex g applied to the
+// tile values around p (stride between neighbouring vertices).
+__device__ __forceinline__ double krow_tile(const OpDev& op, const Dir& d, int g, const double* p,
+                                            int stride) {
+  const int N = d.N, n = N + 1;
+  const int e = g / N, a = g - e * N;
+  double s = 0.0;
+  if (a != 0) {
+    const double* k = op.Kh + a * n;
+    const double* q = p - a * stride;
+    for (int b = 0; b < n; b++) s = fma(k[b], q[b * stride], s);
+    return s;
+  }
+  if (e > 0 || d.periodic) {
+    const double* k = op.Kh + N * n;
+    const double* q = p - N * stride;
+    for (int b = 0; b < n; b++) s = fma(k[b], q[b * stride], s);
+  }
+  if (e < d.nE) {
+    const double* k = op.Kh;
+    for (int b = 0; b < n; b++) s = fma(k[b], p[b * stride], s);
+  }
+  return s;
+}
+
+// Fill the tile at unknown origin (x0, y0) with val(ux, uy) (only the cross
+// the stencil reads: the tile's rows at full width, its columns at full
+// height), then __syncthreads.
+template <class F>
+__device__ __forceinline__ void load_tile(const OpDev& op, int x0, int y0, double* P, const F& val) {
+  const int N = op.d[0].N, W = tile_w(N), H = tile_h(N);
+  const int gx0 = x0 + op.d[0].lo - N, gy0 = y0 + op.d[1].lo - N;
+  for (int k = threadIdx.x; k < W * H; k += blockDim.x) {
+    const int i = k % W, j = k / W;
+    double v = 0.0;
+    if ((j >= N && j < N + kCgTileY) || (i >= N && i < N + kCgTileX)) {
+      const int ux = unknown_of(op.d[0], gx0 + i), uy = unknown_of(op.d[1], gy0 + j);
+      if (ux >= 0 && uy >= 0) v = val(ux, uy);
+    }
+    P[k] = v;
+  }
+  __syncthreads();
+}
+
+// (A p) at this thread's unknown of the tile, from the staged tile.
+__device__ __forceinline__ double apply_tile(const OpDev& op, int gx, int gy, const double* P,
+                                             int tx, int ty) {
+  const int N = op.d[0].N, W = tile_w(N);
+  const double* c = P + (ty + N) * W + (tx + N);
+  const double wx = wsum(op, op.d[0], gx), wy = wsum(op, op.d[1], gy);
+  const double kx = krow_tile(op, op.d[0], gx, c, 1);
+  const double ky = krow_tile(op, op.d[1], gy, c, W);
+  return op.alpha * wx * wy * c[0] + op.beta[0] * wy * kx + op.beta[1] * wx * ky;
+}
+
+__global__ void __launch_bounds__(kCgThreads) op_apply_tile_kernel(const OpDev op,
+                                                                    const double* __restrict__ x,
+                                                                    double* __restrict__ y) {
+  extern __shared__ double smem[];
+  const int x0 = blockIdx.x * kCgTileX, y0 = blockIdx.y * kCgTileY;
   const int G0 = op.G[0];
-  auto xv = [&](int a, int b) { return __ldg(x + (size_t)b * G0 + a); };
-  y[(size_t)uy * G0 + ux] = apply_at(op, ux + op.d[0].lo, uy + op.d[1].lo, xv);
+  load_tile(op, x0, y0, smem, [&](int a, int b) { return __ldg(x + (size_t)b * G0 + a); });
+  const int tx = threadIdx.x % kCgTileX, ty = threadIdx.x / kCgTileX;
+  const int ux = x0 + tx, uy = y0 + ty;
+  if (ux >= op.G[0] || uy >= op.G[1]) return;
+  y[(size_t)uy * G0 + ux] = apply_tile(op, ux + op.d[0].lo, uy + op.d[1].lo, smem, tx, ty);
 }
 
 __global__ void op_diag_kernel(const OpDev op, double* __restrict__ d) {
@@ -267,11 +347,21 @@ __device__ __forceinline__ void block_sum4(double v[4]) {
 }
 
 // Sum of partial slot q over a solve's segments, fixed order; result valid in
-// every lane of warp 0.
+// every lane of the calling warp. Lane l sums segments l, l+32, ... in order;
+// the loads of a lane are issued eight at a time so that the L2 round trips
+// overlap.
 __device__ __forceinline__ double seg_sum(const CgBatch& B, const CgSolve& S, int q) {
   const int l = threadIdx.x & 31;
   double s = 0.0;
-  for (int k = S.seg_begin + l; k < S.seg_end; k += 32) s += B.partials[(size_t)k * 4 + q];
+  int k = S.seg_begin + l;
+  for (; k + 7 * 32 < S.seg_end; k += 8 * 32) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) v[u] = B.partials[(size_t)(k + u * 32) * 4 + q];
+#pragma unroll
+    for (int u = 0; u < 8; u++) s += v[u];
+  }
+  for (; k < S.seg_end; k += 32) s += B.partials[(size_t)k * 4 + q];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   return s;
@@ -281,7 +371,7 @@ enum { PH_INIT = 0, PH_NULL, PH_APPLY, PH_UPDATE };
 
 // One pass over this block's tiles. Accumulates per-segment partial sums.
 template <int PH>
-__device__ void cg_pass(const CgBatch& B, int t0, int t1) {
+__device__ void cg_pass(const CgBatch& B, int t0, int t1, double* smem) {
   const int tx = threadIdx.x & (kCgTileX - 1), ty = threadIdx.x / kCgTileX;
   int cur_seg = -1;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
@@ -300,6 +390,34 @@ __device__ void cg_pass(const CgBatch& B, int t0, int t1) {
       for (int q = 0; q < 4; q++) acc[q] = 0.0;
     }
     if (S.done) continue;
+    if (PH == PH_APPLY) {
+      // p = z + bcoef p_old (p = z on the first iteration) staged with its
+      // halo; w = A p; the current p is (pbuf ? p1 : p0) and the new one goes
+      // to the other buffer. z and p are rewritten by this kernel between
+      // passes: plain coherent loads, never the read-only path.
+      const int G0 = S.op.G[0];
+      const double* z = S.z;
+      const double* po = S.pbuf ? S.p1 : S.p0;
+      double* pn = S.pbuf ? S.p0 : S.p1;
+      const bool first = S.its == 0;
+      const double bc = S.bcoef;
+      load_tile(S.op, T.x0, T.y0, smem, [&](int a, int b) {
+        const size_t q = (size_t)b * G0 + a;
+        return first ? z[q] : fma(bc, po[q], z[q]);
+      });
+      const int ux = T.x0 + tx, uy = T.y0 + ty;
+      if (ux < S.op.G[0] && uy < S.op.G[1]) {
+        const int N = S.op.d[0].N;
+        const double p = smem[(ty + N) * tile_w(N) + (tx + N)];
+        const double w = apply_tile(S.op, ux + S.op.d[0].lo, uy + S.op.d[1].lo, smem, tx, ty);
+        const size_t k = (size_t)uy * G0 + ux;
+        pn[k] = p;
+        S.w[k] = w;
+        acc[0] += p * w;
+      }
+      __syncthreads();  // the next tile reuses the shared buffer
+      continue;
+    }
     const int ux = T.x0 + tx, uy = T.y0 + ty;
     if (ux >= S.op.G[0] || uy >= S.op.G[1]) continue;
     const int G0 = S.op.G[0];
@@ -325,23 +443,7 @@ __device__ void cg_pass(const CgBatch& B, int t0, int t1) {
       acc[1] += z * r;
       acc[2] += r * r;
     } else if (PH == PH_APPLY) {
-      // p = z + bcoef p_old (p = z on the first iteration); w = A p. The
-      // current p is (pbuf ? p1 : p0); the new one goes to the other buffer.
-      const double* z = S.z;
-      const double* po = S.pbuf ? S.p1 : S.p0;
-      double* pn = S.pbuf ? S.p0 : S.p1;
-      const double bc = S.its == 0 ? 0.0 : S.bcoef;
-      // z and p are rewritten by this kernel between passes: plain coherent
-      // loads, never the read-only (non-coherent) path.
-      auto pv = [&](int a, int b) {
-        const size_t q = (size_t)b * G0 + a;
-        return S.its == 0 ? z[q] : fma(bc, po[q], z[q]);
-      };
-      const double p = pv(ux, uy);
-      const double w = apply_at(S.op, gx, gy, pv);
-      pn[k] = p;
-      S.w[k] = w;
-      acc[0] += p * w;
+      // handled per tile by cg_apply_tile
     } else {
       // x += a p; r -= a w; z = D^{-1} r (p is the buffer the apply wrote;
       // the barrier after the apply flipped pbuf to point at it)
@@ -396,6 +498,7 @@ __device__ __forceinline__ void cg_converged(CgSolve& S, int n, double dp) {
 }
 
 __global__ void __launch_bounds__(kCgThreads) cg_kernel(const CgBatch B) {
+  extern __shared__ double smem[];
   const int t0 = B.block_tile_begin[blockIdx.x], t1 = B.block_tile_begin[blockIdx.x + 1];
   const bool any_null = [&] {
     for (int s = 0; s < B.nsolves; s++)
@@ -404,7 +507,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(const CgBatch B) {
   }();
 
   // ---- r = b, z = D^{-1} r; norms; beta = z.r
-  cg_pass<PH_INIT>(B, t0, t1);
+  cg_pass<PH_INIT>(B, t0, t1, smem);
   grid_barrier(B, [&] {
     if (threadIdx.x >= 32) return;
     for (int s = 0; s < B.nsolves; s++) {
@@ -415,7 +518,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(const CgBatch B) {
   });
   if (*B.err) return;
   if (any_null) {
-    cg_pass<PH_NULL>(B, t0, t1);
+    cg_pass<PH_NULL>(B, t0, t1, smem);
     grid_barrier(B, [] {});
     if (*B.err) return;
   }
@@ -453,7 +556,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(const CgBatch B) {
 
   while (*(volatile int*)B.n_active > 0) {
     // ---- p = z + (beta/betaold) p; w = A p; dpi = p.w
-    cg_pass<PH_APPLY>(B, t0, t1);
+    cg_pass<PH_APPLY>(B, t0, t1, smem);
     grid_barrier(B, [&] {
       if (threadIdx.x >= 32) return;
       for (int s = 0; s < B.nsolves; s++) {
@@ -477,7 +580,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(const CgBatch B) {
     });
     if (*B.err) return;
     // ---- x += a p, r -= a w, z = D^{-1} r; norms
-    cg_pass<PH_UPDATE>(B, t0, t1);
+    cg_pass<PH_UPDATE>(B, t0, t1, smem);
     if (any_null) {
       grid_barrier(B, [&] {
         if (threadIdx.x >= 32) return;
@@ -488,7 +591,7 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(const CgBatch B) {
         }
       });
       if (*B.err) return;
-      cg_pass<PH_NULL>(B, t0, t1);
+      cg_pass<PH_NULL>(B, t0, t1, smem);
     }
     grid_barrier(B, [&] {
       if (threadIdx.x >= 32) return;
@@ -529,9 +632,13 @@ __global__ void __launch_bounds__(kCgThreads) cg_kernel(const CgBatch B) {
 
 }  // namespace
 
+size_t cg_smem_bytes(int maxN) {
+  return sizeof(double) * (size_t)(kCgTileX + 2 * maxN) * (kCgTileY + 2 * maxN);
+}
+
 cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, cudaStream_t s) {
-  dim3 block(32, 8), grid((op.G[0] + 31) / 32, (op.G[1] + 7) / 8);
-  op_apply_kernel<<<grid, block, 0, s>>>(op, x, y);
+  dim3 grid((op.G[0] + kCgTileX - 1) / kCgTileX, (op.G[1] + kCgTileY - 1) / kCgTileY);
+  op_apply_tile_kernel<<<grid, kCgThreads, cg_smem_bytes(op.d[0].N), s>>>(op, x, y);
   return cudaGetLastError();
 }
 cudaError_t launch_op_diag(const OpDev& op, double* d, cudaStream_t s) {
@@ -558,20 +665,20 @@ cudaError_t launch_update_field(const OpDev& op, const MeshDev& m, const double*
   return cudaGetLastError();
 }
 
-int cg_max_grid(int device) {
+int cg_max_grid(int device, int maxN) {
   int sms = 0, per_sm = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
     return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_kernel, kCgThreads, 0) !=
-      cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_kernel, kCgThreads,
+                                                    cg_smem_bytes(maxN)) != cudaSuccess)
     return 0;
   return sms * per_sm;
 }
 
-cudaError_t launch_cg(const CgBatch& batch, int grid, cudaStream_t s) {
+cudaError_t launch_cg(const CgBatch& batch, int grid, int maxN, cudaStream_t s) {
   void* args[] = {const_cast<CgBatch*>(&batch)};
   return cudaLaunchCooperativeKernel((const void*)cg_kernel, dim3(grid), dim3(kCgThreads), args,
-                                     0, s);
+                                     cg_smem_bytes(maxN), s);
 }
 
 }  // namespace seg

@@ -65,11 +65,12 @@ class SolverOpts(ctypes.Structure):
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("reason", ctypes.c_int), ("its", ctypes.c_int), ("outer_its", ctypes.c_int),
-                ("rnorm", ctypes.c_double), ("rnorm0", ctypes.c_double)]
+                ("rnorm", ctypes.c_double), ("rnorm0", ctypes.c_double),
+                ("kernel_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {"reason": self.reason, "its": self.its, "outer_its": self.outer_its,
-                "rnorm": self.rnorm, "rnorm0": self.rnorm0}
+                "rnorm": self.rnorm, "rnorm0": self.rnorm0, "kernel_ms": self.kernel_ms}
 
 
 _lib = None

@@ -3,7 +3,11 @@ persistent Jacobi-PCG (src/linsys/HelmholtzEqn.cpp, PoissonEqn.cpp) against
 the oracle's assembled AIJ operator and restated PETSc KSPCG, through the
 C-ABI.
 
-Tolerances (FP64): operator apply within 1e-13 of |A||x| row scale;
+Tolerances (FP64): operator apply within 2e-11 of the |A||x| row scale --
+the reference builds every element matrix through a numerically computed
+Jacobian, so its own element matrices differ from element to element by up
+to 5.1e-12 relative on these cases (identical in exact arithmetic on SE's
+uniform meshes);
 solutions of rtol=1e-12 solves within 1e-8 relative; iteration counts within
 2 of the oracle's; repeated solves bit-identical.
 """
@@ -61,12 +65,12 @@ def test_apply_matches_assembled_operator(segpu, oracle, case, quirk):
     torch.cuda.synchronize()
     rowptr, col, val, _ = A.arrays()
     scale = np.array([np.abs(val[rowptr[i]:rowptr[i + 1]]).sum() for i in range(n)]) * np.abs(x).max()
-    assert (np.abs(yd.cpu().numpy() - ref) / scale).max() < 1e-13
+    assert (np.abs(yd.cpu().numpy() - ref) / scale).max() < 2e-11
     d = torch.zeros(n, device="cuda", dtype=torch.float64)
     ls.diagonal(d.data_ptr())
     torch.cuda.synchronize()
     diag = np.array([val[rowptr[i]:rowptr[i + 1]][col[rowptr[i]:rowptr[i + 1]] == i][0] for i in range(n)])
-    assert np.abs(d.cpu().numpy() - diag).max() <= 1e-13 * np.abs(diag).max()
+    assert np.abs(d.cpu().numpy() - diag).max() <= 2e-11 * np.abs(diag).max()
 
 
 @pytest.mark.parametrize("case", range(len(CASES)))
@@ -90,6 +94,7 @@ def test_solve_deterministic_and_reusable(segpu, oracle):
     v1 = fs.vals
     b = ls.Solve("helm_")
     v2 = fs.vals
+    a.pop("kernel_ms"), b.pop("kernel_ms")
     assert a == b and np.array_equal(v1, v2)
 
 
@@ -127,12 +132,16 @@ def test_config0_exact_modal_solution(segpu, oracle):
 
 
 def test_poisson_null_space(segpu, oracle):
-    """Doubly periodic Poisson with a constant null space removed."""
+    """Doubly periodic Poisson with a constant null space removed, for a
+    consistent right-hand side (zero mean): converges like the oracle. With an
+    inconsistent one (nonzero mean) the projected Jacobi-CG breaks down and
+    both report KSP_DIVERGED_INDEFINITE_PC at the same iteration."""
     case = (6, 6, 5, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False))
     om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, case, -1.0, 0, 0, True,
                                                      poisson=True)
     X = om.verts()
-    rhs = om.periodic_update(np.sin(2 * np.pi * X[:, 0]) * np.cos(4 * np.pi * X[:, 1]) + 0.3)
+    rhs = om.periodic_update(np.sin(2 * np.pi * X[:, 0]) * np.cos(4 * np.pi * X[:, 1])
+                             + np.cos(2 * np.pi * X[:, 1]))
     fr.vals = rhs
     ref_sol, st = oracle.helmholtz_solve(om, sol, rhs, -1.0, 0, 0, quirk=True, rtol=1e-10,
                                          remove_null_space=True, poisson=True)
@@ -141,6 +150,13 @@ def test_poisson_null_space(segpu, oracle):
     assert abs(out["its"] - st["its"]) <= 2
     got = fs.vals
     assert np.abs(got - ref_sol).max() <= 1e-7 * np.abs(ref_sol).max()
+    bad = om.periodic_update(rhs + 0.3)
+    fr.vals = bad
+    _, st2 = oracle.helmholtz_solve(om, sol, bad, -1.0, 0, 0, quirk=True, rtol=1e-10,
+                                    remove_null_space=True, poisson=True)
+    out2 = ls.Solve(removeNullSpace=True)
+    assert st2["reason"] == out2["reason"] == -8
+    assert abs(st2["its"] - out2["its"]) <= 1
 
 
 def test_solver_reasons(segpu, oracle):
