@@ -198,6 +198,29 @@ int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev);
 int se_linsys_diagonal(se_linsys* ls, double* d_dev);
 int se_linsys_vec_size(const se_linsys* ls, int* n);
 
+/* No counterpart in the reference: HelmholtzEqn/PoissonEqn construction,
+ * Assemble and Solve in one call that allocates no memory, for callers that
+ * cannot call cudaMalloc (a driver that reserves its whole device-memory
+ * budget at start-up while other components share the GPU, or a time loop
+ * that cannot take the device-wide synchronisation cudaMalloc/cudaFree may
+ * cause mid-step). The mesh is given by the Mesh/BCs constructor arguments
+ * (bcs = {bottom, top, left, right}); rhs_dev (nullable) and sol_dev are
+ * caller-owned device arrays of nVertsTotal doubles in the reference's vertex
+ * order; sol_dev holds the Dirichlet values on entry and the solution on
+ * return. poisson != 0 selects A = c*Laplacian (nu, dt ignored).
+ * Limit: at most 65536 vector unknowns (e.g. 32x32 elements at N = 8);
+ * larger systems return SE_ERR_UNSUPPORTED. All temporaries live in one
+ * static device array of about 4.5 MB that every GPU loading the library
+ * holds until exit; every call shares it, so calls whose device work
+ * overlaps race and must be serialised by the caller. The first call on a
+ * device looks the array up (cudaGetSymbolAddress) and should come before
+ * any stream capture. */
+int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double min[2],
+                               const double max[2], const int periodic[2], const int bcs[4],
+                               double c, double nu, double dt, int poisson,
+                               const se_solver_opts* opts, int remove_null_space,
+                               const double* rhs_dev, double* sol_dev, se_solve_stats* stats);
+
 /* ------------------------------------------------------------ utilities -- */
 /* CalcTimeStep(velocity, courantNo) (src/base/Utils.cpp:23-40). */
 int se_calc_time_step(const se_field* velocity, double courant, double* dt);

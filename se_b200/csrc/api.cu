@@ -1031,3 +1031,222 @@ int se_field_error(const se_field* numeric, const se_field* analytic, int dof, i
 }
 
 }  // extern "C"
+
+// ===================================================== no-allocation solve ==
+// se_helmholtz_solve_noalloc: the whole HelmholtzEqn/PoissonEqn
+// construct-assemble-solve sequence in one call that allocates nothing. It
+// is for callers that cannot call cudaMalloc: a model driver that reserves
+// its whole device-memory budget at start-up (other components share the
+// GPU and a later allocation may fail or evict them), or a time loop that
+// cannot afford the implicit device-wide synchronisation cudaMalloc/cudaFree
+// may cause in the middle of a step. The caller passes the field arrays;
+// every temporary lives in g_noalloc_scratch below.
+//
+// Limits and sharing: at most kNoAllocMaxUnknowns vector unknowns and
+// kNoAllocMaxTiles tiles of 32x16 unknowns per solve; larger systems are
+// rejected with SE_ERR_UNSUPPORTED. The array is held by every GPU that loads
+// the library until the process exits, and every call on a device shares it
+// and leaves its contents behind: calls whose device work overlaps (other
+// streams, other host threads) race on it and must be serialised by the
+// caller. The first call on each device looks up the array's device address
+// (cudaGetSymbolAddress, with that device current); make that first call
+// before any stream capture.
+namespace {
+constexpr int kNoAllocMaxUnknowns = 65536;
+constexpr int kNoAllocMaxTiles = 8192;
+constexpr int kNoAllocMaxGrid = 4096;
+constexpr size_t kNoAllocVecDoubles = 8 * (size_t)kNoAllocMaxUnknowns;  // f lift x r z p0 p1 w
+constexpr size_t kNoAllocPartialDoubles = 4 * (size_t)kNoAllocMaxGrid;
+constexpr size_t kNoAllocSolveDoubles = (sizeof(CgSolve) + 255) / 256 * 256 / sizeof(double);
+constexpr size_t kNoAllocTileDoubles = (sizeof(CgTile) * kNoAllocMaxTiles + 255) / 256 * 256 / sizeof(double);
+constexpr size_t kNoAllocBeginDoubles = (sizeof(int) * (kNoAllocMaxGrid + 1) + 255) / 256 * 256 / sizeof(double);
+// barrier count, generation, active count and error word, each on its own
+// 128-byte line: 128 unsigned words
+constexpr size_t kNoAllocWordDoubles = 64;
+constexpr size_t kNoAllocDoubles = kNoAllocVecDoubles + kNoAllocPartialDoubles + kNoAllocSolveDoubles +
+                                   kNoAllocTileDoubles + kNoAllocBeginDoubles + kNoAllocWordDoubles;
+}  // namespace
+
+// About 4.4 MB per device: 8 vectors of 65536 doubles plus the schedule.
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;                // guards the host-side tables below
+double* g_noalloc_dev[kMaxDevices];     // device address of the scratch, per device
+CgTile g_noalloc_tiles[kNoAllocMaxTiles];
+int g_noalloc_begin[kNoAllocMaxGrid + 1];
+}  // namespace
+
+extern "C" int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double min[2],
+                                          const double max[2], const int periodic[2],
+                                          const int bcs[4], double c, double nu, double dt,
+                                          int poisson, const se_solver_opts* opts,
+                                          int remove_null_space, const double* rhs_dev,
+                                          double* sol_dev, se_solve_stats* stats) {
+  if (!nEls || !min || !max || !periodic || !bcs || !sol_dev)
+    return fail(SE_ERR_ARG, "null argument");
+  if (N < 2 || N > SE_MAXN)
+    return fail(SE_ERR_UNSUPPORTED, "polynomial order %d outside [2, %d]", N, SE_MAXN);
+  if (nEls[0] < 1 || nEls[1] < 1) return fail(SE_ERR_ARG, "element counts must be positive");
+  if (!(max[0] > min[0]) || !(max[1] > min[1])) return fail(SE_ERR_ARG, "empty domain");
+  const bool b = bcs[0] != 0, t = bcs[1] != 0, l = bcs[2] != 0, r = bcs[3] != 0;
+  const int perx = periodic[0] != 0, pery = periodic[1] != 0;
+  if ((b || t) && pery) return fail(SE_ERR_ARG, "both periodic and non-periodic conditions in y");
+  if ((l || r) && perx) return fail(SE_ERR_ARG, "both periodic and non-periodic conditions in x");
+  if (pery && !perx) return fail(SE_ERR_UNSUPPORTED, "periodic in y only is not built by the reference");
+  if (perx && !pery && b && !t)
+    return fail(SE_ERR_UNSUPPORTED, "periodic x with a bottom wall only (reference: bc error)");
+  if ((perx && nEls[0] < 2) || (pery && nEls[1] < 2))
+    return fail(SE_ERR_UNSUPPORTED, "a periodic direction needs at least 2 elements");
+  se_solver_opts o;
+  if (opts) o = *opts; else se_solver_opts_default(&o);
+
+  // host tables on the stack: mesh, boundary ranges, operator
+  se_mesh mesh;
+  gll_build(N, mesh.gll);
+  MeshDev& md = mesh.dev;
+  std::memset(&md, 0, sizeof(md));
+  md.N = N;
+  for (int k = 0; k < 2; k++) {
+    md.nEls[k] = nEls[k];
+    md.nVerts[k] = nEls[k] * N + 1;
+    md.periodic[k] = k == 0 ? perx : pery;
+    md.min[k] = min[k];
+    md.max[k] = max[k];
+    md.dx[k] = (md.max[k] - md.min[k]) / md.nEls[k];
+    md.two_over_dx[k] = 2.0 / md.dx[k];
+    md.span[k] = md.max[k] - md.min[k];
+    md.nspan[k] = md.min[k] - md.max[k];
+  }
+  for (int i = 0; i <= N; i++) {
+    md.abcissa[i] = mesh.gll.x[i];
+    md.lambda[i] = mesh.gll.lambda[i];
+    md.w[i] = mesh.gll.w[i];
+  }
+  OpDev op;
+  std::memset(&op, 0, sizeof(op));
+  op.d[0] = make_dir(md, 0, l, r);
+  op.d[1] = make_dir(md, 1, b, t || pery);
+  op.G[0] = op.d[0].hi - op.d[0].lo;
+  op.G[1] = op.d[1].hi - op.d[1].lo;
+  const long n = (long)op.G[0] * op.G[1];
+  if (n > kNoAllocMaxUnknowns)
+    return fail(SE_ERR_UNSUPPORTED,
+                "%ld unknowns exceed the no-allocation limit of %d; use se_helmholtz_create", n,
+                kNoAllocMaxUnknowns);
+  const long ntiles = (long)((op.G[0] + kCgTileX - 1) / kCgTileX) * ((op.G[1] + kCgTileY - 1) / kCgTileY);
+  if (ntiles > kNoAllocMaxTiles)
+    return fail(SE_ERR_UNSUPPORTED, "%ld tiles exceed the no-allocation limit of %d", ntiles,
+                kNoAllocMaxTiles);
+  const double hx = md.dx[0], hy = md.dx[1];
+  const double s = poisson ? c : nu * dt;
+  op.alpha = (poisson ? 0.0 : c) * (0.5 * hx) * (0.5 * hy);
+  if (o.mode == SE_MODE_EXACT) {
+    op.beta[0] = s * (hy / hx);
+    op.beta[1] = s * (hx / hy);
+  } else {
+    op.beta[0] = s * (2.0 / hx) * (2.0 / hx);
+    op.beta[1] = s * (2.0 / hy) * (2.0 / hy);
+  }
+  for (int a = 0; a < (N + 1) * (N + 1); a++) op.Kh[a] = mesh.gll.Kh[a];
+  for (int a = 0; a <= N; a++) op.w[a] = mesh.gll.w[a];
+
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(SE_ERR_UNSUPPORTED, "device index %d", dev);
+  if (!g_noalloc_dev[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_dev[dev] = static_cast<double*>(p);
+  }
+  double* base = g_noalloc_dev[dev];
+  const size_t vn = kNoAllocMaxUnknowns;
+  double *f = base, *lift = base + vn, *x = base + 2 * vn, *rr = base + 3 * vn, *z = base + 4 * vn,
+         *p0 = base + 5 * vn, *p1 = base + 6 * vn, *w = base + 7 * vn;
+  double* partials = base + kNoAllocVecDoubles;
+  CgSolve* d_solve = reinterpret_cast<CgSolve*>(partials + kNoAllocPartialDoubles);
+  CgTile* d_tiles = reinterpret_cast<CgTile*>(partials + kNoAllocPartialDoubles + kNoAllocSolveDoubles);
+  int* d_begin = reinterpret_cast<int*>(partials + kNoAllocPartialDoubles + kNoAllocSolveDoubles +
+                                        kNoAllocTileDoubles);
+  unsigned* words = reinterpret_cast<unsigned*>(partials + kNoAllocPartialDoubles + kNoAllocSolveDoubles +
+                                                kNoAllocTileDoubles + kNoAllocBeginDoubles);
+
+  // schedule: same tile order and contiguous block chunks as the allocating path
+  int maxg = cg_max_grid(dev, N);
+  if (maxg <= 0) return fail(SE_ERR_CUDA, "cannot size the cooperative CG launch");
+  {
+    int sms = 1, per = 2;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (const char* ev = std::getenv("SE_CG_BLOCKS_PER_SM")) per = std::max(1, std::atoi(ev));
+    maxg = std::min(std::min(maxg, sms * per), kNoAllocMaxGrid);
+  }
+  int nt = 0;
+  for (int y = 0; y < op.G[1]; y += kCgTileY)
+    for (int xx = 0; xx < op.G[0]; xx += kCgTileX) g_noalloc_tiles[nt++] = {0, xx, y, 0};
+  const int grid = std::max(1, std::min(maxg, nt));
+  for (int k = 0; k <= grid; k++) g_noalloc_begin[k] = (int)((long)nt * k / grid);
+  for (int k = 0; k < grid; k++)
+    for (int q = g_noalloc_begin[k]; q < g_noalloc_begin[k + 1]; q++) g_noalloc_tiles[q].seg = k;
+
+  CgSolve cs;
+  std::memset(&cs, 0, sizeof(cs));
+  cs.op = op;
+  cs.b = f;
+  cs.x = x;
+  cs.r = rr;
+  cs.z = z;
+  cs.p0 = p0;
+  cs.p1 = p1;
+  cs.w = w;
+  cs.rtol = o.rtol;
+  cs.atol = o.atol;
+  cs.dtol = o.dtol;
+  cs.max_it = o.max_it;
+  cs.norm_type = o.norm_type;
+  cs.remove_null = remove_null_space;
+  cs.n = (int)n;
+  cs.seg_begin = 0;
+  cs.seg_end = grid;
+
+  cudaStream_t st = g_stream;
+  // what must start at zero: the barrier words, the active count, the error word
+  CK(cudaMemsetAsync(words, 0, sizeof(double) * kNoAllocWordDoubles, st));
+  CK(cudaMemcpyAsync(d_tiles, g_noalloc_tiles, sizeof(CgTile) * nt, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_begin, g_noalloc_begin, sizeof(int) * (grid + 1), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_solve, &cs, sizeof(cs), cudaMemcpyHostToDevice, st));
+  CK(launch_lift(op, md, sol_dev, lift, st));
+  CK(launch_rhs_assemble(op, md, rhs_dev, lift, f, st));
+  CgBatch B;
+  B.solves = d_solve;
+  B.nsolves = 1;
+  B.tiles = d_tiles;
+  B.block_tile_begin = d_begin;
+  B.partials = partials;
+  B.nseg = grid;
+  B.bar_count = words;
+  B.bar_gen = words + 32;   // another 128-byte line
+  B.n_active = reinterpret_cast<int*>(words + 64);
+  B.err = words + 96;
+  CK(launch_cg(B, grid, N, st));
+  CgSolve out;
+  unsigned err = 0;
+  CK(cudaMemcpyAsync(&out, d_solve, sizeof(out), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&err, B.err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  CK(launch_update_field(op, md, x, sol_dev, st));
+  CK(cudaStreamSynchronize(st));
+  if (err & KERR_BARRIER_TIMEOUT) return fail(SE_ERR_TIMEOUT, "CG grid barrier timed out");
+  if (stats) {
+    stats->reason = out.reason;
+    stats->its = out.its;
+    stats->outer_its = 0;
+    stats->rnorm = out.dp;
+    stats->rnorm0 = out.rnorm0;
+    stats->kernel_ms = 0.0;
+  }
+  if (out.reason < 0)
+    return fail(SE_ERR_NOT_CONVERGED, "KSP diverged, reason %d after %d its", out.reason, out.its);
+  return SE_OK;
+}

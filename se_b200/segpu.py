@@ -111,6 +111,10 @@ SIGNATURES = {
     "se_linsys_vec_size": [_vp, _I],
     "se_calc_time_step": [_vp, ctypes.c_double, _D],
     "se_field_error": [_vp, _vp, ctypes.c_int, ctypes.c_int, _D],
+    "se_helmholtz_solve_noalloc": [_I, ctypes.c_int, _D, _D, _I, _I, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                   ctypes.POINTER(SolverOpts), ctypes.c_int, _vp, _vp,
+                                   ctypes.POINTER(SolveStats)],
 }
 
 
