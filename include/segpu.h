@@ -41,6 +41,7 @@ extern "C" {
 #define SE_KSP_CONVERGED_ATOL 3
 #define SE_KSP_DIVERGED_ITS (-3)
 #define SE_KSP_DIVERGED_DTOL (-4)
+#define SE_KSP_DIVERGED_BREAKDOWN (-5) /* FDM refinement stalled at the rounding floor */
 #define SE_KSP_DIVERGED_INDEFINITE_PC (-8)
 #define SE_KSP_DIVERGED_NANORINF (-9)
 #define SE_KSP_DIVERGED_INDEFINITE_MAT (-10)
@@ -139,7 +140,10 @@ int se_advector_departures(se_advector* adv, int* el, double* xy);
 #define SE_MODE_REFERENCE 0 /* the reference's Laplacian with detJac forced to 1 (src/base/Operator.cpp:72) */
 #define SE_MODE_EXACT 1     /* the Laplacian with its true Jacobian */
 #define SE_PREC_FP64 0      /* every operation in FP64: the drop-in */
-#define SE_PREC_MIXED 1     /* FP32 inner CG, FP64 iterative refinement */
+#define SE_PREC_MIXED 1     /* FP32 data, TF32 tensor-core inner solves, FP64 refinement */
+#define SE_PREC_BF16 2      /* BF16 data, FP32-accumulated tensor-core inner solves, FP64 refinement */
+#define SE_METHOD_CG 0      /* PETSc KSPCG + PCJACOBI semantics: the drop-in */
+#define SE_METHOD_FDM 1     /* fast diagonalization: exact inverse by 1-D eigenvector transforms */
 typedef struct {
   double rtol;    /* default 1e-5 (PETSc) */
   double atol;    /* default 1e-50 */
@@ -148,8 +152,12 @@ typedef struct {
   int norm_type;  /* SE_NORM_*, default preconditioned */
   int mode;       /* SE_MODE_*, default SE_MODE_REFERENCE */
   int precision;  /* SE_PREC_*, default SE_PREC_FP64 */
-  int inner_max_it; /* mixed: inner CG iteration cap per refinement step (default 2000) */
-  double inner_rtol; /* mixed: inner CG relative tolerance (default 1e-6) */
+  int inner_max_it; /* reserved (default 2000) */
+  double inner_rtol; /* reserved (default 1e-6) */
+  int method;     /* SE_METHOD_*, default SE_METHOD_CG. FDM: the solution of
+                     A x = b by fast diagonalization, refined in FP64 until the
+                     chosen residual norm meets rtol/atol (its = refinement
+                     steps); precision selects the GEMM arithmetic. */
 } se_solver_opts;
 
 typedef struct {
@@ -210,7 +218,7 @@ int se_linsys_vec_size(const se_linsys* ls, int* n);
  * return. poisson != 0 selects A = c*Laplacian (nu, dt ignored).
  * Limit: at most 65536 vector unknowns (e.g. 32x32 elements at N = 8);
  * larger systems return SE_ERR_UNSUPPORTED. All temporaries live in one
- * static device array of about 4.5 MB that every GPU loading the library
+ * static device array of about 5 MB that every GPU loading the library
  * holds until exit; every call shares it, so calls whose device work
  * overlaps race and must be serialised by the caller. The first call on a
  * device looks the array up (cudaGetSymbolAddress) and should come before

@@ -8,7 +8,8 @@ over that C-ABI.
 """
 from .segpu import (BCs, Advector, CalcTimeStep, Field, FieldError, HelmholtzEqn, Mesh,  # noqa: F401
                     PoissonEqn, SEError, load_library, set_stream, solver_opts, synchronize,
-                    MODE_EXACT, MODE_REFERENCE, PREC_FP64, PREC_MIXED, NORM_NATURAL,
+                    MODE_EXACT, MODE_REFERENCE, PREC_FP64, PREC_MIXED, PREC_BF16, METHOD_CG,
+                    METHOD_FDM, NORM_NATURAL,
                     NORM_PRECONDITIONED, NORM_UNPRECONDITIONED)
 
 __all__ = ["Mesh", "BCs", "Field", "Advector", "HelmholtzEqn", "PoissonEqn", "CalcTimeStep",

@@ -1,6 +1,9 @@
 // Host side of the segpu C-ABI (include/segpu.h): object lifetimes, the
 // mesh/GLL/boundary tables, device memory and kernel launches.
+#include <cublas_v2.h>
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cusolverDn.h>
 
 #include <algorithm>
 #include <cmath>
@@ -242,7 +245,8 @@ struct se_linsys {
   OpDev op;
   int n;
   bool assembled;
-  double *f, *lift, *x, *r, *z, *p0, *p1, *w;
+  double *f, *lift, *x, *r, *z, *p0, *p1, *w, *dinv;
+  bool resident;
   // single-solve CG schedule
   CgSolve* d_solve;
   CgTile* d_tiles;
@@ -253,6 +257,15 @@ struct se_linsys {
   unsigned* d_err;
   int grid, nseg, seg_begin, seg_end;
   cudaEvent_t ev[2];
+  // fast diagonalization (built on the first FDM solve)
+  bool fdm_ready;
+  int fdm_prec;
+  double *Sx, *Sy, *lx, *ly;  // eigenvectors (column-major, W-orthonormal), eigenvalues
+  void *Sx_lo, *Sy_lo;        // low-precision copies of Sx, Sy
+  double *X1, *X2, *ax;       // FP64 work: two transform buffers, A x
+  void *L1, *L2, *L3;         // low-precision work
+  double* fpart;              // reduction partials [2*1184] + results [8]
+  double lmax[2];  // largest 1-D eigenvalue magnitude per direction
 };
 
 namespace {
@@ -352,6 +365,7 @@ CgSolve make_solve(const se_linsys* ls, const double* b, double* x, double rtol,
   cs.p0 = ls->p0;
   cs.p1 = ls->p1;
   cs.w = ls->w;
+  cs.dinv = ls->dinv;
   cs.rtol = rtol;
   cs.atol = atol;
   cs.dtol = dtol;
@@ -373,6 +387,7 @@ void linsys_free(se_linsys* ls) {
   dfree(ls->p0);
   dfree(ls->p1);
   dfree(ls->w);
+  dfree(ls->dinv);
   dfree(ls->d_solve);
   dfree(ls->d_tiles);
   dfree(ls->d_block_begin);
@@ -380,10 +395,47 @@ void linsys_free(se_linsys* ls) {
   dfree(ls->d_bar);
   dfree(ls->d_active);
   dfree(ls->d_err);
+  dfree(ls->Sx);
+  dfree(ls->Sy);
+  dfree(ls->lx);
+  dfree(ls->ly);
+  if (ls->Sx_lo) cudaFree(ls->Sx_lo);
+  if (ls->Sy_lo) cudaFree(ls->Sy_lo);
+  dfree(ls->X1);
+  dfree(ls->X2);
+  dfree(ls->ax);
+  if (ls->L1) cudaFree(ls->L1);
+  if (ls->L2) cudaFree(ls->L2);
+  if (ls->L3) cudaFree(ls->L3);
+  dfree(ls->fpart);
   if (ls->ev[0]) cudaEventDestroy(ls->ev[0]);
   if (ls->ev[1]) cudaEventDestroy(ls->ev[1]);
   delete ls->own_bcs;
   delete ls;
+}
+
+// Number of CG tiles of an operator's unknown grid.
+long cg_tiles(const OpDev& op) {
+  return (long)((op.G[0] + kCgTileX - 1) / kCgTileX) * ((op.G[1] + kCgTileY - 1) / kCgTileY);
+}
+
+// Grid and mode of the persistent CG for ntiles tiles of order N: resident
+// (state in registers) when every block can own at most kCgResidentTiles
+// tiles; otherwise streaming with SE_CG_BLOCKS_PER_SM (default 2) blocks per
+// SM. Returns the grid (0 on failure).
+int cg_plan(int dev, int N, long ntiles, int nsolves, bool* resident) {
+  const int maxr = cg_max_grid(dev, N, true, nsolves);
+  if (maxr > 0 && ntiles <= (long)maxr * kCgResidentTiles) {
+    *resident = true;
+    return (int)std::min<long>(maxr, ntiles);
+  }
+  int maxs = cg_max_grid(dev, N, false, nsolves);
+  if (maxs <= 0) return 0;
+  int sms = 1, per = 2;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (const char* e = std::getenv("SE_CG_BLOCKS_PER_SM")) per = std::max(1, std::atoi(e));
+  *resident = false;
+  return (int)std::min<long>(std::min(maxs, sms * per), ntiles);
 }
 
 int linsys_alloc(se_linsys* ls) {
@@ -391,30 +443,21 @@ int linsys_alloc(se_linsys* ls) {
   int rc;
   if ((rc = dalloc(&ls->f, n)) || (rc = dalloc(&ls->lift, n)) || (rc = dalloc(&ls->x, n)) ||
       (rc = dalloc(&ls->r, n)) || (rc = dalloc(&ls->z, n)) || (rc = dalloc(&ls->p0, n)) ||
-      (rc = dalloc(&ls->p1, n)) || (rc = dalloc(&ls->w, n)))
+      (rc = dalloc(&ls->p1, n)) || (rc = dalloc(&ls->w, n)) || (rc = dalloc(&ls->dinv, n)))
     return rc;
   CK(cudaMemset(ls->lift, 0, sizeof(double) * n));
   int dev = 0;
   CK(cudaGetDevice(&dev));
-  int maxg = cg_max_grid(dev, ls->op.d[0].N);
-  if (maxg <= 0) return fail(SE_ERR_CUDA, "cannot size the cooperative CG launch");
-  {
-    // Blocks per SM for the persistent CG: fewer blocks mean fewer barrier
-    // arrivals and partial sums per iteration; the default of 2 was the best
-    // of 1..4 on the 64x64, p=8 solve. SE_CG_BLOCKS_PER_SM overrides it.
-    int sms = 1, per = 2;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (const char* e = std::getenv("SE_CG_BLOCKS_PER_SM")) per = std::max(1, std::atoi(e));
-    maxg = std::min(maxg, sms * per);
-  }
-  Schedule S = make_schedule({&ls->op}, maxg);
+  const int grid = cg_plan(dev, ls->op.d[0].N, cg_tiles(ls->op), 1, &ls->resident);
+  if (grid <= 0) return fail(SE_ERR_CUDA, "cannot size the cooperative CG launch");
+  Schedule S = make_schedule({&ls->op}, grid);
   ls->grid = (int)S.block_begin.size() - 1;
   ls->nseg = S.nseg;
   ls->seg_begin = S.seg_begin[0];
   ls->seg_end = S.seg_end[0];
   if ((rc = dalloc(&ls->d_solve, 1)) || (rc = dalloc(&ls->d_tiles, S.tiles.size())) ||
       (rc = dalloc(&ls->d_block_begin, S.block_begin.size())) ||
-      (rc = dalloc(&ls->d_partials, (size_t)S.nseg * 4)) || (rc = dalloc(&ls->d_bar, 2)) ||
+      (rc = dalloc(&ls->d_partials, (size_t)S.nseg * 8)) || (rc = dalloc(&ls->d_bar, 2)) ||
       (rc = dalloc(&ls->d_active, 1)) || (rc = dalloc(&ls->d_err, 1)))
     return rc;
   CK(cudaMemcpy(ls->d_tiles, S.tiles.data(), sizeof(CgTile) * S.tiles.size(),
@@ -432,7 +475,7 @@ int run_cg(se_linsys* ls, const double* b, double* x, double rtol, double atol, 
   CgSolve cs = make_solve(ls, b, x, rtol, atol, dtol, max_it, remove_null);
   cudaStream_t s = g_stream;
   CK(cudaMemcpyAsync(ls->d_solve, &cs, sizeof(cs), cudaMemcpyHostToDevice, s));
-  CK(cudaMemsetAsync(ls->d_bar, 0, sizeof(unsigned), s));  // arrivals; generation keeps counting
+  CK(cudaMemsetAsync(ls->d_bar, 0, sizeof(unsigned), s));  // barrier word starts at 0
   CK(cudaMemsetAsync(ls->d_err, 0, sizeof(unsigned), s));
   CgBatch B;
   B.solves = ls->d_solve;
@@ -450,7 +493,7 @@ int run_cg(se_linsys* ls, const double* b, double* x, double rtol, double atol, 
     CK(cudaEventCreate(&ls->ev[1]));
   }
   CK(cudaEventRecord(ls->ev[0], s));
-  CK(launch_cg(B, ls->grid, ls->op.d[0].N, s));
+  CK(launch_cg(B, ls->grid, ls->op.d[0].N, ls->resident, s));
   CK(cudaEventRecord(ls->ev[1], s));
   unsigned err = 0;
   CK(cudaMemcpyAsync(out_state, ls->d_solve, sizeof(CgSolve), cudaMemcpyDeviceToHost, s));
@@ -463,6 +506,322 @@ int run_cg(se_linsys* ls, const double* b, double* x, double rtol, double atol, 
 
 int check_field(const se_field* f) {
   if (!f || !f->mesh || !f->vals) return fail(SE_ERR_ARG, "null field");
+  return SE_OK;
+}
+}  // namespace
+
+
+// ------------------------------------------------- fast diagonalization ----
+namespace {
+constexpr int kFdmPartials = 1184;
+cublasHandle_t g_cublas[64];
+
+int cublas_for(cublasHandle_t* out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(SE_ERR_UNSUPPORTED, "device index %d", dev);
+  if (!g_cublas[dev]) {
+    if (cublasCreate(&g_cublas[dev]) != CUBLAS_STATUS_SUCCESS)
+      return fail(SE_ERR_CUDA, "cublasCreate failed");
+  }
+  *out = g_cublas[dev];
+  return SE_OK;
+}
+
+// 1-D assembled stiffness (dense, n x n) and weights on one direction's
+// unknowns: element rows of Kh and w added at the vertices they map to
+// (periodic end folded onto the start, Dirichlet vertices dropped).
+void assemble_1d(const Dir& d, const double* Kh, const double* w, std::vector<double>& K,
+                 std::vector<double>& W) {
+  const int n = d.hi - d.lo, N = d.N;
+  K.assign((size_t)n * n, 0.0);
+  W.assign(n, 0.0);
+  auto u = [&](int g) {
+    if (d.periodic && g == d.nV - 1) g = 0;
+    return (g >= d.lo && g < d.hi) ? g - d.lo : -1;
+  };
+  for (int e = 0; e < d.nE; e++)
+    for (int a = 0; a <= N; a++) {
+      const int ua = u(e * N + a);
+      if (ua < 0) continue;
+      W[ua] += w[a];
+      for (int b = 0; b <= N; b++) {
+        const int ub = u(e * N + b);
+        if (ub >= 0) K[(size_t)ua * n + ub] += Kh[a * (N + 1) + b];
+      }
+    }
+}
+
+uint16_t to_bf16(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u += 0x7fffu + ((u >> 16) & 1u);  // round to nearest even
+  return (uint16_t)(u >> 16);
+}
+
+// Generalised eigenvectors S (S^T K S = diag(lam), S^T W S = I) of one
+// direction, on the device: eigenvectors of W^-1/2 K W^-1/2 by cuSOLVER
+// syevd (setup only), then scaled by W^-1/2.
+int eig_1d(const Dir& d, const double* Kh, const double* w, double** S_dev, double** lam_dev,
+           std::vector<double>& S_host) {
+  std::vector<double> K, W;
+  assemble_1d(d, Kh, w, K, W);
+  const int n = d.hi - d.lo;
+  std::vector<double> A((size_t)n * n);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) A[(size_t)j * n + i] = K[(size_t)i * n + j] / std::sqrt(W[i] * W[j]);
+  double *dA = nullptr, *dlam = nullptr, *work = nullptr;
+  int* info = nullptr;
+  int rc;
+  if ((rc = dalloc(&dA, (size_t)n * n)) || (rc = dalloc(&dlam, n)) || (rc = dalloc(&info, 1))) {
+    dfree(dA);
+    dfree(dlam);
+    dfree(info);
+    return rc;
+  }
+  cusolverDnHandle_t h = nullptr;
+  int lwork = 0, hinfo = 0;
+  bool ok = cusolverDnCreate(&h) == CUSOLVER_STATUS_SUCCESS;
+  ok = ok && cudaMemcpy(dA, A.data(), sizeof(double) * A.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+  ok = ok && cusolverDnDsyevd_bufferSize(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dA, n,
+                                         dlam, &lwork) == CUSOLVER_STATUS_SUCCESS;
+  ok = ok && dalloc(&work, (size_t)lwork) == SE_OK;
+  ok = ok && cusolverDnDsyevd(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, dA, n, dlam,
+                              work, lwork, info) == CUSOLVER_STATUS_SUCCESS;
+  ok = ok && cudaMemcpy(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess && hinfo == 0;
+  ok = ok && cudaMemcpy(A.data(), dA, sizeof(double) * A.size(), cudaMemcpyDeviceToHost) == cudaSuccess;
+  if (h) cusolverDnDestroy(h);
+  dfree(work);
+  dfree(info);
+  if (!ok) {
+    dfree(dA);
+    dfree(dlam);
+    return fail(SE_ERR_CUDA, "eigendecomposition of the 1-D operator failed (n=%d)", n);
+  }
+  for (int j = 0; j < n; j++)
+    for (int i = 0; i < n; i++) A[(size_t)j * n + i] /= std::sqrt(W[i]);
+  S_host = A;
+  CK(cudaMemcpy(dA, A.data(), sizeof(double) * A.size(), cudaMemcpyHostToDevice));
+  *S_dev = dA;
+  *lam_dev = dlam;
+  return SE_OK;
+}
+
+int upload_low(const std::vector<double>& S, int prec, void** out) {
+  const size_t n = S.size();
+  if (prec == 1) {
+    std::vector<float> v(n);
+    for (size_t k = 0; k < n; k++) v[k] = (float)S[k];
+    float* d = nullptr;
+    if (int rc = dalloc(&d, n)) return rc;
+    CK(cudaMemcpy(d, v.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    *out = d;
+  } else {
+    std::vector<uint16_t> v(n);
+    for (size_t k = 0; k < n; k++) v[k] = to_bf16((float)S[k]);
+    uint16_t* d = nullptr;
+    if (int rc = dalloc(&d, n)) return rc;
+    CK(cudaMemcpy(d, v.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
+    *out = d;
+  }
+  return SE_OK;
+}
+
+int fdm_setup(se_linsys* ls, int prec) {
+  if (ls->fdm_ready && ls->fdm_prec == prec) return SE_OK;
+  const OpDev& op = ls->op;
+  const size_t n = (size_t)ls->n;
+  int rc;
+  if (!ls->Sx) {
+    std::vector<double> Sxh, Syh;
+    if ((rc = eig_1d(op.d[0], op.Kh, op.w, &ls->Sx, &ls->lx, Sxh))) return rc;
+    if ((rc = eig_1d(op.d[1], op.Kh, op.w, &ls->Sy, &ls->ly, Syh))) return rc;
+    if ((rc = dalloc(&ls->X1, n)) || (rc = dalloc(&ls->X2, n)) || (rc = dalloc(&ls->ax, n)) ||
+        (rc = dalloc(&ls->fpart, 2 * kFdmPartials + 8)))
+      return rc;
+    // Jacobi inverse for the preconditioned residual norm
+    CK(launch_op_diag(op, ls->dinv, g_stream));
+    CK(launch_invert(ls->dinv, n, g_stream));
+    // spectral range for the null-mode tolerance
+    std::vector<double> lx(op.G[0]), ly(op.G[1]);
+    CK(cudaMemcpy(lx.data(), ls->lx, sizeof(double) * lx.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(ly.data(), ls->ly, sizeof(double) * ly.size(), cudaMemcpyDeviceToHost));
+    ls->lmax[0] = ls->lmax[1] = 0.0;
+    for (double v : lx) ls->lmax[0] = std::max(ls->lmax[0], std::fabs(v));
+    for (double v : ly) ls->lmax[1] = std::max(ls->lmax[1], std::fabs(v));
+    if (prec != 0) {
+      if ((rc = upload_low(Sxh, prec, &ls->Sx_lo)) || (rc = upload_low(Syh, prec, &ls->Sy_lo)))
+        return rc;
+    }
+    ls->fdm_prec = prec;
+  } else if (prec != 0 && (!ls->Sx_lo || ls->fdm_prec != prec)) {
+    // re-derive the low-precision copies from the FP64 eigenvectors
+    std::vector<double> Sxh((size_t)op.G[0] * op.G[0]), Syh((size_t)op.G[1] * op.G[1]);
+    CK(cudaMemcpy(Sxh.data(), ls->Sx, sizeof(double) * Sxh.size(), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(Syh.data(), ls->Sy, sizeof(double) * Syh.size(), cudaMemcpyDeviceToHost));
+    if (ls->Sx_lo) cudaFree(ls->Sx_lo);
+    if (ls->Sy_lo) cudaFree(ls->Sy_lo);
+    ls->Sx_lo = ls->Sy_lo = nullptr;
+    if ((rc = upload_low(Sxh, prec, &ls->Sx_lo)) || (rc = upload_low(Syh, prec, &ls->Sy_lo))) return rc;
+    ls->fdm_prec = prec;
+  }
+  if (prec != 0) {
+    const size_t es = prec == 1 ? sizeof(float) : sizeof(uint16_t);
+    if (ls->L1) cudaFree(ls->L1);
+    if (ls->L2) cudaFree(ls->L2);
+    if (ls->L3) cudaFree(ls->L3);
+    ls->L1 = ls->L2 = ls->L3 = nullptr;
+    char *l1 = nullptr, *l2 = nullptr, *l3 = nullptr;
+    if ((rc = dalloc(&l1, n * es)) || (rc = dalloc(&l2, n * es)) || (rc = dalloc(&l3, n * es)))
+      return rc;
+    ls->L1 = l1;
+    ls->L2 = l2;
+    ls->L3 = l3;
+  }
+  ls->fdm_ready = true;
+  return SE_OK;
+}
+
+#define CB(call)                                                              \
+  do {                                                                        \
+    cublasStatus_t s_ = (call);                                               \
+    if (s_ != CUBLAS_STATUS_SUCCESS) return fail(SE_ERR_CUDA, "%s: cublas status %d", #call, (int)s_); \
+  } while (0)
+
+// Spectral entries below this magnitude are a null mode (constant null space
+// of a periodic Poisson operator) and are zeroed.
+double null_tol(const se_linsys* ls) {
+  const OpDev& op = ls->op;
+  return 1e-12 * (std::fabs(op.alpha) + std::fabs(op.beta[0]) * ls->lmax[0] +
+                  std::fabs(op.beta[1]) * ls->lmax[1]);
+}
+
+// out (= or +=) A^{-1} in by four FP64 GEMMs (column-major G_x x G_y views of
+// the row-major unknown arrays).
+int fdm_apply64(se_linsys* ls, cublasHandle_t h, const double* in, double* out, bool accumulate) {
+  const int gx = ls->op.G[0], gy = ls->op.G[1];
+  const double one = 1.0, zero = 0.0;
+  CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, gx, gy, gy, &one, in, gx, ls->Sy, gy, &zero, ls->X1, gx));
+  CB(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, gx, gy, gx, &one, ls->Sx, gx, ls->X1, gx, &zero, ls->X2, gx));
+  CK(launch_spectral_divide(0, ls->X2, gx, gy, ls->lx, ls->ly, ls->op.alpha, ls->op.beta[0],
+                            ls->op.beta[1], null_tol(ls), g_stream));
+  CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, gx, gy, gy, &one, ls->X2, gx, ls->Sy, gy, &zero, ls->X1, gx));
+  CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, gx, gy, gx, &one, ls->Sx, gx, ls->X1, gx,
+                 accumulate ? &one : &zero, out, gx));
+  return SE_OK;
+}
+
+// Low-precision A^{-1} in (in: FP64, scaled by 1/max|in| into L1; result
+// added to out in FP64). prec 1: FP32 data, TF32 tensor cores; prec 2: BF16
+// data, FP32 accumulation.
+int fdm_apply_low(se_linsys* ls, cublasHandle_t h, const double* in, double* out) {
+  const int gx = ls->op.G[0], gy = ls->op.G[1];
+  const size_t n = (size_t)gx * gy;
+  const int prec = ls->fdm_prec;
+  double* mx = ls->fpart + 2 * kFdmPartials;
+  CK(launch_maxabs(in, n, ls->fpart, kFdmPartials, mx, g_stream));
+  double hmax = 0.0;
+  CK(cudaMemcpyAsync(&hmax, mx, sizeof(double), cudaMemcpyDeviceToHost, g_stream));
+  CK(cudaStreamSynchronize(g_stream));
+  if (!(hmax > 0.0)) return SE_OK;
+  const double scale = 1.0 / hmax;
+  CK(launch_to_low(prec, in, ls->L1, n, scale, g_stream));
+  const float one = 1.0f, zero = 0.0f;
+  const cudaDataType_t t = prec == 1 ? CUDA_R_32F : CUDA_R_16BF;
+  const cublasComputeType_t ct = prec == 1 ? CUBLAS_COMPUTE_32F_FAST_TF32 : CUBLAS_COMPUTE_32F;
+  CB(cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, gx, gy, gy, &one, ls->L1, t, gx, ls->Sy_lo, t, gy,
+                  &zero, ls->L2, t, gx, ct, CUBLAS_GEMM_DEFAULT));
+  CB(cublasGemmEx(h, CUBLAS_OP_T, CUBLAS_OP_N, gx, gy, gx, &one, ls->Sx_lo, t, gx, ls->L2, t, gx,
+                  &zero, ls->L3, t, gx, ct, CUBLAS_GEMM_DEFAULT));
+  CK(launch_spectral_divide(prec, ls->L3, gx, gy, ls->lx, ls->ly, ls->op.alpha, ls->op.beta[0],
+                            ls->op.beta[1], null_tol(ls), g_stream));
+  CB(cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_T, gx, gy, gy, &one, ls->L3, t, gx, ls->Sy_lo, t, gy,
+                  &zero, ls->L2, t, gx, ct, CUBLAS_GEMM_DEFAULT));
+  CB(cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, gx, gy, gx, &one, ls->Sx_lo, t, gx, ls->L2, t, gx,
+                  &zero, ls->L1, t, gx, ct, CUBLAS_GEMM_DEFAULT));
+  CK(launch_add_low(prec, out, ls->L1, n, hmax, g_stream));
+  return SE_OK;
+}
+
+// Residual norms of r: returns the chosen norm (preconditioned: |D^-1 r|,
+// unpreconditioned: |r|, natural: sqrt|r.D^-1 r|).
+int residual_norm(se_linsys* ls, const double* r, double* out) {
+  const size_t n = (size_t)ls->n;
+  double* res = ls->fpart + 2 * kFdmPartials + 2;
+  double h[2];
+  const int nt = ls->opts.norm_type;
+  CK(launch_norms(r, nt == SE_NORM_UNPRECONDITIONED ? nullptr : ls->dinv, n,
+                  nt == SE_NORM_NATURAL, ls->fpart, kFdmPartials, res, g_stream));
+  CK(cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, g_stream));
+  CK(cudaStreamSynchronize(g_stream));
+  *out = std::sqrt(std::fabs(h[0]));
+  return SE_OK;
+}
+
+// Solve A x = f by fast diagonalization with FP64 iterative refinement until
+// the chosen residual norm is <= max(rtol |f|, atol) in that norm.
+int run_fdm(se_linsys* ls, int remove_null, CgSolve* st, float* kernel_ms) {
+  const int prec = ls->opts.precision == SE_PREC_FP64 ? 0 : (ls->opts.precision == SE_PREC_MIXED ? 1 : 2);
+  if (int rc = fdm_setup(ls, prec)) return rc;
+  cublasHandle_t h;
+  if (int rc = cublas_for(&h)) return rc;
+  CB(cublasSetStream(h, g_stream));
+  const size_t n = (size_t)ls->n;
+  std::memset(st, 0, sizeof(*st));
+  if (!ls->ev[0]) {
+    CK(cudaEventCreate(&ls->ev[0]));
+    CK(cudaEventCreate(&ls->ev[1]));
+  }
+  CK(cudaEventRecord(ls->ev[0], g_stream));
+  double rn0 = 0.0;
+  if (int rc = residual_norm(ls, ls->f, &rn0)) return rc;
+  st->rnorm0 = rn0;
+  const double ttol = std::max(ls->opts.rtol * rn0, ls->opts.atol);
+  CK(cudaMemsetAsync(ls->x, 0, sizeof(double) * n, g_stream));
+  double dp = rn0;
+  int its = 0, reason = 0;
+  if (!(dp == dp) || std::isinf(dp)) reason = -9;
+  else if (dp <= ttol) reason = dp < ls->opts.atol ? 3 : 2;
+  const double* rhs = ls->f;
+  // refinement stalls at the rounding floor of the true residual
+  // (~eps |A| |x|): three steps without halving it end the solve with
+  // SE_KSP_DIVERGED_BREAKDOWN
+  double best = dp;
+  int stalled = 0;
+  while (!reason) {
+    if (its >= ls->opts.max_it) {
+      reason = -3;
+      break;
+    }
+    // x += A^{-1} r  (r = f on the first step)
+    if (prec == 0) {
+      if (int rc = fdm_apply64(ls, h, rhs, ls->x, its > 0)) return rc;
+    } else {
+      if (int rc = fdm_apply_low(ls, h, rhs, ls->x)) return rc;
+    }
+    if (remove_null) CK(launch_remove_mean(ls->x, n, ls->fpart, kFdmPartials, ls->fpart + 2 * kFdmPartials + 4, g_stream));
+    its++;
+    // r = f - A x
+    CK(launch_op_apply(ls->op, ls->x, ls->ax, g_stream));
+    CK(launch_sub(ls->f, ls->ax, ls->r, n, g_stream));
+    rhs = ls->r;
+    if (int rc = residual_norm(ls, ls->r, &dp)) return rc;
+    if (!(dp == dp) || std::isinf(dp)) reason = -9;
+    else if (dp <= ttol) reason = dp < ls->opts.atol ? 3 : 2;
+    else if (dp >= ls->opts.dtol * rn0) reason = -4;
+    else if (dp > 0.5 * best) {
+      if (++stalled >= 3) reason = SE_KSP_DIVERGED_BREAKDOWN;
+    } else {
+      stalled = 0;
+    }
+    best = std::min(best, dp);
+  }
+  CK(cudaEventRecord(ls->ev[1], g_stream));
+  CK(cudaEventSynchronize(ls->ev[1]));
+  if (kernel_ms) CK(cudaEventElapsedTime(kernel_ms, ls->ev[0], ls->ev[1]));
+  st->its = its;
+  st->reason = reason;
+  st->dp = dp;
   return SE_OK;
 }
 }  // namespace
@@ -838,6 +1197,7 @@ int se_solver_opts_default(se_solver_opts* o) {
   o->precision = SE_PREC_FP64;
   o->inner_max_it = 2000;
   o->inner_rtol = 1e-6;
+  o->method = SE_METHOD_CG;
   return SE_OK;
 }
 
@@ -865,9 +1225,13 @@ int se_solver_opts_parse(se_solver_opts* o, const char* prefix, const char* opti
     if (!val.empty()) i++;
     char* end = nullptr;
     if (key == "ksp_type") {
-      if (val != "cg") return fail(SE_ERR_UNSUPPORTED, "ksp_type %s (only cg)", val.c_str());
+      if (val == "cg") o->method = SE_METHOD_CG;
+      else if (val == "preonly") o->method = SE_METHOD_FDM;
+      else return fail(SE_ERR_UNSUPPORTED, "ksp_type %s (cg, or preonly with pc_type fdm)", val.c_str());
     } else if (key == "pc_type") {
-      if (val != "jacobi") return fail(SE_ERR_UNSUPPORTED, "pc_type %s (only jacobi)", val.c_str());
+      if (val == "fdm") o->method = SE_METHOD_FDM;
+      else if (val != "jacobi")
+        return fail(SE_ERR_UNSUPPORTED, "pc_type %s (jacobi, or fdm)", val.c_str());
     } else if (key == "ksp_rtol") {
       o->rtol = std::strtod(val.c_str(), &end);
     } else if (key == "ksp_atol") {
@@ -966,14 +1330,16 @@ int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats)
   CK(launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, g_stream));
   CgSolve st;
   float kms = 0.f;
-  int rc = run_cg(ls, ls->f, ls->x, ls->opts.rtol, ls->opts.atol, ls->opts.dtol, ls->opts.max_it,
-                  remove_null_space, &st, &kms);
+  int rc = ls->opts.method == SE_METHOD_FDM
+               ? run_fdm(ls, remove_null_space, &st, &kms)
+               : run_cg(ls, ls->f, ls->x, ls->opts.rtol, ls->opts.atol, ls->opts.dtol,
+                        ls->opts.max_it, remove_null_space, &st, &kms);
   if (rc) return rc;
   CK(launch_update_field(ls->op, m, ls->x, ls->sol->vals, g_stream));
   if (stats) {
     stats->reason = st.reason;
     stats->its = st.its;
-    stats->outer_its = 0;
+    stats->outer_its = ls->opts.method == SE_METHOD_FDM ? st.its : 0;
     stats->rnorm = st.dp;
     stats->rnorm0 = st.rnorm0;
     stats->kernel_ms = kms;
@@ -1055,8 +1421,8 @@ namespace {
 constexpr int kNoAllocMaxUnknowns = 65536;
 constexpr int kNoAllocMaxTiles = 8192;
 constexpr int kNoAllocMaxGrid = 4096;
-constexpr size_t kNoAllocVecDoubles = 8 * (size_t)kNoAllocMaxUnknowns;  // f lift x r z p0 p1 w
-constexpr size_t kNoAllocPartialDoubles = 4 * (size_t)kNoAllocMaxGrid;
+constexpr size_t kNoAllocVecDoubles = 9 * (size_t)kNoAllocMaxUnknowns;  // f lift x r z p0 p1 w dinv
+constexpr size_t kNoAllocPartialDoubles = 8 * (size_t)kNoAllocMaxGrid;  // two buffers
 constexpr size_t kNoAllocSolveDoubles = (sizeof(CgSolve) + 255) / 256 * 256 / sizeof(double);
 constexpr size_t kNoAllocTileDoubles = (sizeof(CgTile) * kNoAllocMaxTiles + 255) / 256 * 256 / sizeof(double);
 constexpr size_t kNoAllocBeginDoubles = (sizeof(int) * (kNoAllocMaxGrid + 1) + 255) / 256 * 256 / sizeof(double);
@@ -1067,7 +1433,7 @@ constexpr size_t kNoAllocDoubles = kNoAllocVecDoubles + kNoAllocPartialDoubles +
                                    kNoAllocTileDoubles + kNoAllocBeginDoubles + kNoAllocWordDoubles;
 }  // namespace
 
-// About 4.4 MB per device: 8 vectors of 65536 doubles plus the schedule.
+// About 5 MB per device: 9 vectors of 65536 doubles plus the schedule.
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
 namespace {
@@ -1165,7 +1531,7 @@ extern "C" int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double
   double* base = g_noalloc_dev[dev];
   const size_t vn = kNoAllocMaxUnknowns;
   double *f = base, *lift = base + vn, *x = base + 2 * vn, *rr = base + 3 * vn, *z = base + 4 * vn,
-         *p0 = base + 5 * vn, *p1 = base + 6 * vn, *w = base + 7 * vn;
+         *p0 = base + 5 * vn, *p1 = base + 6 * vn, *w = base + 7 * vn, *dinv = base + 8 * vn;
   double* partials = base + kNoAllocVecDoubles;
   CgSolve* d_solve = reinterpret_cast<CgSolve*>(partials + kNoAllocPartialDoubles);
   CgTile* d_tiles = reinterpret_cast<CgTile*>(partials + kNoAllocPartialDoubles + kNoAllocSolveDoubles);
@@ -1174,15 +1540,11 @@ extern "C" int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double
   unsigned* words = reinterpret_cast<unsigned*>(partials + kNoAllocPartialDoubles + kNoAllocSolveDoubles +
                                                 kNoAllocTileDoubles + kNoAllocBeginDoubles);
 
-  // schedule: same tile order and contiguous block chunks as the allocating path
-  int maxg = cg_max_grid(dev, N);
+  // schedule: same tile order, mode and contiguous block chunks as the
+  // allocating path
+  bool resident = false;
+  const int maxg = std::min(cg_plan(dev, N, ntiles, 1, &resident), kNoAllocMaxGrid);
   if (maxg <= 0) return fail(SE_ERR_CUDA, "cannot size the cooperative CG launch");
-  {
-    int sms = 1, per = 2;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (const char* ev = std::getenv("SE_CG_BLOCKS_PER_SM")) per = std::max(1, std::atoi(ev));
-    maxg = std::min(std::min(maxg, sms * per), kNoAllocMaxGrid);
-  }
   int nt = 0;
   for (int y = 0; y < op.G[1]; y += kCgTileY)
     for (int xx = 0; xx < op.G[0]; xx += kCgTileX) g_noalloc_tiles[nt++] = {0, xx, y, 0};
@@ -1201,6 +1563,7 @@ extern "C" int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double
   cs.p0 = p0;
   cs.p1 = p1;
   cs.w = w;
+  cs.dinv = dinv;
   cs.rtol = o.rtol;
   cs.atol = o.atol;
   cs.dtol = o.dtol;
@@ -1230,7 +1593,7 @@ extern "C" int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double
   B.bar_gen = words + 32;   // another 128-byte line
   B.n_active = reinterpret_cast<int*>(words + 64);
   B.err = words + 96;
-  CK(launch_cg(B, grid, N, st));
+  CK(launch_cg(B, grid, N, resident, st));
   CgSolve out;
   unsigned err = 0;
   CK(cudaMemcpyAsync(&out, d_solve, sizeof(out), cudaMemcpyDeviceToHost, st));

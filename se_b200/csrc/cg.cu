@@ -1,0 +1,649 @@
+// Persistent, deterministic Jacobi-preconditioned CG over a batch of
+// Helmholtz/Poisson solves of one polynomial order N, sm_100a.
+//
+// One cooperative launch runs every iteration of every solve in the batch.
+// The unknown grid of each solve is cut into tiles of kCgTileX x kCgTileY
+// unknowns, assigned in contiguous chunks to the resident blocks, one
+// unknown per thread and tile.
+//
+//  * Resident mode (K > 0, each block owns at most K tiles): x, r, the
+//    Jacobi inverse, p and A p of a thread's unknowns stay in registers for
+//    the whole solve. Only z and p go to memory each iteration, because the
+//    neighbouring tiles read them as their stencil halo.
+//  * Streaming mode (K == 0, any size): the same iteration with x, r, w and
+//    the Jacobi inverse in memory; bounded by HBM bandwidth.
+//
+// The operator is the tensor-product form of SE's assembled c*Mass +
+// s*Laplacian (see linsys.cu); each tile is staged with its halo in shared
+// memory and every unknown sums its row of the assembled 1-D operators in a
+// fixed order, so there are no atomics and results are bit-for-bit
+// repeatable.
+//
+// Dot products: every block accumulates per-segment partial sums (a
+// segment is a run of one solve's tiles inside one block) and, after each
+// grid barrier, every block sums every solve's segments in the same fixed
+// order; all blocks therefore hold identical scalars and take identical
+// decisions without another round trip. The iteration and its tests are
+// PETSc's KSPCG with PCJACOBI as SE runs it (src/linsys/HelmholtzEqn.cpp:
+// 141-150): zero initial guess, preconditioned/unpreconditioned/natural
+// norm, RTOL/ATOL/DTOL/ITS, and the sign checks for an indefinite matrix
+// or preconditioner; a constant null space is projected out of every
+// preconditioned residual.
+#include "common.cuh"
+
+namespace seg {
+namespace {
+
+struct SolveState {
+  double beta, betaold, dpi, bcoef, a, rnorm0, ttol, dp, zmean;
+  int its, done, reason, pbuf;
+};
+struct SolveMeta {
+  int seg_begin, seg_end, max_it, norm_type, remove_null, n;
+  double rtol, atol, dtol;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Grid barrier for a cooperative launch: block 0 adds 2^31 - (nblocks - 1),
+// every other block adds 1, so the word's top bit flips exactly when all
+// blocks have arrived; no reset is needed between uses. The wait is bounded:
+// after 2^26 polls a block records KERR_BARRIER_TIMEOUT and returns false.
+constexpr long kPollLimit = 1L << 26;
+__device__ __forceinline__ bool grid_sync(unsigned* bar, unsigned* err) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned inc = blockIdx.x == 0 ? 0x80000000u - (gridDim.x - 1u) : 1u;
+    __threadfence();
+    const unsigned old = atomicAdd(bar, inc);
+    long polls = 0;
+    int ok = 1;
+    while (((ld_acquire_u32(bar) ^ old) & 0x80000000u) == 0u) {
+      if (++polls > kPollLimit) {
+        atomicOr(err, KERR_BARRIER_TIMEOUT);
+        ok = 0;
+        break;
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok;
+}
+
+// Fixed-order block reduction of 4 sums; the result is valid in thread 0.
+__device__ __forceinline__ void block_sum4(double v[4], double (*sm)[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; q++)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0)
+#pragma unroll
+    for (int q = 0; q < 4; q++) sm[w][q] = v[q];
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      v[q] = l < kCgThreads / 32 ? sm[l][q] : 0.0;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+    }
+  }
+  __syncthreads();
+}
+
+// All four partial slots of one solve's segments at once (one 32-byte load
+// per segment), fixed order; every lane of the calling warp gets the sums.
+__device__ __forceinline__ void seg_sum4(const double* partials, int b, int e, double out[4]) {
+  const int l = threadIdx.x & 31;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  for (int k = b + l; k < e; k += 32) {
+    const double2* p = reinterpret_cast<const double2*>(partials + (size_t)k * 4);
+    const double2 u = p[0], v = p[1];
+    s0 += u.x;
+    s1 += u.y;
+    s2 += v.x;
+    s3 += v.y;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+  }
+  out[0] = s0;
+  out[1] = s1;
+  out[2] = s2;
+  out[3] = s3;
+}
+
+// ---------------------------------------------------------------- operator --
+template <int N>
+struct Geo {
+  static constexpr int n = N + 1;
+  static constexpr int W = kCgTileX + 2 * N;
+  static constexpr int H = kCgTileY + 2 * N;
+  static constexpr int kRows = kCgTileY * W;       // tile rows, full width
+  static constexpr int kCols = 2 * N * kCgTileX;   // tile columns, y-halo only
+};
+
+// Unknown index of unwrapped vertex g along d (-1: Dirichlet or outside).
+__device__ __forceinline__ int unknown_1d(const Dir& d, int g) {
+  if (d.periodic) {
+    const int L = d.nV - 1;
+    if (g < 0) g += L;
+    else if (g >= L) g -= L;
+  } else if (g < 0 || g >= d.nV) {
+    return -1;
+  }
+  return (g >= d.lo && g < d.hi) ? g - d.lo : -1;
+}
+
+// Assembled 1-D GLL weight and stiffness diagonal at vertex g (e = g/N, a).
+template <int N>
+__device__ __forceinline__ double wsum_n(const Dir& d, const double* w, int e, int a) {
+  double s = 0.0;
+  if (e < d.nE) s += w[a];
+  if (a == 0 && (e > 0 || d.periodic)) s += w[N];
+  return s;
+}
+template <int N>
+__device__ __forceinline__ double kdiag_n(const Dir& d, const double* Kh, int e, int a) {
+  constexpr int n = N + 1;
+  double s = 0.0;
+  if (e < d.nE) s += Kh[a * n + a];
+  if (a == 0 && (e > 0 || d.periodic)) s += Kh[N * n + N];
+  return s;
+}
+// Row of the assembled 1-D stiffness at vertex (e, a) applied to the staged
+// values around c (stride between neighbouring vertices).
+template <int N, int STRIDE>
+__device__ __forceinline__ double krow_n(const Dir& d, const double* Kh, int e, int a,
+                                         const double* c) {
+  constexpr int n = N + 1;
+  double s = 0.0;
+  if (a != 0) {
+    const double* k = Kh + a * n;
+    const double* q = c - a * STRIDE;
+#pragma unroll
+    for (int b = 0; b < n; b++) s = fma(k[b], q[b * STRIDE], s);
+    return s;
+  }
+  if (e > 0 || d.periodic) {
+    const double* k = Kh + N * n;
+#pragma unroll
+    for (int b = 0; b < n; b++) s = fma(k[b], c[(b - N) * STRIDE], s);
+  }
+  if (e < d.nE) {
+#pragma unroll
+    for (int b = 0; b < n; b++) s = fma(Kh[b], c[b * STRIDE], s);
+  }
+  return s;
+}
+
+// Per-block copy of one solve's operator coefficients.
+struct OpSm {
+  double Kh[SE_MAXN1 * SE_MAXN1];
+  double w[SE_MAXN1];
+  double alpha, beta0, beta1;
+  Dir dx, dy;
+  int G0, G1;
+  int solve;
+  const double* b;
+  double *x, *r, *z, *p0, *p1, *wv, *dinv;
+};
+
+__device__ __forceinline__ void load_op(OpSm& o, const CgSolve& S, int solve) {
+  if (o.solve == solve) return;
+  __syncthreads();
+  const OpDev& op = S.op;
+  const int n = op.d[0].N + 1;
+  for (int k = threadIdx.x; k < n * n; k += blockDim.x) o.Kh[k] = op.Kh[k];
+  if (threadIdx.x < n) o.w[threadIdx.x] = op.w[threadIdx.x];
+  if (threadIdx.x == 0) {
+    o.alpha = op.alpha;
+    o.beta0 = op.beta[0];
+    o.beta1 = op.beta[1];
+    o.dx = op.d[0];
+    o.dy = op.d[1];
+    o.G0 = op.G[0];
+    o.G1 = op.G[1];
+    o.solve = solve;
+    o.b = S.b;
+    o.x = S.x;
+    o.r = S.r;
+    o.z = S.z;
+    o.p0 = S.p0;
+    o.p1 = S.p1;
+    o.wv = S.w;
+    o.dinv = S.dinv;
+  }
+  __syncthreads();
+}
+
+// Stage p = z + bc*p_old (p = z when first) for the tile and its halo.
+template <int N>
+__device__ __forceinline__ void stage_p(const OpSm& o, int x0, int y0, const double* z,
+                                        const double* po, bool first, double bc, double* P) {
+  typedef Geo<N> G;
+  const int gx0 = x0 + o.dx.lo - N, gy0 = y0 + o.dy.lo - N;
+  for (int k = threadIdx.x; k < G::kRows + G::kCols; k += kCgThreads) {
+    int i, j;
+    if (k < G::kRows) {
+      j = N + k / G::W;
+      i = k - (j - N) * G::W;
+    } else {
+      const int q = k - G::kRows;
+      const int jj = q / kCgTileX;
+      i = N + (q - jj * kCgTileX);
+      j = jj < N ? jj : jj + kCgTileY;
+    }
+    double v = 0.0;
+    const int ux = unknown_1d(o.dx, gx0 + i), uy = unknown_1d(o.dy, gy0 + j);
+    if (ux >= 0 && uy >= 0) {
+      const size_t q = (size_t)uy * o.G0 + ux;
+      v = first ? z[q] : fma(bc, po[q], z[q]);
+    }
+    P[j * G::W + i] = v;
+  }
+  __syncthreads();
+}
+
+// (A p) at the thread's unknown (tile coordinates tx, ty; vertex gx, gy).
+template <int N>
+__device__ __forceinline__ double apply_n(const OpSm& o, const double* P, int tx, int ty, int gx,
+                                          int gy) {
+  typedef Geo<N> G;
+  const double* c = P + (ty + N) * G::W + (tx + N);
+  const int ex = gx / N, ax = gx - ex * N, ey = gy / N, ay = gy - ey * N;
+  const double wx = wsum_n<N>(o.dx, o.w, ex, ax), wy = wsum_n<N>(o.dy, o.w, ey, ay);
+  const double kx = krow_n<N, 1>(o.dx, o.Kh, ex, ax, c);
+  const double ky = krow_n<N, G::W>(o.dy, o.Kh, ey, ay, c);
+  return o.alpha * wx * wy * c[0] + o.beta0 * wy * kx + o.beta1 * wx * ky;
+}
+
+template <int N>
+__device__ __forceinline__ double dinv_n(const OpSm& o, int gx, int gy) {
+  const int ex = gx / N, ax = gx - ex * N, ey = gy / N, ay = gy - ey * N;
+  const double wx = wsum_n<N>(o.dx, o.w, ex, ax), wy = wsum_n<N>(o.dy, o.w, ey, ay);
+  const double d = o.alpha * wx * wy + o.beta0 * kdiag_n<N>(o.dx, o.Kh, ex, ax) * wy +
+                   o.beta1 * wx * kdiag_n<N>(o.dy, o.Kh, ey, ay);
+  return 1.0 / d;
+}
+
+// --------------------------------------------------------------- scalars --
+// KSPConvergedDefault on the residual norm dp at iteration n.
+__device__ __forceinline__ void converged(SolveState& s, const SolveMeta& m, int n, double dp) {
+  if (!(dp == dp) || isinf(dp)) {
+    s.reason = -9;
+    s.done = 1;
+    return;
+  }
+  if (n == 0) {
+    s.rnorm0 = dp;
+    s.ttol = fmax(m.rtol * dp, m.atol);
+  }
+  if (dp <= s.ttol) {
+    s.reason = dp < m.atol ? 3 : 2;
+    s.done = 1;
+  } else if (n > 0 && dp >= m.dtol * s.rnorm0) {
+    s.reason = -4;
+    s.done = 1;
+  }
+}
+__device__ __forceinline__ double norm_of(const SolveMeta& m, double zz, double zr, double rr) {
+  return m.norm_type == 0 ? sqrt(zz) : (m.norm_type == 1 ? sqrt(rr) : sqrt(fabs(zr)));
+}
+
+enum Step { ST_MEAN = 0, ST_START, ST_APPLY, ST_UPDATE };
+
+// After a barrier: every block updates every solve's state from the partial
+// sums, warp w taking solves w, w + nwarps, ...; then counts active solves.
+template <int STEP>
+__device__ __forceinline__ int update_states(const CgBatch& B, const double* part, SolveState* st,
+                                             const SolveMeta* mt) {
+  __shared__ int s_active;
+  if (threadIdx.x == 0) s_active = 0;
+  __syncthreads();
+  const int w = threadIdx.x >> 5, nw = kCgThreads / 32, l = threadIdx.x & 31;
+  for (int s = w; s < B.nsolves; s += nw) {
+    SolveState& S = st[s];
+    const SolveMeta& M = mt[s];
+    if (STEP != ST_MEAN && S.done) continue;
+    double v[4];
+    seg_sum4(part, M.seg_begin, M.seg_end, v);
+    if (l != 0) continue;
+    if (STEP == ST_MEAN) {
+      S.zmean = M.remove_null ? v[3] / M.n : 0.0;
+    } else if (STEP == ST_START) {
+      const double dp = norm_of(M, v[0], v[1], v[2]);
+      S.dp = dp;
+      converged(S, M, 0, dp);
+      S.beta = v[1];
+      if (!S.done && M.max_it <= 0) {
+        S.reason = -3;
+        S.done = 1;
+      }
+      if (!S.done && S.beta == 0.0) {
+        S.reason = 3;
+        S.done = 1;
+      }
+    } else if (STEP == ST_APPLY) {
+      const double dpi = v[0];
+      const double dpiold = S.dpi;
+      S.dpi = dpi;
+      S.betaold = S.beta;
+      S.pbuf ^= 1;
+      if (dpi == 0.0 || (S.its > 0 && dpi * dpiold <= 0.0)) {
+        S.reason = -10;
+        S.done = 1;
+      } else {
+        S.a = S.beta / dpi;
+      }
+    } else {
+      const double zr = v[1];
+      S.its += 1;
+      const double dp = norm_of(M, v[0], v[1], v[2]);
+      S.dp = dp;
+      converged(S, M, S.its, dp);
+      if (!S.done) {
+        if (zr == 0.0) {
+          S.reason = 3;
+          S.done = 1;
+        } else if (zr * S.betaold < 0.0) {
+          S.reason = -8;
+          S.done = 1;
+        } else if (S.its >= M.max_it) {
+          S.reason = -3;
+          S.done = 1;
+        } else {
+          S.beta = zr;
+          S.bcoef = zr / S.betaold;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < B.nsolves; s += kCgThreads)
+    if (!st[s].done) atomicAdd(&s_active, 1);
+  __syncthreads();
+  return s_active;
+}
+
+enum Pass { PS_INIT = 0, PS_NULL, PS_APPLY, PS_UPDATE };
+
+template <int N, int K>
+struct Regs {
+  double x[K > 0 ? K : 1], r[K > 0 ? K : 1], dinv[K > 0 ? K : 1], p[K > 0 ? K : 1],
+      w[K > 0 ? K : 1], z[K > 0 ? K : 1];
+};
+
+// One pass over the block's tiles; writes the block's segment partials.
+constexpr int kTileCache = 64;  // tile descriptors a block keeps in shared memory
+
+template <int N, int K, int PASS>
+__device__ __forceinline__ void pass(const CgBatch& B, double* part, const SolveState* st, OpSm& o,
+                                     double* P, double (*red)[4], Regs<N, K>& R, int t0, int t1,
+                                     const CgTile* tcache) {
+  const int tx = threadIdx.x & (kCgTileX - 1), ty = threadIdx.x / kCgTileX;
+  int seg = -1;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  // The tile loop body; `continue` in it means "next tile".
+  auto tile = [&](int kk, int t) {
+    const CgTile T = t - t0 < kTileCache ? tcache[t - t0] : B.tiles[t];
+    if (T.seg != seg) {
+      if (seg >= 0) {
+        block_sum4(acc, red);
+        if (threadIdx.x == 0)
+#pragma unroll
+          for (int q = 0; q < 4; q++) part[(size_t)seg * 4 + q] = acc[q];
+      }
+      seg = T.seg;
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[q] = 0.0;
+    }
+    const SolveState& S = st[T.solve];
+    if (S.done && PASS != PS_INIT) return;
+    load_op(o, B.solves[T.solve], T.solve);
+    const int ux = T.x0 + tx, uy = T.y0 + ty;
+    const bool in = ux < o.G0 && uy < o.G1;
+    const size_t k = (size_t)uy * o.G0 + ux;
+    const int gx = ux + o.dx.lo, gy = uy + o.dy.lo;
+    if (PASS == PS_APPLY) {
+      const double* po = S.pbuf ? o.p1 : o.p0;
+      double* pn = S.pbuf ? o.p0 : o.p1;
+      stage_p<N>(o, T.x0, T.y0, o.z, po, S.its == 0, S.bcoef, P);
+      if (in) {
+        const double p = P[(ty + N) * Geo<N>::W + (tx + N)];
+        const double w = apply_n<N>(o, P, tx, ty, gx, gy);
+        pn[k] = p;
+        if (K > 0) {
+          R.p[kk] = p;
+          R.w[kk] = w;
+        } else {
+          o.wv[k] = w;
+        }
+        acc[0] += p * w;
+      }
+      __syncthreads();  // the next tile reuses P
+      return;
+    }
+    if (!in) return;
+    if (PASS == PS_INIT) {
+      const double r = o.b[k];
+      const double di = dinv_n<N>(o, gx, gy);
+      const double z = r * di;
+      if (K > 0) {
+        R.x[kk] = 0.0;
+        R.r[kk] = r;
+        R.dinv[kk] = di;
+        R.z[kk] = z;
+      } else {
+        o.x[k] = 0.0;
+        o.r[k] = r;
+        o.dinv[k] = di;
+      }
+      o.z[k] = z;
+      acc[0] += z * z;
+      acc[1] += z * r;
+      acc[2] += r * r;
+      acc[3] += z;
+    } else if (PASS == PS_NULL) {
+      const double z = (K > 0 ? R.z[kk] : o.z[k]) - S.zmean;
+      const double r = K > 0 ? R.r[kk] : o.r[k];
+      if (K > 0) R.z[kk] = z;
+      o.z[k] = z;
+      acc[0] += z * z;
+      acc[1] += z * r;
+      acc[2] += r * r;
+    } else {  // PS_UPDATE: x += a p; r -= a w; z = D^-1 r
+      const double a = S.a;
+      double x, r, di;
+      if (K > 0) {
+        x = fma(a, R.p[kk], R.x[kk]);
+        r = fma(-a, R.w[kk], R.r[kk]);
+        di = R.dinv[kk];
+        R.x[kk] = x;
+        R.r[kk] = r;
+      } else {
+        const double* pc = S.pbuf ? o.p1 : o.p0;  // pbuf already points at the new p
+        x = fma(a, pc[k], o.x[k]);
+        r = fma(-a, o.wv[k], o.r[k]);
+        di = o.dinv[k];
+        o.x[k] = x;
+        o.r[k] = r;
+      }
+      const double z = r * di;
+      if (K > 0) R.z[kk] = z;
+      o.z[k] = z;
+      acc[0] += z * z;
+      acc[1] += z * r;
+      acc[2] += r * r;
+      acc[3] += z;
+    }
+    };
+  if (K > 0) {
+#pragma unroll
+    for (int kk = 0; kk < (K > 0 ? K : 1); kk++)
+      if (t0 + kk < t1) tile(kk, t0 + kk);
+  } else {
+    for (int t = t0; t < t1; t++) tile(0, t);
+  }
+  if (seg >= 0) {
+    block_sum4(acc, red);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int q = 0; q < 4; q++) part[(size_t)seg * 4 + q] = acc[q];
+  }
+}
+
+template <int N, int K>
+__global__ void __launch_bounds__(kCgThreads, 1) cg_n_kernel(const CgBatch B) {
+  extern __shared__ double dyn[];
+  SolveState* st = reinterpret_cast<SolveState*>(dyn);
+  SolveMeta* mt = reinterpret_cast<SolveMeta*>(st + B.nsolves);
+  double* P = reinterpret_cast<double*>(mt + B.nsolves);
+  P = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(P) + 15) & ~uintptr_t(15));
+  __shared__ OpSm o;
+  __shared__ double red[kCgThreads / 32][4];
+  __shared__ CgTile tcache[kTileCache];
+  Regs<N, K> R;
+  const int t0 = B.block_tile_begin[blockIdx.x], t1 = B.block_tile_begin[blockIdx.x + 1];
+  if (threadIdx.x == 0) o.solve = -1;
+  for (int t = t0 + threadIdx.x; t < t1 && t - t0 < kTileCache; t += kCgThreads)
+    tcache[t - t0] = B.tiles[t];
+  bool any_null = false;
+  for (int s = threadIdx.x; s < B.nsolves; s += kCgThreads) {
+    const CgSolve& C = B.solves[s];
+    SolveMeta& M = mt[s];
+    M.seg_begin = C.seg_begin;
+    M.seg_end = C.seg_end;
+    M.max_it = C.max_it;
+    M.norm_type = C.norm_type;
+    M.remove_null = C.remove_null;
+    M.n = C.n;
+    M.rtol = C.rtol;
+    M.atol = C.atol;
+    M.dtol = C.dtol;
+    SolveState& S = st[s];
+    S.beta = S.betaold = S.dpi = S.bcoef = S.a = S.rnorm0 = S.ttol = S.dp = S.zmean = 0.0;
+    S.its = S.done = S.reason = S.pbuf = 0;
+  }
+  __syncthreads();
+  for (int s = 0; s < B.nsolves; s++) any_null |= mt[s].remove_null != 0;
+
+  // Partial sums alternate between two buffers pass by pass: a block that
+  // has passed barrier k may write pass k+1's sums while a slower block still
+  // reads pass k's, but nobody writes pass k+2's before every block has
+  // arrived at barrier k+1, i.e. finished reading pass k's.
+  int pc = 0;
+  auto part = [&]() { return B.partials + (size_t)(pc & 1) * B.nseg * 4; };
+  pass<N, K, PS_INIT>(B, part(), st, o, P, red, R, t0, t1, tcache);
+  if (!grid_sync(B.bar_count, B.err)) return;
+  update_states<ST_MEAN>(B, part(), st, mt);
+  if (any_null) {
+    ++pc;
+    pass<N, K, PS_NULL>(B, part(), st, o, P, red, R, t0, t1, tcache);
+    if (!grid_sync(B.bar_count, B.err)) return;
+  }
+  int active = update_states<ST_START>(B, part(), st, mt);
+  while (active > 0) {
+    ++pc;
+    pass<N, K, PS_APPLY>(B, part(), st, o, P, red, R, t0, t1, tcache);
+    if (!grid_sync(B.bar_count, B.err)) return;
+    update_states<ST_APPLY>(B, part(), st, mt);
+    ++pc;
+    pass<N, K, PS_UPDATE>(B, part(), st, o, P, red, R, t0, t1, tcache);
+    if (!grid_sync(B.bar_count, B.err)) return;
+    if (any_null) {
+      update_states<ST_MEAN>(B, part(), st, mt);
+      ++pc;
+      pass<N, K, PS_NULL>(B, part(), st, o, P, red, R, t0, t1, tcache);
+      if (!grid_sync(B.bar_count, B.err)) return;
+    }
+    active = update_states<ST_UPDATE>(B, part(), st, mt);
+  }
+  // results: x back to memory (resident mode), states by block 0
+  if (K > 0) {
+    const int tx = threadIdx.x & (kCgTileX - 1), ty = threadIdx.x / kCgTileX;
+#pragma unroll
+    for (int kk = 0; kk < (K > 0 ? K : 1); kk++) {
+      const int t = t0 + kk;
+      if (t >= t1) break;
+      const CgTile T = B.tiles[t];
+      const CgSolve& C = B.solves[T.solve];
+      const int ux = T.x0 + tx, uy = T.y0 + ty;
+      if (ux < C.op.G[0] && uy < C.op.G[1]) C.x[(size_t)uy * C.op.G[0] + ux] = R.x[kk];
+    }
+  }
+  if (blockIdx.x == 0)
+    for (int s = threadIdx.x; s < B.nsolves; s += kCgThreads) {
+      CgSolve& C = B.solves[s];
+      const SolveState& S = st[s];
+      C.its = S.its;
+      C.reason = S.reason;
+      C.done = S.done;
+      C.dp = S.dp;
+      C.rnorm0 = S.rnorm0;
+      C.beta = S.beta;
+    }
+}
+
+template <int N, int K>
+const void* kernel_ptr() {
+  return (const void*)cg_n_kernel<N, K>;
+}
+
+const void* pick(int N, int K) {
+#define SE_CASE(n)                                         \
+  case n:                                                  \
+    return K > 0 ? kernel_ptr<n, kCgResidentTiles>() : kernel_ptr<n, 0>();
+  switch (N) {
+    SE_CASE(2) SE_CASE(3) SE_CASE(4) SE_CASE(5) SE_CASE(6) SE_CASE(7) SE_CASE(8) SE_CASE(9)
+    SE_CASE(10) SE_CASE(11) SE_CASE(12)
+    default:
+      return nullptr;
+  }
+#undef SE_CASE
+}
+
+}  // namespace
+
+size_t cg_dyn_smem_bytes(int N, int nsolves) {
+  return sizeof(SolveState) * nsolves + sizeof(SolveMeta) * nsolves + 16 +
+         sizeof(double) * (size_t)(kCgTileX + 2 * N) * (kCgTileY + 2 * N);
+}
+
+int cg_max_grid(int device, int N, bool resident, int nsolves) {
+  const void* f = pick(N, resident ? 1 : 0);
+  if (!f) return 0;
+  int sms = 0, per_sm = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
+    return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, kCgThreads,
+                                                    cg_dyn_smem_bytes(N, nsolves)) != cudaSuccess)
+    return 0;
+  return sms * per_sm;
+}
+
+cudaError_t launch_cg(const CgBatch& batch, int grid, int N, bool resident, cudaStream_t s) {
+  const void* f = pick(N, resident ? 1 : 0);
+  if (!f) return cudaErrorInvalidValue;
+  const size_t smem = cg_dyn_smem_bytes(N, batch.nsolves);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  void* args[] = {const_cast<CgBatch*>(&batch)};
+  return cudaLaunchCooperativeKernel(f, dim3(grid), dim3(kCgThreads), args, smem, s);
+}
+
+}  // namespace seg

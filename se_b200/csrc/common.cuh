@@ -115,6 +115,7 @@ struct CgSolve {
   OpDev op;
   const double* b;  // right-hand side (unknowns)
   double *x, *r, *z, *p0, *p1, *w;
+  double* dinv;     // Jacobi inverse (streaming mode only)
   double rtol, atol, dtol;
   int max_it;
   int norm_type;
@@ -136,7 +137,7 @@ struct CgBatch {
   int nsolves;
   const CgTile* tiles;  // device array, grouped by block (contiguous chunks)
   const int* block_tile_begin;  // [grid+1]
-  double* partials;  // [nseg][4]
+  double* partials;  // [2][nseg][4]: double-buffered by pass parity
   int nseg;
   unsigned* bar_count;
   unsigned* bar_gen;
@@ -146,10 +147,35 @@ struct CgBatch {
 constexpr int kCgTileX = 32;
 constexpr int kCgTileY = 16;
 constexpr int kCgThreads = kCgTileX * kCgTileY;
-// Shared memory of one CG block for polynomial orders up to maxN.
+// Shared memory of the standalone operator apply for order maxN.
 size_t cg_smem_bytes(int maxN);
-// Blocks of kCgThreads that can be co-resident on this device.
-int cg_max_grid(int device, int maxN);
-cudaError_t launch_cg(const CgBatch& batch, int grid, int maxN, cudaStream_t s);
+// Tiles a block may own in the register-resident CG mode.
+constexpr int kCgResidentTiles = 4;
+// Dynamic shared memory of one CG block (order N, nsolves per launch).
+size_t cg_dyn_smem_bytes(int N, int nsolves);
+// Blocks of kCgThreads that can be co-resident for the CG kernel.
+int cg_max_grid(int device, int N, bool resident, int nsolves);
+// Persistent CG over a batch of same-order solves; resident needs every block
+// to own at most kCgResidentTiles tiles.
+cudaError_t launch_cg(const CgBatch& batch, int grid, int N, bool resident, cudaStream_t s);
+
+// Fast-diagonalization pieces (fdm.cu). prec: 0 FP64, 1 FP32, 2 BF16.
+cudaError_t launch_spectral_divide(int prec, void* v, int gx, int gy, const double* lx,
+                                   const double* ly, double alpha, double bx, double by,
+                                   double null_tol, cudaStream_t s);
+cudaError_t launch_to_low(int prec, const double* x, void* y, size_t n, double scale,
+                          cudaStream_t s);
+cudaError_t launch_add_low(int prec, double* x, const void* y, size_t n, double inv_scale,
+                           cudaStream_t s);
+// out2 = {sum (w r)^2 or, natural != 0, sum r w r; sum r^2} (w == nullptr:
+// w = 1), deterministic.
+cudaError_t launch_norms(const double* r, const double* w, size_t n, int natural, double* partial,
+                         int npart, double* out2, cudaStream_t s);
+cudaError_t launch_maxabs(const double* x, size_t n, double* partial, int npart, double* out,
+                          cudaStream_t s);
+cudaError_t launch_sub(const double* b, const double* y, double* r, size_t n, cudaStream_t s);
+cudaError_t launch_invert(double* x, size_t n, cudaStream_t s);
+cudaError_t launch_remove_mean(double* x, size_t n, double* partial, int npart, double* sum2,
+                               cudaStream_t s);
 
 }  // namespace seg

@@ -16,16 +16,7 @@
 // unknown sums its own row of the assembled 1-D operators in a fixed order,
 // so the result is deterministic and needs no atomics.
 //
-// CG. One cooperative launch runs all iterations of a batch of solves.
-// Tiles of 32x8 unknowns are statically assigned in contiguous chunks to the
-// resident blocks; every dot product is reduced in a fixed order
-// (warp shuffles, then block, then segment by segment in the last block to
-// reach the grid barrier), so repeated solves are bit-for-bit identical.
-// Two grid barriers per iteration (three with a constant null space).
-// The iteration is PETSc's KSPCG with PCJACOBI (zero initial guess,
-// preconditioned/unpreconditioned/natural norm, RTOL/ATOL/DTOL tests and
-// the sign checks for an indefinite matrix or preconditioner), as SE runs
-// it from src/linsys/HelmholtzEqn.cpp:141-150.
+// The persistent CG that drives this operator is in cg.cu.
 #include "common.cuh"
 
 namespace seg {
@@ -273,363 +264,6 @@ __global__ void update_field_kernel(const OpDev op, const MeshDev m, const doubl
   if (cx && cy) sol[(size_t)nvy * nvx - 1] = v;
 }
 
-// ------------------------------------------------------------ grid barrier --
-__device__ __forceinline__ unsigned ld_acquire(const unsigned* p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release(unsigned* p, unsigned v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Grid-wide barrier for a cooperative launch. The last block to arrive runs
-// last_fn (with the whole block) before releasing the others. Waits are
-// bounded: after ~2^26 polls a block records KERR_BARRIER_TIMEOUT and goes
-// on; callers check the error word after every barrier and return.
-constexpr long kBarrierPolls = 1L << 26;
-template <class F>
-__device__ __forceinline__ void grid_barrier(const CgBatch& B, F&& last_fn) {
-  __shared__ unsigned s_last, s_gen;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned gen = ld_acquire(B.bar_gen);
-    __threadfence();
-    unsigned arrived = atomicAdd(B.bar_count, 1u) + 1u;
-    s_last = arrived == gridDim.x;
-    s_gen = gen;
-  }
-  __syncthreads();
-  if (s_last) {
-    __threadfence();
-    last_fn();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      atomicExch(B.bar_count, 0u);
-      __threadfence();
-      st_release(B.bar_gen, s_gen + 1u);
-    }
-  } else if (threadIdx.x == 0) {
-    long polls = 0;
-    while (ld_acquire(B.bar_gen) == s_gen) {
-      if (++polls > kBarrierPolls) {
-        atomicOr(B.err, KERR_BARRIER_TIMEOUT);
-        break;
-      }
-      if (polls > 256) __nanosleep(64);
-    }
-    __threadfence();
-  }
-  __syncthreads();
-}
-
-// Fixed-order block reduction of 4 sums into lane 0 of warp 0.
-__device__ __forceinline__ void block_sum4(double v[4]) {
-  __shared__ double sm[kCgThreads / 32][4];
-#pragma unroll
-  for (int q = 0; q < 4; q++)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0)
-#pragma unroll
-    for (int q = 0; q < 4; q++) sm[w][q] = v[q];
-  __syncthreads();
-  if (w == 0) {
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      v[q] = l < kCgThreads / 32 ? sm[l][q] : 0.0;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
-    }
-  }
-  __syncthreads();
-}
-
-// Sum of partial slot q over a solve's segments, fixed order; result valid in
-// every lane of the calling warp. Lane l sums segments l, l+32, ... in order;
-// the loads of a lane are issued eight at a time so that the L2 round trips
-// overlap.
-__device__ __forceinline__ double seg_sum(const CgBatch& B, const CgSolve& S, int q) {
-  const int l = threadIdx.x & 31;
-  double s = 0.0;
-  int k = S.seg_begin + l;
-  for (; k + 7 * 32 < S.seg_end; k += 8 * 32) {
-    double v[8];
-#pragma unroll
-    for (int u = 0; u < 8; u++) v[u] = B.partials[(size_t)(k + u * 32) * 4 + q];
-#pragma unroll
-    for (int u = 0; u < 8; u++) s += v[u];
-  }
-  for (; k < S.seg_end; k += 32) s += B.partials[(size_t)k * 4 + q];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  return s;
-}
-
-enum { PH_INIT = 0, PH_NULL, PH_APPLY, PH_UPDATE };
-
-// One pass over this block's tiles. Accumulates per-segment partial sums.
-template <int PH>
-__device__ void cg_pass(const CgBatch& B, int t0, int t1, double* smem) {
-  const int tx = threadIdx.x & (kCgTileX - 1), ty = threadIdx.x / kCgTileX;
-  int cur_seg = -1;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int t = t0; t < t1; t++) {
-    const CgTile T = B.tiles[t];
-    const CgSolve& S = B.solves[T.solve];
-    if (T.seg != cur_seg) {
-      if (cur_seg >= 0) {
-        block_sum4(acc);
-        if (threadIdx.x == 0)
-#pragma unroll
-          for (int q = 0; q < 4; q++) B.partials[(size_t)cur_seg * 4 + q] = acc[q];
-      }
-      cur_seg = T.seg;
-#pragma unroll
-      for (int q = 0; q < 4; q++) acc[q] = 0.0;
-    }
-    if (S.done) continue;
-    if (PH == PH_APPLY) {
-      // p = z + bcoef p_old (p = z on the first iteration) staged with its
-      // halo; w = A p; the current p is (pbuf ? p1 : p0) and the new one goes
-      // to the other buffer. z and p are rewritten by this kernel between
-      // passes: plain coherent loads, never the read-only path.
-      const int G0 = S.op.G[0];
-      const double* z = S.z;
-      const double* po = S.pbuf ? S.p1 : S.p0;
-      double* pn = S.pbuf ? S.p0 : S.p1;
-      const bool first = S.its == 0;
-      const double bc = S.bcoef;
-      load_tile(S.op, T.x0, T.y0, smem, [&](int a, int b) {
-        const size_t q = (size_t)b * G0 + a;
-        return first ? z[q] : fma(bc, po[q], z[q]);
-      });
-      const int ux = T.x0 + tx, uy = T.y0 + ty;
-      if (ux < S.op.G[0] && uy < S.op.G[1]) {
-        const int N = S.op.d[0].N;
-        const double p = smem[(ty + N) * tile_w(N) + (tx + N)];
-        const double w = apply_tile(S.op, ux + S.op.d[0].lo, uy + S.op.d[1].lo, smem, tx, ty);
-        const size_t k = (size_t)uy * G0 + ux;
-        pn[k] = p;
-        S.w[k] = w;
-        acc[0] += p * w;
-      }
-      __syncthreads();  // the next tile reuses the shared buffer
-      continue;
-    }
-    const int ux = T.x0 + tx, uy = T.y0 + ty;
-    if (ux >= S.op.G[0] || uy >= S.op.G[1]) continue;
-    const int G0 = S.op.G[0];
-    const size_t k = (size_t)uy * G0 + ux;
-    const int gx = ux + S.op.d[0].lo, gy = uy + S.op.d[1].lo;
-    if (PH == PH_INIT) {
-      // r = b (x = 0), z = D^{-1} r
-      double r = S.b[k];
-      double z = r / diag_at(S.op, gx, gy);
-      S.x[k] = 0.0;
-      S.r[k] = r;
-      S.z[k] = z;
-      acc[0] += z * z;
-      acc[1] += z * r;
-      acc[2] += r * r;
-      acc[3] += z;
-    } else if (PH == PH_NULL) {
-      // z -= mean(z)
-      double z = S.z[k] - S.zmean;
-      double r = S.r[k];
-      S.z[k] = z;
-      acc[0] += z * z;
-      acc[1] += z * r;
-      acc[2] += r * r;
-    } else if (PH == PH_APPLY) {
-      // handled per tile by cg_apply_tile
-    } else {
-      // x += a p; r -= a w; z = D^{-1} r (p is the buffer the apply wrote;
-      // the barrier after the apply flipped pbuf to point at it)
-      const double* pn = S.pbuf ? S.p1 : S.p0;
-      const double a = S.a;
-      double p = pn[k], w = S.w[k];
-      double x = S.x[k] + a * p;
-      double r = S.r[k] - a * w;
-      double z = r / diag_at(S.op, gx, gy);
-      S.x[k] = x;
-      S.r[k] = r;
-      S.z[k] = z;
-      acc[0] += z * z;
-      acc[1] += z * r;
-      acc[2] += r * r;
-      acc[3] += z;
-    }
-  }
-  if (cur_seg >= 0) {
-    block_sum4(acc);
-    if (threadIdx.x == 0)
-#pragma unroll
-      for (int q = 0; q < 4; q++) B.partials[(size_t)cur_seg * 4 + q] = acc[q];
-  }
-}
-
-// Residual norm in the chosen norm from the partials of the last pass.
-__device__ __forceinline__ double cg_norm(const CgSolve& S, double zz, double zr, double rr) {
-  if (S.norm_type == 0) return sqrt(zz);
-  if (S.norm_type == 1) return sqrt(rr);
-  return sqrt(fabs(zr));
-}
-
-// Convergence test of KSPConvergedDefault; sets reason/done. n = iteration.
-__device__ __forceinline__ void cg_converged(CgSolve& S, int n, double dp) {
-  if (!(dp == dp) || isinf(dp)) {
-    S.reason = -9;
-    S.done = 1;
-    return;
-  }
-  if (n == 0) {
-    S.rnorm0 = dp;
-    S.ttol = fmax(S.rtol * dp, S.atol);
-  }
-  if (dp <= S.ttol) {
-    S.reason = dp < S.atol ? 3 : 2;
-    S.done = 1;
-  } else if (n > 0 && dp >= S.dtol * S.rnorm0) {
-    S.reason = -4;
-    S.done = 1;
-  }
-}
-
-__global__ void __launch_bounds__(kCgThreads) cg_kernel(const CgBatch B) {
-  extern __shared__ double smem[];
-  const int t0 = B.block_tile_begin[blockIdx.x], t1 = B.block_tile_begin[blockIdx.x + 1];
-  const bool any_null = [&] {
-    for (int s = 0; s < B.nsolves; s++)
-      if (B.solves[s].remove_null) return true;
-    return false;
-  }();
-
-  // ---- r = b, z = D^{-1} r; norms; beta = z.r
-  cg_pass<PH_INIT>(B, t0, t1, smem);
-  grid_barrier(B, [&] {
-    if (threadIdx.x >= 32) return;
-    for (int s = 0; s < B.nsolves; s++) {
-      CgSolve& S = B.solves[s];
-      const double zsum = seg_sum(B, S, 3);
-      if (threadIdx.x == 0) S.zmean = S.remove_null ? zsum / S.n : 0.0;
-    }
-  });
-  if (*B.err) return;
-  if (any_null) {
-    cg_pass<PH_NULL>(B, t0, t1, smem);
-    grid_barrier(B, [] {});
-    if (*B.err) return;
-  }
-  grid_barrier(B, [&] {
-    if (threadIdx.x >= 32) return;
-    int active = 0;
-    for (int s = 0; s < B.nsolves; s++) {
-      CgSolve& S = B.solves[s];
-      const double zz = seg_sum(B, S, 0), zr = seg_sum(B, S, 1), rr = seg_sum(B, S, 2);
-      if (threadIdx.x == 0) {
-        S.its = 0;
-        S.reason = 0;
-        S.done = 0;
-        S.pbuf = 0;
-        S.dpi = 0.0;
-        S.betaold = 0.0;
-        const double dp = cg_norm(S, zz, zr, rr);
-        S.dp = dp;
-        cg_converged(S, 0, dp);
-        S.beta = zr;
-        if (!S.done && S.max_it <= 0) {
-          S.reason = -3;
-          S.done = 1;
-        }
-        if (!S.done && S.beta == 0.0) {
-          S.reason = 3;
-          S.done = 1;
-        }
-        active += !S.done;
-      }
-    }
-    if (threadIdx.x == 0) *B.n_active = active;
-  });
-  if (*B.err) return;
-
-  while (*(volatile int*)B.n_active > 0) {
-    // ---- p = z + (beta/betaold) p; w = A p; dpi = p.w
-    cg_pass<PH_APPLY>(B, t0, t1, smem);
-    grid_barrier(B, [&] {
-      if (threadIdx.x >= 32) return;
-      for (int s = 0; s < B.nsolves; s++) {
-        CgSolve& S = B.solves[s];
-        if (S.done) continue;
-        const double dpi = seg_sum(B, S, 0);
-        if (threadIdx.x == 0) {
-          const double dpiold = S.dpi;
-          S.dpiold = dpiold;
-          S.dpi = dpi;
-          S.betaold = S.beta;
-          S.pbuf ^= 1;  // the apply wrote the other buffer
-          if (dpi == 0.0 || (S.its > 0 && dpi * dpiold <= 0.0)) {
-            S.reason = -10;
-            S.done = 1;
-          } else {
-            S.a = S.beta / dpi;
-          }
-        }
-      }
-    });
-    if (*B.err) return;
-    // ---- x += a p, r -= a w, z = D^{-1} r; norms
-    cg_pass<PH_UPDATE>(B, t0, t1, smem);
-    if (any_null) {
-      grid_barrier(B, [&] {
-        if (threadIdx.x >= 32) return;
-        for (int s = 0; s < B.nsolves; s++) {
-          CgSolve& S = B.solves[s];
-          const double zsum = seg_sum(B, S, 3);
-          if (threadIdx.x == 0) S.zmean = S.remove_null ? zsum / S.n : 0.0;
-        }
-      });
-      if (*B.err) return;
-      cg_pass<PH_NULL>(B, t0, t1, smem);
-    }
-    grid_barrier(B, [&] {
-      if (threadIdx.x >= 32) return;
-      int active = 0;
-      for (int s = 0; s < B.nsolves; s++) {
-        CgSolve& S = B.solves[s];
-        if (S.done) continue;
-        const double zz = seg_sum(B, S, 0), zr = seg_sum(B, S, 1), rr = seg_sum(B, S, 2);
-        if (threadIdx.x == 0) {
-          S.its += 1;
-          const double dp = cg_norm(S, zz, zr, rr);
-          S.dp = dp;
-          cg_converged(S, S.its, dp);
-          if (!S.done) {
-            const double beta = zr;
-            if (beta == 0.0) {
-              S.reason = 3;
-              S.done = 1;
-            } else if (beta * S.betaold < 0.0) {
-              S.reason = -8;
-              S.done = 1;
-            } else if (S.its >= S.max_it) {
-              S.reason = -3;
-              S.done = 1;
-            } else {
-              S.beta = beta;
-              S.bcoef = beta / S.betaold;
-            }
-          }
-          active += !S.done;
-        }
-      }
-      if (threadIdx.x == 0) *B.n_active = active;
-    });
-    if (*B.err) return;
-  }
-}
-
 }  // namespace
 
 size_t cg_smem_bytes(int maxN) {
@@ -663,22 +297,6 @@ cudaError_t launch_update_field(const OpDev& op, const MeshDev& m, const double*
   dim3 block(32, 8), grid((op.G[0] + 31) / 32, (op.G[1] + 7) / 8);
   update_field_kernel<<<grid, block, 0, s>>>(op, m, x, sol_vals);
   return cudaGetLastError();
-}
-
-int cg_max_grid(int device, int maxN) {
-  int sms = 0, per_sm = 0;
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
-    return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, cg_kernel, kCgThreads,
-                                                    cg_smem_bytes(maxN)) != cudaSuccess)
-    return 0;
-  return sms * per_sm;
-}
-
-cudaError_t launch_cg(const CgBatch& batch, int grid, int maxN, cudaStream_t s) {
-  void* args[] = {const_cast<CgBatch*>(&batch)};
-  return cudaLaunchCooperativeKernel((const void*)cg_kernel, dim3(grid), dim3(kCgThreads), args,
-                                     cg_smem_bytes(maxN), s);
 }
 
 }  // namespace seg

@@ -42,7 +42,8 @@ SE_ERR_DOMAIN = -7
 
 NORM_PRECONDITIONED, NORM_UNPRECONDITIONED, NORM_NATURAL = 0, 1, 2
 MODE_REFERENCE, MODE_EXACT = 0, 1
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_BF16 = 0, 1, 2
+METHOD_CG, METHOD_FDM = 0, 1
 
 KSP_REASONS = {2: "CONVERGED_RTOL", 3: "CONVERGED_ATOL", -3: "DIVERGED_ITS",
                -4: "DIVERGED_DTOL", -8: "DIVERGED_INDEFINITE_PC",
@@ -60,7 +61,7 @@ class SolverOpts(ctypes.Structure):
                 ("dtol", ctypes.c_double), ("max_it", ctypes.c_int),
                 ("norm_type", ctypes.c_int), ("mode", ctypes.c_int),
                 ("precision", ctypes.c_int), ("inner_max_it", ctypes.c_int),
-                ("inner_rtol", ctypes.c_double)]
+                ("inner_rtol", ctypes.c_double), ("method", ctypes.c_int)]
 
 
 class SolveStats(ctypes.Structure):

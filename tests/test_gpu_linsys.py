@@ -191,3 +191,65 @@ def test_field_error_calc_time_step(segpu, oracle):
     fv = segpu.Field("v", m, 2, None)
     fv.vals = v
     assert abs(segpu.CalcTimeStep(fv, 2.0) - om.calc_time_step(v, 2.0)) <= 1e-15
+
+
+# ------------------------------------------------- fast diagonalization ----
+@pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("prec", [0, 1, 2])
+def test_fdm_solve_matches_oracle(segpu, oracle, case, prec):
+    """FDM (exact 1-D eigenvector transforms) refined in FP64 to rtol 1e-10 in
+    the true preconditioned residual reaches the oracle's CG solution of the
+    same system (run to rtol 1e-14), for FP64, TF32 and BF16 transform
+    arithmetic."""
+    om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, CASES[case], -3.0, -1.0, 1.0,
+                                                     True, seed=case + 20)
+    ref_sol, st = oracle.helmholtz_solve(om, sol, rhs, -3.0, -1.0, 1.0, bcs=CASES[case][6],
+                                         quirk=True, rtol=1e-14)
+    ls.set_opts(segpu.solver_opts(rtol=1e-10, method=segpu.METHOD_FDM, precision=prec,
+                                  max_it=40))
+    out = ls.Solve("helm_")
+    assert out["reason"] == 2, out
+    if prec == 0:
+        assert out["its"] <= 2
+    got = fs.vals
+    assert np.abs(got - ref_sol).max() <= 1e-8 * np.abs(ref_sol).max()
+    assert np.array_equal(got[f2v < 0], sol[f2v < 0])
+
+
+def test_fdm_config0_exact_modal_and_null_space(segpu, oracle):
+    rng = np.random.default_rng(0)
+    m = segpu.Mesh("m", [16, 16], "legendre", 6, [0, 0], [1, 1], [True, True])
+    X = m.verts
+    f, u = np.zeros(len(X)), np.zeros(len(X))
+    for _ in range(8):
+        kx, ky = rng.integers(1, 7, size=2)
+        a, b = rng.standard_normal(2)
+        ph = 2 * np.pi * (kx * X[:, 0] + ky * X[:, 1])
+        mode = a * np.cos(ph) + b * np.sin(ph)
+        f += mode
+        u += mode / (-(4 * np.pi ** 2 * (kx * kx + ky * ky)) - 1.0)
+    bc = segpu.BCs(False, False, False, False, m)
+    fs, fr = segpu.Field("u", m, 1, bc), segpu.Field("f", m, 1, bc)
+    fr.vals = f
+    for prec in (0, 2):
+        ls = segpu.HelmholtzEqn(fs, fr, -1.0, -1.0, 1.0, 0,
+                                segpu.solver_opts(rtol=1e-10, mode=segpu.MODE_EXACT,
+                                                  method=segpu.METHOD_FDM, precision=prec))
+        st = ls.Solve("helm_")
+        assert st["reason"] == 2
+        assert np.linalg.norm(fs.vals - u) / np.linalg.norm(u) < 1e-7
+    # periodic Poisson with the constant null space: matches the oracle CG
+    om = oracle.Mesh(16, 16, 6)
+    g = om.periodic_update(np.sin(2 * np.pi * X[:, 0]) * np.cos(4 * np.pi * X[:, 1]))
+    fr.vals = g
+    ref, st = oracle.helmholtz_solve(om, np.zeros(om.nv), g, -1.0, 0, 0, quirk=True, rtol=1e-13,
+                                     remove_null_space=True, poisson=True)
+    ps = segpu.PoissonEqn(fs, fr, -1.0, segpu.solver_opts(rtol=1e-10, method=segpu.METHOD_FDM))
+    out = ps.Solve(removeNullSpace=True)
+    assert out["reason"] == 2
+    assert np.abs(fs.vals - ref).max() <= 1e-8 * np.abs(ref).max()
+
+
+def test_fdm_options_string(segpu):
+    o = segpu.solver_opts("helm_", "-helm_ksp_type preonly -helm_pc_type fdm -helm_ksp_rtol 1e-9")
+    assert o.method == segpu.METHOD_FDM and o.rtol == 1e-9
