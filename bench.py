@@ -72,48 +72,62 @@ def config(extra=None):
 
 # --------------------------------------------------------------- clocks ----
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled through NVML every
+    2 ms on a background thread during the timed region. NVML is initialised
+    and queried on that thread only."""
 
-    def __init__(self, index=0):
-        self.index, self.proc, self.path = index, None, None
+    BITS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+            0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown"}
+
+    def __init__(self, bus_id=None):
+        self.bus_id, self.thread, self.samples, self.reasons = bus_id, None, [], 0
+        self.stop_flag, self.max_mhz, self.error = False, None, None
 
     def start(self):
-        self.path = os.path.join("/tmp", f"se_clocks_{os.getpid()}.csv")
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "100",
-                 "-i", str(self.index)], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+        import threading
+
+        def run():
+            try:
+                import pynvml
+                pynvml.nvmlInit()
+                h = None
+                if self.bus_id:
+                    try:
+                        h = pynvml.nvmlDeviceGetHandleByPciBusId(self.bus_id.encode())
+                    except Exception:
+                        h = None
+                if h is None:
+                    h = pynvml.nvmlDeviceGetHandleByIndex(0)
+                self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM)
+                get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None)
+                while not self.stop_flag:
+                    self.samples.append(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                    if get_reasons is not None:
+                        self.reasons |= int(get_reasons(h))
+                    time.sleep(0.002)
+                pynvml.nvmlShutdown()
+            except Exception as e:  # no NVML: report unavailable
+                self.error = repr(e)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
 
     def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            f = [t.strip() for t in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        os.unlink(self.path)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
-                "samples": len(sm), "reasons": sorted(reasons)}
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "samples": 0, "reasons": ["unavailable"]}
+        self.stop_flag = True
+        self.thread.join()
+        names = sorted(v for b, v in self.BITS.items() if self.reasons & b)
+        out = {"sm_mhz": float(np.median(self.samples)) if self.samples else None,
+               "sm_max_mhz": float(self.max_mhz) if self.max_mhz else None,
+               "samples": len(self.samples), "reasons": names}
+        if self.error:
+            out["error"] = self.error
+        return out
+
+
+def log(msg):
+    print(f"[bench] {msg}", file=sys.stderr, flush=True)
 
 
 # ------------------------------------------------------------- GPU arm ----
@@ -174,7 +188,9 @@ def run_gpu(args, rank, world):
             if world > 1:
                 torch.distributed.barrier()
             steps = args.steps if name == HEADLINE else max(3, min(args.steps, 5))
-            sampler = ClockSampler(dev) if name == HEADLINE else None
+            bus = getattr(torch.cuda.get_device_properties(dev), "pci_bus_id", None)
+            sampler = ClockSampler(bus) if name == HEADLINE else None
+            log(f"variant {name}: timing {steps} steps")
             if sampler:
                 sampler.start()
             times, its, solve_ms = [], [], []
@@ -223,6 +239,35 @@ def run_gpu(args, rank, world):
                 results[name]["e2e_ms"] = float(np.mean(e2e_ms))
             del helm
 
+        log("SL kernel timing")
+        # the SL advection kernel alone (the largest kernel of the step that
+        # is this library's), CUDA events on its stream, L2 flushed
+        phi.vals = phi0
+        sl_ms = []
+        for _ in range(max(5, min(args.steps, 20))):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            adv.Advect(dt)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            sl_ms.append(e0.elapsed_time(e1))
+        log("FP64 DGEMM reference")
+        # FP64 peak of this GPU: a large cuBLAS DGEMM (denominator for the
+        # FP64-bound SL kernel)
+        a = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+        bm = torch.randn(8192, 8192, dtype=torch.float64, device="cuda")
+        torch.matmul(a, bm)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(3):
+            torch.matmul(a, bm)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fp64_tflops = 3 * 2 * 8192 ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+        del a, bm
+
     head = results[HEADLINE]
     step_ms, e2e = head["ms"], head["e2e_ms"]
     if world > 1:
@@ -230,7 +275,7 @@ def run_gpu(args, rank, world):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         step_ms, e2e = float(t[0]), float(t[1])
     return {"step_ms": step_ms, "e2e_ms": e2e, "ng": ng, "nv": m.nVertsTotal, "clocks": clock,
-            "variants": results}
+            "variants": results, "sl_ms": float(np.median(sl_ms)), "fp64_tflops": fp64_tflops}
 
 
 # Kernels of the library launched per headline step: SL advection, RHS
@@ -240,14 +285,36 @@ def run_gpu(args, rank, world):
 GPU_LAUNCHES_PER_STEP = 1 + 1 + 2 * 5 + 2 + 1
 
 
+# Algorithmic bytes and flops of one first-order SL vertex update at p=8:
+# tracer in 8 B + velocity in 16 B + value out 8 B; FP64 flops of the two
+# interpolations at non-node points (velocity at the midpoint, tracer at the
+# departure point; the one at the vertex itself snaps to the node): two
+# 9-point cardinal evaluations (5 flops per node) and a 9x9 tensor
+# contraction (2 flops per node and component) each.
+SL_BYTES_PER_VERTEX = 32.0
+SL_FLOPS_PER_VERTEX = (2 * 9 * 5 + 2 * 81 * 2 + 2 * 9 * 2) + (2 * 9 * 5 + 2 * 81 + 2 * 9)
+# Traffic of one SL launch (dram read + write bytes), from the ncu capture
+# summarised in profiles/sl_first_kernel_64x64_p8.md; None until captured.
+SL_TRAFFIC_BYTES = None
+
+
 def roofline(r):
-    """Roofline of the SL advection kernel, the largest kernel of the step
-    that is ours: FP64-bound gathers; reported against HBM with its
-    algorithmic bytes (tracer 8 + velocity 16 + output 8 per vertex)."""
+    """Roofline of the SL advection kernel, the largest of this library's
+    kernels in the step: achieved = algorithmic bytes per launch / measured
+    launch time, against the measured HBM copy bandwidth; the kernel is bound
+    by its FP64 gathers, so its FP64 rate against a measured DGEMM is beside it."""
     peaks = read_peaks()
-    return {"kernel": "sl_first_kernel<8> (see profiles/)", "bound": "hbm", "achieved": None,
-            "peak": peaks[0], "peak_source": peaks[1], "unit": "GB/s", "frac": None,
-            "traffic": None}
+    nv = r["nv"]
+    t = r["sl_ms"] * 1e-3
+    achieved = SL_BYTES_PER_VERTEX * nv / t / 1e9
+    fp64 = SL_FLOPS_PER_VERTEX * nv / t / 1e12
+    return {"kernel": "sl_first_kernel<8> (SL advection, FP64)", "bound": "hbm",
+            "achieved": achieved, "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
+            "peak_source": peaks[1] + " (MEASURED_PEAKS.json hbm_gbs)",
+            "launch_ms": r["sl_ms"], "algorithmic_bytes_per_launch": SL_BYTES_PER_VERTEX * nv,
+            "traffic": SL_TRAFFIC_BYTES,
+            "fp64_tflops_achieved": fp64, "fp64_tflops_peak_measured_dgemm": r["fp64_tflops"],
+            "fp64_frac": fp64 / r["fp64_tflops"]}
 
 
 def read_peaks():
@@ -345,6 +412,7 @@ def main():
         torch.distributed.destroy_process_group()
     if rank != 0:
         return
+    log("GPU arm done")
     cpu = None
     if not args.no_cpu_baseline:
         per_step, ng, its = cpu_sample(args.cpu_steps, nthreads)

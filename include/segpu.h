@@ -41,7 +41,7 @@ extern "C" {
 #define SE_KSP_CONVERGED_ATOL 3
 #define SE_KSP_DIVERGED_ITS (-3)
 #define SE_KSP_DIVERGED_DTOL (-4)
-#define SE_KSP_DIVERGED_BREAKDOWN (-5) /* FDM refinement stalled at the rounding floor */
+#define SE_KSP_DIVERGED_BREAKDOWN (-5) /* FDM refinement stalled: no 10% gain in 3 steps */
 #define SE_KSP_DIVERGED_INDEFINITE_PC (-8)
 #define SE_KSP_DIVERGED_NANORINF (-9)
 #define SE_KSP_DIVERGED_INDEFINITE_MAT (-10)
@@ -141,7 +141,10 @@ int se_advector_departures(se_advector* adv, int* el, double* xy);
 #define SE_MODE_EXACT 1     /* the Laplacian with its true Jacobian */
 #define SE_PREC_FP64 0      /* every operation in FP64: the drop-in */
 #define SE_PREC_MIXED 1     /* FP32 data, TF32 tensor-core inner solves, FP64 refinement */
-#define SE_PREC_BF16 2      /* BF16 data, FP32-accumulated tensor-core inner solves, FP64 refinement */
+#define SE_PREC_BF16 2      /* BF16 data, FP32-accumulated tensor-core inner solves, FP64 refinement;
+                               refinement converges only while 2^-8 times the operator's
+                               condition number stays below 1 (small or well-conditioned
+                               systems) and otherwise stops with SE_KSP_DIVERGED_BREAKDOWN */
 #define SE_METHOD_CG 0      /* PETSc KSPCG + PCJACOBI semantics: the drop-in */
 #define SE_METHOD_FDM 1     /* fast diagonalization: exact inverse by 1-D eigenvector transforms */
 typedef struct {

@@ -264,8 +264,15 @@ struct se_linsys {
   void *Sx_lo, *Sy_lo;        // low-precision copies of Sx, Sy
   double *X1, *X2, *ax;       // FP64 work: two transform buffers, A x
   void *L1, *L2, *L3;         // low-precision work
-  double* fpart;              // reduction partials [2*1184] + results [8]
+  double* fpart;              // reduction partials [2*fpart_n] + results [16]
+  int fpart_n;
   double lmax[2];  // largest 1-D eigenvalue magnitude per direction
+  cudaGraphExec_t fdm_exec;  // the captured FDM solve
+  int fdm_key;
+  void* cublas_ws;
+  FdmParams* d_fparams;
+  FdmState* d_fstate;
+  FdmParams h_fparams;  // staging copy for the asynchronous upload
 };
 
 namespace {
@@ -408,6 +415,10 @@ void linsys_free(se_linsys* ls) {
   if (ls->L2) cudaFree(ls->L2);
   if (ls->L3) cudaFree(ls->L3);
   dfree(ls->fpart);
+  if (ls->fdm_exec) cudaGraphExecDestroy(ls->fdm_exec);
+  if (ls->cublas_ws) cudaFree(ls->cublas_ws);
+  dfree(ls->d_fparams);
+  dfree(ls->d_fstate);
   if (ls->ev[0]) cudaEventDestroy(ls->ev[0]);
   if (ls->ev[1]) cudaEventDestroy(ls->ev[1]);
   delete ls->own_bcs;
@@ -636,8 +647,9 @@ int fdm_setup(se_linsys* ls, int prec) {
     std::vector<double> Sxh, Syh;
     if ((rc = eig_1d(op.d[0], op.Kh, op.w, &ls->Sx, &ls->lx, Sxh))) return rc;
     if ((rc = eig_1d(op.d[1], op.Kh, op.w, &ls->Sy, &ls->ly, Syh))) return rc;
+    ls->fpart_n = std::max(kFdmPartials, residual_blocks(op));
     if ((rc = dalloc(&ls->X1, n)) || (rc = dalloc(&ls->X2, n)) || (rc = dalloc(&ls->ax, n)) ||
-        (rc = dalloc(&ls->fpart, 2 * kFdmPartials + 8)))
+        (rc = dalloc(&ls->fpart, 2 * (size_t)ls->fpart_n + 16)))
       return rc;
     // Jacobi inverse for the preconditioned residual norm
     CK(launch_op_diag(op, ls->dinv, g_stream));
@@ -711,21 +723,16 @@ int fdm_apply64(se_linsys* ls, cublasHandle_t h, const double* in, double* out, 
   return SE_OK;
 }
 
-// Low-precision A^{-1} in (in: FP64, scaled by 1/max|in| into L1; result
-// added to out in FP64). prec 1: FP32 data, TF32 tensor cores; prec 2: BF16
-// data, FP32 accumulation.
+// Low-precision x += A^{-1} in: in scaled by 1/max|in| (max kept in device
+// memory) into L1, four GEMMs, result added back scaled. prec 1: FP32 data,
+// TF32 tensor cores; prec 2: BF16 data, FP32 accumulation.
 int fdm_apply_low(se_linsys* ls, cublasHandle_t h, const double* in, double* out) {
   const int gx = ls->op.G[0], gy = ls->op.G[1];
   const size_t n = (size_t)gx * gy;
   const int prec = ls->fdm_prec;
-  double* mx = ls->fpart + 2 * kFdmPartials;
+  double* mx = ls->fpart + 2 * ls->fpart_n;
   CK(launch_maxabs(in, n, ls->fpart, kFdmPartials, mx, g_stream));
-  double hmax = 0.0;
-  CK(cudaMemcpyAsync(&hmax, mx, sizeof(double), cudaMemcpyDeviceToHost, g_stream));
-  CK(cudaStreamSynchronize(g_stream));
-  if (!(hmax > 0.0)) return SE_OK;
-  const double scale = 1.0 / hmax;
-  CK(launch_to_low(prec, in, ls->L1, n, scale, g_stream));
+  CK(launch_to_low(prec, in, ls->L1, n, mx, g_stream));
   const float one = 1.0f, zero = 0.0f;
   const cudaDataType_t t = prec == 1 ? CUDA_R_32F : CUDA_R_16BF;
   const cublasComputeType_t ct = prec == 1 ? CUBLAS_COMPUTE_32F_FAST_TF32 : CUBLAS_COMPUTE_32F;
@@ -739,89 +746,159 @@ int fdm_apply_low(se_linsys* ls, cublasHandle_t h, const double* in, double* out
                   &zero, ls->L2, t, gx, ct, CUBLAS_GEMM_DEFAULT));
   CB(cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, gx, gy, gx, &one, ls->Sx_lo, t, gx, ls->L2, t, gx,
                   &zero, ls->L1, t, gx, ct, CUBLAS_GEMM_DEFAULT));
-  CK(launch_add_low(prec, out, ls->L1, n, hmax, g_stream));
+  CK(launch_add_low(prec, out, ls->L1, n, mx, g_stream));
   return SE_OK;
 }
 
-// Residual norms of r: returns the chosen norm (preconditioned: |D^-1 r|,
-// unpreconditioned: |r|, natural: sqrt|r.D^-1 r|).
-int residual_norm(se_linsys* ls, const double* r, double* out) {
-  const size_t n = (size_t)ls->n;
-  double* res = ls->fpart + 2 * kFdmPartials + 2;
-  double h[2];
-  const int nt = ls->opts.norm_type;
-  CK(launch_norms(r, nt == SE_NORM_UNPRECONDITIONED ? nullptr : ls->dinv, n,
-                  nt == SE_NORM_NATURAL, ls->fpart, kFdmPartials, res, g_stream));
-  CK(cudaMemcpyAsync(h, res, sizeof(h), cudaMemcpyDeviceToHost, g_stream));
-  CK(cudaStreamSynchronize(g_stream));
-  *out = std::sqrt(std::fabs(h[0]));
-  return SE_OK;
+constexpr size_t kCublasWorkspace = 32u << 20;
+
+// The whole FDM solve as one CUDA graph: right-hand side assembly, r = f,
+// x = 0, the initial norm and test, then a conditional while-node whose body
+// refines x += A^{-1} r, forms r = f - A x with its norm and runs the
+// convergence test that sets the loop condition; finally the field update.
+// Parameters (rtol, atol, dtol, max_it) and the loop state live in device
+// memory, so one solve is one graph launch and one read of the state.
+int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
+  cublasHandle_t h;
+  if (int rc = cublas_for(&h)) return rc;
+  if (!ls->cublas_ws) {
+    if (int rc = dalloc(&ls->cublas_ws, kCublasWorkspace)) return rc;
+  }
+  if (!ls->d_fparams) {
+    int rc;
+    if ((rc = dalloc(&ls->d_fparams, 1)) || (rc = dalloc(&ls->d_fstate, 1))) return rc;
+  }
+  if (ls->fdm_exec) {
+    cudaGraphExecDestroy(ls->fdm_exec);
+    ls->fdm_exec = nullptr;
+  }
+  const cudaStream_t saved = g_stream;
+  cudaStream_t cs = nullptr, bs = nullptr;
+  CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
+  auto cleanup = [&]() {
+    g_stream = saved;
+    cublasSetStream(h, saved);
+    cudaStreamDestroy(cs);
+    cudaStreamDestroy(bs);
+  };
+  int rc = SE_OK;
+  cudaGraph_t graph = nullptr;
+  do {
+    if (cublasSetWorkspace(h, ls->cublas_ws, kCublasWorkspace) != CUBLAS_STATUS_SUCCESS) {
+      rc = fail(SE_ERR_CUDA, "cublasSetWorkspace failed");
+      break;
+    }
+    const MeshDev& m = ls->sol->mesh->dev;
+    const size_t n = (size_t)ls->n;
+    const int nt = ls->opts.norm_type;
+    const double* wv = nt == SE_NORM_UNPRECONDITIONED ? nullptr : ls->dinv;
+    double* res = ls->fpart + 2 * ls->fpart_n + 2;
+    g_stream = cs;
+    cublasSetStream(h, cs);
+    cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) { rc = cuda_fail(e, "begin capture"); break; }
+    cudaStreamCaptureStatus status;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    cudaGraphConditionalHandle hc;
+    bool ok = cudaStreamGetCaptureInfo(cs, &status, nullptr, &cg, &deps, &ndeps) == cudaSuccess &&
+              cudaGraphConditionalHandleCreate(&hc, cg, 0, 0) == cudaSuccess;
+    // prologue
+    ok = ok && launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, cs) == cudaSuccess;
+    ok = ok && cudaMemcpyAsync(ls->r, ls->f, sizeof(double) * n, cudaMemcpyDeviceToDevice, cs) == cudaSuccess;
+    ok = ok && cudaMemsetAsync(ls->x, 0, sizeof(double) * n, cs) == cudaSuccess;
+    ok = ok && launch_norms(ls->f, wv, n, nt == SE_NORM_NATURAL, ls->fpart, kFdmPartials, res, cs) == cudaSuccess;
+    ok = ok && launch_fdm_init(ls->d_fparams, ls->d_fstate, res, hc, cs) == cudaSuccess;
+    // the while-node, depending on the prologue
+    cudaGraphNode_t cn = nullptr;
+    cudaGraph_t body = nullptr;
+    if (ok) {
+      ok = cudaStreamGetCaptureInfo(cs, &status, nullptr, &cg, &deps, &ndeps) == cudaSuccess;
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = hc;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      ok = ok && cudaGraphAddNode(&cn, cg, deps, ndeps, &cp) == cudaSuccess;
+      ok = ok && cudaStreamUpdateCaptureDependencies(cs, &cn, 1, cudaStreamSetCaptureDependencies) == cudaSuccess;
+      if (ok) body = cp.conditional.phGraph_out[0];
+    }
+    // the loop body, captured on its own stream
+    if (ok) {
+      g_stream = bs;
+      cublasSetStream(h, bs);
+      ok = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      int brc = SE_OK;
+      if (ok) {
+        brc = prec == 0 ? fdm_apply64(ls, h, ls->r, ls->x, true) : fdm_apply_low(ls, h, ls->r, ls->x);
+        if (!brc && remove_null)
+          brc = launch_remove_mean(ls->x, n, ls->fpart, kFdmPartials, ls->fpart + 2 * ls->fpart_n + 4, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
+        if (!brc) brc = launch_residual(ls->op, ls->x, ls->f, ls->r, wv, nt == SE_NORM_NATURAL, ls->fpart, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
+        if (!brc) brc = launch_norm_final(ls->fpart, residual_blocks(ls->op), res, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
+        if (!brc) brc = launch_fdm_check(ls->d_fparams, ls->d_fstate, res, hc, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
+        cudaGraph_t bodyg = body;
+        const bool ended = cudaStreamEndCapture(bs, &bodyg) == cudaSuccess;
+        ok = ended && brc == SE_OK;
+      }
+      g_stream = cs;
+      cublasSetStream(h, cs);
+    }
+    // epilogue
+    ok = ok && launch_update_field(ls->op, m, ls->x, ls->sol->vals, cs) == cudaSuccess;
+    const bool ended = cudaStreamEndCapture(cs, &graph) == cudaSuccess;
+    if (!ok || !ended) {
+      cudaGetLastError();
+      rc = fail(SE_ERR_CUDA, "capturing the FDM solve graph failed");
+      break;
+    }
+    e = cudaGraphInstantiate(&ls->fdm_exec, graph, 0);
+    if (e != cudaSuccess) {
+      rc = cuda_fail(e, "cudaGraphInstantiate");
+      ls->fdm_exec = nullptr;
+      break;
+    }
+    ls->fdm_key = prec | (remove_null << 2) | (nt << 3) | (ls->opts.mode << 6);
+  } while (0);
+  if (graph) cudaGraphDestroy(graph);
+  cleanup();
+  return rc;
 }
 
 // Solve A x = f by fast diagonalization with FP64 iterative refinement until
-// the chosen residual norm is <= max(rtol |f|, atol) in that norm.
+// the chosen residual norm is <= max(rtol |f|, atol) in that norm; the right
+// hand side assembly and the field update are part of the graph.
 int run_fdm(se_linsys* ls, int remove_null, CgSolve* st, float* kernel_ms) {
   const int prec = ls->opts.precision == SE_PREC_FP64 ? 0 : (ls->opts.precision == SE_PREC_MIXED ? 1 : 2);
   if (int rc = fdm_setup(ls, prec)) return rc;
-  cublasHandle_t h;
-  if (int rc = cublas_for(&h)) return rc;
-  CB(cublasSetStream(h, g_stream));
-  const size_t n = (size_t)ls->n;
-  std::memset(st, 0, sizeof(*st));
+  const int key = prec | ((remove_null != 0) << 2) | (ls->opts.norm_type << 3) | (ls->opts.mode << 6);
+  if (!ls->fdm_exec || ls->fdm_key != key)
+    if (int rc = fdm_build_graph(ls, prec, remove_null != 0)) return rc;
+  FdmParams p;
+  p.rtol = ls->opts.rtol;
+  p.atol = ls->opts.atol;
+  p.dtol = ls->opts.dtol;
+  p.max_it = ls->opts.max_it;
+  p.pad = 0;
   if (!ls->ev[0]) {
     CK(cudaEventCreate(&ls->ev[0]));
     CK(cudaEventCreate(&ls->ev[1]));
   }
+  std::memcpy(&ls->h_fparams, &p, sizeof(p));
+  CK(cudaMemcpyAsync(ls->d_fparams, &ls->h_fparams, sizeof(p), cudaMemcpyHostToDevice, g_stream));
   CK(cudaEventRecord(ls->ev[0], g_stream));
-  double rn0 = 0.0;
-  if (int rc = residual_norm(ls, ls->f, &rn0)) return rc;
-  st->rnorm0 = rn0;
-  const double ttol = std::max(ls->opts.rtol * rn0, ls->opts.atol);
-  CK(cudaMemsetAsync(ls->x, 0, sizeof(double) * n, g_stream));
-  double dp = rn0;
-  int its = 0, reason = 0;
-  if (!(dp == dp) || std::isinf(dp)) reason = -9;
-  else if (dp <= ttol) reason = dp < ls->opts.atol ? 3 : 2;
-  const double* rhs = ls->f;
-  // refinement stalls at the rounding floor of the true residual
-  // (~eps |A| |x|): three steps without halving it end the solve with
-  // SE_KSP_DIVERGED_BREAKDOWN
-  double best = dp;
-  int stalled = 0;
-  while (!reason) {
-    if (its >= ls->opts.max_it) {
-      reason = -3;
-      break;
-    }
-    // x += A^{-1} r  (r = f on the first step)
-    if (prec == 0) {
-      if (int rc = fdm_apply64(ls, h, rhs, ls->x, its > 0)) return rc;
-    } else {
-      if (int rc = fdm_apply_low(ls, h, rhs, ls->x)) return rc;
-    }
-    if (remove_null) CK(launch_remove_mean(ls->x, n, ls->fpart, kFdmPartials, ls->fpart + 2 * kFdmPartials + 4, g_stream));
-    its++;
-    // r = f - A x
-    CK(launch_op_apply(ls->op, ls->x, ls->ax, g_stream));
-    CK(launch_sub(ls->f, ls->ax, ls->r, n, g_stream));
-    rhs = ls->r;
-    if (int rc = residual_norm(ls, ls->r, &dp)) return rc;
-    if (!(dp == dp) || std::isinf(dp)) reason = -9;
-    else if (dp <= ttol) reason = dp < ls->opts.atol ? 3 : 2;
-    else if (dp >= ls->opts.dtol * rn0) reason = -4;
-    else if (dp > 0.5 * best) {
-      if (++stalled >= 3) reason = SE_KSP_DIVERGED_BREAKDOWN;
-    } else {
-      stalled = 0;
-    }
-    best = std::min(best, dp);
-  }
+  CK(cudaGraphLaunch(ls->fdm_exec, g_stream));
   CK(cudaEventRecord(ls->ev[1], g_stream));
-  CK(cudaEventSynchronize(ls->ev[1]));
+  FdmState s;
+  CK(cudaMemcpyAsync(&s, ls->d_fstate, sizeof(s), cudaMemcpyDeviceToHost, g_stream));
+  CK(cudaStreamSynchronize(g_stream));
   if (kernel_ms) CK(cudaEventElapsedTime(kernel_ms, ls->ev[0], ls->ev[1]));
-  st->its = its;
-  st->reason = reason;
-  st->dp = dp;
+  std::memset(st, 0, sizeof(*st));
+  st->its = s.its;
+  st->reason = s.reason;
+  st->dp = s.dp;
+  st->rnorm0 = s.rnorm0;
   return SE_OK;
 }
 }  // namespace
@@ -1327,15 +1404,20 @@ int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats)
   if (!ls->assembled)
     if (int rc = se_linsys_assemble(ls)) return rc;
   const MeshDev& m = ls->sol->mesh->dev;
-  CK(launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, g_stream));
   CgSolve st;
   float kms = 0.f;
-  int rc = ls->opts.method == SE_METHOD_FDM
-               ? run_fdm(ls, remove_null_space, &st, &kms)
-               : run_cg(ls, ls->f, ls->x, ls->opts.rtol, ls->opts.atol, ls->opts.dtol,
-                        ls->opts.max_it, remove_null_space, &st, &kms);
-  if (rc) return rc;
-  CK(launch_update_field(ls->op, m, ls->x, ls->sol->vals, g_stream));
+  int rc;
+  if (ls->opts.method == SE_METHOD_FDM) {
+    // right-hand side assembly and field update are inside the FDM graph
+    rc = run_fdm(ls, remove_null_space, &st, &kms);
+    if (rc) return rc;
+  } else {
+    CK(launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, g_stream));
+    rc = run_cg(ls, ls->f, ls->x, ls->opts.rtol, ls->opts.atol, ls->opts.dtol, ls->opts.max_it,
+                remove_null_space, &st, &kms);
+    if (rc) return rc;
+    CK(launch_update_field(ls->op, m, ls->x, ls->sol->vals, g_stream));
+  }
   if (stats) {
     stats->reason = st.reason;
     stats->its = st.its;

@@ -597,6 +597,70 @@ __global__ void __launch_bounds__(kCgThreads, 1) cg_n_kernel(const CgBatch B) {
     }
 }
 
+
+// ------------------------------------------- standalone apply / residual --
+// y = A x, or with b: r = b - A x together with per-block partial sums of
+// (w r)^2 (or r w r when natural) and r^2 (w = Jacobi inverse, nullptr: 1).
+template <int N>
+__global__ void __launch_bounds__(kCgThreads) apply_kernel(const OpDev op, const double* __restrict__ x,
+                                                           const double* __restrict__ b,
+                                                           double* __restrict__ y,
+                                                           const double* __restrict__ w,
+                                                           int natural, double* __restrict__ partial) {
+  extern __shared__ double P[];
+  __shared__ OpSm o;
+  __shared__ double red[kCgThreads / 32][4];
+  {
+    const int n = N + 1;
+    for (int k = threadIdx.x; k < n * n; k += kCgThreads) o.Kh[k] = op.Kh[k];
+    if (threadIdx.x < n) o.w[threadIdx.x] = op.w[threadIdx.x];
+    if (threadIdx.x == 0) {
+      o.alpha = op.alpha;
+      o.beta0 = op.beta[0];
+      o.beta1 = op.beta[1];
+      o.dx = op.d[0];
+      o.dy = op.d[1];
+      o.G0 = op.G[0];
+      o.G1 = op.G[1];
+    }
+    __syncthreads();
+  }
+  const int x0 = blockIdx.x * kCgTileX, y0 = blockIdx.y * kCgTileY;
+  stage_p<N>(o, x0, y0, x, nullptr, true, 0.0, P);
+  const int tx = threadIdx.x & (kCgTileX - 1), ty = threadIdx.x / kCgTileX;
+  const int ux = x0 + tx, uy = y0 + ty;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  if (ux < o.G0 && uy < o.G1) {
+    const size_t k = (size_t)uy * o.G0 + ux;
+    const double ax = apply_n<N>(o, P, tx, ty, ux + o.dx.lo, uy + o.dy.lo);
+    if (b) {
+      const double r = b[k] - ax;
+      y[k] = r;
+      const double z = w ? r * w[k] : r;
+      acc[0] = natural ? z * r : z * z;
+      acc[1] = r * r;
+    } else {
+      y[k] = ax;
+    }
+  }
+  if (partial) {
+    block_sum4(acc, red);
+    if (threadIdx.x == 0) {
+      partial[2 * (blockIdx.y * gridDim.x + blockIdx.x)] = acc[0];
+      partial[2 * (blockIdx.y * gridDim.x + blockIdx.x) + 1] = acc[1];
+    }
+  }
+}
+
+template <int N>
+cudaError_t launch_apply_n(const OpDev& op, const double* x, const double* b, double* y,
+                           const double* w, int natural, double* partial, cudaStream_t s) {
+  dim3 grid((op.G[0] + kCgTileX - 1) / kCgTileX, (op.G[1] + kCgTileY - 1) / kCgTileY);
+  const size_t smem = sizeof(double) * (size_t)Geo<N>::W * Geo<N>::H;
+  apply_kernel<N><<<grid, kCgThreads, smem, s>>>(op, x, b, y, w, natural, partial);
+  return cudaGetLastError();
+}
+
 template <int N, int K>
 const void* kernel_ptr() {
   return (const void*)cg_n_kernel<N, K>;
@@ -616,6 +680,30 @@ const void* pick(int N, int K) {
 }
 
 }  // namespace
+
+#define SE_APPLY_CASE(n) \
+  case n:                \
+    return launch_apply_n<n>(op, x, b, y, w, natural, partial, s);
+
+cudaError_t launch_residual(const OpDev& op, const double* x, const double* b, double* y,
+                            const double* w, int natural, double* partial, cudaStream_t s) {
+  switch (op.d[0].N) {
+    SE_APPLY_CASE(2) SE_APPLY_CASE(3) SE_APPLY_CASE(4) SE_APPLY_CASE(5) SE_APPLY_CASE(6)
+    SE_APPLY_CASE(7) SE_APPLY_CASE(8) SE_APPLY_CASE(9) SE_APPLY_CASE(10) SE_APPLY_CASE(11)
+    SE_APPLY_CASE(12)
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+#undef SE_APPLY_CASE
+
+cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, cudaStream_t s) {
+  return launch_residual(op, x, nullptr, y, nullptr, 0, nullptr, s);
+}
+
+int residual_blocks(const OpDev& op) {
+  return ((op.G[0] + kCgTileX - 1) / kCgTileX) * ((op.G[1] + kCgTileY - 1) / kCgTileY);
+}
 
 size_t cg_dyn_smem_bytes(int N, int nsolves) {
   return sizeof(SolveState) * nsolves + sizeof(SolveMeta) * nsolves + 16 +

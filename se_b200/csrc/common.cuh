@@ -99,6 +99,11 @@ cudaError_t launch_max_speed_sq(int nv, const double* vel, double* scratch, int 
 
 // Linear-system pieces.
 cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, cudaStream_t s);
+// r = b - A x with per-block partial sums (partial[2*block]: (w r)^2 or, when
+// natural, r w r; and r^2) over residual_blocks(op) blocks (cg.cu).
+cudaError_t launch_residual(const OpDev& op, const double* x, const double* b, double* r,
+                            const double* w, int natural, double* partial, cudaStream_t s);
+int residual_blocks(const OpDev& op);
 cudaError_t launch_op_diag(const OpDev& op, double* d, cudaStream_t s);
 // f = Mass*rhs over the unknowns (FieldRHS + Vector::Assemble), plus lift.
 cudaError_t launch_rhs_assemble(const OpDev& op, const MeshDev& m, const double* rhs_vals,
@@ -159,18 +164,41 @@ int cg_max_grid(int device, int N, bool resident, int nsolves);
 // to own at most kCgResidentTiles tiles.
 cudaError_t launch_cg(const CgBatch& batch, int grid, int N, bool resident, cudaStream_t s);
 
+// Device-resident parameters and state of an FDM refinement loop.
+struct FdmParams {
+  double rtol, atol, dtol;
+  int max_it, pad;
+};
+struct FdmState {
+  double rnorm0, ttol, dp, best;
+  int its, reason, stalled, pad;
+};
+// Set up the loop from res = {norm^2 of f, .}: rnorm0, tolerance, the
+// iteration-0 test; sets the while-condition (1 = iterate).
+cudaError_t launch_fdm_init(const FdmParams* p, FdmState* st, const double* res,
+                            cudaGraphConditionalHandle h, cudaStream_t s);
+// After a refinement step: iteration count, the residual tests (RTOL, ATOL,
+// DTOL, NANORINF, ITS, and stagnation at the rounding floor) and the
+// while-condition.
+cudaError_t launch_fdm_check(const FdmParams* p, FdmState* st, const double* res,
+                             cudaGraphConditionalHandle h, cudaStream_t s);
+
 // Fast-diagonalization pieces (fdm.cu). prec: 0 FP64, 1 FP32, 2 BF16.
 cudaError_t launch_spectral_divide(int prec, void* v, int gx, int gy, const double* lx,
                                    const double* ly, double alpha, double bx, double by,
                                    double null_tol, cudaStream_t s);
-cudaError_t launch_to_low(int prec, const double* x, void* y, size_t n, double scale,
+// y = x / max (max read from device memory; 0 leaves y = 0).
+cudaError_t launch_to_low(int prec, const double* x, void* y, size_t n, const double* max,
                           cudaStream_t s);
-cudaError_t launch_add_low(int prec, double* x, const void* y, size_t n, double inv_scale,
+// x += y * max.
+cudaError_t launch_add_low(int prec, double* x, const void* y, size_t n, const double* max,
                            cudaStream_t s);
 // out2 = {sum (w r)^2 or, natural != 0, sum r w r; sum r^2} (w == nullptr:
 // w = 1), deterministic.
 cudaError_t launch_norms(const double* r, const double* w, size_t n, int natural, double* partial,
                          int npart, double* out2, cudaStream_t s);
+// Sum np pairs of partials into out2 (deterministic order).
+cudaError_t launch_norm_final(const double* partial, int np, double* out2, cudaStream_t s);
 cudaError_t launch_maxabs(const double* x, size_t n, double* partial, int npart, double* out,
                           cudaStream_t s);
 cudaError_t launch_sub(const double* b, const double* y, double* r, size_t n, cudaStream_t s);

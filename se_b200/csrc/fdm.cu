@@ -40,21 +40,68 @@ __global__ void spectral_divide_kernel(T* __restrict__ v, int gx, int gy,
   v[k] = (T)(fabs(d) <= null_tol ? 0.0 : val / d);
 }
 
+// y = x / max|x| in low precision (max from device memory).
 template <class T>
 __global__ void to_low_kernel(const double* __restrict__ x, T* __restrict__ y, size_t n,
-                              double scale) {
+                              const double* __restrict__ mx) {
+  const double m = *mx;
+  const double scale = m > 0.0 ? 1.0 / m : 0.0;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
        k += (size_t)gridDim.x * blockDim.x)
     y[k] = (T)(x[k] * scale);
 }
 
-// x += y / scale (y in low precision); optionally also d = y / scale.
+// x += y * max (undoing the scale of to_low).
 template <class T>
 __global__ void add_low_kernel(double* __restrict__ x, const T* __restrict__ y, size_t n,
-                               double inv_scale) {
+                               const double* __restrict__ mx) {
+  const double m = *mx;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
        k += (size_t)gridDim.x * blockDim.x)
-    x[k] += (double)y[k] * inv_scale;
+    x[k] += (double)y[k] * m;
+}
+
+// ------------------------------------------------- refinement loop control --
+__global__ void fdm_init_kernel(const FdmParams* __restrict__ p, FdmState* __restrict__ st,
+                                const double* __restrict__ res, cudaGraphConditionalHandle h) {
+  const double dp = sqrt(fabs(res[0]));
+  st->rnorm0 = dp;
+  st->ttol = fmax(p->rtol * dp, p->atol);
+  st->dp = dp;
+  st->best = dp;
+  st->its = 0;
+  st->stalled = 0;
+  int reason = 0;
+  if (!(dp == dp) || isinf(dp)) reason = -9;
+  else if (dp <= st->ttol) reason = dp < p->atol ? 3 : 2;
+  else if (p->max_it <= 0) reason = -3;
+  st->reason = reason;
+  cudaGraphSetConditional(h, reason == 0 ? 1u : 0u);
+}
+
+__global__ void fdm_check_kernel(const FdmParams* __restrict__ p, FdmState* __restrict__ st,
+                                 const double* __restrict__ res, cudaGraphConditionalHandle h) {
+  const double dp = sqrt(fabs(res[0]));
+  const int its = st->its + 1;
+  st->its = its;
+  st->dp = dp;
+  int reason = 0;
+  if (!(dp == dp) || isinf(dp)) reason = -9;
+  else if (dp <= st->ttol) reason = dp < p->atol ? 3 : 2;
+  else if (dp >= p->dtol * st->rnorm0) reason = -4;
+  else {
+    // three steps without a 10% gain on the best residual: stalled (the
+    // rounding floor, or a low precision too coarse for this operator)
+    if (dp > 0.9 * st->best) {
+      if (++st->stalled >= 3) reason = -5;
+    } else {
+      st->stalled = 0;
+    }
+    if (!reason && its >= p->max_it) reason = -3;
+  }
+  st->best = fmin(st->best, dp);
+  st->reason = reason;
+  cudaGraphSetConditional(h, reason == 0 ? 1u : 0u);
 }
 
 // Fixed-order block reduction of one sum (256 threads); result in thread 0.
@@ -190,22 +237,33 @@ cudaError_t launch_spectral_divide(int prec, void* v, int gx, int gy, const doub
   return cudaGetLastError();
 }
 
-cudaError_t launch_to_low(int prec, const double* x, void* y, size_t n, double scale,
+cudaError_t launch_to_low(int prec, const double* x, void* y, size_t n, const double* mx,
                           cudaStream_t s) {
   if (prec == 1)
-    to_low_kernel<float><<<blocks_for(n), 256, 0, s>>>(x, (float*)y, n, scale);
+    to_low_kernel<float><<<blocks_for(n), 256, 0, s>>>(x, (float*)y, n, mx);
   else
-    to_low_kernel<__nv_bfloat16><<<blocks_for(n), 256, 0, s>>>(x, (__nv_bfloat16*)y, n, scale);
+    to_low_kernel<__nv_bfloat16><<<blocks_for(n), 256, 0, s>>>(x, (__nv_bfloat16*)y, n, mx);
   return cudaGetLastError();
 }
 
-cudaError_t launch_add_low(int prec, double* x, const void* y, size_t n, double inv_scale,
+cudaError_t launch_add_low(int prec, double* x, const void* y, size_t n, const double* mx,
                            cudaStream_t s) {
   if (prec == 1)
-    add_low_kernel<float><<<blocks_for(n), 256, 0, s>>>(x, (const float*)y, n, inv_scale);
+    add_low_kernel<float><<<blocks_for(n), 256, 0, s>>>(x, (const float*)y, n, mx);
   else
-    add_low_kernel<__nv_bfloat16><<<blocks_for(n), 256, 0, s>>>(x, (const __nv_bfloat16*)y, n,
-                                                                inv_scale);
+    add_low_kernel<__nv_bfloat16><<<blocks_for(n), 256, 0, s>>>(x, (const __nv_bfloat16*)y, n, mx);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fdm_init(const FdmParams* p, FdmState* st, const double* res,
+                            cudaGraphConditionalHandle h, cudaStream_t s) {
+  fdm_init_kernel<<<1, 1, 0, s>>>(p, st, res, h);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fdm_check(const FdmParams* p, FdmState* st, const double* res,
+                             cudaGraphConditionalHandle h, cudaStream_t s) {
+  fdm_check_kernel<<<1, 1, 0, s>>>(p, st, res, h);
   return cudaGetLastError();
 }
 
@@ -220,6 +278,11 @@ cudaError_t launch_norms(const double* r, const double* w, size_t n, int natural
 
 cudaError_t launch_invert(double* x, size_t n, cudaStream_t s) {
   invert_kernel<<<blocks_for(n), 256, 0, s>>>(x, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_norm_final(const double* partial, int np, double* out2, cudaStream_t s) {
+  norm_final_kernel<<<1, 256, 0, s>>>(partial, np, out2);
   return cudaGetLastError();
 }
 

@@ -163,19 +163,6 @@ __device__ __forceinline__ double apply_tile(const OpDev& op, int gx, int gy, co
   return op.alpha * wx * wy * c[0] + op.beta[0] * wy * kx + op.beta[1] * wx * ky;
 }
 
-__global__ void __launch_bounds__(kCgThreads) op_apply_tile_kernel(const OpDev op,
-                                                                    const double* __restrict__ x,
-                                                                    double* __restrict__ y) {
-  extern __shared__ double smem[];
-  const int x0 = blockIdx.x * kCgTileX, y0 = blockIdx.y * kCgTileY;
-  const int G0 = op.G[0];
-  load_tile(op, x0, y0, smem, [&](int a, int b) { return __ldg(x + (size_t)b * G0 + a); });
-  const int tx = threadIdx.x % kCgTileX, ty = threadIdx.x / kCgTileX;
-  const int ux = x0 + tx, uy = y0 + ty;
-  if (ux >= op.G[0] || uy >= op.G[1]) return;
-  y[(size_t)uy * G0 + ux] = apply_tile(op, ux + op.d[0].lo, uy + op.d[1].lo, smem, tx, ty);
-}
-
 __global__ void op_diag_kernel(const OpDev op, double* __restrict__ d) {
   const int ux = blockIdx.x * blockDim.x + threadIdx.x;
   const int uy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -270,11 +257,6 @@ size_t cg_smem_bytes(int maxN) {
   return sizeof(double) * (size_t)(kCgTileX + 2 * maxN) * (kCgTileY + 2 * maxN);
 }
 
-cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, cudaStream_t s) {
-  dim3 grid((op.G[0] + kCgTileX - 1) / kCgTileX, (op.G[1] + kCgTileY - 1) / kCgTileY);
-  op_apply_tile_kernel<<<grid, kCgThreads, cg_smem_bytes(op.d[0].N), s>>>(op, x, y);
-  return cudaGetLastError();
-}
 cudaError_t launch_op_diag(const OpDev& op, double* d, cudaStream_t s) {
   dim3 block(32, 8), grid((op.G[0] + 31) / 32, (op.G[1] + 7) / 8);
   op_diag_kernel<<<grid, block, 0, s>>>(op, d);
