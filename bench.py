@@ -167,7 +167,11 @@ def run_gpu(args, rank, world):
     results, ref_u = {}, None
     clock = None
     with torch.cuda.stream(stream):
-        for name, (meth, prec) in VARIANTS.items():
+        chosen = [v for v in args.variants.split(",") if v in VARIANTS] or [HEADLINE]
+        if HEADLINE not in chosen:
+            chosen = [HEADLINE] + chosen
+        for name in chosen:
+            meth, prec = VARIANTS[name]
             opts = S.solver_opts(rtol=RTOL, mode=S.MODE_EXACT, method=getattr(S, meth),
                                  precision=getattr(S, prec), max_it=10000)
             helm = S.HelmholtzEqn(u, adv.fieldSL, -LAMBDA, -1.0, 1.0, 0, opts)
@@ -293,9 +297,9 @@ GPU_LAUNCHES_PER_STEP = 1 + 1 + 2 * 5 + 2 + 1
 # contraction (2 flops per node and component) each.
 SL_BYTES_PER_VERTEX = 32.0
 SL_FLOPS_PER_VERTEX = (2 * 9 * 5 + 2 * 81 * 2 + 2 * 9 * 2) + (2 * 9 * 5 + 2 * 81 + 2 * 9)
-# Traffic of one SL launch (dram read + write bytes), from the ncu capture
-# summarised in profiles/sl_first_kernel_64x64_p8.md; None until captured.
-SL_TRAFFIC_BYTES = None
+# DRAM traffic of one SL launch (dram__bytes_read.sum + dram__bytes_write.sum)
+# from the ncu capture summarised in profiles/sl_first_kernel_64x64_p8.md.
+SL_TRAFFIC_BYTES = 6.358016e6
 
 
 def roofline(r):
@@ -369,6 +373,8 @@ def main():
     ap.add_argument("--impl", default="segpu", choices=["segpu", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=1, help="steps in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variants", default=",".join(VARIANTS),
+                    help="comma-separated solver variants to time (the first timed is the headline)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -203,6 +203,17 @@ int se_linsys_assemble(se_linsys* ls);
  * copied into sol's unknowns and periodic copies. stats may be NULL.
  * Returns SE_ERR_NOT_CONVERGED if the reason is negative. */
 int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats);
+/* Several solves in one call (the batched ensemble; no counterpart in the
+ * reference, which solves one system at a time through the same Solve).
+ * Systems using SE_METHOD_CG and the same polynomial order run as one
+ * persistent cooperative launch (up to 256 per launch) whose launch shape is
+ * chosen by a built-in autotuner on the first batch of a given signature;
+ * SE_METHOD_FDM systems run their solve graphs overlapped on a pool of 8
+ * streams. stats (nullable) gets one entry per system; the return value is
+ * SE_ERR_NOT_CONVERGED if any system diverged. The caller's stream is ordered
+ * after all solves. */
+int se_linsys_solve_batch(se_linsys** systems, int n, int remove_null_space,
+                          se_solve_stats* stats);
 /* y = A x on vector unknowns (device pointers, vec_size entries each). */
 int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev);
 /* The Jacobi diagonal of A (device pointer, vec_size entries). */

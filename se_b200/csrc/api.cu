@@ -11,7 +11,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -23,7 +25,7 @@ using namespace seg;
 // ------------------------------------------------------------- errors -----
 namespace {
 thread_local std::string g_err;
-cudaStream_t g_stream = nullptr;
+thread_local cudaStream_t g_stream = nullptr;  // the calling thread's stream
 std::mutex g_scratch_mu;
 double* g_scratch = nullptr;  // reductions: partials + results
 constexpr int kScratch = 8192;
@@ -260,8 +262,9 @@ struct se_linsys {
   // fast diagonalization (built on the first FDM solve)
   bool fdm_ready;
   int fdm_prec;
-  double *Sx, *Sy, *lx, *ly;  // eigenvectors (column-major, W-orthonormal), eigenvalues
-  void *Sx_lo, *Sy_lo;        // low-precision copies of Sx, Sy
+  double *Sx, *Sy, *lx, *ly;  // eigenvectors (column-major, W-orthonormal), eigenvalues (cached, shared)
+  void *Sx_lo, *Sy_lo;        // low-precision copies of Sx, Sy (cached, shared)
+  int fdm_lbuf_prec;          // precision the L1..L3 buffers were sized for
   double *X1, *X2, *ax;       // FP64 work: two transform buffers, A x
   void *L1, *L2, *L3;         // low-precision work
   double* fpart;              // reduction partials [2*fpart_n] + results [16]
@@ -272,7 +275,8 @@ struct se_linsys {
   void* cublas_ws;
   FdmParams* d_fparams;
   FdmState* d_fstate;
-  FdmParams h_fparams;  // staging copy for the asynchronous upload
+  FdmParams* h_fparams;  // pinned host copies for asynchronous transfers
+  FdmState* h_fstate;
 };
 
 namespace {
@@ -402,12 +406,6 @@ void linsys_free(se_linsys* ls) {
   dfree(ls->d_bar);
   dfree(ls->d_active);
   dfree(ls->d_err);
-  dfree(ls->Sx);
-  dfree(ls->Sy);
-  dfree(ls->lx);
-  dfree(ls->ly);
-  if (ls->Sx_lo) cudaFree(ls->Sx_lo);
-  if (ls->Sy_lo) cudaFree(ls->Sy_lo);
   dfree(ls->X1);
   dfree(ls->X2);
   dfree(ls->ax);
@@ -419,6 +417,7 @@ void linsys_free(se_linsys* ls) {
   if (ls->cublas_ws) cudaFree(ls->cublas_ws);
   dfree(ls->d_fparams);
   dfree(ls->d_fstate);
+  if (ls->h_fparams) cudaFreeHost(ls->h_fparams);
   if (ls->ev[0]) cudaEventDestroy(ls->ev[0]);
   if (ls->ev[1]) cudaEventDestroy(ls->ev[1]);
   delete ls->own_bcs;
@@ -638,15 +637,71 @@ int upload_low(const std::vector<double>& S, int prec, void** out) {
   return SE_OK;
 }
 
+// Process-wide cache of 1-D generalised eigendecompositions, per device.
+// The 1-D assembled operators depend only on the element count, the order
+// and the boundary ends of a direction (not on h, the coefficients or the
+// Laplacian scaling), so every system with the same direction shares one
+// setup; entries live until the process exits.
+struct Eig1D {
+  int n = 0;
+  double* S = nullptr;    // W-orthonormal eigenvectors, column-major n x n
+  double* lam = nullptr;  // eigenvalues
+  double lmax = 0.0;
+  void* low[3] = {nullptr, nullptr, nullptr};  // [1] FP32, [2] BF16 copies of S
+};
+typedef std::tuple<int, int, int, int, int, int> EigKey;
+std::mutex g_eig_mu;
+std::map<EigKey, Eig1D*> g_eig[64];
+
+int eig_get(const Dir& d, const double* Kh, const double* w, int prec, Eig1D** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(SE_ERR_UNSUPPORTED, "device index %d", dev);
+  std::lock_guard<std::mutex> lk(g_eig_mu);
+  const EigKey key(d.nE, d.N, d.periodic, d.lo, d.hi, d.nV);
+  Eig1D*& e = g_eig[dev][key];
+  std::vector<double> Sh;
+  if (!e) {
+    Eig1D* ne = new Eig1D();
+    ne->n = d.hi - d.lo;
+    if (int rc = eig_1d(d, Kh, w, &ne->S, &ne->lam, Sh)) {
+      delete ne;
+      g_eig[dev].erase(key);
+      return rc;
+    }
+    std::vector<double> lam(ne->n);
+    CK(cudaMemcpy(lam.data(), ne->lam, sizeof(double) * ne->n, cudaMemcpyDeviceToHost));
+    for (double v : lam) ne->lmax = std::max(ne->lmax, std::fabs(v));
+    e = ne;
+  }
+  if (prec != 0 && !e->low[prec]) {
+    if (Sh.empty()) {
+      Sh.resize((size_t)e->n * e->n);
+      CK(cudaMemcpy(Sh.data(), e->S, sizeof(double) * Sh.size(), cudaMemcpyDeviceToHost));
+    }
+    if (int rc = upload_low(Sh, prec, &e->low[prec])) return rc;
+  }
+  *out = e;
+  return SE_OK;
+}
+
 int fdm_setup(se_linsys* ls, int prec) {
   if (ls->fdm_ready && ls->fdm_prec == prec) return SE_OK;
   const OpDev& op = ls->op;
   const size_t n = (size_t)ls->n;
   int rc;
-  if (!ls->Sx) {
-    std::vector<double> Sxh, Syh;
-    if ((rc = eig_1d(op.d[0], op.Kh, op.w, &ls->Sx, &ls->lx, Sxh))) return rc;
-    if ((rc = eig_1d(op.d[1], op.Kh, op.w, &ls->Sy, &ls->ly, Syh))) return rc;
+  Eig1D *ex = nullptr, *ey = nullptr;
+  if ((rc = eig_get(op.d[0], op.Kh, op.w, prec, &ex)) || (rc = eig_get(op.d[1], op.Kh, op.w, prec, &ey)))
+    return rc;
+  ls->Sx = ex->S;
+  ls->Sy = ey->S;
+  ls->lx = ex->lam;
+  ls->ly = ey->lam;
+  ls->lmax[0] = ex->lmax;
+  ls->lmax[1] = ey->lmax;
+  ls->Sx_lo = prec ? ex->low[prec] : nullptr;
+  ls->Sy_lo = prec ? ey->low[prec] : nullptr;
+  if (!ls->X1) {
     ls->fpart_n = std::max(kFdmPartials, residual_blocks(op));
     if ((rc = dalloc(&ls->X1, n)) || (rc = dalloc(&ls->X2, n)) || (rc = dalloc(&ls->ax, n)) ||
         (rc = dalloc(&ls->fpart, 2 * (size_t)ls->fpart_n + 16)))
@@ -654,30 +709,8 @@ int fdm_setup(se_linsys* ls, int prec) {
     // Jacobi inverse for the preconditioned residual norm
     CK(launch_op_diag(op, ls->dinv, g_stream));
     CK(launch_invert(ls->dinv, n, g_stream));
-    // spectral range for the null-mode tolerance
-    std::vector<double> lx(op.G[0]), ly(op.G[1]);
-    CK(cudaMemcpy(lx.data(), ls->lx, sizeof(double) * lx.size(), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(ly.data(), ls->ly, sizeof(double) * ly.size(), cudaMemcpyDeviceToHost));
-    ls->lmax[0] = ls->lmax[1] = 0.0;
-    for (double v : lx) ls->lmax[0] = std::max(ls->lmax[0], std::fabs(v));
-    for (double v : ly) ls->lmax[1] = std::max(ls->lmax[1], std::fabs(v));
-    if (prec != 0) {
-      if ((rc = upload_low(Sxh, prec, &ls->Sx_lo)) || (rc = upload_low(Syh, prec, &ls->Sy_lo)))
-        return rc;
-    }
-    ls->fdm_prec = prec;
-  } else if (prec != 0 && (!ls->Sx_lo || ls->fdm_prec != prec)) {
-    // re-derive the low-precision copies from the FP64 eigenvectors
-    std::vector<double> Sxh((size_t)op.G[0] * op.G[0]), Syh((size_t)op.G[1] * op.G[1]);
-    CK(cudaMemcpy(Sxh.data(), ls->Sx, sizeof(double) * Sxh.size(), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(Syh.data(), ls->Sy, sizeof(double) * Syh.size(), cudaMemcpyDeviceToHost));
-    if (ls->Sx_lo) cudaFree(ls->Sx_lo);
-    if (ls->Sy_lo) cudaFree(ls->Sy_lo);
-    ls->Sx_lo = ls->Sy_lo = nullptr;
-    if ((rc = upload_low(Sxh, prec, &ls->Sx_lo)) || (rc = upload_low(Syh, prec, &ls->Sy_lo))) return rc;
-    ls->fdm_prec = prec;
   }
-  if (prec != 0) {
+  if (prec != 0 && ls->fdm_lbuf_prec != prec) {
     const size_t es = prec == 1 ? sizeof(float) : sizeof(uint16_t);
     if (ls->L1) cudaFree(ls->L1);
     if (ls->L2) cudaFree(ls->L2);
@@ -689,7 +722,9 @@ int fdm_setup(se_linsys* ls, int prec) {
     ls->L1 = l1;
     ls->L2 = l2;
     ls->L3 = l3;
+    ls->fdm_lbuf_prec = prec;
   }
+  ls->fdm_prec = prec;
   ls->fdm_ready = true;
   return SE_OK;
 }
@@ -866,39 +901,199 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
   return rc;
 }
 
-// Solve A x = f by fast diagonalization with FP64 iterative refinement until
-// the chosen residual norm is <= max(rtol |f|, atol) in that norm; the right
-// hand side assembly and the field update are part of the graph.
-int run_fdm(se_linsys* ls, int remove_null, CgSolve* st, float* kernel_ms) {
+// Queue the FDM solve of A x = f (fast diagonalization with FP64 iterative
+// refinement until the chosen residual norm is <= max(rtol |f|, atol)) on the
+// calling thread's stream: parameter upload, the solve graph (right-hand side
+// assembly through the field update) and the state read-back into pinned
+// memory. fdm_finish reads the state once the stream is done.
+int fdm_launch(se_linsys* ls, int remove_null) {
   const int prec = ls->opts.precision == SE_PREC_FP64 ? 0 : (ls->opts.precision == SE_PREC_MIXED ? 1 : 2);
   if (int rc = fdm_setup(ls, prec)) return rc;
   const int key = prec | ((remove_null != 0) << 2) | (ls->opts.norm_type << 3) | (ls->opts.mode << 6);
   if (!ls->fdm_exec || ls->fdm_key != key)
     if (int rc = fdm_build_graph(ls, prec, remove_null != 0)) return rc;
-  FdmParams p;
+  if (!ls->h_fparams) {
+    void* p = nullptr;
+    CK(cudaMallocHost(&p, sizeof(FdmParams) + sizeof(FdmState)));
+    ls->h_fparams = static_cast<FdmParams*>(p);
+    ls->h_fstate = reinterpret_cast<FdmState*>(ls->h_fparams + 1);
+  }
+  if (!ls->ev[0]) {
+    CK(cudaEventCreate(&ls->ev[0]));
+    CK(cudaEventCreate(&ls->ev[1]));
+  }
+  FdmParams& p = *ls->h_fparams;
   p.rtol = ls->opts.rtol;
   p.atol = ls->opts.atol;
   p.dtol = ls->opts.dtol;
   p.max_it = ls->opts.max_it;
   p.pad = 0;
-  if (!ls->ev[0]) {
-    CK(cudaEventCreate(&ls->ev[0]));
-    CK(cudaEventCreate(&ls->ev[1]));
-  }
-  std::memcpy(&ls->h_fparams, &p, sizeof(p));
-  CK(cudaMemcpyAsync(ls->d_fparams, &ls->h_fparams, sizeof(p), cudaMemcpyHostToDevice, g_stream));
+  CK(cudaMemcpyAsync(ls->d_fparams, ls->h_fparams, sizeof(FdmParams), cudaMemcpyHostToDevice, g_stream));
   CK(cudaEventRecord(ls->ev[0], g_stream));
   CK(cudaGraphLaunch(ls->fdm_exec, g_stream));
   CK(cudaEventRecord(ls->ev[1], g_stream));
-  FdmState s;
-  CK(cudaMemcpyAsync(&s, ls->d_fstate, sizeof(s), cudaMemcpyDeviceToHost, g_stream));
-  CK(cudaStreamSynchronize(g_stream));
+  CK(cudaMemcpyAsync(ls->h_fstate, ls->d_fstate, sizeof(FdmState), cudaMemcpyDeviceToHost, g_stream));
+  return SE_OK;
+}
+int fdm_finish(se_linsys* ls, CgSolve* st, float* kernel_ms) {
+  CK(cudaEventSynchronize(ls->ev[1]));
   if (kernel_ms) CK(cudaEventElapsedTime(kernel_ms, ls->ev[0], ls->ev[1]));
   std::memset(st, 0, sizeof(*st));
-  st->its = s.its;
-  st->reason = s.reason;
-  st->dp = s.dp;
-  st->rnorm0 = s.rnorm0;
+  st->its = ls->h_fstate->its;
+  st->reason = ls->h_fstate->reason;
+  st->dp = ls->h_fstate->dp;
+  st->rnorm0 = ls->h_fstate->rnorm0;
+  return SE_OK;
+}
+int run_fdm(se_linsys* ls, int remove_null, CgSolve* st, float* kernel_ms) {
+  if (int rc = fdm_launch(ls, remove_null)) return rc;
+  CK(cudaStreamSynchronize(g_stream));
+  return fdm_finish(ls, st, kernel_ms);
+}
+
+// ---------------------------------------------------------- batched CG ----
+// Workspace of batched CG launches (grow-only, per device).
+struct BatchWs {
+  CgSolve* solves = nullptr;
+  CgTile* tiles = nullptr;
+  int* begin = nullptr;
+  double* partials = nullptr;
+  unsigned* words = nullptr;  // barrier, error
+  size_t cap_solves = 0, cap_tiles = 0, cap_begin = 0, cap_part = 0;
+  std::vector<CgSolve> h_solves;
+};
+std::mutex g_batch_mu;
+BatchWs g_batch[64];
+
+template <class T>
+int grow(T** p, size_t* cap, size_t need) {
+  if (*cap >= need) return SE_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  size_t n = std::max(need, (size_t)(*cap * 2));
+  if (int rc = dalloc(p, n)) return rc;
+  *cap = n;
+  return SE_OK;
+}
+
+// Launch-shape autotuner for batched CG: for a batch signature (order,
+// number of solves, tile count rounded up to a power of two) it times short
+// capped runs (30 iterations) of each candidate -- the register-resident
+// mode when it fits, and the streaming mode at 1, 2 and 4 blocks per SM --
+// and keeps the fastest. Decisions are cached for the process.
+struct TuneChoice {
+  bool resident;
+  int grid;
+};
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, TuneChoice> g_tune;
+
+int run_cg_batch_once(int dev, std::vector<se_linsys*>& sys, const std::vector<const OpDev*>& ops,
+                      int N, bool resident, int grid, int max_it_cap, int remove_null, float* ms) {
+  BatchWs& W = g_batch[dev];
+  Schedule S = make_schedule(ops, grid);
+  const int g = (int)S.block_begin.size() - 1;
+  const size_t ns = sys.size();
+  int rc;
+  if ((rc = grow(&W.solves, &W.cap_solves, ns)) || (rc = grow(&W.tiles, &W.cap_tiles, S.tiles.size())) ||
+      (rc = grow(&W.begin, &W.cap_begin, S.block_begin.size())) ||
+      (rc = grow(&W.partials, &W.cap_part, (size_t)S.nseg * 8)))
+    return rc;
+  if (!W.words && (rc = dalloc(&W.words, 64))) return rc;
+  W.h_solves.resize(ns);
+  for (size_t i = 0; i < ns; i++) {
+    se_linsys* ls = sys[i];
+    CgSolve& cs = W.h_solves[i];
+    cs = make_solve(ls, ls->f, ls->x, ls->opts.rtol, ls->opts.atol, ls->opts.dtol,
+                    max_it_cap > 0 ? std::min(max_it_cap, ls->opts.max_it) : ls->opts.max_it, remove_null);
+    cs.seg_begin = S.seg_begin[i];
+    cs.seg_end = S.seg_end[i];
+  }
+  cudaStream_t s = g_stream;
+  CK(cudaMemcpyAsync(W.solves, W.h_solves.data(), sizeof(CgSolve) * ns, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(W.tiles, S.tiles.data(), sizeof(CgTile) * S.tiles.size(), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(W.begin, S.block_begin.data(), sizeof(int) * S.block_begin.size(), cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(W.words, 0, 64 * sizeof(unsigned), s));
+  CgBatch B;
+  B.solves = W.solves;
+  B.nsolves = (int)ns;
+  B.tiles = W.tiles;
+  B.block_tile_begin = W.begin;
+  B.partials = W.partials;
+  B.nseg = S.nseg;
+  B.bar_count = W.words;
+  B.bar_gen = W.words + 32;
+  B.n_active = reinterpret_cast<int*>(W.words + 40);
+  B.err = W.words + 48;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, s));
+  cudaError_t le = launch_cg(B, g, N, resident, s);
+  CK(cudaEventRecord(e1, s));
+  CK(cudaMemcpyAsync(W.h_solves.data(), W.solves, sizeof(CgSolve) * ns, cudaMemcpyDeviceToHost, s));
+  unsigned err = 0;
+  CK(cudaMemcpyAsync(&err, B.err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (ms) cudaEventElapsedTime(ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (le != cudaSuccess) return cuda_fail(le, "batched CG launch");
+  if (err & KERR_BARRIER_TIMEOUT) return fail(SE_ERR_TIMEOUT, "CG grid barrier timed out");
+  return SE_OK;
+}
+
+int solve_cg_group(std::vector<se_linsys*>& sys, int remove_null, std::vector<CgSolve>& out, float* ms) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(g_batch_mu);
+  const int N = sys[0]->op.d[0].N;
+  std::vector<const OpDev*> ops;
+  long ntiles = 0;
+  for (se_linsys* ls : sys) {
+    ops.push_back(&ls->op);
+    ntiles += cg_tiles(ls->op);
+  }
+  int bucket = 1;
+  while (bucket < ntiles) bucket <<= 1;
+  const auto key = std::make_tuple(dev, N, (int)sys.size(), bucket);
+  TuneChoice choice{false, 0};
+  bool have = false;
+  {
+    std::lock_guard<std::mutex> tl(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      choice = it->second;
+      have = true;
+    }
+  }
+  if (!have) {
+    int sms = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    std::vector<TuneChoice> cands;
+    const int maxr = cg_max_grid(dev, N, true, (int)sys.size());
+    if (maxr > 0 && ntiles <= (long)maxr * kCgResidentTiles)
+      cands.push_back({true, (int)std::min<long>(maxr, ntiles)});
+    const int maxs = cg_max_grid(dev, N, false, (int)sys.size());
+    for (int per : {1, 2, 4})
+      if (maxs > 0 && sms * per <= maxs) cands.push_back({false, (int)std::min<long>(sms * per, ntiles)});
+    if (cands.empty()) return fail(SE_ERR_CUDA, "no co-resident launch shape for the batched CG");
+    float best = 1e30f;
+    for (const TuneChoice& c : cands) {
+      float t = 0.f;
+      if (int rc = run_cg_batch_once(dev, sys, ops, N, c.resident, c.grid, 30, remove_null, &t)) return rc;
+      if (t < best) {
+        best = t;
+        choice = c;
+      }
+    }
+    std::lock_guard<std::mutex> tl(g_tune_mu);
+    g_tune[key] = choice;
+  }
+  if (int rc = run_cg_batch_once(dev, sys, ops, N, choice.resident, choice.grid, 0, remove_null, ms))
+    return rc;
+  out.assign(g_batch[dev].h_solves.begin(), g_batch[dev].h_solves.begin() + sys.size());
   return SE_OK;
 }
 }  // namespace
@@ -1428,6 +1623,93 @@ int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats)
   }
   if (st.reason < 0) return fail(SE_ERR_NOT_CONVERGED, "KSP diverged, reason %d after %d its",
                                  st.reason, st.its);
+  return SE_OK;
+}
+int se_linsys_solve_batch(se_linsys** systems, int n, int remove_null_space, se_solve_stats* stats) {
+  if (!systems || n < 0) return fail(SE_ERR_ARG, "bad argument");
+  for (int i = 0; i < n; i++)
+    if (!systems[i]) return fail(SE_ERR_ARG, "null system %d", i);
+  for (int i = 0; i < n; i++)
+    if (!systems[i]->assembled)
+      if (int rc = se_linsys_assemble(systems[i])) return rc;
+  std::vector<CgSolve> st(n);
+  std::vector<float> kms(n, 0.f);
+  // fast-diagonalization solves: graphs overlapped over a pool of streams
+  static thread_local std::vector<cudaStream_t> pool;
+  if (pool.empty()) {
+    for (int k = 0; k < 8; k++) {
+      cudaStream_t s;
+      CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      pool.push_back(s);
+    }
+  }
+  const cudaStream_t saved = g_stream;
+  cudaEvent_t ready;
+  CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  CK(cudaEventRecord(ready, saved));
+  std::vector<int> fdm_idx;
+  std::map<int, std::vector<int>> cg_groups;
+  for (int i = 0; i < n; i++) {
+    if (systems[i]->opts.method == SE_METHOD_FDM) fdm_idx.push_back(i);
+    else cg_groups[systems[i]->op.d[0].N].push_back(i);
+  }
+  int rc = SE_OK;
+  for (size_t k = 0; k < fdm_idx.size() && !rc; k++) {
+    g_stream = pool[k % pool.size()];
+    if (k < pool.size()) cudaStreamWaitEvent(g_stream, ready, 0);
+    rc = fdm_launch(systems[fdm_idx[k]], remove_null_space);
+  }
+  g_stream = saved;
+  for (auto& grp : cg_groups) {
+    if (rc) break;
+    std::vector<int>& idx = grp.second;
+    for (size_t off = 0; off < idx.size() && !rc; off += 256) {
+      std::vector<se_linsys*> sys;
+      for (size_t j = off; j < std::min(idx.size(), off + 256); j++) {
+        se_linsys* ls = systems[idx[j]];
+        const MeshDev& m = ls->sol->mesh->dev;
+        CK(launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, g_stream));
+        sys.push_back(ls);
+      }
+      std::vector<CgSolve> out;
+      float t = 0.f;
+      rc = solve_cg_group(sys, remove_null_space, out, &t);
+      for (size_t j = 0; j < sys.size() && !rc; j++) {
+        st[idx[off + j]] = out[j];
+        kms[idx[off + j]] = t;
+        const MeshDev& m = sys[j]->sol->mesh->dev;
+        if (launch_update_field(sys[j]->op, m, sys[j]->x, sys[j]->sol->vals, g_stream) != cudaSuccess)
+          rc = fail(SE_ERR_CUDA, "field update");
+      }
+    }
+  }
+  for (size_t k = 0; k < fdm_idx.size() && !rc; k++)
+    rc = fdm_finish(systems[fdm_idx[k]], &st[fdm_idx[k]], &kms[fdm_idx[k]]);
+  // the caller's stream sees every solve's result
+  for (size_t k = 0; k < pool.size() && k < fdm_idx.size(); k++) {
+    cudaEvent_t done;
+    if (cudaEventCreateWithFlags(&done, cudaEventDisableTiming) == cudaSuccess) {
+      cudaEventRecord(done, pool[k]);
+      cudaStreamWaitEvent(saved, done, 0);
+      cudaEventDestroy(done);
+    }
+  }
+  cudaEventDestroy(ready);
+  if (rc) return rc;
+  int worst = SE_OK;
+  for (int i = 0; i < n; i++) {
+    if (stats) {
+      se_solve_stats& o = stats[i];
+      o.reason = st[i].reason;
+      o.its = st[i].its;
+      o.outer_its = systems[i]->opts.method == SE_METHOD_FDM ? st[i].its : 0;
+      o.rnorm = st[i].dp;
+      o.rnorm0 = st[i].rnorm0;
+      o.kernel_ms = kms[i];
+    }
+    if (st[i].reason < 0) worst = SE_ERR_NOT_CONVERGED;
+  }
+  if (worst) return fail(worst, "at least one system did not converge");
   return SE_OK;
 }
 int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev) {

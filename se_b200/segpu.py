@@ -108,6 +108,8 @@ SIGNATURES = {
     "se_linsys_destroy": [_vp], "se_linsys_set_opts": [_vp, ctypes.POINTER(SolverOpts)],
     "se_linsys_assemble": [_vp],
     "se_linsys_solve": [_vp, ctypes.c_int, ctypes.POINTER(SolveStats)],
+    "se_linsys_solve_batch": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
+                              ctypes.POINTER(SolveStats)],
     "se_linsys_apply": [_vp, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
     "se_linsys_vec_size": [_vp, _I],
     "se_calc_time_step": [_vp, ctypes.c_double, _D],
@@ -452,6 +454,22 @@ class PoissonEqn(_LinSys):
             _check(_lib.se_solver_opts_parse(ctypes.byref(o), b"poisson_", options.encode()))
             self.set_opts(o)
         return self._solve(removeNullSpace, raise_on_diverge)
+
+
+def solve_batch(systems, removeNullSpace: bool = False, raise_on_diverge: bool = False):
+    """Solve several HelmholtzEqn/PoissonEqn systems in one call
+    (se_linsys_solve_batch); returns one stats dict per system."""
+    n = len(systems)
+    arr = (_vp * n)(*[s._h for s in systems])
+    st = (SolveStats * n)()
+    rc = load_library().se_linsys_solve_batch(arr, n, int(bool(removeNullSpace)), st)
+    if rc == SE_ERR_NOT_CONVERGED and not raise_on_diverge:
+        rc = SE_OK
+    _check(rc)
+    out = [s.as_dict() for s in st]
+    for sys_, o in zip(systems, out):
+        sys_.stats = o
+    return out
 
 
 def CalcTimeStep(velocity: Field, courantNo: float) -> float:
