@@ -214,6 +214,14 @@ int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats)
  * after all solves. */
 int se_linsys_solve_batch(se_linsys** systems, int n, int remove_null_space,
                           se_solve_stats* stats);
+/* Queue a solve on the calling thread's stream without waiting (no
+ * counterpart in the reference; for callers that overlap solves with other
+ * work, such as the serving loop). SE_METHOD_FDM solves are fully
+ * asynchronous; SE_METHOD_CG solves run to completion inside this call.
+ * Exactly one se_linsys_solve_finish must follow: it waits for the solve,
+ * fills stats (nullable) and returns what se_linsys_solve would have. */
+int se_linsys_solve_async(se_linsys* ls, int remove_null_space);
+int se_linsys_solve_finish(se_linsys* ls, se_solve_stats* stats);
 /* y = A x on vector unknowns (device pointers, vec_size entries each). */
 int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev);
 /* The Jacobi diagonal of A (device pointer, vec_size entries). */
@@ -242,6 +250,51 @@ int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double min[2],
                                double c, double nu, double dt, int poisson,
                                const se_solver_opts* opts, int remove_null_space,
                                const double* rhs_dev, double* sol_dev, se_solve_stats* stats);
+
+/* ---------------------------------------------------------------- serving --
+ * A continuous-batching request server (no counterpart in the reference,
+ * which runs one model in one process). A worker thread admits queued
+ * requests in arrival order into free execution slots (one CUDA stream each)
+ * whenever the device-memory budget allows their resources, queues each
+ * request's device work without waiting, and completes requests as their
+ * streams finish, so requests that arrive while others run overlap on the
+ * device. Resources are cached per configuration and reused; least recently
+ * used idle ones are released when a new configuration needs the memory.
+ * Results do not depend on what else runs: the kernels are deterministic. */
+#define SE_REQ_HELMHOLTZ 0 /* one HelmholtzEqn/PoissonEqn solve */
+#define SE_REQ_ADVECT 1    /* steps of first-order SL advection of a tracer */
+typedef struct {
+  int kind;                 /* SE_REQ_* */
+  int nEls[2];              /* mesh, as se_mesh_create */
+  int N;
+  double min[2], max[2];
+  int periodic[2];
+  int bcs[4];               /* Helmholtz: Dirichlet bottom, top, left, right */
+  double c, nu, dt;         /* Helmholtz: A = c*Mass + nu*dt*Laplacian */
+  int poisson;              /* Helmholtz: nonzero for A = c*Laplacian */
+  se_solver_opts opts;      /* Helmholtz: solver options */
+  int steps;                /* advection: number of steps */
+  double sl_dt;             /* advection: time step */
+  const double* in;         /* host [nVertsTotal]: right-hand side field / tracer */
+  const double* aux;        /* host: solution field with its Dirichlet values [nVertsTotal]
+                               (NULL: zeros) / velocity [nVertsTotal][2] */
+  double* out;              /* host [nVertsTotal]: solution / advected tracer */
+} se_request;                /* host buffers must stay valid until se_server_wait returns */
+typedef struct {
+  int status;               /* SE_OK or SE_ERR_* */
+  int reason, its;          /* Helmholtz: solver reason and iterations */
+  double queued_ms;         /* submission to admission */
+  double latency_ms;        /* submission to result in out */
+} se_result;
+typedef struct se_server se_server;
+/* slots: concurrent requests (1..64); device_gib: memory budget for cached
+ * request resources. Work runs on the device current at creation. */
+int se_server_create(int slots, double device_gib, se_server** out);
+int se_server_submit(se_server* srv, const se_request* req, long long* ticket);
+/* Wait for a request; res (nullable) gets its status and timings. */
+int se_server_wait(se_server* srv, long long ticket, se_result* res);
+/* Finish queued work, then release everything. */
+int se_server_destroy(se_server* srv);
 
 /* ------------------------------------------------------------ utilities -- */
 /* CalcTimeStep(velocity, courantNo) (src/base/Utils.cpp:23-40). */

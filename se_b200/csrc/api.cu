@@ -277,6 +277,9 @@ struct se_linsys {
   FdmState* d_fstate;
   FdmParams* h_fparams;  // pinned host copies for asynchronous transfers
   FdmState* h_fstate;
+  int async_pending;       // 1: FDM solve queued; 2: synchronous result held
+  int async_rc;
+  se_solve_stats async_stats;
 };
 
 namespace {
@@ -1710,6 +1713,43 @@ int se_linsys_solve_batch(se_linsys** systems, int n, int remove_null_space, se_
     if (st[i].reason < 0) worst = SE_ERR_NOT_CONVERGED;
   }
   if (worst) return fail(worst, "at least one system did not converge");
+  return SE_OK;
+}
+int se_linsys_solve_async(se_linsys* ls, int remove_null_space) {
+  if (!ls) return fail(SE_ERR_ARG, "null system");
+  if (!ls->assembled)
+    if (int rc = se_linsys_assemble(ls)) return rc;
+  if (ls->opts.method != SE_METHOD_FDM) {
+    // the CG path reads its state back on the host: solve now, keep the stats
+    ls->async_rc = se_linsys_solve(ls, remove_null_space, &ls->async_stats);
+    ls->async_pending = 2;
+    return ls->async_rc == SE_ERR_NOT_CONVERGED ? SE_OK : ls->async_rc;
+  }
+  if (int rc = fdm_launch(ls, remove_null_space)) return rc;
+  ls->async_pending = 1;
+  return SE_OK;
+}
+int se_linsys_solve_finish(se_linsys* ls, se_solve_stats* stats) {
+  if (!ls || !ls->async_pending) return fail(SE_ERR_ARG, "no solve queued");
+  if (ls->async_pending == 2) {
+    ls->async_pending = 0;
+    if (stats) *stats = ls->async_stats;
+    return ls->async_rc;
+  }
+  ls->async_pending = 0;
+  CgSolve st;
+  float kms = 0.f;
+  if (int rc = fdm_finish(ls, &st, &kms)) return rc;
+  if (stats) {
+    stats->reason = st.reason;
+    stats->its = st.its;
+    stats->outer_its = st.its;
+    stats->rnorm = st.dp;
+    stats->rnorm0 = st.rnorm0;
+    stats->kernel_ms = kms;
+  }
+  if (st.reason < 0) return fail(SE_ERR_NOT_CONVERGED, "KSP diverged, reason %d after %d its",
+                                 st.reason, st.its);
   return SE_OK;
 }
 int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev) {

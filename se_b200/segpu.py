@@ -74,6 +74,23 @@ class SolveStats(ctypes.Structure):
                 "rnorm": self.rnorm, "rnorm0": self.rnorm0, "kernel_ms": self.kernel_ms}
 
 
+class Request(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("nEls", ctypes.c_int * 2), ("N", ctypes.c_int),
+                ("min", ctypes.c_double * 2), ("max", ctypes.c_double * 2),
+                ("periodic", ctypes.c_int * 2), ("bcs", ctypes.c_int * 4),
+                ("c", ctypes.c_double), ("nu", ctypes.c_double), ("dt", ctypes.c_double),
+                ("poisson", ctypes.c_int), ("opts", SolverOpts), ("steps", ctypes.c_int),
+                ("sl_dt", ctypes.c_double), ("in_", ctypes.c_void_p), ("aux", ctypes.c_void_p),
+                ("out", ctypes.c_void_p)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("reason", ctypes.c_int), ("its", ctypes.c_int),
+                ("queued_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
+
+
+REQ_HELMHOLTZ, REQ_ADVECT = 0, 1
+
 _lib = None
 _vp = ctypes.c_void_p
 _D = ctypes.POINTER(ctypes.c_double)
@@ -110,10 +127,16 @@ SIGNATURES = {
     "se_linsys_solve": [_vp, ctypes.c_int, ctypes.POINTER(SolveStats)],
     "se_linsys_solve_batch": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
                               ctypes.POINTER(SolveStats)],
+    "se_linsys_solve_async": [_vp, ctypes.c_int],
+    "se_linsys_solve_finish": [_vp, ctypes.POINTER(SolveStats)],
     "se_linsys_apply": [_vp, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
     "se_linsys_vec_size": [_vp, _I],
     "se_calc_time_step": [_vp, ctypes.c_double, _D],
     "se_field_error": [_vp, _vp, ctypes.c_int, ctypes.c_int, _D],
+    "se_server_create": [ctypes.c_int, ctypes.c_double, ctypes.POINTER(_vp)],
+    "se_server_submit": [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)],
+    "se_server_wait": [_vp, ctypes.c_longlong, ctypes.POINTER(Result)],
+    "se_server_destroy": [_vp],
     "se_helmholtz_solve_noalloc": [_I, ctypes.c_int, _D, _D, _I, _I, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.POINTER(SolverOpts), ctypes.c_int, _vp, _vp,
@@ -470,6 +493,63 @@ def solve_batch(systems, removeNullSpace: bool = False, raise_on_diverge: bool =
     for sys_, o in zip(systems, out):
         sys_.stats = o
     return out
+
+
+class Server:
+    """The continuous-batching request server (se_server_*). Arrays passed to
+    submit() are kept alive until wait() returns their result."""
+
+    def __init__(self, slots: int = 8, device_gib: float = 16.0):
+        h = _vp()
+        rc = load_library().se_server_create(int(slots), float(device_gib), ctypes.byref(h))
+        if rc:
+            raise SEError(rc, "se_server_create failed")
+        self._h = h
+        self._keep = {}
+
+    def submit(self, kind, nEls, N, lo, hi, periodic, field_in, aux=None, bcs=(0, 0, 0, 0),
+               c=-1.0, nu=-1.0, dt=1.0, poisson=False, opts=None, steps=0, sl_dt=0.0):
+        fin = np.ascontiguousarray(field_in, dtype=np.float64)
+        fa = None if aux is None else np.ascontiguousarray(aux, dtype=np.float64)
+        out = np.empty(len(fin))
+        r = Request()
+        r.kind = kind
+        r.nEls[:] = [int(nEls[0]), int(nEls[1])]
+        r.N = int(N)
+        r.min[:] = [float(lo[0]), float(lo[1])]
+        r.max[:] = [float(hi[0]), float(hi[1])]
+        r.periodic[:] = [int(bool(periodic[0])), int(bool(periodic[1]))]
+        r.bcs[:] = [int(bool(b)) for b in bcs]
+        r.c, r.nu, r.dt, r.poisson = float(c), float(nu), float(dt), int(bool(poisson))
+        r.opts = opts if opts is not None else solver_opts(rtol=1e-10, mode=MODE_EXACT,
+                                                           method=METHOD_FDM)
+        r.steps, r.sl_dt = int(steps), float(sl_dt)
+        r.in_ = fin.ctypes.data
+        r.aux = None if fa is None else fa.ctypes.data
+        r.out = out.ctypes.data
+        t = ctypes.c_longlong()
+        rc = _lib.se_server_submit(self._h, ctypes.byref(r), ctypes.byref(t))
+        if rc:
+            raise SEError(rc, "se_server_submit failed")
+        self._keep[t.value] = (fin, fa, out, r)
+        return t.value
+
+    def wait(self, ticket):
+        res = Result()
+        rc = _lib.se_server_wait(self._h, ctypes.c_longlong(ticket), ctypes.byref(res))
+        if rc:
+            raise SEError(rc, "se_server_wait failed")
+        fin, fa, out, r = self._keep.pop(ticket)
+        return out, {"status": res.status, "reason": res.reason, "its": res.its,
+                     "queued_ms": res.queued_ms, "latency_ms": res.latency_ms}
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.se_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
 
 
 def CalcTimeStep(velocity: Field, courantNo: float) -> float:
