@@ -330,6 +330,192 @@ def read_peaks():
         return 6650.0, "fallback"
 
 
+
+# ------------------------------------------------------ ensemble (config 3) --
+def run_ensemble(count=256, seed=2024):
+    """256 independent Helmholtz solves, mesh n x n elements with n uniform in
+    8..64, p in {4, 6, 8}, lambda log-uniform in [1e-2, 1e2], RHS a seeded sum
+    of 8 Fourier modes; doubly periodic unit square; rtol 1e-10. Timed with
+    the batch call (FDM: graphs overlapped on 8 streams; CG: one persistent
+    launch per order, autotuned)."""
+    import torch
+    import se_b200 as S
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(count):
+        specs.append((int(rng.integers(8, 65)), int(rng.choice([4, 6, 8])),
+                      float(10 ** rng.uniform(-2, 2)), int(rng.integers(0, 2 ** 31))))
+    out = {"workload": "256 solves, n x n elements n~U{8..64}, p~U{4,6,8}, lambda~logU[1e-2,1e2], "
+                       "8-mode RHS, rtol 1e-10"}
+    for name, method in (("fdm_fp64", S.METHOD_FDM), ("cg_fp64", S.METHOD_CG)):
+        systems = []
+        for ne, p, lam, sd in specs:
+            m = S.Mesh("m", [ne, ne], "legendre", p, [0, 0], [1, 1], [True, True])
+            X = m.verts
+            r2 = np.random.default_rng(sd)
+            f = np.zeros(len(X))
+            for _ in range(8):
+                kx, ky = r2.integers(1, 7, size=2)
+                a, b = r2.standard_normal(2)
+                ph = 2 * np.pi * (kx * X[:, 0] + ky * X[:, 1])
+                f += a * np.cos(ph) + b * np.sin(ph)
+            bc = S.BCs(False, False, False, False, m)
+            u, rr = S.Field("u", m, 1, bc), S.Field("f", m, 1, bc)
+            rr.vals = f
+            ls = S.HelmholtzEqn(u, rr, -lam, -1.0, 1.0, 0,
+                                S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=method))
+            systems.append((m, bc, u, rr, ls))
+        lss = [s[4] for s in systems]
+        ng = sum(ls.vecSize for ls in lss)
+        S.solve_batch(lss)  # setup: eigen cache, graphs, autotuned launch shape
+        times = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st = S.solve_batch(lss)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        t = float(np.median(times))
+        its = [s["its"] for s in st]
+        out[name] = {"dofs": ng, "ms": 1e3 * t, "dof_per_s": ng / t,
+                     "its_median": float(np.median(its)), "its_max": int(max(its)),
+                     "all_converged": all(s["reason"] > 0 for s in st)}
+        del systems, lss
+    return out
+
+
+# ------------------------------------------------------- serving (config 4) --
+def run_serving(rate=2000.0, seconds=2.0, seed=77):
+    """Poisson arrivals (mean `rate` req/s) for `seconds`, half Helmholtz
+    solves (lambda = 1, rtol 1e-10, FDM) and half 10-step first-order SL
+    jobs (Taylor-Green velocity, Courant 1), on n x n element doubly periodic
+    meshes with n in {8, 16, 32, 64, 128} (the powers of two of 8..128) and p
+    uniform in 4..8. Every configuration is warmed once before the stream.
+    Reports completed-request throughput, DOF-updates/s (Helmholtz: unknowns;
+    SL: vertices x steps) and p50/p99 latency from submission to result,
+    for FP64 solves and for TF32 solves refined in FP64."""
+    import se_b200 as S
+    rng = np.random.default_rng(seed)
+    sizes, orders = [8, 16, 32, 64, 128], [4, 5, 6, 7, 8]
+    inputs = {}
+
+    def inp(kind, n, p):
+        key = (kind, n, p)
+        if key not in inputs:
+            m = S.Mesh("m", [n, n], "legendre", p, [0, 0], [1, 1], [True, True])
+            X = m.verts
+            x, y = X[:, 0], X[:, 1]
+            if kind == S.REQ_HELMHOLTZ:
+                f = np.sin(2 * np.pi * x) * np.cos(4 * np.pi * y) + np.exp(-((x - .3) ** 2 + (y - .6) ** 2) / .02)
+                inputs[key] = (f, None, 0.0, n * p * n * p)
+            else:
+                vel = np.stack([-np.sin(np.pi * x) ** 2 * np.sin(2 * np.pi * y),
+                                np.sin(np.pi * y) ** 2 * np.sin(2 * np.pi * x)], 1)
+                phi = np.exp(-((x - .4) ** 2 + (y - .6) ** 2) / .05 ** 2)
+                dt = 1.0 * (1.0 / n) / np.sqrt((vel ** 2).sum(1).max())
+                inputs[key] = (phi, vel, dt, len(X) * 10)
+        return inputs[key]
+
+    import torch
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        return t  # keep the tensor alive; .numpy() shares its page-locked memory
+
+    keep = []
+
+    def inp_pinned(kind, n, p):
+        f, aux, dt, d = inp(kind, n, p)
+        key = ("pinned", kind, n, p)
+        if key not in inputs:
+            tf = pinned(f)
+            ta = None if aux is None else pinned(aux)
+            keep.extend([tf, ta])
+            inputs[key] = (tf.numpy(), None if ta is None else ta.numpy())
+        return inputs[key][0], inputs[key][1], dt, d
+
+    n_req = int(rate * seconds)
+    gaps = rng.exponential(1.0 / rate, size=n_req)
+    kinds = rng.integers(0, 2, size=n_req)
+    ns = rng.choice(sizes, size=n_req)
+    ps = rng.choice(orders, size=n_req)
+    out = {"workload": f"Poisson arrivals {rate:.0f} req/s for {seconds:.1f} s, Helmholtz (FDM, "
+                       "rtol 1e-10) and 10-step SL jobs, n x n elements n in {8,16,32,64,128}, "
+                       "p in 4..8", "requests": n_req}
+    for label, prec in (("fp64", S.PREC_FP64), ("tf32_refined_fp64", S.PREC_MIXED)):
+        opts = S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=S.METHOD_FDM, precision=prec)
+        srv = S.Server(slots=16, device_gib=60.0)
+        keys = sorted({(int(k), int(n), int(p)) for k, n, p in zip(kinds, ns, ps)})
+        warm = []
+        for k, n, p in keys:
+            f, aux, dt, _ = inp(k, n, p)
+            warm.append(srv.submit(k, (n, n), p, (0, 0), (1, 1), (1, 1), f, aux, opts=opts,
+                                   c=-1.0, nu=-1.0, dt=1.0, steps=10, sl_dt=dt))
+        for t in warm:
+            srv.wait(t)
+        # Page-locked result buffers per configuration, recycled by a
+        # collector thread that waits for results in submission order (as a
+        # client of the server would); the pool is primed before timing.
+        import queue
+        import threading
+        pool = {key: [] for key in keys}
+        pool_mu = threading.Lock()
+        for k, n, p in keys:
+            nv = (n * p + 1) ** 2
+            for _ in range(4):
+                pool[(k, n, p)].append(torch.empty(nv, dtype=torch.float64, pin_memory=True))
+        for k, n, p in keys:
+            inp_pinned(k, n, p)
+        pending = queue.Queue()
+        lat, fails = [], {}
+
+        def collect():
+            while True:
+                item = pending.get()
+                if item is None:
+                    return
+                t, key, buf = item
+                _, res = srv.wait(t)
+                lat.append(res["latency_ms"])
+                if res["status"] != 0 or res["reason"] < 0:
+                    tag = (f"status={res['status']} reason={res['reason']}: {res['error']}")
+                    fails[tag] = fails.get(tag, 0) + 1
+                with pool_mu:
+                    pool[key].append(buf)
+
+        th = threading.Thread(target=collect)
+        th.start()
+        dofs, grown = 0, 0
+        t_start = time.perf_counter()
+        due = t_start
+        for g, k, n, p in zip(gaps, kinds, ns, ps):
+            due += g
+            while time.perf_counter() < due:
+                pass
+            key = (int(k), int(n), int(p))
+            f, aux, dt, d = inp_pinned(*key)
+            with pool_mu:
+                buf = pool[key].pop() if pool[key] else None
+            if buf is None:
+                buf = torch.empty(len(f), dtype=torch.float64, pin_memory=True)
+                grown += 1
+            t = srv.submit(key[0], (key[1], key[1]), key[2], (0, 0), (1, 1), (1, 1), f, aux,
+                           opts=opts, c=-1.0, nu=-1.0, dt=1.0, steps=10, sl_dt=dt,
+                           out=buf.numpy())
+            pending.put((t, key, buf))
+            dofs += d
+        pending.put(None)
+        th.join()
+        wall = time.perf_counter() - t_start
+        bad = sum(fails.values())
+        srv.close()
+        out[label] = {"req_per_s": n_req / wall, "dof_updates_per_s": dofs / wall,
+                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                      "failed": int(bad), "failures": fails, "pinned_buffers_grown": grown}
+    return out
+
+
 # ------------------------------------------------------------- CPU arm ----
 def cpu_sample(steps: int, nthreads: int, cg_cap: int = 0, full_its: int = 0):
     """Time `steps` SL+Helmholtz steps of the workload with the CPU oracle.
@@ -373,6 +559,8 @@ def main():
     ap.add_argument("--impl", default="segpu", choices=["segpu", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=1, help="steps in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the ensemble (256-solve batch) and serving measurements")
     ap.add_argument("--variants", default=",".join(VARIANTS),
                     help="comma-separated solver variants to time (the first timed is the headline)")
     args = ap.parse_args()
@@ -419,6 +607,12 @@ def main():
     if rank != 0:
         return
     log("GPU arm done")
+    extras = {}
+    if not args.no_extras:
+        log("ensemble")
+        extras["ensemble"] = run_ensemble()
+        log("serving")
+        extras["serving"] = run_serving()
     cpu = None
     if not args.no_cpu_baseline:
         per_step, ng, its = cpu_sample(args.cpu_steps, nthreads)
@@ -443,6 +637,7 @@ def main():
         "gpu_launches": GPU_LAUNCHES_PER_STEP * args.steps,
         "clocks": r["clocks"],
         "variants": variants,
+        **extras,
     }), flush=True)
 
 

@@ -279,12 +279,15 @@ typedef struct {
   const double* aux;        /* host: solution field with its Dirichlet values [nVertsTotal]
                                (NULL: zeros) / velocity [nVertsTotal][2] */
   double* out;              /* host [nVertsTotal]: solution / advected tracer */
-} se_request;                /* host buffers must stay valid until se_server_wait returns */
+} se_request;                /* host buffers must stay valid until se_server_wait returns;
+                               page-locked ones (cudaMallocHost / cudaHostRegister) are
+                               copied directly, others through the server's staging */
 typedef struct {
   int status;               /* SE_OK or SE_ERR_* */
   int reason, its;          /* Helmholtz: solver reason and iterations */
   double queued_ms;         /* submission to admission */
   double latency_ms;        /* submission to result in out */
+  char error[160];          /* status != SE_OK: the failing call's message */
 } se_result;
 typedef struct se_server se_server;
 /* slots: concurrent requests (1..64); device_gib: memory budget for cached

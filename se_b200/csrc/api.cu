@@ -1,6 +1,5 @@
 // Host side of the segpu C-ABI (include/segpu.h): object lifetimes, the
 // mesh/GLL/boundary tables, device memory and kernel launches.
-#include <cublas_v2.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cusolverDn.h>
@@ -29,7 +28,6 @@ thread_local cudaStream_t g_stream = nullptr;  // the calling thread's stream
 std::mutex g_scratch_mu;
 double* g_scratch = nullptr;  // reductions: partials + results
 constexpr int kScratch = 8192;
-unsigned* g_err_word = nullptr;  // device error bits of SL kernels
 
 int fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -55,8 +53,6 @@ int ensure_globals() {
   cudaError_t e = cudaGetDeviceCount(&n);
   if (e != cudaSuccess || n == 0) return fail(SE_ERR_CUDA, "no CUDA device available");
   CK(cudaMalloc(&g_scratch, sizeof(double) * (kScratch + 8)));
-  CK(cudaMalloc(&g_err_word, sizeof(unsigned)));
-  CK(cudaMemset(g_err_word, 0, sizeof(unsigned)));
   return SE_OK;
 }
 
@@ -236,6 +232,7 @@ struct se_advector {
   se_field* sl;
   int* dep_el;
   double* dep_xy;
+  unsigned* err;  // device error bits of this advector's SL kernels
   bool record;
 };
 struct se_linsys {
@@ -262,17 +259,18 @@ struct se_linsys {
   // fast diagonalization (built on the first FDM solve)
   bool fdm_ready;
   int fdm_prec;
-  double *Sx, *Sy, *lx, *ly;  // eigenvectors (column-major, W-orthonormal), eigenvalues (cached, shared)
-  void *Sx_lo, *Sy_lo;        // low-precision copies of Sx, Sy (cached, shared)
-  int fdm_lbuf_prec;          // precision the L1..L3 buffers were sized for
+  // eigenvectors E per direction (W-orthonormal; cached, shared): S = row-major
+  // E^T, ST = row-major E; eigenvalues lx, ly
+  double *Sx, *Sy, *SxT, *SyT, *lx, *ly;
+  void *Sx_lo, *Sy_lo, *SxT_lo, *SyT_lo;  // low-precision copies (cached, shared)
+  int fdm_lbuf_prec;          // precision the L2, L3 buffers were sized for
   double *X1, *X2, *ax;       // FP64 work: two transform buffers, A x
-  void *L1, *L2, *L3;         // low-precision work
+  void *L1, *L2, *L3;         // low-precision work (L1 unused)
   double* fpart;              // reduction partials [2*fpart_n] + results [16]
   int fpart_n;
   double lmax[2];  // largest 1-D eigenvalue magnitude per direction
   cudaGraphExec_t fdm_exec;  // the captured FDM solve
   int fdm_key;
-  void* cublas_ws;
   FdmParams* d_fparams;
   FdmState* d_fstate;
   FdmParams* h_fparams;  // pinned host copies for asynchronous transfers
@@ -417,7 +415,6 @@ void linsys_free(se_linsys* ls) {
   if (ls->L3) cudaFree(ls->L3);
   dfree(ls->fpart);
   if (ls->fdm_exec) cudaGraphExecDestroy(ls->fdm_exec);
-  if (ls->cublas_ws) cudaFree(ls->cublas_ws);
   dfree(ls->d_fparams);
   dfree(ls->d_fstate);
   if (ls->h_fparams) cudaFreeHost(ls->h_fparams);
@@ -527,20 +524,6 @@ int check_field(const se_field* f) {
 // ------------------------------------------------- fast diagonalization ----
 namespace {
 constexpr int kFdmPartials = 1184;
-cublasHandle_t g_cublas[64];
-
-int cublas_for(cublasHandle_t* out) {
-  int dev = 0;
-  CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) return fail(SE_ERR_UNSUPPORTED, "device index %d", dev);
-  if (!g_cublas[dev]) {
-    if (cublasCreate(&g_cublas[dev]) != CUBLAS_STATUS_SUCCESS)
-      return fail(SE_ERR_CUDA, "cublasCreate failed");
-  }
-  *out = g_cublas[dev];
-  return SE_OK;
-}
-
 // 1-D assembled stiffness (dense, n x n) and weights on one direction's
 // unknowns: element rows of Kh and w added at the vertices they map to
 // (periodic end folded onto the start, Dirichlet vertices dropped).
@@ -575,8 +558,8 @@ uint16_t to_bf16(float f) {
 // Generalised eigenvectors S (S^T K S = diag(lam), S^T W S = I) of one
 // direction, on the device: eigenvectors of W^-1/2 K W^-1/2 by cuSOLVER
 // syevd (setup only), then scaled by W^-1/2.
-int eig_1d(const Dir& d, const double* Kh, const double* w, double** S_dev, double** lam_dev,
-           std::vector<double>& S_host) {
+int eig_1d(const Dir& d, const double* Kh, const double* w, double** S_dev, double** ST_dev,
+           double** lam_dev, std::vector<double>& S_host) {
   std::vector<double> K, W;
   assemble_1d(d, Kh, w, K, W);
   const int n = d.hi - d.lo;
@@ -615,7 +598,18 @@ int eig_1d(const Dir& d, const double* Kh, const double* w, double** S_dev, doub
     for (int i = 0; i < n; i++) A[(size_t)j * n + i] /= std::sqrt(W[i]);
   S_host = A;
   CK(cudaMemcpy(dA, A.data(), sizeof(double) * A.size(), cudaMemcpyHostToDevice));
+  std::vector<double> T((size_t)n * n);
+  for (int j = 0; j < n; j++)
+    for (int i = 0; i < n; i++) T[(size_t)i * n + j] = A[(size_t)j * n + i];
+  double* dT = nullptr;
+  if (int rc2 = dalloc(&dT, (size_t)n * n)) {
+    dfree(dA);
+    dfree(dlam);
+    return rc2;
+  }
+  CK(cudaMemcpy(dT, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice));
   *S_dev = dA;
+  *ST_dev = dT;
   *lam_dev = dlam;
   return SE_OK;
 }
@@ -647,10 +641,12 @@ int upload_low(const std::vector<double>& S, int prec, void** out) {
 // setup; entries live until the process exits.
 struct Eig1D {
   int n = 0;
-  double* S = nullptr;    // W-orthonormal eigenvectors, column-major n x n
+  double* S = nullptr;    // W-orthonormal eigenvectors E, column-major (= row-major E^T)
+  double* ST = nullptr;   // row-major E
   double* lam = nullptr;  // eigenvalues
   double lmax = 0.0;
-  void* low[3] = {nullptr, nullptr, nullptr};  // [1] FP32, [2] BF16 copies of S
+  void* low[3] = {nullptr, nullptr, nullptr};   // [1] FP32, [2] BF16 copies of S
+  void* lowT[3] = {nullptr, nullptr, nullptr};  // and of ST
 };
 typedef std::tuple<int, int, int, int, int, int> EigKey;
 std::mutex g_eig_mu;
@@ -667,7 +663,7 @@ int eig_get(const Dir& d, const double* Kh, const double* w, int prec, Eig1D** o
   if (!e) {
     Eig1D* ne = new Eig1D();
     ne->n = d.hi - d.lo;
-    if (int rc = eig_1d(d, Kh, w, &ne->S, &ne->lam, Sh)) {
+    if (int rc = eig_1d(d, Kh, w, &ne->S, &ne->ST, &ne->lam, Sh)) {
       delete ne;
       g_eig[dev].erase(key);
       return rc;
@@ -683,6 +679,11 @@ int eig_get(const Dir& d, const double* Kh, const double* w, int prec, Eig1D** o
       CK(cudaMemcpy(Sh.data(), e->S, sizeof(double) * Sh.size(), cudaMemcpyDeviceToHost));
     }
     if (int rc = upload_low(Sh, prec, &e->low[prec])) return rc;
+    const int n = e->n;
+    std::vector<double> T((size_t)n * n);
+    for (int j = 0; j < n; j++)
+      for (int i = 0; i < n; i++) T[(size_t)i * n + j] = Sh[(size_t)j * n + i];
+    if (int rc = upload_low(T, prec, &e->lowT[prec])) return rc;
   }
   *out = e;
   return SE_OK;
@@ -698,12 +699,16 @@ int fdm_setup(se_linsys* ls, int prec) {
     return rc;
   ls->Sx = ex->S;
   ls->Sy = ey->S;
+  ls->SxT = ex->ST;
+  ls->SyT = ey->ST;
   ls->lx = ex->lam;
   ls->ly = ey->lam;
   ls->lmax[0] = ex->lmax;
   ls->lmax[1] = ey->lmax;
   ls->Sx_lo = prec ? ex->low[prec] : nullptr;
   ls->Sy_lo = prec ? ey->low[prec] : nullptr;
+  ls->SxT_lo = prec ? ex->lowT[prec] : nullptr;
+  ls->SyT_lo = prec ? ey->lowT[prec] : nullptr;
   if (!ls->X1) {
     ls->fpart_n = std::max(kFdmPartials, residual_blocks(op));
     if ((rc = dalloc(&ls->X1, n)) || (rc = dalloc(&ls->X2, n)) || (rc = dalloc(&ls->ax, n)) ||
@@ -719,10 +724,8 @@ int fdm_setup(se_linsys* ls, int prec) {
     if (ls->L2) cudaFree(ls->L2);
     if (ls->L3) cudaFree(ls->L3);
     ls->L1 = ls->L2 = ls->L3 = nullptr;
-    char *l1 = nullptr, *l2 = nullptr, *l3 = nullptr;
-    if ((rc = dalloc(&l1, n * es)) || (rc = dalloc(&l2, n * es)) || (rc = dalloc(&l3, n * es)))
-      return rc;
-    ls->L1 = l1;
+    char *l2 = nullptr, *l3 = nullptr;
+    if ((rc = dalloc(&l2, n * es)) || (rc = dalloc(&l3, n * es))) return rc;
     ls->L2 = l2;
     ls->L3 = l3;
     ls->fdm_lbuf_prec = prec;
@@ -732,12 +735,6 @@ int fdm_setup(se_linsys* ls, int prec) {
   return SE_OK;
 }
 
-#define CB(call)                                                              \
-  do {                                                                        \
-    cublasStatus_t s_ = (call);                                               \
-    if (s_ != CUBLAS_STATUS_SUCCESS) return fail(SE_ERR_CUDA, "%s: cublas status %d", #call, (int)s_); \
-  } while (0)
-
 // Spectral entries below this magnitude are a null mode (constant null space
 // of a periodic Poisson operator) and are zeroed.
 double null_tol(const se_linsys* ls) {
@@ -745,50 +742,47 @@ double null_tol(const se_linsys* ls) {
   return 1e-12 * (std::fabs(op.alpha) + std::fabs(op.beta[0]) * ls->lmax[0] +
                   std::fabs(op.beta[1]) * ls->lmax[1]);
 }
-
-// out (= or +=) A^{-1} in by four FP64 GEMMs (column-major G_x x G_y views of
-// the row-major unknown arrays).
-int fdm_apply64(se_linsys* ls, cublasHandle_t h, const double* in, double* out, bool accumulate) {
+// out (= or +=) A^{-1} in by four FP64 products on the row-major
+// G_y x G_x unknown arrays F:  Ey^T (F Ex), spectral divide, then
+// Ey ((.) Ex^T), the divide fused into the second product's epilogue and the
+// accumulation into the fourth's (gemm.cu).
+int fdm_apply64(se_linsys* ls, const double* in, double* out, bool accumulate) {
   const int gx = ls->op.G[0], gy = ls->op.G[1];
-  const double one = 1.0, zero = 0.0;
-  CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, gx, gy, gy, &one, in, gx, ls->Sy, gy, &zero, ls->X1, gx));
-  CB(cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, gx, gy, gx, &one, ls->Sx, gx, ls->X1, gx, &zero, ls->X2, gx));
-  CK(launch_spectral_divide(0, ls->X2, gx, gy, ls->lx, ls->ly, ls->op.alpha, ls->op.beta[0],
-                            ls->op.beta[1], null_tol(ls), g_stream));
-  CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, gx, gy, gy, &one, ls->X2, gx, ls->Sy, gy, &zero, ls->X1, gx));
-  CB(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, gx, gy, gx, &one, ls->Sx, gx, ls->X1, gx,
-                 accumulate ? &one : &zero, out, gx));
+  const OpDev& op = ls->op;
+  const double nt = null_tol(ls);
+  CK(launch_fdm_gemm(0, 0, in, 1, ls->SxT, ls->X1, 1, gy, gx, gx, gx, gx, gx, nullptr, nullptr,
+                     nullptr, nullptr, 0, 0, 0, 0, g_stream));
+  CK(launch_fdm_gemm(0, 1, ls->Sy, 1, ls->X1, ls->X2, 1, gy, gx, gy, gy, gx, gx, nullptr, nullptr,
+                     ls->lx, ls->ly, op.alpha, op.beta[0], op.beta[1], nt, g_stream));
+  CK(launch_fdm_gemm(0, 0, ls->X2, 1, ls->Sx, ls->X1, 1, gy, gx, gx, gx, gx, gx, nullptr, nullptr,
+                     nullptr, nullptr, 0, 0, 0, 0, g_stream));
+  CK(launch_fdm_gemm(0, accumulate ? 2 : 0, ls->SyT, 1, ls->X1, out, 1, gy, gx, gy, gy, gx, gx,
+                     nullptr, nullptr, nullptr, nullptr, 0, 0, 0, 0, g_stream));
   return SE_OK;
 }
 
-// Low-precision x += A^{-1} in: in scaled by 1/max|in| (max kept in device
-// memory) into L1, four GEMMs, result added back scaled. prec 1: FP32 data,
-// TF32 tensor cores; prec 2: BF16 data, FP32 accumulation.
-int fdm_apply_low(se_linsys* ls, cublasHandle_t h, const double* in, double* out) {
+// Low-precision x += A^{-1} in: the first product reads in scaled by
+// 1/max|in| (max kept in device memory) and rounds it to the low type, the
+// last adds its result back scaled by max. prec 1: FP32 data, TF32 tensor
+// cores; prec 2: BF16 data; both accumulate in FP32.
+int fdm_apply_low(se_linsys* ls, const double* in, double* out) {
   const int gx = ls->op.G[0], gy = ls->op.G[1];
   const size_t n = (size_t)gx * gy;
   const int prec = ls->fdm_prec;
+  const OpDev& op = ls->op;
   double* mx = ls->fpart + 2 * ls->fpart_n;
   CK(launch_maxabs(in, n, ls->fpart, kFdmPartials, mx, g_stream));
-  CK(launch_to_low(prec, in, ls->L1, n, mx, g_stream));
-  const float one = 1.0f, zero = 0.0f;
-  const cudaDataType_t t = prec == 1 ? CUDA_R_32F : CUDA_R_16BF;
-  const cublasComputeType_t ct = prec == 1 ? CUBLAS_COMPUTE_32F_FAST_TF32 : CUBLAS_COMPUTE_32F;
-  CB(cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, gx, gy, gy, &one, ls->L1, t, gx, ls->Sy_lo, t, gy,
-                  &zero, ls->L2, t, gx, ct, CUBLAS_GEMM_DEFAULT));
-  CB(cublasGemmEx(h, CUBLAS_OP_T, CUBLAS_OP_N, gx, gy, gx, &one, ls->Sx_lo, t, gx, ls->L2, t, gx,
-                  &zero, ls->L3, t, gx, ct, CUBLAS_GEMM_DEFAULT));
-  CK(launch_spectral_divide(prec, ls->L3, gx, gy, ls->lx, ls->ly, ls->op.alpha, ls->op.beta[0],
-                            ls->op.beta[1], null_tol(ls), g_stream));
-  CB(cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_T, gx, gy, gy, &one, ls->L3, t, gx, ls->Sy_lo, t, gy,
-                  &zero, ls->L2, t, gx, ct, CUBLAS_GEMM_DEFAULT));
-  CB(cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, gx, gy, gx, &one, ls->Sx_lo, t, gx, ls->L2, t, gx,
-                  &zero, ls->L1, t, gx, ct, CUBLAS_GEMM_DEFAULT));
-  CK(launch_add_low(prec, out, ls->L1, n, mx, g_stream));
+  CK(launch_fdm_gemm(prec, 0, in, 1, ls->SxT_lo, ls->L2, 0, gy, gx, gx, gx, gx, gx, mx, nullptr,
+                     nullptr, nullptr, 0, 0, 0, 0, g_stream));
+  CK(launch_fdm_gemm(prec, 1, ls->Sy_lo, 0, ls->L2, ls->L3, 0, gy, gx, gy, gy, gx, gx, nullptr,
+                     nullptr, ls->lx, ls->ly, op.alpha, op.beta[0], op.beta[1], null_tol(ls), g_stream));
+  CK(launch_fdm_gemm(prec, 0, ls->L3, 0, ls->Sx_lo, ls->L2, 0, gy, gx, gx, gx, gx, gx, nullptr,
+                     nullptr, nullptr, nullptr, 0, 0, 0, 0, g_stream));
+  CK(launch_fdm_gemm(prec, 2, ls->SyT_lo, 0, ls->L2, out, 1, gy, gx, gy, gy, gx, gx, nullptr, mx,
+                     nullptr, nullptr, 0, 0, 0, 0, g_stream));
   return SE_OK;
 }
 
-constexpr size_t kCublasWorkspace = 32u << 20;
 
 // The whole FDM solve as one CUDA graph: right-hand side assembly, r = f,
 // x = 0, the initial norm and test, then a conditional while-node whose body
@@ -796,12 +790,53 @@ constexpr size_t kCublasWorkspace = 32u << 20;
 // convergence test that sets the loop condition; finally the field update.
 // Parameters (rtol, atol, dtol, max_it) and the loop state live in device
 // memory, so one solve is one graph launch and one read of the state.
-int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
-  cublasHandle_t h;
-  if (int rc = cublas_for(&h)) return rc;
-  if (!ls->cublas_ws) {
-    if (int rc = dalloc(&ls->cublas_ws, kCublasWorkspace)) return rc;
+// Node and edge kinds of a captured graph, for error messages.
+std::string describe_graph(cudaGraph_t g) {
+  if (!g) return "none";
+  size_t nn = 0;
+  if (cudaGraphGetNodes(g, nullptr, &nn) != cudaSuccess) return "?";
+  std::vector<cudaGraphNode_t> nodes(nn);
+  cudaGraphGetNodes(g, nodes.data(), &nn);
+  int kinds[16] = {0}, clusters = 0, pdl_attr = 0;
+  for (auto nd : nodes) {
+    cudaGraphNodeType t;
+    if (cudaGraphNodeGetType(nd, &t) != cudaSuccess) continue;
+    kinds[(int)t & 15]++;
+    if (t == cudaGraphNodeTypeKernel) {
+      cudaLaunchAttributeValue v;
+      if (cudaGraphKernelNodeGetAttribute(nd, cudaLaunchAttributeClusterDimension, &v) == cudaSuccess &&
+          v.clusterDim.x * v.clusterDim.y * v.clusterDim.z > 1)
+        clusters++;
+      if (cudaGraphKernelNodeGetAttribute(nd, cudaLaunchAttributeProgrammaticStreamSerialization, &v) == cudaSuccess &&
+          v.programmaticStreamSerializationAllowed)
+        pdl_attr++;
+    }
   }
+  size_t ne = 0;
+  int prog = 0;
+  if (cudaGraphGetEdges_v2(g, nullptr, nullptr, nullptr, &ne) == cudaSuccess && ne) {
+    std::vector<cudaGraphNode_t> from(ne), to(ne);
+    std::vector<cudaGraphEdgeData> ed(ne);
+    if (cudaGraphGetEdges_v2(g, from.data(), to.data(), ed.data(), &ne) == cudaSuccess)
+      for (size_t k = 0; k < ne; k++)
+        if (ed[k].type != cudaGraphDependencyTypeDefault) prog++;
+  }
+  cudaGetLastError();
+  char buf[256];
+  snprintf(buf, sizeof(buf),
+           "%zu nodes: %d kernel, %d memcpy, %d memset, %d host, %d graph, %d empty, %d other; "
+           "%d clustered, %d with programmatic serialization; %zu edges, %d programmatic",
+           nn, kinds[cudaGraphNodeTypeKernel], kinds[cudaGraphNodeTypeMemcpy],
+           kinds[cudaGraphNodeTypeMemset], kinds[cudaGraphNodeTypeHost], kinds[cudaGraphNodeTypeGraph],
+           kinds[cudaGraphNodeTypeEmpty],
+           (int)nn - kinds[cudaGraphNodeTypeKernel] - kinds[cudaGraphNodeTypeMemcpy] -
+               kinds[cudaGraphNodeTypeMemset] - kinds[cudaGraphNodeTypeHost] -
+               kinds[cudaGraphNodeTypeGraph] - kinds[cudaGraphNodeTypeEmpty],
+           clusters, pdl_attr, ne, prog);
+  return buf;
+}
+
+int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
   if (!ls->d_fparams) {
     int rc;
     if ((rc = dalloc(&ls->d_fparams, 1)) || (rc = dalloc(&ls->d_fstate, 1))) return rc;
@@ -816,24 +851,18 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
   CK(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
   auto cleanup = [&]() {
     g_stream = saved;
-    cublasSetStream(h, saved);
     cudaStreamDestroy(cs);
     cudaStreamDestroy(bs);
   };
   int rc = SE_OK;
   cudaGraph_t graph = nullptr;
   do {
-    if (cublasSetWorkspace(h, ls->cublas_ws, kCublasWorkspace) != CUBLAS_STATUS_SUCCESS) {
-      rc = fail(SE_ERR_CUDA, "cublasSetWorkspace failed");
-      break;
-    }
     const MeshDev& m = ls->sol->mesh->dev;
     const size_t n = (size_t)ls->n;
     const int nt = ls->opts.norm_type;
     const double* wv = nt == SE_NORM_UNPRECONDITIONED ? nullptr : ls->dinv;
     double* res = ls->fpart + 2 * ls->fpart_n + 2;
     g_stream = cs;
-    cublasSetStream(h, cs);
     cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess) { rc = cuda_fail(e, "begin capture"); break; }
     cudaStreamCaptureStatus status;
@@ -866,11 +895,10 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
     // the loop body, captured on its own stream
     if (ok) {
       g_stream = bs;
-      cublasSetStream(h, bs);
       ok = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
       int brc = SE_OK;
       if (ok) {
-        brc = prec == 0 ? fdm_apply64(ls, h, ls->r, ls->x, true) : fdm_apply_low(ls, h, ls->r, ls->x);
+        brc = prec == 0 ? fdm_apply64(ls, ls->r, ls->x, true) : fdm_apply_low(ls, ls->r, ls->x);
         if (!brc && remove_null)
           brc = launch_remove_mean(ls->x, n, ls->fpart, kFdmPartials, ls->fpart + 2 * ls->fpart_n + 4, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
         if (!brc) brc = launch_residual(ls->op, ls->x, ls->f, ls->r, wv, nt == SE_NORM_NATURAL, ls->fpart, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
@@ -881,7 +909,6 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
         ok = ended && brc == SE_OK;
       }
       g_stream = cs;
-      cublasSetStream(h, cs);
     }
     // epilogue
     ok = ok && launch_update_field(ls->op, m, ls->x, ls->sol->vals, cs) == cudaSuccess;
@@ -893,7 +920,9 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
     }
     e = cudaGraphInstantiate(&ls->fdm_exec, graph, 0);
     if (e != cudaSuccess) {
-      rc = cuda_fail(e, "cudaGraphInstantiate");
+      rc = fail(SE_ERR_CUDA, "cudaGraphInstantiate: %s (loop body: %s)", cudaGetErrorString(e),
+                describe_graph(body).c_str());
+      cudaGetLastError();
       ls->fdm_exec = nullptr;
       break;
     }
@@ -1400,14 +1429,20 @@ int se_advector_create(se_field* field, se_field* velocity, se_field* field_prev
   a->vel = velocity;
   a->field_prev = field_prev;
   a->vel_prev = vel_prev;
-  int rc = se_field_create(field->mesh, field->ndofs, field->bcs, &a->sl);
+  int rc = dalloc(&a->err, 1);
   if (rc) {
+    delete a;
+    return rc;
+  }
+  if ((rc = se_field_create(field->mesh, field->ndofs, field->bcs, &a->sl))) {
+    dfree(a->err);
     delete a;
     return rc;
   }
   // fieldSL starts as a copy of the field (src/base/Advector.cpp:64-65)
   if ((rc = se_field_copy(a->sl, field))) {
     se_field_destroy(a->sl);
+    dfree(a->err);
     delete a;
     return rc;
   }
@@ -1419,18 +1454,19 @@ int se_advector_destroy(se_advector* adv) {
   se_field_destroy(adv->sl);
   dfree(adv->dep_el);
   dfree(adv->dep_xy);
+  dfree(adv->err);
   delete adv;
   return SE_OK;
 }
 int se_advect(se_advector* adv, double dt) {
   if (!adv) return fail(SE_ERR_ARG, "null advector");
   const se_mesh* me = adv->field->mesh;
-  CK(cudaMemsetAsync(g_err_word, 0, sizeof(unsigned), g_stream));
+  CK(cudaMemsetAsync(adv->err, 0, sizeof(unsigned), g_stream));
   CK(launch_sl(me->dev, adv->field->ndofs, adv->field->vals, adv->vel->vals,
                adv->field_prev ? adv->field_prev->vals : nullptr,
                adv->vel_prev ? adv->vel_prev->vals : nullptr, dt, adv->sl->vals,
                adv->record ? adv->dep_el : nullptr, adv->record ? adv->dep_xy : nullptr,
-               g_err_word, g_stream));
+               adv->err, g_stream));
   return SE_OK;
 }
 int se_advector_field_sl(se_advector* adv, se_field** field_sl) {
@@ -1455,7 +1491,7 @@ int se_advector_departures(se_advector* adv, int* el, double* xy) {
                        g_stream));
   CK(cudaStreamSynchronize(g_stream));
   unsigned err = 0;
-  CK(cudaMemcpy(&err, g_err_word, sizeof(err), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&err, adv->err, sizeof(err), cudaMemcpyDeviceToHost));
   if (err & KERR_DOMAIN) return fail(SE_ERR_DOMAIN, "a departure point left the mesh");
   return SE_OK;
 }

@@ -598,8 +598,78 @@ __global__ void __launch_bounds__(kCgThreads, 1) cg_n_kernel(const CgBatch B) {
 }
 
 
+
+// ------------------------------------------- extended-precision residual --
+// Error-free transformations (Knuth TwoSum; TwoProd with an FMA): the pair
+// (hi, lo) carries a value to about twice double precision.
+// The _rn intrinsics keep each operation a single IEEE operation: the
+// compiler must not fuse a product into a following sum here.
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+}
+__device__ __forceinline__ void dd_add(double& hi, double& lo, double x) {
+  double s, e;
+  two_sum(hi, x, s, e);
+  hi = s;
+  lo += e;
+}
+__device__ __forceinline__ void dd_fma(double& hi, double& lo, double a, double b) {
+  const double p = __dmul_rn(a, b);
+  const double pe = fma(a, b, -p);  // exact: a*b - p
+  dd_add(hi, lo, p);
+  lo += pe;
+}
+// krow_n in double-double: the stiffness rows sum to zero, so the taps cancel
+// and a plain FP64 sum loses the digits a 1e-10 residual needs.
+template <int N, int STRIDE>
+__device__ __forceinline__ void krow_dd(const Dir& d, const double* Kh, int e, int a, const double* c,
+                                        double& hi, double& lo) {
+  constexpr int n = N + 1;
+  hi = 0.0;
+  lo = 0.0;
+  if (a != 0) {
+    const double* k = Kh + a * n;
+    const double* q = c - a * STRIDE;
+#pragma unroll
+    for (int b = 0; b < n; b++) dd_fma(hi, lo, k[b], q[b * STRIDE]);
+    return;
+  }
+  if (e > 0 || d.periodic) {
+    const double* k = Kh + N * n;
+#pragma unroll
+    for (int b = 0; b < n; b++) dd_fma(hi, lo, k[b], c[(b - N) * STRIDE]);
+  }
+  if (e < d.nE) {
+#pragma unroll
+    for (int b = 0; b < n; b++) dd_fma(hi, lo, Kh[b], c[b * STRIDE]);
+  }
+}
+// b - (A p) at the thread's unknown, accumulated in double-double and
+// rounded once.
+template <int N>
+__device__ __forceinline__ double residual_dd(const OpSm& o, const double* P, int tx, int ty, int gx,
+                                              int gy, double bval) {
+  typedef Geo<N> G;
+  const double* c = P + (ty + N) * G::W + (tx + N);
+  const int ex = gx / N, ax = gx - ex * N, ey = gy / N, ay = gy - ey * N;
+  const double wx = wsum_n<N>(o.dx, o.w, ex, ax), wy = wsum_n<N>(o.dy, o.w, ey, ay);
+  double kxh, kxl, kyh, kyl;
+  krow_dd<N, 1>(o.dx, o.Kh, ex, ax, c, kxh, kxl);
+  krow_dd<N, G::W>(o.dy, o.Kh, ey, ay, c, kyh, kyl);
+  double hi = bval, lo = 0.0;
+  const double cm = -o.alpha * wx * wy, cx = -o.beta0 * wy, cy = -o.beta1 * wx;
+  dd_fma(hi, lo, cm, c[0]);
+  dd_fma(hi, lo, cx, kxh);
+  lo = fma(cx, kxl, lo);
+  dd_fma(hi, lo, cy, kyh);
+  lo = fma(cy, kyl, lo);
+  return hi + lo;
+}
+
 // ------------------------------------------- standalone apply / residual --
-// y = A x, or with b: r = b - A x together with per-block partial sums of
+// y = A x, or with b: r = b - A x (extended precision) with per-block partial sums of
 // (w r)^2 (or r w r when natural) and r^2 (w = Jacobi inverse, nullptr: 1).
 template <int N>
 __global__ void __launch_bounds__(kCgThreads) apply_kernel(const OpDev op, const double* __restrict__ x,
@@ -632,15 +702,14 @@ __global__ void __launch_bounds__(kCgThreads) apply_kernel(const OpDev op, const
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   if (ux < o.G0 && uy < o.G1) {
     const size_t k = (size_t)uy * o.G0 + ux;
-    const double ax = apply_n<N>(o, P, tx, ty, ux + o.dx.lo, uy + o.dy.lo);
     if (b) {
-      const double r = b[k] - ax;
+      const double r = residual_dd<N>(o, P, tx, ty, ux + o.dx.lo, uy + o.dy.lo, b[k]);
       y[k] = r;
       const double z = w ? r * w[k] : r;
       acc[0] = natural ? z * r : z * z;
       acc[1] = r * r;
     } else {
-      y[k] = ax;
+      y[k] = apply_n<N>(o, P, tx, ty, ux + o.dx.lo, uy + o.dy.lo);
     }
   }
   if (partial) {

@@ -183,6 +183,18 @@ cudaError_t launch_fdm_init(const FdmParams* p, FdmState* st, const double* res,
 cudaError_t launch_fdm_check(const FdmParams* p, FdmState* st, const double* res,
                              cudaGraphConditionalHandle h, cudaStream_t s);
 
+// C = A B (row-major, leading dimensions lda/ldb/ldc) on the tensor cores
+// (gemm.cu). prec: 0 FP64, 1 TF32 on FP32 data, 2 BF16. epi: 0 store,
+// 1 store after the spectral divide by alpha + bx lx[col] + by ly[row]
+// (|divisor| <= null_tol gives 0), 2 accumulate into FP64 C scaled by *cmax
+// (cmax == nullptr: 1). a_fp64: A is FP64 (scaled by 1/*amax when amax is
+// given) whatever prec; c_fp64: C is FP64 (required for epi 2).
+cudaError_t launch_fdm_gemm(int prec, int epi, const void* A, int a_fp64, const void* B, void* C,
+                            int c_fp64, int M, int N, int K, int lda, int ldb, int ldc,
+                            const double* amax, const double* cmax, const double* lx,
+                            const double* ly, double alpha, double bx, double by, double null_tol,
+                            cudaStream_t s);
+
 // Fast-diagonalization pieces (fdm.cu). prec: 0 FP64, 1 FP32, 2 BF16.
 cudaError_t launch_spectral_divide(int prec, void* v, int gx, int gy, const double* lx,
                                    const double* ly, double alpha, double bx, double by,

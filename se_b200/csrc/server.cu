@@ -69,8 +69,20 @@ struct Job {
   Instance* inst = nullptr;
   int slot = -1;
   bool done = false;
+  bool out_direct = false;  // the result is copied straight into req.out
   se_result res;
 };
+
+// Page-locked host memory can be the source or destination of an
+// asynchronous copy directly; other memory goes through the slot's staging.
+bool pinned(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
+}
 
 struct Slot {
   cudaStream_t s = nullptr;
@@ -182,7 +194,19 @@ int acquire(se_server* S, const se_request& r, Instance** out) {
   return create(S, r, out);
 }
 
+// The worker thread's last library message, or the CUDA error pending on it.
+void note_error(Job* j, int rc) {
+  if (rc == SE_OK || j->res.error[0]) return;
+  const char* m = se_last_error();
+  const cudaError_t e = cudaGetLastError();
+  if (m && m[0])
+    snprintf(j->res.error, sizeof(j->res.error), "%s", m);
+  else
+    snprintf(j->res.error, sizeof(j->res.error), "%s", cudaGetErrorString(e));
+}
+
 void fail_job(se_server* S, Job* j, int rc) {
+  note_error(j, rc);
   j->res.status = rc;
   j->t_done = now_ms();
   j->res.queued_ms = (j->t_admit > 0 ? j->t_admit : j->t_done) - j->t_submit;
@@ -191,16 +215,25 @@ void fail_job(se_server* S, Job* j, int rc) {
   S->cv_done.notify_all();
 }
 
+// Record a failed CUDA runtime call in the job's result.
+int cuda_failed(Job* j, cudaError_t e, const char* what) {
+  snprintf(j->res.error, sizeof(j->res.error), "%s: %s", what, cudaGetErrorString(e));
+  cudaGetLastError();
+  return e == cudaErrorMemoryAllocation ? SE_ERR_OOM : SE_ERR_CUDA;
+}
+
 // Queue the request's device work on the slot's stream.
 int start(se_server* S, Job* j, Slot& sl) {
   const se_request& r = j->req;
   Instance* in = j->inst;
   const size_t nv = (size_t)in->nv;
+  cudaError_t e;
   if (sl.cap < nv) {
     if (sl.h) cudaFreeHost(sl.h);
     sl.h = nullptr;
     sl.cap = 0;
-    if (cudaMallocHost((void**)&sl.h, sizeof(double) * 4 * nv) != cudaSuccess) return SE_ERR_OOM;
+    if ((e = cudaMallocHost((void**)&sl.h, sizeof(double) * 4 * nv)) != cudaSuccess)
+      return cuda_failed(j, e, "staging cudaMallocHost");
     sl.cap = nv;
   }
   double *h_in = sl.h, *h_aux = sl.h + sl.cap, *h_out = sl.h + 3 * sl.cap;
@@ -208,35 +241,44 @@ int start(se_server* S, Job* j, Slot& sl) {
   double *da = nullptr, *db = nullptr;
   se_field_device_ptr(in->a, &da);
   se_field_device_ptr(in->b, &db);
-  std::memcpy(h_in, r.in, sizeof(double) * nv);
-  if (cudaMemcpyAsync(da, h_in, sizeof(double) * nv, cudaMemcpyHostToDevice, sl.s) != cudaSuccess)
-    return SE_ERR_CUDA;
+  // host -> device through staging unless the caller's array is page-locked
+  auto upload = [&](double* dst, const double* src, double* stage, size_t count) {
+    const double* from = src;
+    if (!pinned(src)) {
+      std::memcpy(stage, src, sizeof(double) * count);
+      from = stage;
+    }
+    const cudaError_t ue =
+        cudaMemcpyAsync(dst, from, sizeof(double) * count, cudaMemcpyHostToDevice, sl.s);
+    return ue == cudaSuccess ? SE_OK : cuda_failed(j, ue, "input upload");
+  };
+  j->out_direct = pinned(r.out);
+  double* dst_out = j->out_direct ? r.out : h_out;
+  if (int rc = upload(da, r.in, h_in, nv)) return rc;
   int rc = SE_OK;
   if (r.kind == SE_REQ_HELMHOLTZ) {
     if (r.aux) {
-      std::memcpy(h_aux, r.aux, sizeof(double) * nv);
-      if (cudaMemcpyAsync(db, h_aux, sizeof(double) * nv, cudaMemcpyHostToDevice, sl.s) != cudaSuccess)
-        return SE_ERR_CUDA;
-    } else if (cudaMemsetAsync(db, 0, sizeof(double) * nv, sl.s) != cudaSuccess) {
-      return SE_ERR_CUDA;
+      if (int rc2 = upload(db, r.aux, h_aux, nv)) return rc2;
+    } else if ((e = cudaMemsetAsync(db, 0, sizeof(double) * nv, sl.s)) != cudaSuccess) {
+      return cuda_failed(j, e, "solution clear");
     }
     rc = se_linsys_assemble(in->ls);  // the Dirichlet lifting of this request's values
     if (!rc) rc = se_linsys_solve_async(in->ls, 0);
-    if (!rc && cudaMemcpyAsync(h_out, db, sizeof(double) * nv, cudaMemcpyDeviceToHost, sl.s) != cudaSuccess)
-      rc = SE_ERR_CUDA;
+    if (rc) return rc;
+    if ((e = cudaMemcpyAsync(dst_out, db, sizeof(double) * nv, cudaMemcpyDeviceToHost, sl.s)) != cudaSuccess)
+      return cuda_failed(j, e, "result download");
   } else {
-    std::memcpy(h_aux, r.aux, sizeof(double) * 2 * nv);
-    if (cudaMemcpyAsync(db, h_aux, sizeof(double) * 2 * nv, cudaMemcpyHostToDevice, sl.s) != cudaSuccess)
-      return SE_ERR_CUDA;
+    if (int rc2 = upload(db, r.aux, h_aux, 2 * nv)) return rc2;
     for (int k = 0; k < r.steps && !rc; k++) {
       rc = se_advect(in->adv, r.sl_dt);
       if (!rc) rc = se_field_copy(in->a, in->sl);
     }
-    if (!rc && cudaMemcpyAsync(h_out, da, sizeof(double) * nv, cudaMemcpyDeviceToHost, sl.s) != cudaSuccess)
-      rc = SE_ERR_CUDA;
+    if (rc) return rc;
+    if ((e = cudaMemcpyAsync(dst_out, da, sizeof(double) * nv, cudaMemcpyDeviceToHost, sl.s)) != cudaSuccess)
+      return cuda_failed(j, e, "result download");
   }
-  if (!rc && cudaEventRecord(sl.ev, sl.s) != cudaSuccess) rc = SE_ERR_CUDA;
-  return rc;
+  if ((e = cudaEventRecord(sl.ev, sl.s)) != cudaSuccess) return cuda_failed(j, e, "completion event");
+  return SE_OK;
 }
 
 void finish(se_server* S, Slot& sl) {
@@ -251,7 +293,8 @@ void finish(se_server* S, Slot& sl) {
     j->res.its = st.its;
     if (rc == SE_ERR_NOT_CONVERGED) rc = SE_OK;  // reported through reason
   }
-  std::memcpy(j->req.out, sl.h + 3 * sl.cap, sizeof(double) * in->nv);
+  note_error(j, rc);
+  if (!j->out_direct) std::memcpy(j->req.out, sl.h + 3 * sl.cap, sizeof(double) * in->nv);
   std::lock_guard<std::mutex> lk(S->mu);
   in->busy = false;
   in->last_used = ++S->clock;

@@ -86,7 +86,8 @@ class Request(ctypes.Structure):
 
 class Result(ctypes.Structure):
     _fields_ = [("status", ctypes.c_int), ("reason", ctypes.c_int), ("its", ctypes.c_int),
-                ("queued_ms", ctypes.c_double), ("latency_ms", ctypes.c_double)]
+                ("queued_ms", ctypes.c_double), ("latency_ms", ctypes.c_double),
+                ("error", ctypes.c_char * 160)]
 
 
 REQ_HELMHOLTZ, REQ_ADVECT = 0, 1
@@ -508,10 +509,13 @@ class Server:
         self._keep = {}
 
     def submit(self, kind, nEls, N, lo, hi, periodic, field_in, aux=None, bcs=(0, 0, 0, 0),
-               c=-1.0, nu=-1.0, dt=1.0, poisson=False, opts=None, steps=0, sl_dt=0.0):
+               c=-1.0, nu=-1.0, dt=1.0, poisson=False, opts=None, steps=0, sl_dt=0.0, out=None):
+        """Queue a request; `out` (optional) is a preallocated float64 result
+        array (page-locked memory avoids the server's staging copies)."""
         fin = np.ascontiguousarray(field_in, dtype=np.float64)
         fa = None if aux is None else np.ascontiguousarray(aux, dtype=np.float64)
-        out = np.empty(len(fin))
+        if out is None:
+            out = np.empty(len(fin))
         r = Request()
         r.kind = kind
         r.nEls[:] = [int(nEls[0]), int(nEls[1])]
@@ -541,7 +545,8 @@ class Server:
             raise SEError(rc, "se_server_wait failed")
         fin, fa, out, r = self._keep.pop(ticket)
         return out, {"status": res.status, "reason": res.reason, "its": res.its,
-                     "queued_ms": res.queued_ms, "latency_ms": res.latency_ms}
+                     "queued_ms": res.queued_ms, "latency_ms": res.latency_ms,
+                     "error": res.error.decode(errors="replace")}
 
     def close(self):
         if getattr(self, "_h", None) and _lib is not None:
