@@ -331,6 +331,61 @@ def read_peaks():
 
 
 
+# ------------------------------------------------------- operator apply ----
+def run_apply_roofline(ne=768, p=8, reps=20):
+    """The matrix-free Helmholtz apply y = A x on a doubly periodic
+    ne x ne element mesh of order p (ne = 768, p = 8: 37.7M unknowns, larger
+    than L2 in every precision), timed with CUDA events on the launching
+    stream over `reps` back-to-back launches after 3 warm-up launches.
+    Algorithmic bytes per unknown: FP64 in + FP64 out = 16; BF16 in + FP32
+    out = 6. Achieved = bytes / launch time, against the measured HBM copy
+    bandwidth."""
+    import torch
+    import se_b200 as S
+    hbm, src = read_peaks()
+    m = S.Mesh("m", [ne, ne], "legendre", p, [0, 0], [1, 1], [True, True])
+    bc = S.BCs(False, False, False, False, m)
+    u, f = S.Field("u", m, 1, bc), S.Field("f", m, 1, bc)
+    ls = S.HelmholtzEqn(u, f, -1.0, -1.0, 1.0, 0,
+                        S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=S.METHOD_FDM))
+    n = ls.vecSize
+    stream = torch.cuda.Stream()
+    S.set_stream(stream.cuda_stream)  # the library launches on the stream the events record on
+    g = torch.Generator(device="cuda").manual_seed(5)
+    out = {"workload": f"y = A x, {ne}x{ne} elements, p={p}, doubly periodic, {n} unknowns",
+           "unknowns": n}
+    with torch.cuda.stream(stream):
+        for name, bpd in (("fp64", 16), ("bf16_in_fp32_out", 6)):
+            if name == "fp64":
+                x = torch.randn(n, device="cuda", dtype=torch.float64, generator=g)
+                y = torch.empty(n, device="cuda", dtype=torch.float64)
+                call = lambda: ls.apply(x.data_ptr(), y.data_ptr())  # noqa: E731
+            else:
+                x = torch.randn(n, device="cuda", dtype=torch.float32, generator=g).to(torch.bfloat16)
+                y = torch.empty(n, device="cuda", dtype=torch.float32)
+                call = lambda: ls.apply_low(x.data_ptr(), y.data_ptr(), S.PREC_BF16)  # noqa: E731
+            for _ in range(3):
+                call()
+            stream.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                call()
+            e1.record(stream)
+            stream.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            gbs = bpd * n / (ms * 1e-3) / 1e9
+            out[name] = {"kernel": ("apply_tile_kernel<8, double>" if name == "fp64"
+                                    else "apply_tile_kernel<8, bf16 -> float>"),
+                         "launch_ms": ms, "bytes_per_unknown": bpd, "achieved_gbs": gbs,
+                         "peak_gbs": hbm, "frac": gbs / hbm,
+                         "peak_source": src + " (MEASURED_PEAKS.json hbm_gbs)",
+                         "dof_applies_per_s": n / (ms * 1e-3)}
+            del x, y
+    del ls, u, f, bc, m
+    return out
+
+
 # ------------------------------------------------------ ensemble (config 3) --
 def run_ensemble(count=256, seed=2024):
     """256 independent Helmholtz solves, mesh n x n elements with n uniform in
@@ -347,7 +402,9 @@ def run_ensemble(count=256, seed=2024):
                       float(10 ** rng.uniform(-2, 2)), int(rng.integers(0, 2 ** 31))))
     out = {"workload": "256 solves, n x n elements n~U{8..64}, p~U{4,6,8}, lambda~logU[1e-2,1e2], "
                        "8-mode RHS, rtol 1e-10"}
-    for name, method in (("fdm_fp64", S.METHOD_FDM), ("cg_fp64", S.METHOD_CG)):
+    for name, method, prec in (("fdm_fp64", S.METHOD_FDM, S.PREC_FP64),
+                               ("fdm_tf32_refined_fp64", S.METHOD_FDM, S.PREC_MIXED),
+                               ("cg_fp64", S.METHOD_CG, S.PREC_FP64)):
         systems = []
         for ne, p, lam, sd in specs:
             m = S.Mesh("m", [ne, ne], "legendre", p, [0, 0], [1, 1], [True, True])
@@ -363,7 +420,8 @@ def run_ensemble(count=256, seed=2024):
             u, rr = S.Field("u", m, 1, bc), S.Field("f", m, 1, bc)
             rr.vals = f
             ls = S.HelmholtzEqn(u, rr, -lam, -1.0, 1.0, 0,
-                                S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=method))
+                                S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=method,
+                                              precision=prec))
             systems.append((m, bc, u, rr, ls))
         lss = [s[4] for s in systems]
         ng = sum(ls.vecSize for ls in lss)
@@ -385,19 +443,35 @@ def run_ensemble(count=256, seed=2024):
 
 
 # ------------------------------------------------------- serving (config 4) --
-def run_serving(rate=2000.0, seconds=2.0, seed=77):
-    """Poisson arrivals (mean `rate` req/s) for `seconds`, half Helmholtz
-    solves (lambda = 1, rtol 1e-10, FDM) and half 10-step first-order SL
-    jobs (Taylor-Green velocity, Courant 1), on n x n element doubly periodic
-    meshes with n in {8, 16, 32, 64, 128} (the powers of two of 8..128) and p
-    uniform in 4..8. Every configuration is warmed once before the stream.
-    Reports completed-request throughput, DOF-updates/s (Helmholtz: unknowns;
-    SL: vertices x steps) and p50/p99 latency from submission to result,
-    for FP64 solves and for TF32 solves refined in FP64."""
+def run_serving(seconds=2.0, seed=77, load=0.7):
+    """Serving through the continuous-batching server (se_server_*): half
+    Helmholtz solves (lambda = 1, rtol 1e-10, FDM) and half 10-step
+    first-order SL jobs (Courant 1), on n x n element doubly periodic meshes
+    with n in {8, 16, 32, 64, 128} and p uniform in 4..8. Every
+    configuration is warmed once. The client holds page-locked inputs and a
+    pool of page-locked result buffers per configuration (a result buffer is
+    reused once its result was collected; submission waits for a free one).
+
+    Two phases per precision: (1) capacity, the whole request stream
+    submitted as fast as the pools allow; (2) latency, Poisson arrivals at
+    `load` x capacity for `seconds`, with p50/p99 from submission to result.
+    DOF-updates: Helmholtz unknowns; SL vertices x steps."""
+    import queue
+    import threading
+
+    import torch
+
     import se_b200 as S
     rng = np.random.default_rng(seed)
     sizes, orders = [8, 16, 32, 64, 128], [4, 5, 6, 7, 8]
     inputs = {}
+    keep = []
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+        t.numpy()[...] = a
+        keep.append(t)
+        return t.numpy()  # shares the tensor's page-locked memory
 
     def inp(kind, n, p):
         key = (kind, n, p)
@@ -407,66 +481,24 @@ def run_serving(rate=2000.0, seconds=2.0, seed=77):
             x, y = X[:, 0], X[:, 1]
             if kind == S.REQ_HELMHOLTZ:
                 f = np.sin(2 * np.pi * x) * np.cos(4 * np.pi * y) + np.exp(-((x - .3) ** 2 + (y - .6) ** 2) / .02)
-                inputs[key] = (f, None, 0.0, n * p * n * p)
+                inputs[key] = (pinned(f), None, 0.0, n * p * n * p)
             else:
                 vel = np.stack([-np.sin(np.pi * x) ** 2 * np.sin(2 * np.pi * y),
                                 np.sin(np.pi * y) ** 2 * np.sin(2 * np.pi * x)], 1)
                 phi = np.exp(-((x - .4) ** 2 + (y - .6) ** 2) / .05 ** 2)
                 dt = 1.0 * (1.0 / n) / np.sqrt((vel ** 2).sum(1).max())
-                inputs[key] = (phi, vel, dt, len(X) * 10)
+                inputs[key] = (pinned(phi), pinned(vel), dt, len(X) * 10)
         return inputs[key]
 
-    import torch
+    def stream(n_req):
+        kinds = rng.integers(0, 2, size=n_req)
+        ns = rng.choice(sizes, size=n_req)
+        ps = rng.choice(orders, size=n_req)
+        return [(int(k), int(n), int(p)) for k, n, p in zip(kinds, ns, ps)]
 
-    def pinned(a):
-        t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
-        t.numpy()[...] = a
-        return t  # keep the tensor alive; .numpy() shares its page-locked memory
-
-    keep = []
-
-    def inp_pinned(kind, n, p):
-        f, aux, dt, d = inp(kind, n, p)
-        key = ("pinned", kind, n, p)
-        if key not in inputs:
-            tf = pinned(f)
-            ta = None if aux is None else pinned(aux)
-            keep.extend([tf, ta])
-            inputs[key] = (tf.numpy(), None if ta is None else ta.numpy())
-        return inputs[key][0], inputs[key][1], dt, d
-
-    n_req = int(rate * seconds)
-    gaps = rng.exponential(1.0 / rate, size=n_req)
-    kinds = rng.integers(0, 2, size=n_req)
-    ns = rng.choice(sizes, size=n_req)
-    ps = rng.choice(orders, size=n_req)
-    out = {"workload": f"Poisson arrivals {rate:.0f} req/s for {seconds:.1f} s, Helmholtz (FDM, "
-                       "rtol 1e-10) and 10-step SL jobs, n x n elements n in {8,16,32,64,128}, "
-                       "p in 4..8", "requests": n_req}
-    for label, prec in (("fp64", S.PREC_FP64), ("tf32_refined_fp64", S.PREC_MIXED)):
-        opts = S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=S.METHOD_FDM, precision=prec)
-        srv = S.Server(slots=16, device_gib=60.0)
-        keys = sorted({(int(k), int(n), int(p)) for k, n, p in zip(kinds, ns, ps)})
-        warm = []
-        for k, n, p in keys:
-            f, aux, dt, _ = inp(k, n, p)
-            warm.append(srv.submit(k, (n, n), p, (0, 0), (1, 1), (1, 1), f, aux, opts=opts,
-                                   c=-1.0, nu=-1.0, dt=1.0, steps=10, sl_dt=dt))
-        for t in warm:
-            srv.wait(t)
-        # Page-locked result buffers per configuration, recycled by a
-        # collector thread that waits for results in submission order (as a
-        # client of the server would); the pool is primed before timing.
-        import queue
-        import threading
-        pool = {key: [] for key in keys}
-        pool_mu = threading.Lock()
-        for k, n, p in keys:
-            nv = (n * p + 1) ** 2
-            for _ in range(4):
-                pool[(k, n, p)].append(torch.empty(nv, dtype=torch.float64, pin_memory=True))
-        for k, n, p in keys:
-            inp_pinned(k, n, p)
+    def serve(srv, opts, reqs, gaps, pools, cv):
+        """Submit reqs (after gaps; None: back to back) and collect them in
+        submission order on a second thread."""
         pending = queue.Queue()
         lat, fails = [], {}
 
@@ -479,40 +511,69 @@ def run_serving(rate=2000.0, seconds=2.0, seed=77):
                 _, res = srv.wait(t)
                 lat.append(res["latency_ms"])
                 if res["status"] != 0 or res["reason"] < 0:
-                    tag = (f"status={res['status']} reason={res['reason']}: {res['error']}")
+                    tag = f"status={res['status']} reason={res['reason']}: {res['error']}"
                     fails[tag] = fails.get(tag, 0) + 1
-                with pool_mu:
-                    pool[key].append(buf)
+                with cv:
+                    pools[key].append(buf)
+                    cv.notify_all()
 
         th = threading.Thread(target=collect)
         th.start()
-        dofs, grown = 0, 0
-        t_start = time.perf_counter()
-        due = t_start
-        for g, k, n, p in zip(gaps, kinds, ns, ps):
-            due += g
-            while time.perf_counter() < due:
-                pass
-            key = (int(k), int(n), int(p))
-            f, aux, dt, d = inp_pinned(*key)
-            with pool_mu:
-                buf = pool[key].pop() if pool[key] else None
-            if buf is None:
-                buf = torch.empty(len(f), dtype=torch.float64, pin_memory=True)
-                grown += 1
+        dofs = 0
+        t0 = time.perf_counter()
+        due = t0
+        for i, key in enumerate(reqs):
+            if gaps is not None:
+                due += gaps[i]
+                while time.perf_counter() < due:
+                    pass
+            f, aux, dt, d = inp(*key)
+            with cv:
+                while not pools[key]:
+                    cv.wait()
+                buf = pools[key].pop()
             t = srv.submit(key[0], (key[1], key[1]), key[2], (0, 0), (1, 1), (1, 1), f, aux,
-                           opts=opts, c=-1.0, nu=-1.0, dt=1.0, steps=10, sl_dt=dt,
-                           out=buf.numpy())
+                           opts=opts, c=-1.0, nu=-1.0, dt=1.0, steps=10, sl_dt=dt, out=buf.numpy())
             pending.put((t, key, buf))
             dofs += d
         pending.put(None)
         th.join()
-        wall = time.perf_counter() - t_start
-        bad = sum(fails.values())
+        wall = time.perf_counter() - t0
+        return {"req_per_s": len(reqs) / wall, "dof_updates_per_s": dofs / wall,
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "failed": int(sum(fails.values())), "failures": fails}
+
+    keys = sorted({(k, n, p) for k in (0, 1) for n in sizes for p in orders})
+    for key in keys:
+        inp(*key)
+    out = {"workload": "Helmholtz (FDM, rtol 1e-10) and 10-step SL requests, n x n elements "
+                       "n in {8,16,32,64,128}, p in 4..8, page-locked client buffers",
+           "load": load}
+    cap_reqs = stream(4000)
+    for label, prec in (("fp64", S.PREC_FP64), ("tf32_refined_fp64", S.PREC_MIXED)):
+        opts = S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=S.METHOD_FDM, precision=prec)
+        srv = S.Server(slots=16, device_gib=60.0)
+        cv = threading.Condition()
+        pools = {key: [torch.empty((key[1] * key[2] + 1) ** 2, dtype=torch.float64, pin_memory=True)
+                       for _ in range(8)] for key in keys}
+        for key in keys:  # warm every configuration
+            f, aux, dt, _ = inp(*key)
+            srv.wait(srv.submit(key[0], (key[1], key[1]), key[2], (0, 0), (1, 1), (1, 1), f, aux,
+                                opts=opts, c=-1.0, nu=-1.0, dt=1.0, steps=10, sl_dt=dt))
+        cap = serve(srv, opts, cap_reqs, None, pools, cv)
+        rate = load * cap["req_per_s"]
+        n_req = int(rate * seconds)
+        lat_reqs = stream(n_req)
+        gaps = rng.exponential(1.0 / rate, size=n_req)
+        lat = serve(srv, opts, lat_reqs, gaps, pools, cv)
         srv.close()
-        out[label] = {"req_per_s": n_req / wall, "dof_updates_per_s": dofs / wall,
-                      "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                      "failed": int(bad), "failures": fails, "pinned_buffers_grown": grown}
+        del pools
+        out[label] = {"capacity_req_per_s": cap["req_per_s"],
+                      "capacity_dof_updates_per_s": cap["dof_updates_per_s"],
+                      "offered_req_per_s": rate, "req_per_s": lat["req_per_s"],
+                      "p50_ms": lat["p50_ms"], "p99_ms": lat["p99_ms"],
+                      "failed": cap["failed"] + lat["failed"],
+                      "failures": {**cap["failures"], **lat["failures"]}}
     return out
 
 
@@ -609,6 +670,8 @@ def main():
     log("GPU arm done")
     extras = {}
     if not args.no_extras:
+        log("apply roofline")
+        extras["apply_roofline"] = run_apply_roofline()
         log("ensemble")
         extras["ensemble"] = run_ensemble()
         log("serving")

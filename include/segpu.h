@@ -145,7 +145,8 @@ int se_advector_departures(se_advector* adv, int* el, double* xy);
                                refinement converges only while 2^-8 times the operator's
                                condition number stays below 1 (small or well-conditioned
                                systems) and otherwise stops with SE_KSP_DIVERGED_BREAKDOWN */
-#define SE_METHOD_CG 0      /* PETSc KSPCG + PCJACOBI semantics: the drop-in */
+#define SE_PREC_FP16 3      /* FP16 data, FP32 arithmetic: se_linsys_apply_low only */
+#define SE_METHOD_CG 0      /* PETSc KSPCG + PCJACOBI semantics: the drop-in (FP64 only) */
 #define SE_METHOD_FDM 1     /* fast diagonalization: exact inverse by 1-D eigenvector transforms */
 typedef struct {
   double rtol;    /* default 1e-5 (PETSc) */
@@ -224,6 +225,10 @@ int se_linsys_solve_async(se_linsys* ls, int remove_null_space);
 int se_linsys_solve_finish(se_linsys* ls, se_solve_stats* stats);
 /* y = A x on vector unknowns (device pointers, vec_size entries each). */
 int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev);
+/* No counterpart in the reference: y = A x with x in BF16 or FP16
+ * (precision SE_PREC_BF16 / SE_PREC_FP16) and y in FP32, the operator and
+ * the arithmetic in FP32 (device pointers, vec_size entries each). */
+int se_linsys_apply_low(se_linsys* ls, int precision, const void* x_dev, float* y_dev);
 /* The Jacobi diagonal of A (device pointer, vec_size entries). */
 int se_linsys_diagonal(se_linsys* ls, double* d_dev);
 int se_linsys_vec_size(const se_linsys* ls, int* n);

@@ -1562,10 +1562,30 @@ int se_solver_opts_parse(se_solver_opts* o, const char* prefix, const char* opti
 }
 
 namespace {
+// Solver options this library can run.
+int check_opts(const se_solver_opts* o) {
+  if (o->method != SE_METHOD_CG && o->method != SE_METHOD_FDM)
+    return fail(SE_ERR_ARG, "unknown method %d", o->method);
+  if (o->precision == SE_PREC_FP16)
+    return fail(SE_ERR_UNSUPPORTED, "SE_PREC_FP16 is an apply precision (se_linsys_apply_low) only");
+  if (o->precision != SE_PREC_FP64 && o->precision != SE_PREC_MIXED && o->precision != SE_PREC_BF16)
+    return fail(SE_ERR_ARG, "unknown precision %d", o->precision);
+  if (o->precision != SE_PREC_FP64 && o->method != SE_METHOD_FDM)
+    return fail(SE_ERR_UNSUPPORTED, "reduced precision needs SE_METHOD_FDM");
+  if (o->norm_type < SE_NORM_PRECONDITIONED || o->norm_type > SE_NORM_NATURAL)
+    return fail(SE_ERR_ARG, "unknown norm type %d", o->norm_type);
+  if (o->mode != SE_MODE_REFERENCE && o->mode != SE_MODE_EXACT)
+    return fail(SE_ERR_ARG, "unknown mode %d", o->mode);
+  if (o->max_it < 0) return fail(SE_ERR_ARG, "negative max_it");
+  return SE_OK;
+}
+
 int linsys_create(se_field* sol, se_field* rhs, bool poisson, double c, double nu, double dt,
                   const se_solver_opts* opts, se_linsys** out) {
   if (!out) return fail(SE_ERR_ARG, "null argument");
   *out = nullptr;
+  if (opts)
+    if (int rc = check_opts(opts)) return rc;
   if (int rc = check_field(sol)) return rc;
   if (sol->ndofs != 1) return fail(SE_ERR_UNSUPPORTED, "only scalar solution fields");
   if (rhs) {
@@ -1619,6 +1639,7 @@ int se_linsys_destroy(se_linsys* ls) {
 }
 int se_linsys_set_opts(se_linsys* ls, const se_solver_opts* opts) {
   if (!ls || !opts) return fail(SE_ERR_ARG, "null argument");
+  if (int rc = check_opts(opts)) return rc;
   int old_mode = ls->opts.mode;
   ls->opts = *opts;
   if (opts->mode != old_mode) {
@@ -1791,6 +1812,13 @@ int se_linsys_solve_finish(se_linsys* ls, se_solve_stats* stats) {
 int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev) {
   if (!ls || !x_dev || !y_dev) return fail(SE_ERR_ARG, "null argument");
   CK(launch_op_apply(ls->op, x_dev, y_dev, g_stream));
+  return SE_OK;
+}
+int se_linsys_apply_low(se_linsys* ls, int precision, const void* x_dev, float* y_dev) {
+  if (!ls || !x_dev || !y_dev) return fail(SE_ERR_ARG, "null argument");
+  if (precision != SE_PREC_BF16 && precision != SE_PREC_FP16)
+    return fail(SE_ERR_ARG, "precision must be SE_PREC_BF16 or SE_PREC_FP16");
+  CK(launch_op_apply_low(ls->op, precision == SE_PREC_FP16, x_dev, y_dev, g_stream));
   return SE_OK;
 }
 int se_linsys_diagonal(se_linsys* ls, double* d_dev) {

@@ -766,9 +766,6 @@ cudaError_t launch_residual(const OpDev& op, const double* x, const double* b, d
 }
 #undef SE_APPLY_CASE
 
-cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, cudaStream_t s) {
-  return launch_residual(op, x, nullptr, y, nullptr, 0, nullptr, s);
-}
 
 int residual_blocks(const OpDev& op) {
   return ((op.G[0] + kCgTileX - 1) / kCgTileX) * ((op.G[1] + kCgTileY - 1) / kCgTileY);

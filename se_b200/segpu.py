@@ -42,7 +42,7 @@ SE_ERR_DOMAIN = -7
 
 NORM_PRECONDITIONED, NORM_UNPRECONDITIONED, NORM_NATURAL = 0, 1, 2
 MODE_REFERENCE, MODE_EXACT = 0, 1
-PREC_FP64, PREC_MIXED, PREC_BF16 = 0, 1, 2
+PREC_FP64, PREC_MIXED, PREC_BF16, PREC_FP16 = 0, 1, 2, 3
 METHOD_CG, METHOD_FDM = 0, 1
 
 KSP_REASONS = {2: "CONVERGED_RTOL", 3: "CONVERGED_ATOL", -3: "DIVERGED_ITS",
@@ -130,7 +130,7 @@ SIGNATURES = {
                               ctypes.POINTER(SolveStats)],
     "se_linsys_solve_async": [_vp, ctypes.c_int],
     "se_linsys_solve_finish": [_vp, ctypes.POINTER(SolveStats)],
-    "se_linsys_apply": [_vp, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
+    "se_linsys_apply": [_vp, _vp, _vp], "se_linsys_apply_low": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
     "se_linsys_vec_size": [_vp, _I],
     "se_calc_time_step": [_vp, ctypes.c_double, _D],
     "se_field_error": [_vp, _vp, ctypes.c_int, ctypes.c_int, _D],
@@ -422,6 +422,10 @@ class _LinSys:
     def apply(self, x_ptr: int, y_ptr: int):
         """y = A x on device pointers of vecSize doubles."""
         _check(_lib.se_linsys_apply(self._h, _vp(x_ptr), _vp(y_ptr)))
+
+    def apply_low(self, x_ptr: int, y_ptr: int, precision: int = PREC_BF16):
+        """y (FP32) = A x for x of vecSize BF16 (or FP16) values; device pointers."""
+        _check(_lib.se_linsys_apply_low(self._h, int(precision), _vp(x_ptr), _vp(y_ptr)))
 
     def diagonal(self, d_ptr: int):
         _check(_lib.se_linsys_diagonal(self._h, _vp(d_ptr)))

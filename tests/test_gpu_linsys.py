@@ -74,6 +74,39 @@ def test_apply_matches_assembled_operator(segpu, oracle, case, quirk):
 
 
 @pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("prec", ["bf16", "fp16"])
+def test_low_precision_apply(segpu, oracle, case, prec):
+    """se_linsys_apply_low: x rounded to BF16/FP16, operator and arithmetic in
+    FP32. Against the oracle's FP64 CSR on the same rounded x, the error is
+    bounded by FP32 rounding of the coefficients and the sums: 1e-6 of the
+    row's absolute sum times max|x|."""
+    om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, CASES[case], -2.0, -1.0, 0.5,
+                                                     False)
+    n = ls.vecSize
+    dt = torch.bfloat16 if prec == "bf16" else torch.float16
+    x = torch.tensor(np.random.default_rng(10 + case).standard_normal(n), dtype=dt)
+    ref = A.matvec(x.double().numpy())
+    xd = x.cuda()
+    yd = torch.zeros(n, device="cuda", dtype=torch.float32)
+    ls.apply_low(xd.data_ptr(), yd.data_ptr(), segpu.PREC_BF16 if prec == "bf16" else segpu.PREC_FP16)
+    torch.cuda.synchronize()
+    rowptr, col, val, _ = A.arrays()
+    scale = np.array([np.abs(val[rowptr[i]:rowptr[i + 1]]).sum() for i in range(n)]) * float(x.abs().max())
+    assert (np.abs(yd.cpu().double().numpy() - ref) / scale).max() < 1e-6
+
+
+def test_option_checks(segpu):
+    m = segpu.Mesh("m", [4, 4], "legendre", 4, [0, 0], [1, 1], [True, True])
+    b = segpu.BCs(False, False, False, False, m)
+    u, r = segpu.Field("u", m, 1, b), segpu.Field("r", m, 1, b)
+    for bad in (dict(precision=segpu.PREC_FP16, method=segpu.METHOD_FDM),
+                dict(precision=segpu.PREC_BF16, method=segpu.METHOD_CG),
+                dict(method=7), dict(norm_type=5)):
+        with pytest.raises(segpu.SEError):
+            segpu.HelmholtzEqn(u, r, -1.0, -1.0, 1.0, 0, segpu.solver_opts(**bad))
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
 def test_helmholtz_solve_matches_oracle(segpu, oracle, case):
     om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, CASES[case], -3.0, -1.0, 1.0,
                                                      True, seed=case + 10)
