@@ -1811,7 +1811,7 @@ int se_linsys_solve_finish(se_linsys* ls, se_solve_stats* stats) {
 }
 int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev) {
   if (!ls || !x_dev || !y_dev) return fail(SE_ERR_ARG, "null argument");
-  CK(launch_op_apply(ls->op, x_dev, y_dev, g_stream));
+  CK(launch_op_apply(ls->op, x_dev, y_dev, ls->d_err, g_stream));
   return SE_OK;
 }
 int se_linsys_apply_low(se_linsys* ls, int precision, const void* x_dev, float* y_dev) {

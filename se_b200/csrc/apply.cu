@@ -26,8 +26,13 @@
 // Instantiated for FP64 (x, arithmetic and y in FP64) and for the reduced-
 // precision apply (x in BF16 or FP16, operator and arithmetic in FP32, y in
 // FP32).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+
+#include <cstdint>
+#include <cstring>
 
 #include "common.cuh"
 
@@ -63,7 +68,6 @@ struct ApplyOp {
   int G0, G1;
 };
 
-__device__ __forceinline__ double to_a(double v, double) { return v; }
 __device__ __forceinline__ float to_a(__nv_bfloat16 v, float) { return __bfloat162float(v); }
 __device__ __forceinline__ float to_a(__half v, float) { return __half2float(v); }
 
@@ -237,15 +241,626 @@ cudaError_t launch_tile(const OpDev& od, const TI* x, TO* y, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// FP64 apply on the FP64 tensor cores (mma.sync m16n8k8 f64), tiles staged
+// by TMA. The 1-D element products are small GEMMs: for element k of a
+// tile, the outputs a = 0..N-1 of 16 grid rows are
+//     Z (16 x N) = W (16 x 8KS) * B (8KS x N),
+// W the staged values of the element's window (its left neighbour's nodes
+// and its own: staged columns kN .. kN+2N, padded to 8KS), and
+//     B[j][a] = Kh[a][j-N] (own element, j >= N) + [a == 0] Kh[N][j] (left
+// element, j <= N), zero in the padding,
+// the same matrix for every element and tile, held in registers as MMA
+// fragments for the whole kernel. The column direction is the same product
+// on the transposed window. At a natural (non-periodic, non-Dirichlet) mesh
+// edge the missing neighbour's term at the edge vertex is subtracted.
+//
+// Persistent blocks take tiles in turn with two shared-memory stages: one
+// thread issues the next tile's 2-D TMA load (a UP x UH box of the unknown
+// array, its first column rounded down to an even unknown so that the copy
+// starts on a 16-byte boundary, out-of-range rows and columns zero-filled)
+// while the block computes the current tile. A tile whose staged vertices
+// wrap around a periodic direction, or any tile when the unknown array does
+// not meet TMA's alignment rules, is staged by ordinary loads instead. Every
+// wait on a stage's barrier is bounded; one that gives up sets
+// KERR_BARRIER_TIMEOUT in the error word and the tile's result is invalid.
+template <int N>
+struct MTile {
+  typedef ATile<N> T;
+  static constexpr int TEX = T::TEX, TEY = T::TEY, TW = T::TW, TH = T::TH;
+  static constexpr int KS = (2 * N + 1 + 7) / 8;  // k-steps of the window
+  static constexpr int NT = (N + 7) / 8;          // n-tiles of the outputs
+  static constexpr int RB = (TH + 15) / 16;       // 16-row blocks
+  static constexpr int CB = (TW + 15) / 16;       // 16-column blocks
+  static constexpr int cmax(int a, int b) { return a > b ? a : b; }
+  // staged rectangle the windows read (the real one plus padding)
+  static constexpr int UW = cmax(cmax(T::UW, (TEX - 1) * N + 8 * KS), CB * 16 + N);
+  static constexpr int UH = cmax(cmax(T::UH, (TEY - 1) * N + 8 * KS), RB * 16 + N);
+  // box width = row pitch: one spare column for the alignment shift, 4 mod 16
+  static constexpr int UP = ((UW + 1 + 11) / 16) * 16 + 4;
+  static constexpr int OP = TW + 1;
+  static constexpr int NU = ((UH * UP * 8 + 127) / 128) * 16;  // doubles per stage (128-byte multiple)
+  static constexpr unsigned BOX_BYTES = (unsigned)(UP * UH * 8);
+  static constexpr int NO = TH * OP;
+  static constexpr size_t SMEM = 128 + 16 + sizeof(double) * (size_t)(2 * NU + NO + TW + TH);
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for a barrier phase, at most 2^20 polls.
+__device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned* err) {
+  for (int it = 0; it < (1 << 20); it++)
+    if (mbar_try_wait(bar, parity)) return;
+  if (err) atomicOr(err, (unsigned)KERR_BARRIER_TIMEOUT);
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+      "%3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double a2, double a3,
+                                     double b0, double b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
+}
+
+// Window matrix entry B[j][a].
+template <int N>
+__device__ __forceinline__ double bwin(const ApplyOp<double>& op, int j, int a) {
+  constexpr int n = N + 1;
+  if (a >= N || j > 2 * N) return 0.0;
+  double v = 0.0;
+  if (j >= N) v += op.Kh[a * n + (j - N)];
+  if (a == 0 && j <= N) v += op.Kh[N * n + j];
+  return v;
+}
+
+// Tile t's staged origin in unknown coordinates, and whether TMA can load it.
+template <int N>
+__device__ __forceinline__ bool tile_tma(const ApplyOp<double>& op, int tma, int tiles_x, int t,
+                                         int& xs, int& ys) {
+  typedef MTile<N> T;
+  const int gx0 = (t % tiles_x) * T::TW, gy0 = (t / tiles_x) * T::TH;
+  xs = gx0 - N - op.dx.lo;
+  ys = gy0 - N - op.dy.lo;
+  if (!tma) return false;
+  if (op.dx.periodic && (xs < 0 || xs + ATile<N>::UW > op.G0)) return false;
+  if (op.dy.periodic && (ys < 0 || ys + ATile<N>::UH > op.G1)) return false;
+  return true;
+}
+
+template <int N>
+__global__ void __launch_bounds__(kThreads) apply_mma_kernel(const __grid_constant__ CUtensorMap map,
+                                                             const ApplyOp<double> op,
+                                                             const double* __restrict__ x,
+                                                             double* __restrict__ y, int tiles_x,
+                                                             int ntiles, int tma,
+                                                             unsigned* err) {
+  typedef MTile<N> T;
+  constexpr int n = N + 1;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base =
+      smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);  // 128-byte aligned stages
+  double* Ubuf = reinterpret_cast<double*>(base);                // [2][NU]
+  double* O = Ubuf + 2 * T::NU;
+  double* Wx = O + T::NO;
+  double* Wy = Wx + T::TW;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(Wy + T::TH);  // [2]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+  if (blockIdx.x >= ntiles) return;
+
+  // B fragments (kept for the whole kernel)
+  double bf[T::KS][T::NT][2];
+#pragma unroll
+  for (int ks = 0; ks < T::KS; ks++)
+#pragma unroll
+    for (int nt = 0; nt < T::NT; nt++) {
+      bf[ks][nt][0] = bwin<N>(op, ks * 8 + tq, nt * 8 + g);
+      bf[ks][nt][1] = bwin<N>(op, ks * 8 + tq + 4, nt * 8 + g);
+    }
+
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int xs, ys;
+    if (tile_tma<N>(op, tma, tiles_x, blockIdx.x, xs, ys)) {
+      mbar_expect_tx(&bar[0], T::BOX_BYTES);
+      tma_load_2d(Ubuf, &map, xs & ~1, ys, &bar[0]);
+    }
+  }
+
+  const bool nat_x = !op.dx.periodic, nat_y = !op.dy.periodic;
+  const int lastx = op.dx.nV - 1, lasty = op.dy.nV - 1;
+  unsigned phase = 0;  // bit s: parity of stage s's next completion
+  int i = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
+    const int s = i & 1;
+    double* U = Ubuf + s * T::NU;
+    const int gx0 = (t % tiles_x) * T::TW, gy0 = (t / tiles_x) * T::TH;
+    const int ex0 = gx0 / N, ey0 = gy0 / N;
+    int xs, ys, off = 0;
+    if (tile_tma<N>(op, tma, tiles_x, t, xs, ys)) {
+      mbar_wait_bounded(&bar[s], (phase >> s) & 1u, err);
+      phase ^= 1u << s;
+      off = xs & 1;
+    } else {
+      // ordinary loads: warp w takes staged rows w, w + 8, ...
+      typedef ATile<N> R;
+      const int vx0 = gx0 - N, vy0 = gy0 - N;
+      for (int j = warp; j < T::UH; j += kThreads / 32)
+        for (int c = lane; c < T::UP; c += 32) {
+          double v = 0.0;
+          if (j < R::UH && c < R::UW) {
+            const int ux = unk(op.dx, vx0 + c), uy = unk(op.dy, vy0 + j);
+            if (ux >= 0 && uy >= 0) v = x[(size_t)uy * op.G0 + ux];
+          }
+          U[j * T::UP + c] = v;
+        }
+    }
+    for (int k = threadIdx.x; k < T::TW + T::TH; k += kThreads) {
+      if (k < T::TW) {
+        const int kx = k / N;
+        Wx[k] = wsum<N>(op.dx, op.w, ex0 + kx, k - kx * N);
+      } else {
+        const int r = k - T::TW, ky = r / N;
+        Wy[r] = wsum<N>(op.dy, op.w, ey0 + ky, r - ky * N);
+      }
+    }
+    __syncthreads();
+
+    // prefetch the next tile into the other stage (last read one iteration ago)
+    const int tn = t + gridDim.x;
+    if (threadIdx.x == 0 && tn < ntiles) {
+      int xn, yn;
+      if (tile_tma<N>(op, tma, tiles_x, tn, xn, yn)) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&bar[s ^ 1], T::BOX_BYTES);
+        tma_load_2d(Ubuf + (s ^ 1) * T::NU, &map, xn & ~1, yn, &bar[s ^ 1]);
+      }
+    }
+
+    const double* Us = U + off;  // staged (row j, column c) at Us[j * UP + c]
+
+    // rows: units (16-row block rb, element k)
+    for (int u = warp; u < T::RB * T::TEX; u += kThreads / 32) {
+      const int rb = (u % T::RB) * 16, k = u / T::RB;
+      double c[T::NT][4];
+#pragma unroll
+      for (int nt = 0; nt < T::NT; nt++) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.0;
+      const double* w0 = Us + (rb + g + N) * T::UP + k * N;
+#pragma unroll
+      for (int ks = 0; ks < T::KS; ks++) {
+        const double a0 = w0[ks * 8 + tq], a1 = w0[8 * T::UP + ks * 8 + tq];
+        const double a2 = w0[ks * 8 + tq + 4], a3 = w0[8 * T::UP + ks * 8 + tq + 4];
+#pragma unroll
+        for (int nt = 0; nt < T::NT; nt++) dmma(c[nt], a0, a1, a2, a3, bf[ks][nt][0], bf[ks][nt][1]);
+      }
+#pragma unroll
+      for (int nt = 0; nt < T::NT; nt++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int r = rb + g + (q >> 1) * 8, a = nt * 8 + 2 * tq + (q & 1);
+          if (r >= T::TH || a >= N) continue;
+          const int cc = k * N + a;
+          const double uval = Us[(r + N) * T::UP + cc + N];
+          double z = c[nt][q];
+          if (nat_x && a == 0) {
+            const int gx = gx0 + cc;
+            if (gx == 0) z = fma(-op.Kh[N * n + N], uval, z);  // no left element
+            if (gx == lastx) z = fma(-op.Kh[0], uval, z);      // no own element
+          }
+          const double wy = Wy[r];
+          O[r * T::OP + cc] = fma(op.alpha * Wx[cc] * wy, uval, op.bx * wy * z);
+        }
+    }
+    __syncthreads();
+
+    // columns: units (16-column block cb, element row k); A = window^T
+    for (int u = warp; u < T::CB * T::TEY; u += kThreads / 32) {
+      const int cb = (u % T::CB) * 16, k = u / T::CB;
+      double c[T::NT][4];
+#pragma unroll
+      for (int nt = 0; nt < T::NT; nt++) c[nt][0] = c[nt][1] = c[nt][2] = c[nt][3] = 0.0;
+      const double* w0 = Us + (k * N) * T::UP + cb + g + N;
+#pragma unroll
+      for (int ks = 0; ks < T::KS; ks++) {
+        const double a0 = w0[(ks * 8 + tq) * T::UP], a1 = w0[(ks * 8 + tq) * T::UP + 8];
+        const double a2 = w0[(ks * 8 + tq + 4) * T::UP], a3 = w0[(ks * 8 + tq + 4) * T::UP + 8];
+#pragma unroll
+        for (int nt = 0; nt < T::NT; nt++) dmma(c[nt], a0, a1, a2, a3, bf[ks][nt][0], bf[ks][nt][1]);
+      }
+#pragma unroll
+      for (int nt = 0; nt < T::NT; nt++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const int cc = cb + g + (q >> 1) * 8, a = nt * 8 + 2 * tq + (q & 1);
+          if (cc >= T::TW || a >= N) continue;
+          const int r = k * N + a;
+          double z = c[nt][q];
+          if (nat_y && a == 0) {
+            const int gy = gy0 + r;
+            const double uval = Us[(r + N) * T::UP + cc + N];
+            if (gy == 0) z = fma(-op.Kh[N * n + N], uval, z);
+            if (gy == lasty) z = fma(-op.Kh[0], uval, z);
+          }
+          const int gx = gx0 + cc, gy = gy0 + r;
+          if (gx >= op.dx.lo && gx < op.dx.hi && gy >= op.dy.lo && gy < op.dy.hi)
+            y[(size_t)(gy - op.dy.lo) * op.G0 + (gx - op.dx.lo)] =
+                fma(op.by * Wx[cc], z, O[r * T::OP + cc]);
+        }
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Order N = 8: both directions in the same MMA fragments. A warp task is two
+// vertically stacked elements (16 grid rows x 8 columns of outputs):
+//   x: Zx (16 x 8) = W (16 rows x 24 window columns) * B (24 x 8), B the
+//      window matrix above, held as fragments;
+//   y: Zy (16 x 8) = A (16 x 32) * V (32 window rows x 8 columns), with the
+//      constant A = [[B^T 0]; [0 B^T]] (lower element: window rows 0..23,
+//      upper element: rows 8..31), also held as fragments.
+// Both accumulators have the same layout (row g / g+8, columns 2t, 2t+1), so
+// y = alpha wx wy u + beta_x wy Zx + beta_y wx Zy is formed in registers and
+// stored to global memory: no output buffer in shared memory. A warp takes
+// three consecutive elements of one 16-row block, sliding the x window's
+// fragments from one element to the next. Tiles are 12 x 4 elements, staged
+// by TMA as above.
+struct N8 {
+  static constexpr int N = 8, TEX = 12, TEY = 4, TW = 96, TH = 32;
+  static constexpr int UW = (TEX - 1) * N + 24;  // 112 staged columns read
+  static constexpr int UH = TH + 16;             // 48 staged rows read
+  static constexpr int UP = ((UW + 1 + 11) / 16) * 16 + 4;  // 116: shift column, 4 mod 16
+  static constexpr int NU = ((UH * UP * 8 + 127) / 128) * 16;
+  static constexpr unsigned BOX_BYTES = (unsigned)(UP * UH * 8);
+  static constexpr int REAL_UW = TW + N + 1, REAL_UH = TH + N + 1;  // staged vertices
+  static constexpr int GROUP = 3;                                   // elements per warp task
+  static constexpr size_t SMEM = 128 + 16 + sizeof(double) * (size_t)(2 * NU);
+};
+
+__device__ __forceinline__ bool tile_tma8(const ApplyOp<double>& op, int tma, int tiles_x, int t,
+                                          int& xs, int& ys) {
+  const int gx0 = (t % tiles_x) * N8::TW, gy0 = (t / tiles_x) * N8::TH;
+  xs = gx0 - N8::N - op.dx.lo;
+  ys = gy0 - N8::N - op.dy.lo;
+  if (!tma) return false;
+  if (op.dx.periodic && (xs < 0 || xs + N8::REAL_UW > op.G0)) return false;
+  if (op.dy.periodic && (ys < 0 || ys + N8::REAL_UH > op.G1)) return false;
+  return true;
+}
+
+// Assembled 1-D weight of node a of element e (e may lie outside the mesh
+// for vertices that are not outputs).
+__device__ __forceinline__ double wnode(const Dir& d, const double* w, int e, int a) {
+  if (a != 0) return w[a];
+  double s = 0.0;
+  if (e < d.nE) s += w[0];
+  if (e > 0 || d.periodic) s += w[8];
+  return s;
+}
+
+__global__ void __launch_bounds__(kThreads, 2) apply_n8_kernel(const __grid_constant__ CUtensorMap map,
+                                                               const ApplyOp<double> op,
+                                                               const double* __restrict__ x,
+                                                               double* __restrict__ y, int tiles_x,
+                                                               int ntiles, int tma, unsigned* err) {
+  constexpr int N = 8, n = 9;
+  typedef N8 T;
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);
+  double* Ubuf = reinterpret_cast<double*>(base);  // [2][NU]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(Ubuf + 2 * T::NU);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, tq = lane & 3;
+  if (blockIdx.x >= ntiles) return;
+
+  // x: B fragments (3 k-steps); y: A fragments of [[B^T 0]; [0 B^T]] (4 k-steps)
+  double bx[3][2], ay[4][4];
+#pragma unroll
+  for (int ks = 0; ks < 3; ks++) {
+    bx[ks][0] = bwin<N>(op, ks * 8 + tq, g);
+    bx[ks][1] = bwin<N>(op, ks * 8 + tq + 4, g);
+  }
+#pragma unroll
+  for (int ks = 0; ks < 4; ks++) {
+    const int k0 = ks * 8 + tq, k1 = k0 + 4;
+    ay[ks][0] = k0 < 24 ? bwin<N>(op, k0, g) : 0.0;           // (m = g,     k0)
+    ay[ks][1] = k0 >= 8 ? bwin<N>(op, k0 - 8, g) : 0.0;       // (m = g + 8, k0)
+    ay[ks][2] = k1 < 24 ? bwin<N>(op, k1, g) : 0.0;           // (m = g,     k1)
+    ay[ks][3] = k1 >= 8 ? bwin<N>(op, k1 - 8, g) : 0.0;       // (m = g + 8, k1)
+  }
+
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int xs, ys;
+    if (tile_tma8(op, tma, tiles_x, blockIdx.x, xs, ys)) {
+      mbar_expect_tx(&bar[0], T::BOX_BYTES);
+      tma_load_2d(Ubuf, &map, xs & ~1, ys, &bar[0]);
+    }
+  }
+
+  const bool nat_x = !op.dx.periodic, nat_y = !op.dy.periodic;
+  const int lastx = op.dx.nV - 1, lasty = op.dy.nV - 1;
+  const int rb = (warp & 1) * 16;              // the warp's 16-row block
+  const int e0 = (warp >> 1) * T::GROUP;       // its first element column
+  unsigned phase = 0;
+  int i = 0;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
+    const int s = i & 1;
+    double* U = Ubuf + s * T::NU;
+    const int gx0 = (t % tiles_x) * T::TW, gy0 = (t / tiles_x) * T::TH;
+    int xs, ys, off = 0;
+    if (tile_tma8(op, tma, tiles_x, t, xs, ys)) {
+      mbar_wait_bounded(&bar[s], (phase >> s) & 1u, err);
+      phase ^= 1u << s;
+      off = xs & 1;
+    } else {
+      const int vx0 = gx0 - N, vy0 = gy0 - N;
+      for (int j = warp; j < T::UH; j += kThreads / 32)
+        for (int c = lane; c < T::UP; c += 32) {
+          double v = 0.0;
+          if (j < T::REAL_UH && c < T::REAL_UW) {
+            const int ux = unk(op.dx, vx0 + c), uy = unk(op.dy, vy0 + j);
+            if (ux >= 0 && uy >= 0) v = x[(size_t)uy * op.G0 + ux];
+          }
+          U[j * T::UP + c] = v;
+        }
+      __syncthreads();
+    }
+
+    // prefetch the next tile into the other stage (last read one iteration ago)
+    const int tn = t + gridDim.x;
+    if (threadIdx.x == 0 && tn < ntiles) {
+      int xn, yn;
+      if (tile_tma8(op, tma, tiles_x, tn, xn, yn)) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&bar[s ^ 1], T::BOX_BYTES);
+        tma_load_2d(Ubuf + (s ^ 1) * T::NU, &map, xn & ~1, yn, &bar[s ^ 1]);
+      }
+    }
+
+    const double* Us = U + off;  // staged (row j, column c) at Us[j * UP + c]
+    const int ey0 = gy0 / N + rb / N;  // element row of the warp's lower element
+    // x window fragments of k-steps e0 .. e0 + GROUP + 1 (sliding)
+    double af[3][4];
+    const double* xr = Us + (rb + N + g) * T::UP + e0 * N + tq;
+#pragma unroll
+    for (int ks = 0; ks < 2; ks++) {
+      af[ks][0] = xr[ks * 8];
+      af[ks][1] = xr[8 * T::UP + ks * 8];
+      af[ks][2] = xr[ks * 8 + 4];
+      af[ks][3] = xr[8 * T::UP + ks * 8 + 4];
+    }
+#pragma unroll
+    for (int el = 0; el < T::GROUP; el++) {
+      const int k = e0 + el;  // element column within the tile
+      {
+        const int ks = el + 2;
+        af[2][0] = xr[ks * 8];
+        af[2][1] = xr[8 * T::UP + ks * 8];
+        af[2][2] = xr[ks * 8 + 4];
+        af[2][3] = xr[8 * T::UP + ks * 8 + 4];
+      }
+      double cx[4] = {0.0, 0.0, 0.0, 0.0}, cy[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int ks = 0; ks < 3; ks++) dmma(cx, af[ks][0], af[ks][1], af[ks][2], af[ks][3], bx[ks][0], bx[ks][1]);
+      // y: V[k][n] = staged (row rb + k, column k*N + N + n)
+      const double* yc = Us + (rb + tq) * T::UP + k * N + N + g;
+#pragma unroll
+      for (int ks = 0; ks < 4; ks++)
+        dmma(cy, ay[ks][0], ay[ks][1], ay[ks][2], ay[ks][3], yc[(ks * 8) * T::UP],
+             yc[(ks * 8 + 4) * T::UP]);
+#pragma unroll
+      for (int af_s = 0; af_s < 2; af_s++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) af[af_s][q] = af[af_s + 1][q];
+
+      // outputs: rows rb + g (+8), columns k*N + 2tq (+1)
+      const int cx0 = k * N + 2 * tq;
+      const int exk = gx0 / N + k;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int r = rb + g + 8 * h;
+        const int gy = gy0 + r;
+        if (gy < op.dy.lo || gy >= op.dy.hi) continue;
+        const int ay_node = g;  // r mod N
+        const double wy = wnode(op.dy, op.w, ey0 + h, ay_node);
+        const double* up = Us + (r + N) * T::UP + cx0 + N;  // may be 8-byte aligned only
+        const double u0 = up[0], u1 = up[1];
+#pragma unroll
+        for (int qq = 0; qq < 2; qq++) {
+          const int cc = cx0 + qq, gx = gx0 + cc;
+          if (gx < op.dx.lo || gx >= op.dx.hi) continue;
+          const double uval = qq ? u1 : u0;
+          double zx = cx[2 * h + qq], zy = cy[2 * h + qq];
+          if (nat_x && cc % N == 0) {
+            if (gx == 0) zx = fma(-op.Kh[N * n + N], uval, zx);
+            if (gx == lastx) zx = fma(-op.Kh[0], uval, zx);
+          }
+          if (nat_y && ay_node == 0) {
+            if (gy == 0) zy = fma(-op.Kh[N * n + N], uval, zy);
+            if (gy == lasty) zy = fma(-op.Kh[0], uval, zy);
+          }
+          const double wx = wnode(op.dx, op.w, exk, 2 * tq + qq);
+          double v = op.alpha * wx * wy * uval;
+          v = fma(op.bx * wy, zx, v);
+          v = fma(op.by * wx, zy, v);
+          y[(size_t)(gy - op.dy.lo) * op.G0 + (gx - op.dx.lo)] = v;
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+template <int N>
+cudaError_t launch_mma(const OpDev& od, const double* x, double* y, unsigned* err, cudaStream_t s) {
+  typedef MTile<N> T;
+  ApplyOp<double> op;
+  for (int k = 0; k < (N + 1) * (N + 1); k++) op.Kh[k] = od.Kh[k];
+  for (int k = 0; k <= N; k++) op.w[k] = od.w[k];
+  op.alpha = od.alpha;
+  op.bx = od.beta[0];
+  op.by = od.beta[1];
+  op.dx = od.d[0];
+  op.dy = od.d[1];
+  op.G0 = od.G[0];
+  op.G1 = od.G[1];
+  static int per_sm[64] = {};  // resident blocks per SM, per instantiation and device
+  static int sms[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!per_sm[dev]) {
+    e = cudaFuncSetAttribute(apply_mma_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)T::SMEM);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    int b = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, apply_mma_kernel<N>, kThreads, T::SMEM);
+    if (e != cudaSuccess) return e;
+    per_sm[dev] = b > 0 ? b : 1;
+  }
+  // the tensor map of the unknown array; TMA needs a 16-byte aligned base
+  // and a row pitch that is a multiple of 16 bytes
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  int tma = 0;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (enc && (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (od.G[0] % 2) == 0) {
+    const cuuint64_t dims[2] = {(cuuint64_t)od.G[0], (cuuint64_t)od.G[1]};
+    const cuuint64_t strides[1] = {(cuuint64_t)od.G[0] * sizeof(double)};
+    const cuuint32_t box[2] = {(cuuint32_t)T::UP, (cuuint32_t)T::UH};
+    const cuuint32_t estr[2] = {1, 1};
+    tma = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(x), dims, strides, box,
+              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  }
+  const int tiles_x = (od.d[0].hi + T::TW - 1) / T::TW;
+  const int tiles_y = (od.d[1].hi + T::TH - 1) / T::TH;
+  const int ntiles = tiles_x * tiles_y;
+  const int grid = ntiles < per_sm[dev] * sms[dev] ? ntiles : per_sm[dev] * sms[dev];
+  apply_mma_kernel<N><<<grid, kThreads, T::SMEM, s>>>(map, op, x, y, tiles_x, ntiles, tma, err);
+  return cudaGetLastError();
+}
+
+// Launch of the order-8 kernel (same set-up as launch_mma).
+cudaError_t launch_n8(const OpDev& od, const double* x, double* y, unsigned* err, cudaStream_t s) {
+  typedef N8 T;
+  ApplyOp<double> op;
+  for (int k = 0; k < 81; k++) op.Kh[k] = od.Kh[k];
+  for (int k = 0; k <= 8; k++) op.w[k] = od.w[k];
+  op.alpha = od.alpha;
+  op.bx = od.beta[0];
+  op.by = od.beta[1];
+  op.dx = od.d[0];
+  op.dy = od.d[1];
+  op.G0 = od.G[0];
+  op.G1 = od.G[1];
+  static int per_sm[64] = {};
+  static int sms[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!per_sm[dev]) {
+    e = cudaFuncSetAttribute(apply_n8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    int b = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, apply_n8_kernel, kThreads, T::SMEM);
+    if (e != cudaSuccess) return e;
+    per_sm[dev] = b > 0 ? b : 1;
+  }
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  int tma = 0;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (enc && (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (od.G[0] % 2) == 0) {
+    const cuuint64_t dims[2] = {(cuuint64_t)od.G[0], (cuuint64_t)od.G[1]};
+    const cuuint64_t strides[1] = {(cuuint64_t)od.G[0] * sizeof(double)};
+    const cuuint32_t box[2] = {(cuuint32_t)T::UP, (cuuint32_t)T::UH};
+    const cuuint32_t estr[2] = {1, 1};
+    tma = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(x), dims, strides, box,
+              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  }
+  const int tiles_x = (od.d[0].hi + T::TW - 1) / T::TW;
+  const int tiles_y = (od.d[1].hi + T::TH - 1) / T::TH;
+  const int ntiles = tiles_x * tiles_y;
+  const int grid = ntiles < per_sm[dev] * sms[dev] ? ntiles : per_sm[dev] * sms[dev];
+  apply_n8_kernel<<<grid, kThreads, T::SMEM, s>>>(map, op, x, y, tiles_x, ntiles, tma, err);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 #define SE_APPLY_N(n) \
   case n:             \
-    return launch_tile<n, double, double, double>(op, x, y, s);
-cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, cudaStream_t s) {
+    return launch_mma<n>(op, x, y, err, s);
+cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, unsigned* err,
+                            cudaStream_t s) {
   switch (op.d[0].N) {
     SE_APPLY_N(2) SE_APPLY_N(3) SE_APPLY_N(4) SE_APPLY_N(5) SE_APPLY_N(6) SE_APPLY_N(7)
-    SE_APPLY_N(8) SE_APPLY_N(9) SE_APPLY_N(10) SE_APPLY_N(11) SE_APPLY_N(12)
+    SE_APPLY_N(9) SE_APPLY_N(10) SE_APPLY_N(11) SE_APPLY_N(12)
+    case 8:
+      return launch_n8(op, x, y, err, s);
     default:
       return cudaErrorInvalidValue;
   }

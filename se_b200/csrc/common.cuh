@@ -100,7 +100,9 @@ cudaError_t launch_max_speed_sq(int nv, const double* vel, double* scratch, int 
 // Linear-system pieces.
 // y = A x, element-structured (apply.cu); the reduced-precision form reads
 // x in FP16 (fp16 != 0) or BF16 and computes and writes FP32.
-cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, cudaStream_t s);
+// err (nullable): device error word for KERR_BARRIER_TIMEOUT.
+cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, unsigned* err,
+                            cudaStream_t s);
 cudaError_t launch_op_apply_low(const OpDev& op, int fp16, const void* x, float* y, cudaStream_t s);
 // r = b - A x with per-block partial sums (partial[2*block]: (w r)^2 or, when
 // natural, r w r; and r^2) over residual_blocks(op) blocks (cg.cu).

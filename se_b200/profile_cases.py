@@ -1,14 +1,16 @@
 """Single-kernel cases for profiling the library with ncu.
 
-    python -m se_b200.profile_cases apply   # operator apply, 64x64 elements, p=8
-    python -m se_b200.profile_cases sl      # first-order SL advection, same mesh
-    python -m se_b200.profile_cases cg      # persistent Jacobi-PCG solve, same mesh
-    python -m se_b200.profile_cases fdm     # one FDM solve (a CUDA graph)
+    python -m se_b200.profile_cases apply [ne]       # FP64 operator apply
+    python -m se_b200.profile_cases apply_bf16 [ne]  # BF16-in, FP32 operator apply
+    python -m se_b200.profile_cases sl [ne]          # first-order SL advection
+    python -m se_b200.profile_cases cg [ne]          # persistent Jacobi-PCG solve
+    python -m se_b200.profile_cases fdm [ne]         # one FDM solve (a CUDA graph)
 
-Each case builds the bench's 64x64-element, p=8, doubly periodic mesh and
-fields and launches the kernel a few times directly (not inside a graph), so
-that ncu can capture individual launches. Prints one line with the mean
-device time of the launches (CUDA events).
+Each case builds an ne x ne element (default 64, the bench's mesh), p=8,
+doubly periodic mesh and the bench's fields and launches the kernel a few
+times directly (not inside a graph), so that ncu can capture individual
+launches. Prints one line with the mean device time of the launches (CUDA
+events).
 """
 from __future__ import annotations
 
@@ -17,14 +19,14 @@ import sys
 import numpy as np
 
 
-def main(case: str, reps: int = 3) -> None:
+def main(case: str, ne: int = 64, reps: int = 3) -> None:
     import torch
 
     from . import segpu as S
 
     S.load_library()
     torch.cuda.init()
-    nx, p = 64, 8
+    nx, p = ne, 8
     m = S.Mesh("m", [nx, nx], "legendre", p, [0.0, 0.0], [1.0, 1.0], [True, True])
     X = m.verts
     x, y = X[:, 0], X[:, 1]
@@ -43,17 +45,21 @@ def main(case: str, reps: int = 3) -> None:
             a.record()
             adv.Advect(dt)
             b.record()
-    elif case in ("apply", "cg", "fdm"):
+    elif case in ("apply", "apply_bf16", "cg", "fdm"):
         method = S.METHOD_FDM if case == "fdm" else S.METHOD_CG
         h = S.HelmholtzEqn(u, phi, -1.0, -1.0, 1.0, 0,
                            S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=method))
         n = h.vecSize
         xin = torch.randn(n, dtype=torch.float64, device="cuda")
         yout = torch.empty_like(xin)
+        xb = xin.float().to(torch.bfloat16)
+        yf = torch.empty(n, dtype=torch.float32, device="cuda")
         for a, b in ev:
             a.record()
             if case == "apply":
                 h.apply(xin.data_ptr(), yout.data_ptr())
+            elif case == "apply_bf16":
+                h.apply_low(xb.data_ptr(), yf.data_ptr(), S.PREC_BF16)
             else:
                 h.Solve("helm_")
             b.record()
@@ -65,4 +71,4 @@ def main(case: str, reps: int = 3) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "apply")
+    main(sys.argv[1] if len(sys.argv) > 1 else "apply", int(sys.argv[2]) if len(sys.argv) > 2 else 64)
