@@ -256,6 +256,27 @@ def run_gpu(args, rank, world):
             e1.record(stream)
             torch.cuda.synchronize()
             sl_ms.append(e0.elapsed_time(e1))
+        log("FDM product kernel timing")
+        # the FDM transform x = A^{-1} r of the bench's system alone: four
+        # FP64 tensor-core product launches (fdm_dgemm_kernel, M = N = K = 512),
+        # CUDA events on the library's stream, L2 flushed before each call
+        helm = S.HelmholtzEqn(u, adv.fieldSL, -LAMBDA, -1.0, 1.0, 0,
+                              S.solver_opts(rtol=RTOL, mode=S.MODE_EXACT, method=S.METHOD_FDM))
+        ngf = helm.vecSize
+        rr = torch.randn(ngf, dtype=torch.float64, device="cuda")
+        xx = torch.empty_like(rr)
+        for _ in range(3):
+            helm.fdm_apply(rr.data_ptr(), xx.data_ptr())
+        fdm_ms = []
+        for _ in range(max(5, min(args.steps, 20))):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            helm.fdm_apply(rr.data_ptr(), xx.data_ptr())
+            e1.record(stream)
+            torch.cuda.synchronize()
+            fdm_ms.append(e0.elapsed_time(e1))
+        del helm, rr, xx
         log("FP64 DGEMM reference")
         # FP64 peak of this GPU: a large cuBLAS DGEMM (denominator for the
         # FP64-bound SL kernel)
@@ -279,14 +300,16 @@ def run_gpu(args, rank, world):
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         step_ms, e2e = float(t[0]), float(t[1])
     return {"step_ms": step_ms, "e2e_ms": e2e, "ng": ng, "nv": m.nVertsTotal, "clocks": clock,
-            "variants": results, "sl_ms": float(np.median(sl_ms)), "fp64_tflops": fp64_tflops}
+            "variants": results, "sl_ms": float(np.median(sl_ms)), "fp64_tflops": fp64_tflops,
+            "fdm_apply_ms": float(np.median(fdm_ms)), "gx": int(round(ng ** 0.5))}
 
 
-# Kernels of the library launched per headline step: SL advection, RHS
-# assembly, per refinement step (2 here) the spectral division, operator
-# apply, residual, norm partials and final, and the field update -- cuBLAS
-# GEMMs not counted (library kernels).
-GPU_LAUNCHES_PER_STEP = 1 + 1 + 2 * 5 + 2 + 1
+# Kernels of the library launched per headline step: SL advection; in the
+# FDM solve graph the right-hand side assembly, the initial norm (partials and
+# final) and test, per refinement step (2 here) four product kernels, the
+# residual with norm partials, the norm final and the test, then the field
+# update.
+GPU_LAUNCHES_PER_STEP = 1 + (1 + 2 + 1) + 2 * (4 + 1 + 1 + 1) + 1
 
 
 # Algorithmic bytes and flops of one first-order SL vertex update at p=8:
@@ -300,13 +323,35 @@ SL_FLOPS_PER_VERTEX = (2 * 9 * 5 + 2 * 81 * 2 + 2 * 9 * 2) + (2 * 9 * 5 + 2 * 81
 # DRAM traffic of one SL launch (dram__bytes_read.sum + dram__bytes_write.sum)
 # from the ncu capture summarised in profiles/sl_first_kernel_64x64_p8.md.
 SL_TRAFFIC_BYTES = 6.358016e6
+# DRAM traffic of one fdm_dgemm_kernel launch (M = N = K = 512), from the ncu
+# capture summarised in profiles/fdm_dgemm_kernel_512.md (cold caches: read 4.21 MB, write 0).
+FDM_GEMM_TRAFFIC_BYTES = 4.211968e6
 
 
 def roofline(r):
-    """Roofline of the SL advection kernel, the largest of this library's
-    kernels in the step: achieved = algorithmic bytes per launch / measured
-    launch time, against the measured HBM copy bandwidth; the kernel is bound
-    by its FP64 gathers, so its FP64 rate against a measured DGEMM is beside it."""
+    """Roofline of the step's dominant kernel, the FDM product kernel
+    (fdm_dgemm_kernel, four launches of M = N = K = 512 per refinement step):
+    achieved = algorithmic FLOPs per launch (2 M N K) / mean launch time,
+    the launch time measured live as one FDM transform (exactly four such
+    launches) / 4, against the FP64 DGEMM rate measured in the same run
+    (MEASURED_PEAKS.json holds no FP64 figure). DRAM traffic per launch from
+    the ncu capture summarised in profiles/fdm_dgemm_kernel_512.md."""
+    g = r["gx"]
+    flops = 2.0 * g ** 3
+    launch_ms = r["fdm_apply_ms"] / 4
+    achieved = flops / (launch_ms * 1e-3) / 1e12
+    return {"kernel": "fdm_dgemm_kernel (FP64 DMMA, 32x32 tiles, M=N=K=512)", "bound": "tensor",
+            "achieved": achieved, "peak": r["fp64_tflops"], "unit": "TFLOP/s",
+            "frac": achieved / r["fp64_tflops"],
+            "peak_source": "FP64 DGEMM (torch.matmul float64 8192^3) measured in this run",
+            "launch_ms": launch_ms, "algorithmic_flops_per_launch": flops,
+            "algorithmic_bytes_per_launch": 3 * 8 * g * g, "traffic": FDM_GEMM_TRAFFIC_BYTES}
+
+
+def sl_roofline(r):
+    """The SL advection kernel: algorithmic bytes per launch / measured
+    launch time against the measured HBM copy bandwidth, and its FP64 rate
+    against the measured DGEMM (the kernel is bound by its FP64 gathers)."""
     peaks = read_peaks()
     nv = r["nv"]
     t = r["sl_ms"] * 1e-3
@@ -694,7 +739,7 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
         "config": config({"solver": "fast diagonalization, FP64, refined to rtol 1e-10",
                           "parallelism": f"replicas{world}"}),
-        "roofline": roofline(r), "cpu_baseline": cpu,
+        "roofline": roofline(r), "sl_roofline": sl_roofline(r), "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * r["nv"],
                 "d2h_bytes_per_step": 8 * r["nv"], "ms_per_step": r["e2e_ms"]},
         "gpu_launches": GPU_LAUNCHES_PER_STEP * args.steps,

@@ -225,6 +225,13 @@ int se_linsys_solve_async(se_linsys* ls, int remove_null_space);
 int se_linsys_solve_finish(se_linsys* ls, se_solve_stats* stats);
 /* y = A x on vector unknowns (device pointers, vec_size entries each). */
 int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev);
+/* No counterpart in the reference: x = A^{-1} r by the fast-diagonalization
+ * transforms in FP64 (four tensor-core products; exact up to rounding, the
+ * null mode of a singular operator set to zero), on the calling thread's
+ * stream; device pointers, vec_size entries each, not aliased. A
+ * preconditioner for callers that run their own Krylov loop. The first call
+ * on a system computes its 1-D eigendecompositions (host work, allocation). */
+int se_linsys_fdm_apply(se_linsys* ls, const double* r_dev, double* x_dev);
 /* No counterpart in the reference: y = A x with x in BF16 or FP16
  * (precision SE_PREC_BF16 / SE_PREC_FP16) and y in FP32, the operator and
  * the arithmetic in FP32 (device pointers, vec_size entries each). */

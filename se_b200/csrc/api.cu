@@ -1814,6 +1814,12 @@ int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev) {
   CK(launch_op_apply(ls->op, x_dev, y_dev, ls->d_err, g_stream));
   return SE_OK;
 }
+int se_linsys_fdm_apply(se_linsys* ls, const double* r_dev, double* x_dev) {
+  if (!ls || !r_dev || !x_dev) return fail(SE_ERR_ARG, "null argument");
+  if (r_dev == x_dev) return fail(SE_ERR_ARG, "r and x must not alias");
+  if (int rc = fdm_setup(ls, 0)) return rc;
+  return fdm_apply64(ls, r_dev, x_dev, false);
+}
 int se_linsys_apply_low(se_linsys* ls, int precision, const void* x_dev, float* y_dev) {
   if (!ls || !x_dev || !y_dev) return fail(SE_ERR_ARG, "null argument");
   if (precision != SE_PREC_BF16 && precision != SE_PREC_FP16)

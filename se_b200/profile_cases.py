@@ -5,6 +5,7 @@
     python -m se_b200.profile_cases sl [ne]          # first-order SL advection
     python -m se_b200.profile_cases cg [ne]          # persistent Jacobi-PCG solve
     python -m se_b200.profile_cases fdm [ne]         # one FDM solve (a CUDA graph)
+    python -m se_b200.profile_cases fdm_apply [ne]   # the FDM transform: 4 product kernels
 
 Each case builds an ne x ne element (default 64, the bench's mesh), p=8,
 doubly periodic mesh and the bench's fields and launches the kernel a few
@@ -45,8 +46,8 @@ def main(case: str, ne: int = 64, reps: int = 3) -> None:
             a.record()
             adv.Advect(dt)
             b.record()
-    elif case in ("apply", "apply_bf16", "cg", "fdm"):
-        method = S.METHOD_FDM if case == "fdm" else S.METHOD_CG
+    elif case in ("apply", "apply_bf16", "cg", "fdm", "fdm_apply"):
+        method = S.METHOD_FDM if case in ("fdm", "fdm_apply") else S.METHOD_CG
         h = S.HelmholtzEqn(u, phi, -1.0, -1.0, 1.0, 0,
                            S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=method))
         n = h.vecSize
@@ -60,6 +61,8 @@ def main(case: str, ne: int = 64, reps: int = 3) -> None:
                 h.apply(xin.data_ptr(), yout.data_ptr())
             elif case == "apply_bf16":
                 h.apply_low(xb.data_ptr(), yf.data_ptr(), S.PREC_BF16)
+            elif case == "fdm_apply":
+                h.fdm_apply(xin.data_ptr(), yout.data_ptr())
             else:
                 h.Solve("helm_")
             b.record()
