@@ -141,6 +141,30 @@ VARIANTS = {
 HEADLINE = "fdm_fp64"
 
 
+def rank_barrier(world: int) -> None:
+    """Barrier over the replicas (no-op for one process)."""
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+
+
+def max_over_ranks(vals, world: int, device) -> list:
+    """Element-wise maximum of per-rank values over all ranks (the job's
+    time is its slowest replica's)."""
+    if world == 1:
+        return [float(v) for v in vals]
+    import torch
+    t = torch.tensor([float(v) for v in vals], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def job_rate(units_per_rank: float, world: int, ms: float) -> float:
+    """Whole-job throughput: every replica processes units_per_rank units in
+    (at most) ms milliseconds."""
+    return units_per_rank * world / (ms * 1e-3)
+
+
 def run_gpu(args, rank, world):
     import ctypes
 
@@ -189,8 +213,7 @@ def run_gpu(args, rank, world):
             torch.cuda.synchronize()
             phi.vals = phi0
             torch.cuda.synchronize()
-            if world > 1:
-                torch.distributed.barrier()
+            rank_barrier(world)
             steps = args.steps if name == HEADLINE else max(3, min(args.steps, 5))
             bus = getattr(torch.cuda.get_device_properties(dev), "pci_bus_id", None)
             sampler = ClockSampler(bus) if name == HEADLINE else None
@@ -208,6 +231,7 @@ def run_gpu(args, rank, world):
                 its.append(st["its"])
                 solve_ms.append(st["kernel_ms"])
             torch.cuda.synchronize()
+            rank_barrier(world)
             if sampler:
                 clock = sampler.stop()
             ms = [a.elapsed_time(b) for a, b in times]
@@ -295,10 +319,7 @@ def run_gpu(args, rank, world):
 
     head = results[HEADLINE]
     step_ms, e2e = head["ms"], head["e2e_ms"]
-    if world > 1:
-        t = torch.tensor([step_ms, e2e], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        step_ms, e2e = float(t[0]), float(t[1])
+    step_ms, e2e = max_over_ranks([step_ms, e2e], world, "cuda")
     return {"step_ms": step_ms, "e2e_ms": e2e, "ng": ng, "nv": m.nVertsTotal, "clocks": clock,
             "variants": results, "sl_ms": float(np.median(sl_ms)), "fp64_tflops": fp64_tflops,
             "fdm_apply_ms": float(np.median(fdm_ms)), "gx": int(round(ng ** 0.5))}
@@ -727,9 +748,9 @@ def main():
         cpu = {"value": ng / per_step, "unit": UNIT, "cores": nthreads, "kind": "port",
                "sample": f"{args.cpu_steps} full step(s) of the workload on the CPU oracle "
                          f"({per_step:.1f} s per step, CG its {its})"}
-    value = r["ng"] * world / (r["step_ms"] * 1e-3)
-    e2e = r["ng"] * world / (r["e2e_ms"] * 1e-3)
-    variants = {k: {"value": r["ng"] * world / (v["ms"] * 1e-3), "ms_per_step": v["ms"],
+    value = job_rate(r["ng"], world, r["step_ms"])
+    e2e = job_rate(r["ng"], world, r["e2e_ms"])
+    variants = {k: {"value": job_rate(r["ng"], world, v["ms"]), "ms_per_step": v["ms"],
                     "solve_ms": v["solve_ms"], "its": v["its"],
                     "rel_err_vs_fdm_fp64": v["rel_err_vs_fdm_fp64"]}
                 for k, v in r["variants"].items()}
