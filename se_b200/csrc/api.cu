@@ -273,6 +273,7 @@ struct se_linsys {
   int fdm_key;
   FdmParams* d_fparams;
   FdmState* d_fstate;
+  unsigned* d_rescount;  // arrival counter of the fused residual + test (zero between launches)
   FdmParams* h_fparams;  // pinned host copies for asynchronous transfers
   FdmState* h_fstate;
   int async_pending;       // 1: FDM solve queued; 2: synchronous result held
@@ -407,6 +408,7 @@ void linsys_free(se_linsys* ls) {
   dfree(ls->d_bar);
   dfree(ls->d_active);
   dfree(ls->d_err);
+  dfree(ls->d_rescount);
   dfree(ls->X1);
   dfree(ls->X2);
   dfree(ls->ax);
@@ -839,7 +841,10 @@ std::string describe_graph(cudaGraph_t g) {
 int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
   if (!ls->d_fparams) {
     int rc;
-    if ((rc = dalloc(&ls->d_fparams, 1)) || (rc = dalloc(&ls->d_fstate, 1))) return rc;
+    if ((rc = dalloc(&ls->d_fparams, 1)) || (rc = dalloc(&ls->d_fstate, 1)) ||
+        (rc = dalloc(&ls->d_rescount, 1)))
+      return rc;
+    CK(cudaMemset(ls->d_rescount, 0, sizeof(unsigned)));
   }
   if (ls->fdm_exec) {
     cudaGraphExecDestroy(ls->fdm_exec);
@@ -901,9 +906,13 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
         brc = prec == 0 ? fdm_apply64(ls, ls->r, ls->x, true) : fdm_apply_low(ls, ls->r, ls->x);
         if (!brc && remove_null)
           brc = launch_remove_mean(ls->x, n, ls->fpart, kFdmPartials, ls->fpart + 2 * ls->fpart_n + 4, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
-        if (!brc) brc = launch_residual(ls->op, ls->x, ls->f, ls->r, wv, nt == SE_NORM_NATURAL, ls->fpart, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
-        if (!brc) brc = launch_norm_final(ls->fpart, residual_blocks(ls->op), res, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
-        if (!brc) brc = launch_fdm_check(ls->d_fparams, ls->d_fstate, res, hc, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
+        // r = f - A x with the norm and the convergence test in one launch
+        if (!brc)
+          brc = launch_residual_check(ls->op, ls->x, ls->f, ls->r, wv, nt == SE_NORM_NATURAL,
+                                      ls->fpart, res, ls->d_rescount, ls->d_fparams,
+                                      ls->d_fstate, hc, bs) == cudaSuccess
+                    ? SE_OK
+                    : SE_ERR_CUDA;
         cudaGraph_t bodyg = body;
         const bool ended = cudaStreamEndCapture(bs, &bodyg) == cudaSuccess;
         ok = ended && brc == SE_OK;

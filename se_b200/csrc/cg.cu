@@ -30,6 +30,7 @@
 // or preconditioner; a constant null space is projected out of every
 // preconditioned residual.
 #include "common.cuh"
+#include "fdm_ctl.cuh"
 
 namespace seg {
 namespace {
@@ -671,12 +672,23 @@ __device__ __forceinline__ double residual_dd(const OpSm& o, const double* P, in
 // ------------------------------------------- standalone apply / residual --
 // y = A x, or with b: r = b - A x (extended precision) with per-block partial sums of
 // (w r)^2 (or r w r when natural) and r^2 (w = Jacobi inverse, nullptr: 1).
+// Tail of the FDM refinement step fused into the residual launch (count ==
+// nullptr: none).
+struct ResTail {
+  double* res;
+  unsigned* count;
+  const FdmParams* p;
+  FdmState* st;
+  cudaGraphConditionalHandle h;
+};
+
 template <int N>
 __global__ void __launch_bounds__(kCgThreads) apply_kernel(const OpDev op, const double* __restrict__ x,
                                                            const double* __restrict__ b,
                                                            double* __restrict__ y,
                                                            const double* __restrict__ w,
-                                                           int natural, double* __restrict__ partial) {
+                                                           int natural, double* __restrict__ partial,
+                                                           const ResTail tail) {
   extern __shared__ double P[];
   __shared__ OpSm o;
   __shared__ double red[kCgThreads / 32][4];
@@ -719,14 +731,38 @@ __global__ void __launch_bounds__(kCgThreads) apply_kernel(const OpDev op, const
       partial[2 * (blockIdx.y * gridDim.x + blockIdx.x) + 1] = acc[1];
     }
   }
+  if (!tail.count) return;
+  // the last block to finish sums the partials in block order and runs the
+  // refinement step's convergence test (no block waits for another)
+  __shared__ unsigned last;
+  __threadfence();
+  __syncthreads();
+  const unsigned nb = gridDim.x * gridDim.y;
+  if (threadIdx.x == 0) last = atomicAdd(tail.count, 1u) == nb - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (unsigned k = threadIdx.x; k < nb; k += kCgThreads) {
+    s[0] += __ldcg(partial + 2 * k);
+    s[1] += __ldcg(partial + 2 * k + 1);
+  }
+  block_sum4(s, red);
+  if (threadIdx.x == 0) {
+    tail.res[0] = s[0];
+    tail.res[1] = s[1];
+    *tail.count = 0u;
+    fdm_check_state(tail.p, tail.st, s[0], tail.h);
+  }
 }
 
 template <int N>
 cudaError_t launch_apply_n(const OpDev& op, const double* x, const double* b, double* y,
-                           const double* w, int natural, double* partial, cudaStream_t s) {
+                           const double* w, int natural, double* partial, const ResTail& tail,
+                           cudaStream_t s) {
   dim3 grid((op.G[0] + kCgTileX - 1) / kCgTileX, (op.G[1] + kCgTileY - 1) / kCgTileY);
   const size_t smem = sizeof(double) * (size_t)Geo<N>::W * Geo<N>::H;
-  apply_kernel<N><<<grid, kCgThreads, smem, s>>>(op, x, b, y, w, natural, partial);
+  apply_kernel<N><<<grid, kCgThreads, smem, s>>>(op, x, b, y, w, natural, partial, tail);
   return cudaGetLastError();
 }
 
@@ -752,10 +788,12 @@ const void* pick(int N, int K) {
 
 #define SE_APPLY_CASE(n) \
   case n:                \
-    return launch_apply_n<n>(op, x, b, y, w, natural, partial, s);
+    return launch_apply_n<n>(op, x, b, y, w, natural, partial, tail, s);
 
-cudaError_t launch_residual(const OpDev& op, const double* x, const double* b, double* y,
-                            const double* w, int natural, double* partial, cudaStream_t s) {
+namespace {
+cudaError_t residual_any(const OpDev& op, const double* x, const double* b, double* y,
+                         const double* w, int natural, double* partial, const ResTail& tail,
+                         cudaStream_t s) {
   switch (op.d[0].N) {
     SE_APPLY_CASE(2) SE_APPLY_CASE(3) SE_APPLY_CASE(4) SE_APPLY_CASE(5) SE_APPLY_CASE(6)
     SE_APPLY_CASE(7) SE_APPLY_CASE(8) SE_APPLY_CASE(9) SE_APPLY_CASE(10) SE_APPLY_CASE(11)
@@ -764,7 +802,23 @@ cudaError_t launch_residual(const OpDev& op, const double* x, const double* b, d
       return cudaErrorInvalidValue;
   }
 }
+}  // namespace
 #undef SE_APPLY_CASE
+
+cudaError_t launch_residual(const OpDev& op, const double* x, const double* b, double* y,
+                            const double* w, int natural, double* partial, cudaStream_t s) {
+  const ResTail none{nullptr, nullptr, nullptr, nullptr, 0};
+  return residual_any(op, x, b, y, w, natural, partial, none, s);
+}
+
+cudaError_t launch_residual_check(const OpDev& op, const double* x, const double* b, double* r,
+                                  const double* w, int natural, double* partial, double* res,
+                                  unsigned* count, const FdmParams* p, FdmState* st,
+                                  cudaGraphConditionalHandle h, cudaStream_t s) {
+  if (!partial || !count) return cudaErrorInvalidValue;
+  const ResTail tail{res, count, p, st, h};
+  return residual_any(op, x, b, r, w, natural, partial, tail, s);
+}
 
 
 int residual_blocks(const OpDev& op) {

@@ -108,6 +108,16 @@ cudaError_t launch_op_apply_low(const OpDev& op, int fp16, const void* x, float*
 // natural, r w r; and r^2) over residual_blocks(op) blocks (cg.cu).
 cudaError_t launch_residual(const OpDev& op, const double* x, const double* b, double* r,
                             const double* w, int natural, double* partial, cudaStream_t s);
+// The same residual with the FDM refinement loop's tail fused in: the block
+// that finishes last (arrival counter *count, zero between launches) sums
+// the partials in block order into res[0..1], runs the convergence test on
+// the loop state and sets the loop's while-condition h.
+struct FdmParams;
+struct FdmState;
+cudaError_t launch_residual_check(const OpDev& op, const double* x, const double* b, double* r,
+                                  const double* w, int natural, double* partial, double* res,
+                                  unsigned* count, const FdmParams* p, FdmState* st,
+                                  cudaGraphConditionalHandle h, cudaStream_t s);
 int residual_blocks(const OpDev& op);
 cudaError_t launch_op_diag(const OpDev& op, double* d, cudaStream_t s);
 // f = Mass*rhs over the unknowns (FieldRHS + Vector::Assemble), plus lift.

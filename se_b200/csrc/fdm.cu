@@ -21,6 +21,7 @@
 #include <cuda_fp16.h>
 
 #include "common.cuh"
+#include "fdm_ctl.cuh"
 
 namespace seg {
 namespace {
@@ -81,27 +82,7 @@ __global__ void fdm_init_kernel(const FdmParams* __restrict__ p, FdmState* __res
 
 __global__ void fdm_check_kernel(const FdmParams* __restrict__ p, FdmState* __restrict__ st,
                                  const double* __restrict__ res, cudaGraphConditionalHandle h) {
-  const double dp = sqrt(fabs(res[0]));
-  const int its = st->its + 1;
-  st->its = its;
-  st->dp = dp;
-  int reason = 0;
-  if (!(dp == dp) || isinf(dp)) reason = -9;
-  else if (dp <= st->ttol) reason = dp < p->atol ? 3 : 2;
-  else if (dp >= p->dtol * st->rnorm0) reason = -4;
-  else {
-    // three steps without a 10% gain on the best residual: stalled (the
-    // rounding floor, or a low precision too coarse for this operator)
-    if (dp > 0.9 * st->best) {
-      if (++st->stalled >= 3) reason = -5;
-    } else {
-      st->stalled = 0;
-    }
-    if (!reason && its >= p->max_it) reason = -3;
-  }
-  st->best = fmin(st->best, dp);
-  st->reason = reason;
-  cudaGraphSetConditional(h, reason == 0 ? 1u : 0u);
+  fdm_check_state(p, st, res[0], h);
 }
 
 // Fixed-order block reduction of one sum (256 threads); result in thread 0.

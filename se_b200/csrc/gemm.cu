@@ -9,9 +9,10 @@
 //          no FP64 kind of the tcgen05 MMA), FP64 accumulation;
 //   P = 1  FP32 data rounded to TF32, m16n8k8 tf32 MMA, FP32 accumulation;
 //   P = 2  BF16 data, m16n8k16 bf16 MMA, FP32 accumulation.
-// 128-thread blocks of 2 x 2 warps own 32 x 32 output tiles while a grid of
-// 64 x 64 tiles would leave SMs idle, 64 x 64 tiles above that. FP64 operands
-// stream through a multi-stage cp.async pipeline; low-precision ones pass
+// While a grid of 64 x 64 tiles would leave SMs idle, 32 x 32 tiles: FP64 by
+// 4 warps that split each K stage and sum their partial tiles in warp order,
+// low precision by 2 x 2 warps; 64 x 64 tiles (2 x 2 warps) above that. FP64
+// operands stream through a multi-stage cp.async pipeline; low-precision ones pass
 // through registers (converted, and the FP64 first operand scaled, on the
 // way) into double-buffered shared memory. Any leading dimension (odd ones
 // included) is accepted.
@@ -428,6 +429,150 @@ cudaError_t run_d(const GemmArgs<double, double, double>& g, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// FP64 products split over K inside the block: a 32 x 32 output tile per
+// block of W warps; stage i holds a 32-wide slice of K and warp w multiplies
+// its w-th 8-wide part, so every warp keeps the whole tile's 8 accumulator
+// fragments (8 independent MMA chains). At the end the W partial tiles are
+// summed through shared memory in warp order (deterministic) and the
+// epilogue is applied.
+template <int W_, int ST_>
+struct KCfg {
+  static constexpr int W = W_, ST = ST_;
+  static constexpr int BM = 32, BN = 32, BK = 8 * W;
+  static constexpr int AS = BK + 4, BS = BN + 4, RS = BN + 1;
+  static constexpr int THREADS = 32 * W;
+  static constexpr int A_ELEMS = BM * AS, B_ELEMS = BK * BS;
+  static constexpr int PIPE = ST * (A_ELEMS + B_ELEMS), RED = W * BM * RS;
+  static constexpr size_t SMEM = sizeof(double) * (size_t)(PIPE > RED ? PIPE : RED);
+};
+
+template <class C, int EPI>
+__global__ void __launch_bounds__(C::THREADS) fdm_dgemm_ksplit_kernel(
+    const GemmArgs<double, double, double> g) {
+  extern __shared__ __align__(16) double dsm[];
+  double* As = dsm;
+  double* Bs = dsm + C::ST * C::A_ELEMS;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int gq = lane >> 2, tq = lane & 3;
+  const int m0 = blockIdx.y * C::BM, n0 = blockIdx.x * C::BN;
+  const int nkt = (g.K + C::BK - 1) / C::BK;
+
+  auto issue = [&](int i) {
+    const int k0 = i * C::BK;
+    double* as = As + (i % C::ST) * C::A_ELEMS;
+    double* bs = Bs + (i % C::ST) * C::B_ELEMS;
+#pragma unroll
+    for (int e = tid; e < C::BM * C::BK; e += C::THREADS) {
+      const int row = e / C::BK, col = e % C::BK;
+      const int gr = m0 + row, gc = k0 + col;
+      const bool ok = gr < g.M && gc < g.K;
+      cp_async8(as + row * C::AS + col, ok ? g.A + (size_t)gr * g.lda + gc : g.A, ok);
+    }
+#pragma unroll
+    for (int e = tid; e < C::BK * C::BN; e += C::THREADS) {
+      const int row = e / C::BN, col = e % C::BN;
+      const int gr = k0 + row, gc = n0 + col;
+      const bool ok = gr < g.K && gc < g.N;
+      cp_async8(bs + row * C::BS + col, ok ? g.B + (size_t)gr * g.ldb + gc : g.B, ok);
+    }
+  };
+
+  double acc[2][4][4];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) acc[i][j][q] = 0.0;
+
+#pragma unroll
+  for (int s = 0; s < C::ST - 1; s++) {
+    if (s < nkt) issue(s);
+    cp_async_commit();
+  }
+  const int kk = warp * 8;
+  for (int i = 0; i < nkt; i++) {
+    cp_async_wait<C::ST - 2>();
+    __syncthreads();
+    if (i + C::ST - 1 < nkt) issue(i + C::ST - 1);
+    cp_async_commit();
+    const double* as = As + (i % C::ST) * C::A_ELEMS;
+    const double* bs = Bs + (i % C::ST) * C::B_ELEMS;
+    double a[2][4], b[4][2];
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
+      const int r0 = mt * 16 + gq;
+      a[mt][0] = as[r0 * C::AS + kk + tq];
+      a[mt][1] = as[(r0 + 8) * C::AS + kk + tq];
+      a[mt][2] = as[r0 * C::AS + kk + tq + 4];
+      a[mt][3] = as[(r0 + 8) * C::AS + kk + tq + 4];
+    }
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++) {
+      const int c0 = nt * 8 + gq;
+      b[nt][0] = bs[(kk + tq) * C::BS + c0];
+      b[nt][1] = bs[(kk + tq + 4) * C::BS + c0];
+    }
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+      for (int nt = 0; nt < 4; nt++) mma_f64(acc[mt][nt], a[mt], b[nt]);
+  }
+  cp_async_wait<0>();
+  __syncthreads();
+
+  // partial tiles of the W warps, summed in warp order
+  double* red = dsm;
+#pragma unroll
+  for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+    for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int r = mt * 16 + gq + (q >> 1) * 8, c = nt * 8 + 2 * tq + (q & 1);
+        red[(warp * C::BM + r) * C::RS + c] = acc[mt][nt][q];
+      }
+  __syncthreads();
+  for (int e = tid; e < C::BM * C::BN; e += C::THREADS) {
+    const int r = e / C::BN, c = e % C::BN;
+    const int gr = m0 + r, gc = n0 + c;
+    if (gr >= g.M || gc >= g.N) continue;
+    double v = red[r * C::RS + c];
+#pragma unroll
+    for (int w = 1; w < C::W; w++) v += red[(w * C::BM + r) * C::RS + c];
+    double* dst = g.C + (size_t)gr * g.ldc + gc;
+    if constexpr (EPI == EPI_DIVIDE) {
+      const double d = g.alpha + g.bx * g.lx[gc] + g.by * g.ly[gr];
+      v = fabs(d) <= g.null_tol ? 0.0 : v / d;
+    }
+    if constexpr (EPI == EPI_ACCUM)
+      *dst += v;
+    else
+      *dst = v;
+  }
+}
+
+template <class C, int EPI>
+cudaError_t run_k(const GemmArgs<double, double, double>& g, cudaStream_t s) {
+  if (g.M <= 0 || g.N <= 0 || g.K <= 0) return cudaErrorInvalidValue;
+  if (C::SMEM > 48 * 1024) {
+    static bool attr[64] = {};  // per kernel instantiation and device
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr[dev]) {
+      e = cudaFuncSetAttribute(fdm_dgemm_ksplit_kernel<C, EPI>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+      if (e != cudaSuccess) return e;
+      attr[dev] = true;
+    }
+  }
+  const dim3 grid((g.N + C::BN - 1) / C::BN, (g.M + C::BM - 1) / C::BM);
+  fdm_dgemm_ksplit_kernel<C, EPI><<<grid, C::THREADS, C::SMEM, s>>>(g);
+  return cudaGetLastError();
+}
+
 // Tile shape by problem size: 32 x 32 tiles (four times the blocks) until
 // the 64 x 64 grid alone covers the GPU's 148 SMs.
 inline bool small_tiles(int M, int N) { return ((M + 63) / 64) * ((N + 63) / 64) < 148; }
@@ -436,7 +581,7 @@ template <int P, class TA, class TB, class TC, int EPI>
 cudaError_t run(const GemmArgs<TA, TB, TC>& g, cudaStream_t s) {
   if (g.M <= 0 || g.N <= 0 || g.K <= 0) return cudaErrorInvalidValue;
   if constexpr (P == 0) {
-    if (small_tiles(g.M, g.N)) return run_d<DCfg<32, 32, 2, 2, 4>, EPI>(g, s);
+    if (small_tiles(g.M, g.N)) return run_k<KCfg<4, 3>, EPI>(g, s);
     return run_d<DCfg<64, 64, 2, 2, 3>, EPI>(g, s);
   } else {
     if (small_tiles(g.M, g.N)) {
