@@ -28,6 +28,18 @@ CASES = [
 ]
 
 
+# Order-8 meshes large enough for tiles that the apply stages with TMA:
+# periodic interior tiles; a Dirichlet left end (staged columns shifted by
+# one to keep the copy 16-byte aligned) with natural right and bottom ends
+# (zero fill); an odd number of unknowns per row (ordinary loads only).
+CASES8 = [
+    (26, 14, 8, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False)),
+    (25, 13, 8, (0.0, 0.0), (2.0, 1.0), (False, False), (False, True, True, False)),
+    (24, 15, 8, (-1.0, 0.0), (1.0, 1.0), (False, False), (False, False, False, False)),
+    (20, 17, 8, (0.0, 0.0), (1.0, 1.0), (True, False), (True, True, False, False)),
+]
+
+
 def build(S, O, case, c, nu, dt, quirk, poisson=False, seed=0):
     nx, ny, N, lo, hi, per, bc = case
     om = O.Mesh(nx, ny, N, lo, hi, per)
@@ -73,18 +85,6 @@ def test_apply_matches_assembled_operator(segpu, oracle, case, quirk):
     assert np.abs(d.cpu().numpy() - diag).max() <= 2e-11 * np.abs(diag).max()
 
 
-# Order-8 meshes large enough for tiles that the apply stages with TMA:
-# periodic interior tiles; a Dirichlet left end (staged columns shifted by
-# one to keep the copy 16-byte aligned) with natural right and bottom ends
-# (zero fill); an odd number of unknowns per row (ordinary loads only).
-CASES8 = [
-    (26, 14, 8, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False)),
-    (25, 13, 8, (0.0, 0.0), (2.0, 1.0), (False, False), (False, True, True, False)),
-    (24, 15, 8, (-1.0, 0.0), (1.0, 1.0), (False, False), (False, False, False, False)),
-    (20, 17, 8, (0.0, 0.0), (1.0, 1.0), (True, False), (True, True, False, False)),
-]
-
-
 @pytest.mark.parametrize("case", range(len(CASES8)))
 def test_apply_order8_tiles(segpu, oracle, case):
     om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, CASES8[case], -2.0, -1.0, 0.5,
@@ -102,18 +102,18 @@ def test_apply_order8_tiles(segpu, oracle, case):
         assert (np.abs(yd.cpu().numpy() - ref) / scale).max() < 2e-11
 
 
-@pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("case", list(range(len(CASES))) + ["o8-" + str(k) for k in range(len(CASES8))])
 @pytest.mark.parametrize("prec", ["bf16", "fp16"])
 def test_low_precision_apply(segpu, oracle, case, prec):
     """se_linsys_apply_low: x rounded to BF16/FP16, operator and arithmetic in
     FP32. Against the oracle's FP64 CSR on the same rounded x, the error is
     bounded by FP32 rounding of the coefficients and the sums: 1e-6 of the
     row's absolute sum times max|x|."""
-    om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, CASES[case], -2.0, -1.0, 0.5,
-                                                     False)
+    spec = CASES8[int(case[3:])] if isinstance(case, str) else CASES[case]
+    om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, spec, -2.0, -1.0, 0.5, False)
     n = ls.vecSize
     dt = torch.bfloat16 if prec == "bf16" else torch.float16
-    x = torch.tensor(np.random.default_rng(10 + case).standard_normal(n), dtype=dt)
+    x = torch.tensor(np.random.default_rng(10 + len(str(case))).standard_normal(n), dtype=dt)
     ref = A.matvec(x.double().numpy())
     xd = x.cuda()
     yd = torch.zeros(n, device="cuda", dtype=torch.float32)
