@@ -111,6 +111,14 @@ int se_field_integrate(const se_field* field, int dof, int average, double* out)
  * out is double[npts][ndofs]. */
 int se_field_interp_global(const se_field* field, const double* pts, int npts, double* out);
 
+/* TwoLayerQGEqn::GenVel / QuasiGeostrophicEqn::GenVel
+ * (src/qg/TwoLayerQGEqn.cpp:335-352, src/qg/QuasiGeostrophicEqn.cpp:207-223):
+ * vel (ndofs 2) = (-d psi/dy, d psi/dx) at every vertex, each derivative by
+ * Field::InterpDerivsGlobal (src/base/Field.cpp:96-118) in the element that
+ * Mesh::GetEl assigns to the vertex (at a shared vertex that element's
+ * one-sided derivative, as in the reference). psi has ndofs 1, same mesh. */
+int se_field_gen_vel(const se_field* psi, se_field* vel);
+
 /* -------------------------------------------------------------- Advector --
  * Replaces Advector(field, velocity) (first order) and
  * Advector(field, velocity, fieldMinusOne, velMinusOne) (second order),

@@ -1389,6 +1389,14 @@ int se_field_integrate(const se_field* field, int dof, int average, double* out)
   *out = average ? r[0] / ((m.max[0] - m.min[0]) * (m.max[1] - m.min[1])) : r[0];
   return SE_OK;
 }
+int se_field_gen_vel(const se_field* psi, se_field* vel) {
+  if (int rc = check_field(psi)) return rc;
+  if (int rc = check_field(vel)) return rc;
+  if (psi->ndofs != 1 || vel->ndofs != 2) return fail(SE_ERR_ARG, "psi needs 1 and vel 2 components");
+  if (psi->mesh != vel->mesh) return fail(SE_ERR_ARG, "psi and vel on different meshes");
+  CK(launch_gen_vel(psi->mesh->dev, psi->vals, vel->vals, nullptr, g_stream));
+  return SE_OK;
+}
 int se_field_interp_global(const se_field* field, const double* pts, int npts, double* out) {
   if (int rc = check_field(field)) return rc;
   if (npts < 0 || (npts && (!pts || !out))) return fail(SE_ERR_ARG, "bad argument");

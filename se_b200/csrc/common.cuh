@@ -85,6 +85,9 @@ cudaError_t launch_global_to_local(const MeshDev& m, const double* pts, int npts
 // Field::InterpGlobal at points (device arrays).
 cudaError_t launch_interp_global(const MeshDev& m, int ndofs, const double* vals,
                                  const double* pts, int npts, double* out, cudaStream_t s);
+// vel[Nv][2] = (-d psi/dy, d psi/dx) at every vertex (GenVel of SE's QG models).
+cudaError_t launch_gen_vel(const MeshDev& m, const double* psi, double* vel, unsigned* err,
+                           cudaStream_t s);
 // Field::PeriodicUpdate.
 cudaError_t launch_periodic_update(const MeshDev& m, int ndofs, double* vals, cudaStream_t s);
 // Quadrature sums over all elements: sum detJ*w*a (Integrate) or, with

@@ -462,6 +462,78 @@ __global__ void max_partials_kernel(const double* partial, int np, double* out) 
   }
 }
 
+// TwoLayerQGEqn::GenVel / QuasiGeostrophicEqn::GenVel
+// (src/qg/TwoLayerQGEqn.cpp:335-352, src/qg/QuasiGeostrophicEqn.cpp:207-223):
+// vel = (-d psi/dy, d psi/dx) at every vertex, each derivative from
+// Field::InterpDerivsGlobal (src/base/Field.cpp:96-118) in the element that
+// GetEl picks for the vertex. A vertex's local coordinates are GLL nodes in
+// both directions, so Mesh::ShapeFuncDerivsAtCoord gives d/dxi = dC[xi][j] on
+// the node's row and d/deta = dC[yi][j] on its column, exact zeros elsewhere;
+// the Jacobian, its inverse and the sums are formed in the reference's order
+// over the row and column entries (the zero products leave the sums as they
+// are), with exactly rounded operations.
+template <int N>
+__global__ void gen_vel_kernel(const MeshDev m, const double* __restrict__ psi,
+                               double2* __restrict__ vel, unsigned* err) {
+  constexpr int n = N + 1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nvx = m.nVerts[0], nvy = m.nVerts[1];
+  if (i >= nvx || j >= nvy) return;
+  const double gx = vertex_coord(m, 0, i), gy = vertex_coord(m, 1, j);
+  const int tx = get_topo(m, 0, gx, err), ty = get_topo(m, 1, gy, err);
+  const int xi = snap_node<N>(m, local_coord(m, 0, gx, tx));
+  const int yi = snap_node<N>(m, local_coord(m, 1, gy, ty));
+  if (xi < 0 || yi < 0) {  // a vertex always lies on a node
+    if (err) atomicOr(err, (unsigned)KERR_BAD_CONFIG);
+    return;
+  }
+  const int base = ty * N * nvx + tx * N;
+  const double* rowd = m.dC + xi * n;  // d/dxi of the cardinals along the row
+  const double* cold = m.dC + yi * n;  // d/deta along the column
+  // Jacobian: J00 = sum g0 x, J01 = sum g0 y, J10 = sum g1 x, J11 = sum g1 y
+  double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
+  const double yrow = vertex_coord(m, 1, ty * N + yi), xcol = vertex_coord(m, 0, tx * N + xi);
+#pragma unroll
+  for (int b = 0; b < n; b++) {
+    const double xb = vertex_coord(m, 0, tx * N + b);
+    J00 = xadd(J00, xmul(rowd[b], xb));
+    J01 = xadd(J01, xmul(rowd[b], yrow));
+  }
+#pragma unroll
+  for (int b = 0; b < n; b++) {
+    const double yb = vertex_coord(m, 1, ty * N + b);
+    J10 = xadd(J10, xmul(cold[b], xcol));
+    J11 = xadd(J11, xmul(cold[b], yb));
+  }
+  const double det = xsub(xmul(J00, J11), xmul(J01, J10));
+  const double I00 = xdiv(J11, det), I11 = xdiv(J00, det);
+  const double I01 = xdiv(-J01, det), I10 = xdiv(-J10, det);
+  // d psi/dx, d psi/dy: sums over the element's nodes in node order (row
+  // yj, column xj); only the node's row and column contribute
+  double dx = 0.0, dy = 0.0;
+#pragma unroll
+  for (int yj = 0; yj < n; yj++) {
+    if (yj == yi) {
+#pragma unroll
+      for (int xj = 0; xj < n; xj++) {
+        const double g0 = rowd[xj], g1 = xj == xi ? cold[yj] : 0.0;
+        const double p = __ldg(psi + base + yj * nvx + xj);
+        const double tx_ = xadd(xmul(g0, I00), xmul(g1, I01));
+        const double ty_ = xadd(xmul(g0, I10), xmul(g1, I11));
+        dx = xadd(dx, xmul(tx_, p));
+        dy = xadd(dy, xmul(ty_, p));
+      }
+    } else {
+      const double g1 = cold[yj];
+      const double p = __ldg(psi + base + yj * nvx + xi);
+      dx = xadd(dx, xmul(xmul(g1, I01), p));
+      dy = xadd(dy, xmul(xmul(g1, I11), p));
+    }
+  }
+  vel[j * nvx + i] = make_double2(-dy, dx);
+}
+
 }  // namespace
 
 // Dispatch a runtime polynomial order onto the compile-time one (NN).
@@ -487,6 +559,16 @@ cudaError_t launch_sl(const MeshDev& m, int ndofs, const double* field, const do
   if (m.N < 3) return cudaErrorInvalidValue;
   SE_DISPATCH_N(m.N, return launch_sl_n<NN>(m, ndofs, field, vel, field_prev, vel_prev, dt, out,
                                             dep_el, dep_xy, err, s));
+}
+
+cudaError_t launch_gen_vel(const MeshDev& m, const double* psi, double* vel, unsigned* err,
+                           cudaStream_t s) {
+  const dim3 block(32, 8);
+  const dim3 grid((m.nVerts[0] + 31) / 32, (m.nVerts[1] + 7) / 8);
+  SE_DISPATCH_N(m.N, {
+    gen_vel_kernel<NN><<<grid, block, 0, s>>>(m, psi, reinterpret_cast<double2*>(vel), err);
+    return cudaGetLastError();
+  });
 }
 
 cudaError_t launch_global_to_local(const MeshDev& m, const double* pts, int npts, int* el,

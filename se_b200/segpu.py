@@ -130,7 +130,7 @@ SIGNATURES = {
                               ctypes.POINTER(SolveStats)],
     "se_linsys_solve_async": [_vp, ctypes.c_int],
     "se_linsys_solve_finish": [_vp, ctypes.POINTER(SolveStats)],
-    "se_linsys_apply": [_vp, _vp, _vp], "se_linsys_fdm_apply": [_vp, _vp, _vp], "se_linsys_apply_low": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
+    "se_linsys_apply": [_vp, _vp, _vp], "se_field_gen_vel": [_vp, _vp], "se_linsys_fdm_apply": [_vp, _vp, _vp], "se_linsys_apply_low": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
     "se_linsys_vec_size": [_vp, _I],
     "se_calc_time_step": [_vp, ctypes.c_double, _D],
     "se_field_error": [_vp, _vp, ctypes.c_int, ctypes.c_int, _D],
@@ -563,6 +563,14 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+def GenVel(psi: Field, name: str = "vel") -> Field:
+    """TwoLayerQGEqn::GenVel: a new 2-component field (-d psi/dy, d psi/dx)
+    at every vertex of psi's mesh (no boundary conditions)."""
+    vel = Field(name, psi.mesh, 2, None)
+    _check(load_library().se_field_gen_vel(psi._h, vel._h))
+    return vel
 
 
 def CalcTimeStep(velocity: Field, courantNo: float) -> float:

@@ -236,3 +236,38 @@ def test_integrate_matches_oracle(segpu, oracle, golden):
         f.vals = g[f"{tag}_field"]
         ref = g[f"{tag}_integrate"][0]
         assert abs(f.Integrate(0) - ref) <= 1e-12 * np.abs(g[f"{tag}_field"]).sum()
+
+
+@pytest.mark.parametrize("tag", ["pp", "px", "nn", "channel"])
+def test_gen_vel_bit_exact(segpu, oracle, golden, tag):
+    """GenVel (TwoLayerQGEqn::GenVel): (-d psi/dy, d psi/dx) at every vertex,
+    bit-exact against the oracle's InterpDerivsGlobal (itself pinned to the
+    reference's compiled code), on the fixture meshes and on the full-size
+    config-2 channel (128 x 64 elements, p=6, periodic in x, walls in y)."""
+    if tag == "channel":
+        nx, ny, N, lo, hi, per = 128, 64, 6, (0.0, 0.0), (2.0, 1.0), (True, False)
+    else:
+        p = golden["mesh"][f"{tag}_params"]
+        nx, ny, N = int(p[0]), int(p[1]), int(p[2])
+        lo, hi, per = (p[3], p[4]), (p[5], p[6]), (bool(p[7]), bool(p[8]))
+    om = oracle.Mesh(nx, ny, N, lo, hi, per)
+    X = om.verts()
+    psi = np.sin(2.1 * X[:, 0] + 0.3) * np.cos(3.3 * X[:, 1]) + 0.05 * X[:, 0] * X[:, 1]
+    psi = om.periodic_update(psi)
+    ref = om.interp_derivs_global(psi, X)
+    m = make(segpu, nx, ny, N, lo, hi, per)
+    f = segpu.Field("psi", m, 1, None)
+    f.vals = psi
+    vel = segpu.GenVel(f).vals.reshape(-1, 2)
+    assert np.array_equal(vel[:, 0], -ref[:, 1])
+    assert np.array_equal(vel[:, 1], ref[:, 0])
+
+
+def test_gen_vel_rejects_bad_fields(segpu):
+    m = make(segpu, 4, 4, 4)
+    with pytest.raises(segpu.SEError):
+        segpu.GenVel(segpu.Field("v", m, 2, None))  # psi must be scalar
+    psi = segpu.Field("psi", m, 1, None)
+    v2 = segpu.Field("v", make(segpu, 5, 4, 4), 2, None)
+    with pytest.raises(segpu.SEError):
+        segpu._check(segpu.load_library().se_field_gen_vel(psi._h, v2._h))
