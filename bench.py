@@ -452,6 +452,95 @@ def run_apply_roofline(ne=768, p=8, reps=20):
     return out
 
 
+# ---------------------------------------------------- configs 0 and 1 ----
+def run_config0(seed=0):
+    """(lap - lambda) u = f, lambda = 1, on the doubly periodic 16 x 16
+    element, p = 6 unit square; f a seeded sum of 8 Fourier modes with
+    wavenumbers 1..6 and N(0,1) amplitudes; exact modal solution
+    u = -f_k / (4 pi^2 |k|^2 + lambda). Solved with the CG drop-in (Jacobi,
+    rtol 1e-10, true Jacobian) and with FDM; reports iterations, device solve
+    time and the relative L2 nodal error against the modal solution."""
+    import se_b200 as S
+    rng = np.random.default_rng(seed)
+    m = S.Mesh("m", [16, 16], "legendre", 6, [0, 0], [1, 1], [True, True])
+    X = m.verts
+    f, u = np.zeros(len(X)), np.zeros(len(X))
+    for _ in range(8):
+        kx, ky = rng.integers(1, 7, size=2)
+        a, b = rng.standard_normal(2)
+        ph = 2 * np.pi * (kx * X[:, 0] + ky * X[:, 1])
+        mode = a * np.cos(ph) + b * np.sin(ph)
+        f += mode
+        u += mode / (-(4 * np.pi ** 2 * (kx * kx + ky * ky)) - 1.0)
+    bc = S.BCs(False, False, False, False, m)
+    out = {"workload": "(lap - 1) u = f, 16x16 elements p=6 doubly periodic, 8 seeded Fourier modes, "
+                       "rtol 1e-10, true Jacobian", "unknowns": 9216}
+    for name, method in (("cg_fp64", S.METHOD_CG), ("fdm_fp64", S.METHOD_FDM)):
+        fs, fr = S.Field("u", m, 1, bc), S.Field("f", m, 1, bc)
+        fr.vals = f
+        ls = S.HelmholtzEqn(fs, fr, -1.0, -1.0, 1.0, 0,
+                            S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=method))
+        ls.Solve("helm_")
+        st = [ls.Solve("helm_") for _ in range(5)]
+        got = fs.vals
+        out[name] = {"its": int(st[-1]["its"]), "reason": int(st[-1]["reason"]),
+                     "solve_ms": float(min(s["kernel_ms"] for s in st)),
+                     "rel_l2_error_vs_modal": float(np.linalg.norm(got - u) / np.linalg.norm(u))}
+    return out
+
+
+def run_config1(steps=200, seed=11):
+    """Config 1: first-order SL (RK2 departure points) of four seeded
+    Gaussian blobs (width 0.05) on the doubly periodic 64 x 64 element, p = 8
+    mesh, Taylor-Green velocity of amplitude 1 reversed in time,
+    u(x, t) = u_TG(x) cos(pi t / T) with T = steps * dt (evaluated at each
+    step's mid time), dt from CalcTimeStep at Courant 2. The flow returns
+    every particle to its start at T, so the exact tracer at T is the initial
+    one. Reports the mass drift (Field::Integrate), the relative L2 error
+    against the initial tracer (FieldError), and the device time per SL step
+    (the velocity upload of each step excluded)."""
+    import torch
+    import se_b200 as S
+    rng = np.random.default_rng(seed)
+    m = S.Mesh("m", [64, 64], "legendre", 8, [0, 0], [1, 1], [True, True])
+    X = m.verts
+    x, y = X[:, 0], X[:, 1]
+    phi0 = np.zeros(len(X))
+    for cx, cy in rng.uniform(0, 1, size=(4, 2)):
+        # periodic images so that the blobs are smooth across the boundary
+        for sx in (-1, 0, 1):
+            for sy in (-1, 0, 1):
+                phi0 += np.exp(-((x - cx - sx) ** 2 + (y - cy - sy) ** 2) / 0.05 ** 2)
+    utg = np.stack([-np.sin(np.pi * x) ** 2 * np.sin(2 * np.pi * y),
+                    np.sin(np.pi * y) ** 2 * np.sin(2 * np.pi * x)], 1)
+    phi, exact = S.Field("phi", m, 1, None), S.Field("phi0", m, 1, None)
+    vel = S.Field("vel", m, 2, None)
+    phi.vals, exact.vals, vel.vals = phi0, phi0, utg
+    dt = S.CalcTimeStep(vel, 2.0)
+    T = steps * dt
+    adv = S.Advector(phi, vel)
+    mass0 = phi.Integrate(0)
+    pin = torch.empty(utg.shape, dtype=torch.float64, pin_memory=True)
+    stream = torch.cuda.Stream()
+    S.set_stream(stream.cuda_stream)  # the events below record on the library's stream
+    sl_ms = 0.0
+    for k in range(steps):
+        pin.numpy()[...] = utg * np.cos(np.pi * (k + 0.5) * dt / T)
+        vel.vals = pin.numpy()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        adv.Advect(dt)
+        e1.record(stream)
+        phi.Copy(adv.fieldSL)
+        torch.cuda.synchronize()
+        sl_ms += e0.elapsed_time(e1)
+    return {"workload": f"first-order SL, 64x64 elements p=8, 4 Gaussian blobs, time-reversed "
+                        f"Taylor-Green at Courant 2, {steps} steps",
+            "dt": dt, "mass_drift": float((phi.Integrate(0) - mass0) / mass0),
+            "rel_l2_error_return": float(S.FieldError(phi, exact)),
+            "sl_ms_per_step": sl_ms / steps}
+
+
 # ------------------------------------------------------ ensemble (config 3) --
 def run_ensemble(count=256, seed=2024):
     """256 independent Helmholtz solves, mesh n x n elements with n uniform in
@@ -736,6 +825,9 @@ def main():
     log("GPU arm done")
     extras = {}
     if not args.no_extras:
+        log("configs 0 and 1")
+        extras["config0"] = run_config0()
+        extras["config1"] = run_config1()
         log("apply roofline")
         extras["apply_roofline"] = run_apply_roofline()
         log("ensemble")
