@@ -320,6 +320,33 @@ int se_server_wait(se_server* srv, long long ticket, se_result* res);
 int se_server_destroy(se_server* srv);
 
 /* ------------------------------------------------------------ utilities -- */
+/* ------------------------------------------------------ two-layer QG step --
+ * Replaces TwoLayerQGEqn(psi1, omega1, psi2, omega2, F1, F2, beta, E2, r, nu,
+ * tau_e, dt) and its Solve (src/qg/TwoLayerQGEqn.h, .cpp:17-433): one step of
+ * the two-layer quasi-geostrophic model, on the device: PV of both layers
+ * (GenPV), SL advection of PV by the GenVel velocities (first order, or
+ * second order when the previous fields are given), baroclinic Helmholtz
+ * (c = -(F1+F2)) and barotropic Poisson (c = -1) inversions with the given
+ * solver options, the dissipative PV update (SolveQ with DissipationRHS),
+ * the second inversions and the update of psi1, psi2, omega1, omega2 in
+ * place. The reference's own step is kept as it is: the first-order step
+ * applies SolveQ to layer 1 only, both layers' dissipation uses the first
+ * baroclinic solution, and the PV mass matrix is scaled by 1.5 from the first
+ * second-order step on. Scalar fields on one mesh; psi1's boundary conditions
+ * (e.g. walls in y of a channel) are those of the inversions; tau_e is the
+ * radiative-equilibrium field of the dissipation. The fields must outlive the
+ * object. */
+typedef struct se_qg2 se_qg2;
+int se_qg2_create(se_field* psi1, se_field* omega1, se_field* psi2, se_field* omega2, double F1,
+                  double F2, double beta, double E2, double r, double nu, se_field* tau_e,
+                  double dt, const se_solver_opts* opts, se_qg2** out);
+/* TwoLayerQGEqn::Solve(psi1Prev, omega1Prev, psi2Prev, omega2Prev): second
+ * order when all four previous fields are given (they are then replaced by
+ * the fields as they were before this step), first order when all are NULL. */
+int se_qg2_solve(se_qg2* qg, se_field* psi1_prev, se_field* omega1_prev, se_field* psi2_prev,
+                 se_field* omega2_prev);
+int se_qg2_destroy(se_qg2* qg);
+
 /* CalcTimeStep(velocity, courantNo) (src/base/Utils.cpp:23-40). */
 int se_calc_time_step(const se_field* velocity, double courant, double* dt);
 /* FieldError(numeric, analytic, dof, normalise) (src/base/Utils.cpp:232-254). */

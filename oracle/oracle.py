@@ -96,6 +96,9 @@ def lib():
         L.or_field_error.argtypes = [_vp, _D, _D, _int]
         L.or_calc_time_step.restype = _dbl
         L.or_calc_time_step.argtypes = [_vp, _D, _dbl]
+        L.or_dissipation_rhs.argtypes = [_vp, _I, _int, _dbl, _D, _D, _D, _D, _dbl, _dbl, _dbl,
+                                         _D]
+        L.or_mass_diag.argtypes = [_vp, _I, _int, _dbl, _D]
         _lib = L
     return _lib
 
@@ -368,3 +371,102 @@ def helmholtz_solve(mesh: Mesh, sol_vals, rhs_vals, c, nu, dt, bcs=(False, False
     stats["x"] = x
     stats["b"] = f
     return out, stats
+
+
+class QG2:
+    """TwoLayerQGEqn (src/qg/TwoLayerQGEqn.cpp:17-433) restated over the
+    oracle's pieces: GenPV, GenVel (InterpDerivsGlobal at the vertices), the
+    restated SL advection, Helmholtz/Poisson solves by the restated CSR +
+    Jacobi-PCG, and SolveQ as the assembled DissipationRHS divided by the
+    diagonal PV mass. Follows the reference's step as written (first order:
+    SolveQ for layer 1 only; dissipation of both layers with tau1; PV mass
+    x 1.5 from the first second-order step). Arrays in the reference's vertex
+    order. TEST INFRASTRUCTURE ONLY."""
+
+    def __init__(self, mesh: Mesh, bcs, psi1, omega1, psi2, omega2, F1, F2, beta, E2, r, nu,
+                 tau_e, dt, quirk=False, rtol=1e-12):
+        self.m, self.bcs, self.quirk, self.rtol = mesh, tuple(bcs), quirk, rtol
+        self.F1, self.F2, self.beta, self.E2, self.r, self.nu, self.dt = F1, F2, beta, E2, r, nu, dt
+        self.psi1, self.omega1 = _f64(psi1).copy(), _f64(omega1).copy()
+        self.psi2, self.omega2 = _f64(psi2).copy(), _f64(omega2).copy()
+        self.tau_e = _f64(tau_e).copy()
+        self.X = mesh.verts()
+        self.y = self.X[:, 1].copy()
+        self.f2v, self.v2f = mesh.bcs_maps(*bcs)
+        self.tau1 = self.psi1 - self.psi2
+        self.chi1 = self.psi1 + self.psi2
+        self.tau2, self.chi2 = self.tau1.copy(), self.chi1.copy()
+        self.alpha1 = self.gen_pv(self.omega1, self.psi1, self.psi2, F1)
+        self.alpha2 = self.gen_pv(self.omega2, self.psi2, self.psi1, F2)
+        self.a_mass, self.second = 1.0, False
+
+    def gen_pv(self, omega, psi_i, psi_j, F):
+        return omega + F * (psi_j - psi_i) + self.beta * self.y
+
+    def gen_vel(self, psi):
+        d = self.m.interp_derivs_global(psi, self.X)
+        return np.stack([-d[:, 1], d[:, 0]], 1)
+
+    def helm(self, sol, rhs):
+        return helmholtz_solve(self.m, sol, rhs, -(self.F1 + self.F2), -1.0, 1.0, self.bcs,
+                               quirk=self.quirk, rtol=self.rtol)[0]
+
+    def fish(self, sol, rhs):
+        return helmholtz_solve(self.m, sol, rhs, -1.0, 0.0, 0.0, self.bcs, quirk=self.quirk,
+                               rtol=self.rtol, poisson=True)[0]
+
+    def solve_q(self, alpha_hat, om_hat, rF, Ei, alpha):
+        ng = len(self.v2f)
+        f2v = np.ascontiguousarray(self.f2v, dtype=np.int32)
+        f, d = np.zeros(ng), np.zeros(ng)
+        self.m.L.or_dissipation_rhs(self.m.h, _pi(f2v), ng, self.dt, _pd(_f64(alpha_hat)),
+                                    _pd(_f64(self.tau1)), _pd(_f64(om_hat)), _pd(self.tau_e),
+                                    rF, Ei, self.nu, _pd(f))
+        self.m.L.or_mass_diag(self.m.h, _pi(f2v), ng, self.a_mass, _pd(d))
+        return update_field(self.m, self.v2f, f / d, alpha)
+
+    def invert(self, a1, a2, tau, chi, cb_fish, cb_update):
+        tau = self.helm(tau, a1 - a2)
+        chi = self.fish(chi, a1 + a2 + (self.F1 - self.F2) * tau - cb_fish * self.y)
+        p1, p2 = 0.5 * (tau + chi), 0.5 * (chi - tau)
+        o1 = a1 - self.F1 * (p2 - p1) - cb_update * self.y
+        o2 = a2 - self.F2 * (p1 - p2) - cb_update * self.y
+        return tau, chi, p1, p2, o1, o2
+
+    def step(self, prev=None):
+        """One TwoLayerQGEqn::Solve; prev = (psi1, omega1, psi2, omega2) of
+        the previous step (second order) or None (first order). Returns the
+        new prev tuple (the fields before this step) for second order."""
+        m, dt, b = self.m, self.dt, self.beta
+        if prev is None:
+            vel1, vel2 = self.gen_vel(self.psi1), self.gen_vel(self.psi2)
+            self.alpha1 = self.gen_pv(self.omega1, self.psi1, self.psi2, self.F1)
+            self.alpha2 = self.gen_pv(self.omega2, self.psi2, self.psi1, self.F2)
+            a1h = m.advect(self.alpha1, vel1, dt)
+            a2h = m.advect(self.alpha2, vel2, dt)
+            self.tau1, self.chi1, _, _, o1h, _ = self.invert(a1h, a2h, self.tau1, self.chi1,
+                                                             2.0 * b, b)
+            self.alpha1 = self.solve_q(a1h, o1h, self.r * self.F1, 0.0, self.alpha1)
+            (self.tau2, self.chi2, self.psi1, self.psi2, self.omega1,
+             self.omega2) = self.invert(self.alpha1, self.alpha2, self.tau2, self.chi2, 2.0 * b, b)
+            return None
+        if not self.second:
+            self.a_mass, self.second = 1.5, True
+        p1p, o1p, p2p, o2p = [_f64(v).copy() for v in prev]
+        saved = (self.psi1.copy(), self.omega1.copy(), self.psi2.copy(), self.omega2.copy())
+        a = 1.5
+        vel1, vel2 = self.gen_vel(self.psi1), self.gen_vel(self.psi2)
+        vel1p, vel2p = self.gen_vel(p1p), self.gen_vel(p2p)
+        self.alpha1 = self.gen_pv(self.omega1, self.psi1, self.psi2, self.F1)
+        self.alpha2 = self.gen_pv(self.omega2, self.psi2, self.psi1, self.F2)
+        a1p = self.gen_pv(o1p, p1p, p2p, self.F1)
+        a2p = self.gen_pv(o2p, p2p, p1p, self.F2)
+        a1h = m.advect(self.alpha1, vel1, dt, a1p, vel1p)
+        a2h = m.advect(self.alpha2, vel2, dt, a2p, vel2p)
+        self.tau1, self.chi1, _, _, o1h, o2h = self.invert(a1h, a2h, self.tau1, self.chi1,
+                                                           a * 2.0 * b, a * b)
+        self.alpha1 = self.solve_q(a1h, o1h, self.r * self.F1, 0.0, self.alpha1)
+        self.alpha2 = self.solve_q(a2h, o2h, -self.r * self.F2, self.E2, self.alpha2)
+        (self.tau2, self.chi2, self.psi1, self.psi2, self.omega1,
+         self.omega2) = self.invert(self.alpha1, self.alpha2, self.tau2, self.chi2, 2.0 * b, b)
+        return saved

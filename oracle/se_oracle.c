@@ -879,6 +879,94 @@ void or_assemble_rhs(const or_mesh* m, const int* f2v, int ng, const double* rhs
   }
 }
 
+/* -------------------------------------------------- two-layer QG pieces --
+ * DissipationRHS::AssembleElement (src/qg/TwoLayerQGEqn.cpp:435-463)
+ * assembled by Vector::Assemble (src/base/Vector.cpp:89-121) into the
+ * unknowns: at every GLL point of every element, detJ w q N + c rF t N
+ * - c Ei omegaHat N - c rF tau_e N - c nu (dN/dx dW/dx + dN/dy dW/dy), with
+ * c = detJ w constant, the point values by InterpLocal (the nodal values),
+ * and the gradient of omegaHat by InterpDerivsGlobal at the point's global
+ * coordinate (Mesh::LocalToGlobal, src/base/Mesh.cpp:178-181), i.e. in the
+ * element GetEl picks there. */
+void or_dissipation_rhs(const or_mesh* m, const int* f2v, int ng, double constant,
+                        const double* field, const double* tau, const double* omega_hat,
+                        const double* tau_e, double rF, double Ei, double nu, double* f) {
+  int nn = m->nn, N = m->N;
+  int nodes[(MAXN + 1) * (MAXN + 1)], nodes2[(MAXN + 1) * (MAXN + 1)];
+  double g0[(MAXN + 1) * (MAXN + 1)], g1[(MAXN + 1) * (MAXN + 1)];
+  double gx[(MAXN + 1) * (MAXN + 1)], gy[(MAXN + 1) * (MAXN + 1)];
+  double h0[(MAXN + 1) * (MAXN + 1)], h1[(MAXN + 1) * (MAXN + 1)];
+  double hx[(MAXN + 1) * (MAXN + 1)], hy[(MAXN + 1) * (MAXN + 1)];
+  double rhs[(MAXN + 1) * (MAXN + 1)];
+  memset(f, 0, sizeof(double) * ng);
+  for (int el = 0; el < m->nElsTotal; el++) {
+    el_nodes(m, el, nodes);
+    memset(rhs, 0, sizeof(double) * nn);
+    for (int pt = 0; pt < nn; pt++) {
+      double weight = m->weights[pt % (N + 1)] * m->weights[pt / (N + 1)];
+      double det, det2, l[2], gc[2], l2[2];
+      ref_derivs_at_pt(m, pt, g0, g1);
+      global_derivs(m, el, g0, g1, gx, gy, &det);
+      double c = det * weight * constant;
+      l[0] = m->abcissa[pt % (N + 1)];
+      l[1] = m->abcissa[pt / (N + 1)];
+      gc[0] = m->min[0] + (el % m->nEls[0]) * m->dx[0] + 0.5 * (l[0] + 1.0) * m->dx[0];
+      gc[1] = m->min[1] + (el / m->nEls[0]) * m->dx[1] + 0.5 * (l[1] + 1.0) * m->dx[1];
+      double q = 0.0, t = 0.0, w = 0.0, te = 0.0;
+      for (int k = 0; k < nn; k++) {
+        double Nk = (k == pt) ? 1.0 : 0.0;
+        q += Nk * field[nodes[k]];
+        t += Nk * tau[nodes[k]];
+        w += Nk * omega_hat[nodes[k]];
+        te += Nk * tau_e[nodes[k]];
+      }
+      int el2 = global_to_local(m, gc, l2);
+      el_nodes(m, el2, nodes2);
+      shape_derivs_at(m, l2, h0, h1);
+      global_derivs(m, el2, h0, h1, hx, hy, &det2);
+      double gW0 = 0.0, gW1 = 0.0;
+      for (int k = 0; k < nn; k++) {
+        gW0 += hx[k] * omega_hat[nodes2[k]];
+        gW1 += hy[k] * omega_hat[nodes2[k]];
+      }
+      for (int k = 0; k < nn; k++) {
+        double Nk = (k == pt) ? 1.0 : 0.0;
+        rhs[k] += det * weight * q * Nk;
+        rhs[k] += c * rF * t * Nk;
+        rhs[k] -= c * Ei * w * Nk;
+        rhs[k] -= c * rF * te * Nk;
+        rhs[k] -= c * nu * (gx[k] * gW0 + gy[k] * gW1);
+      }
+    }
+    for (int k = 0; k < nn; k++) {
+      int v = f2v[nodes[k]];
+      if (v >= 0) f[v] += rhs[k];
+    }
+  }
+}
+
+/* Diagonal of TwoLayerQGEqn::AssembleQMat's matrix (src/qg/TwoLayerQGEqn.cpp:
+ * 354-394): MassMatrix(qi, qi, a) assembled over the unknowns; the GLL mass
+ * matrix is diagonal, so this is the whole matrix (and its Dirichlet lifting
+ * is zero). */
+void or_mass_diag(const or_mesh* m, const int* f2v, int ng, double a, double* d) {
+  int nn = m->nn, N = m->N;
+  int nodes[(MAXN + 1) * (MAXN + 1)];
+  double g0[(MAXN + 1) * (MAXN + 1)], g1[(MAXN + 1) * (MAXN + 1)];
+  memset(d, 0, sizeof(double) * ng);
+  for (int el = 0; el < m->nElsTotal; el++) {
+    el_nodes(m, el, nodes);
+    for (int pt = 0; pt < nn; pt++) {
+      double weight = m->weights[pt % (N + 1)] * m->weights[pt / (N + 1)];
+      double J[2][2], det;
+      ref_derivs_at_pt(m, pt, g0, g1);
+      jac_from_derivs(m, el, g0, g1, J, &det);
+      int v = f2v[nodes[pt]];
+      if (v >= 0) d[v] += det * weight * a;
+    }
+  }
+}
+
 /* ------------------------------------------------------------------ PCG --
  * PETSc KSPCG with PCJACOBI as SE runs it through
  * src/linsys/HelmholtzEqn.cpp:141-150 with -<prefix>ksp_type cg

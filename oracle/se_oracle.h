@@ -104,6 +104,14 @@ double or_field_error(const or_mesh* m, const double* numeric, const double* ana
                       int normalise);
 double or_calc_time_step(const or_mesh* m, const double* vel, double courant);
 
+/* TwoLayerQGEqn pieces (src/qg/TwoLayerQGEqn.cpp): the assembled
+ * DissipationRHS vector and the diagonal of the PV mass matrix, over the
+ * unknowns of f2v. */
+void or_dissipation_rhs(const or_mesh* m, const int* f2v, int ng, double constant,
+                        const double* field, const double* tau, const double* omega_hat,
+                        const double* tau_e, double rF, double Ei, double nu, double* f);
+void or_mass_diag(const or_mesh* m, const int* f2v, int ng, double a, double* d);
+
 #ifdef __cplusplus
 }
 #endif

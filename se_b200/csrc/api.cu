@@ -2104,3 +2104,240 @@ extern "C" int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double
     return fail(SE_ERR_NOT_CONVERGED, "KSP diverged, reason %d after %d its", out.reason, out.its);
   return SE_OK;
 }
+
+// ------------------------------------------------------ two-layer QG step --
+// TwoLayerQGEqn (src/qg/TwoLayerQGEqn.cpp:17-433) composed from this
+// library's objects: GenPV, GenVel and the step's pointwise combinations as
+// kernels (sl.cu), the PV advection by the SL advectors, the baroclinic
+// Helmholtz and barotropic Poisson inversions by se_linsys (the method and
+// precision of the given options), and SolveQ with its DissipationRHS as one
+// kernel per layer. The reference's choices are kept: the first-order step
+// applies SolveQ to layer 1 only; both layers' dissipation uses the first
+// baroclinic solution tau1; the PV mass matrix is scaled by 1.5 from the
+// first second-order step on.
+struct se_qg2 {
+  se_field *psi1, *omega1, *psi2, *omega2, *tau_e;  // the caller's
+  double F1, F2, beta, E2, r, nu, dt;
+  double a_mass;
+  bool second_assembled;
+  se_field *tau1, *chi1, *tau2, *chi2;              // psi1's boundary conditions
+  se_field *psi1h, *psi2h, *om1h, *om2h;            // psi1's boundary conditions
+  se_field *alpha1, *alpha2, *alpha1h, *alpha2h;    // psi1's boundary conditions
+  se_field *alpha1p, *alpha2p;                      // no boundary conditions
+  se_field *hrhs1, *frhs1, *hrhs2, *frhs2;          // no boundary conditions
+  se_field *vel1, *vel2, *vel1p, *vel2p, *grad;     // 2 components
+  se_field *tmp[4];
+  se_linsys *helm1, *helm2, *fish1, *fish2;
+  se_advector *adv1, *adv2, *adv1s, *adv2s;
+};
+
+namespace {
+int qg_release(se_qg2* q) {
+  se_field** fs[] = {&q->tau1, &q->chi1, &q->tau2, &q->chi2, &q->psi1h, &q->psi2h, &q->om1h,
+                     &q->om2h, &q->alpha1, &q->alpha2, &q->alpha1h, &q->alpha2h, &q->alpha1p,
+                     &q->alpha2p, &q->hrhs1, &q->frhs1, &q->hrhs2, &q->frhs2, &q->vel1,
+                     &q->vel2, &q->vel1p, &q->vel2p, &q->grad, &q->tmp[0], &q->tmp[1],
+                     &q->tmp[2], &q->tmp[3]};
+  se_advector* as[] = {q->adv1, q->adv2, q->adv1s, q->adv2s};
+  for (se_advector* a : as)
+    if (a) se_advector_destroy(a);
+  se_linsys* ls[] = {q->helm1, q->helm2, q->fish1, q->fish2};
+  for (se_linsys* l : ls)
+    if (l) se_linsys_destroy(l);
+  for (se_field** f : fs)
+    if (*f) se_field_destroy(*f);
+  delete q;
+  return SE_OK;
+}
+#define QK(call)                  \
+  do {                            \
+    if (int rc_ = (call)) return rc_; \
+  } while (0)
+
+// PV advection of one layer into alpha_hat (first order: prev == nullptr).
+int qg_advect(se_qg2* q, se_advector** adv, se_field* alpha, se_field* vel, se_field* alpha_p,
+              se_field* vel_p, se_field* alpha_hat) {
+  if (!*adv) QK(se_advector_create(alpha, vel, alpha_p, vel_p, adv));
+  QK(se_advect(*adv, q->dt));
+  return se_field_copy(alpha_hat, (*adv)->sl);
+}
+
+// Steps 2-4 (or 6-8) of the reference's step: baroclinic Helmholtz solve for
+// t from a1 - a2, barotropic Poisson solve for c, then psi/omega from them.
+int qg_invert(se_qg2* q, se_field* a1, se_field* a2, se_linsys* helm, se_field* hrhs, se_field* t,
+              se_linsys* fish, se_field* frhs, se_field* c, double cb_fish, double cb_update,
+              se_field* p1, se_field* p2, se_field* o1, se_field* o2) {
+  const MeshDev& m = q->psi1->mesh->dev;
+  CK(launch_qg_combine(m, 0, a1->vals, a2->vals, nullptr, nullptr, 0, 0, 0, hrhs->vals, nullptr,
+                       nullptr, nullptr, g_stream));
+  QK(se_linsys_solve(helm, 0, nullptr));
+  CK(launch_qg_combine(m, 1, a1->vals, a2->vals, t->vals, nullptr, q->F1, q->F2, cb_fish,
+                       frhs->vals, nullptr, nullptr, nullptr, g_stream));
+  QK(se_linsys_solve(fish, 0, nullptr));
+  CK(launch_qg_combine(m, 2, a1->vals, a2->vals, t->vals, c->vals, q->F1, q->F2, cb_update,
+                       p1->vals, p2->vals, o1->vals, o2->vals, g_stream));
+  return SE_OK;
+}
+
+// SolveQ of one layer: alpha (unknowns) = M^-1 DissipationRHS(alpha_hat, tau1, om_hat).
+int qg_solve_q(se_qg2* q, se_field* alpha_hat, se_field* om_hat, double rF, double Ei,
+               se_field* alpha) {
+  const se_mesh* me = q->psi1->mesh;
+  CK(launch_gen_vel(me->dev, om_hat->vals, q->grad->vals, nullptr, g_stream));
+  CK(launch_qg_solve_q(me->dev, q->psi1->bcs->d[0], q->psi1->bcs->d[1], q->dt, alpha_hat->vals,
+                       q->tau1->vals, om_hat->vals, q->grad->vals, q->tau_e->vals, rF, Ei, q->nu,
+                       q->a_mass, alpha->vals, g_stream));
+  return SE_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int se_qg2_create(se_field* psi1, se_field* omega1, se_field* psi2, se_field* omega2, double F1,
+                  double F2, double beta, double E2, double r, double nu, se_field* tau_e,
+                  double dt, const se_solver_opts* opts, se_qg2** out) {
+  if (!out) return fail(SE_ERR_ARG, "null argument");
+  *out = nullptr;
+  se_field* in[] = {psi1, omega1, psi2, omega2, tau_e};
+  for (se_field* f : in) {
+    if (int rc = check_field(f)) return rc;
+    if (f->ndofs != 1 || f->mesh != psi1->mesh) return fail(SE_ERR_ARG, "fields must be scalar on one mesh");
+  }
+  if (!psi1->bcs) return fail(SE_ERR_ARG, "psi1 needs boundary conditions");
+  if (psi1->mesh->dev.N < 3) return fail(SE_ERR_UNSUPPORTED, "N < 3 SL is not built");
+  se_qg2* q = new se_qg2();
+  std::memset((void*)q, 0, sizeof(*q));
+  q->psi1 = psi1;
+  q->omega1 = omega1;
+  q->psi2 = psi2;
+  q->omega2 = omega2;
+  q->tau_e = tau_e;
+  q->F1 = F1;
+  q->F2 = F2;
+  q->beta = beta;
+  q->E2 = E2;
+  q->r = r;
+  q->nu = nu;
+  q->dt = dt;
+  q->a_mass = 1.0;
+  se_mesh* me = psi1->mesh;
+  se_bcs* bc = psi1->bcs;
+  se_field** with_bc[] = {&q->tau1, &q->chi1, &q->tau2, &q->chi2, &q->psi1h, &q->psi2h, &q->om1h,
+                          &q->om2h, &q->alpha1, &q->alpha2, &q->alpha1h, &q->alpha2h};
+  se_field** no_bc[] = {&q->alpha1p, &q->alpha2p, &q->hrhs1, &q->frhs1, &q->hrhs2, &q->frhs2,
+                        &q->tmp[0], &q->tmp[1], &q->tmp[2], &q->tmp[3]};
+  se_field** two[] = {&q->vel1, &q->vel2, &q->vel1p, &q->vel2p, &q->grad};
+  int rc = SE_OK;
+  for (se_field** f : with_bc)
+    if (!rc) rc = se_field_create(me, 1, bc, f);
+  for (se_field** f : no_bc)
+    if (!rc) rc = se_field_create(me, 1, nullptr, f);
+  for (se_field** f : two)
+    if (!rc) rc = se_field_create(me, 2, nullptr, f);
+  // boundary values of the baroclinic (tau = psi1 - psi2) and barotropic
+  // (chi = psi1 + psi2) stream functions (src/qg/TwoLayerQGEqn.cpp:46-53)
+  const MeshDev& m = me->dev;
+  if (!rc && (launch_qg_combine(m, 0, psi1->vals, psi2->vals, nullptr, nullptr, 0, 0, 0,
+                                q->tau1->vals, nullptr, nullptr, nullptr, g_stream) ||
+              launch_qg_combine(m, 0, psi1->vals, psi2->vals, nullptr, nullptr, 0, 0, 0,
+                                q->tau2->vals, nullptr, nullptr, nullptr, g_stream)))
+    rc = fail(SE_ERR_CUDA, "QG set-up launch failed");
+  // chi = psi1 + psi2: the Poisson combination with zero coefficients
+  if (!rc && (launch_qg_combine(m, 1, psi1->vals, psi2->vals, psi1->vals, nullptr, 0, 0, 0,
+                                q->chi1->vals, nullptr, nullptr, nullptr, g_stream) ||
+              launch_qg_combine(m, 1, psi1->vals, psi2->vals, psi1->vals, nullptr, 0, 0, 0,
+                                q->chi2->vals, nullptr, nullptr, nullptr, g_stream)))
+    rc = fail(SE_ERR_CUDA, "QG set-up launch failed");
+  const double cmass = -(F1 + F2);
+  if (!rc) rc = se_helmholtz_create(q->tau1, q->hrhs1, cmass, -1.0, 1.0, 0, opts, &q->helm1);
+  if (!rc) rc = se_helmholtz_create(q->tau2, q->hrhs2, cmass, -1.0, 1.0, 0, opts, &q->helm2);
+  if (!rc) rc = se_poisson_create(q->chi1, q->frhs1, -1.0, opts, &q->fish1);
+  if (!rc) rc = se_poisson_create(q->chi2, q->frhs2, -1.0, opts, &q->fish2);
+  // the PV fields (src/qg/TwoLayerQGEqn.cpp:71-72)
+  if (!rc && (launch_gen_pv(m, omega1->vals, psi1->vals, psi2->vals, F1, beta, q->alpha1->vals,
+                            g_stream) ||
+              launch_gen_pv(m, omega2->vals, psi2->vals, psi1->vals, F2, beta, q->alpha2->vals,
+                            g_stream)))
+    rc = fail(SE_ERR_CUDA, "QG set-up launch failed");
+  if (rc) {
+    qg_release(q);
+    return rc;
+  }
+  *out = q;
+  return SE_OK;
+}
+
+int se_qg2_destroy(se_qg2* q) {
+  if (!q) return SE_OK;
+  return qg_release(q);
+}
+
+int se_qg2_solve(se_qg2* q, se_field* psi1p, se_field* omega1p, se_field* psi2p,
+                 se_field* omega2p) {
+  if (!q) return fail(SE_ERR_ARG, "null QG system");
+  const MeshDev& m = q->psi1->mesh->dev;
+  const bool second = psi1p && omega1p && psi2p && omega2p;
+  if (second) {
+    se_field* pv[] = {psi1p, omega1p, psi2p, omega2p};
+    for (se_field* f : pv) {
+      if (int rc = check_field(f)) return rc;
+      if (f->ndofs != 1 || f->mesh != q->psi1->mesh) return fail(SE_ERR_ARG, "previous fields do not match");
+    }
+  }
+  if (!second) {
+    // TwoLayerQGEqn::FirstOrder (src/qg/TwoLayerQGEqn.cpp:175-243)
+    CK(launch_gen_vel(m, q->psi1->vals, q->vel1->vals, nullptr, g_stream));
+    CK(launch_gen_vel(m, q->psi2->vals, q->vel2->vals, nullptr, g_stream));
+    CK(launch_gen_pv(m, q->omega1->vals, q->psi1->vals, q->psi2->vals, q->F1, q->beta,
+                     q->alpha1->vals, g_stream));
+    CK(launch_gen_pv(m, q->omega2->vals, q->psi2->vals, q->psi1->vals, q->F2, q->beta,
+                     q->alpha2->vals, g_stream));
+    QK(qg_advect(q, &q->adv1, q->alpha1, q->vel1, nullptr, nullptr, q->alpha1h));
+    QK(qg_advect(q, &q->adv2, q->alpha2, q->vel2, nullptr, nullptr, q->alpha2h));
+    QK(qg_invert(q, q->alpha1h, q->alpha2h, q->helm1, q->hrhs1, q->tau1, q->fish1, q->frhs1,
+                 q->chi1, 2.0 * q->beta, q->beta, q->psi1h, q->psi2h, q->om1h, q->om2h));
+    QK(qg_solve_q(q, q->alpha1h, q->om1h, q->r * q->F1, 0.0, q->alpha1));
+    QK(qg_invert(q, q->alpha1, q->alpha2, q->helm2, q->hrhs2, q->tau2, q->fish2, q->frhs2,
+                 q->chi2, 2.0 * q->beta, q->beta, q->psi1, q->psi2, q->omega1, q->omega2));
+    return SE_OK;
+  }
+  // TwoLayerQGEqn::Solve with previous fields (src/qg/TwoLayerQGEqn.cpp:123-172)
+  if (!q->second_assembled) {
+    q->a_mass = 1.5;
+    q->second_assembled = true;
+  }
+  QK(se_field_copy(q->tmp[0], q->psi1));
+  QK(se_field_copy(q->tmp[1], q->psi2));
+  QK(se_field_copy(q->tmp[2], q->omega1));
+  QK(se_field_copy(q->tmp[3], q->omega2));
+  // TwoLayerQGEqn::SecondOrder (src/qg/TwoLayerQGEqn.cpp:245-324)
+  const double a = 1.5;
+  CK(launch_gen_vel(m, q->psi1->vals, q->vel1->vals, nullptr, g_stream));
+  CK(launch_gen_vel(m, q->psi2->vals, q->vel2->vals, nullptr, g_stream));
+  CK(launch_gen_vel(m, psi1p->vals, q->vel1p->vals, nullptr, g_stream));
+  CK(launch_gen_vel(m, psi2p->vals, q->vel2p->vals, nullptr, g_stream));
+  CK(launch_gen_pv(m, q->omega1->vals, q->psi1->vals, q->psi2->vals, q->F1, q->beta,
+                   q->alpha1->vals, g_stream));
+  CK(launch_gen_pv(m, q->omega2->vals, q->psi2->vals, q->psi1->vals, q->F2, q->beta,
+                   q->alpha2->vals, g_stream));
+  CK(launch_gen_pv(m, omega1p->vals, psi1p->vals, psi2p->vals, q->F1, q->beta, q->alpha1p->vals,
+                   g_stream));
+  CK(launch_gen_pv(m, omega2p->vals, psi2p->vals, psi1p->vals, q->F2, q->beta, q->alpha2p->vals,
+                   g_stream));
+  QK(qg_advect(q, &q->adv1s, q->alpha1, q->vel1, q->alpha1p, q->vel1p, q->alpha1h));
+  QK(qg_advect(q, &q->adv2s, q->alpha2, q->vel2, q->alpha2p, q->vel2p, q->alpha2h));
+  QK(qg_invert(q, q->alpha1h, q->alpha2h, q->helm1, q->hrhs1, q->tau1, q->fish1, q->frhs1,
+               q->chi1, a * 2.0 * q->beta, a * q->beta, q->psi1h, q->psi2h, q->om1h, q->om2h));
+  QK(qg_solve_q(q, q->alpha1h, q->om1h, q->r * q->F1, 0.0, q->alpha1));
+  QK(qg_solve_q(q, q->alpha2h, q->om2h, -q->r * q->F2, q->E2, q->alpha2));
+  QK(qg_invert(q, q->alpha1, q->alpha2, q->helm2, q->hrhs2, q->tau2, q->fish2, q->frhs2, q->chi2,
+               2.0 * q->beta, q->beta, q->psi1, q->psi2, q->omega1, q->omega2));
+  QK(se_field_copy(psi1p, q->tmp[0]));
+  QK(se_field_copy(psi2p, q->tmp[1]));
+  QK(se_field_copy(omega1p, q->tmp[2]));
+  QK(se_field_copy(omega2p, q->tmp[3]));
+  return SE_OK;
+}
+
+}  // extern "C"
+#undef QK

@@ -85,6 +85,20 @@ cudaError_t launch_global_to_local(const MeshDev& m, const double* pts, int npts
 // Field::InterpGlobal at points (device arrays).
 cudaError_t launch_interp_global(const MeshDev& m, int ndofs, const double* vals,
                                  const double* pts, int npts, double* out, cudaStream_t s);
+// Two-layer QG step pieces (sl.cu): GenPV; pointwise combinations (kind 0
+// Helmholtz rhs, 1 Poisson rhs, 2 stream functions and vorticities); SolveQ
+// with the dissipation rhs over the unknowns of (dx, dy). grad is
+// vel-layout (-d/dy, d/dx) of omegaHat from launch_gen_vel.
+cudaError_t launch_gen_pv(const MeshDev& m, const double* omega, const double* psi_i,
+                          const double* psi_j, double F, double beta, double* alpha, cudaStream_t s);
+cudaError_t launch_qg_combine(const MeshDev& m, int kind, const double* a, const double* b,
+                              const double* t, const double* c, double F1, double F2, double cb,
+                              double* out0, double* out1, double* out2, double* out3,
+                              cudaStream_t s);
+cudaError_t launch_qg_solve_q(const MeshDev& m, const Dir& dx, const Dir& dy, double dt,
+                              const double* q, const double* tau, const double* omh,
+                              const double* grad, const double* tau_e, double rF, double Ei,
+                              double nu, double a, double* alpha, cudaStream_t s);
 // vel[Nv][2] = (-d psi/dy, d psi/dx) at every vertex (GenVel of SE's QG models).
 cudaError_t launch_gen_vel(const MeshDev& m, const double* psi, double* vel, unsigned* err,
                            cudaStream_t s);

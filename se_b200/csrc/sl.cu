@@ -534,6 +534,124 @@ __global__ void gen_vel_kernel(const MeshDev m, const double* __restrict__ psi,
   vel[j * nvx + i] = make_double2(-dy, dx);
 }
 
+// ------------------------------------------------- two-layer QG pieces ----
+// TwoLayerQGEqn::GenPV (src/qg/TwoLayerQGEqn.cpp:326-333):
+// alpha = omega + F (psi_j - psi_i) + beta y at every vertex.
+__global__ void gen_pv_kernel(const MeshDev m, const double* __restrict__ omega,
+                              const double* __restrict__ psi_i, const double* __restrict__ psi_j,
+                              double F, double beta, double* __restrict__ alpha) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= m.nVerts[0]) return;
+  const int v = j * m.nVerts[0] + i;
+  const double y = vertex_coord(m, 1, j);
+  alpha[v] = omega[v] + F * (psi_j[v] - psi_i[v]) + beta * y;
+}
+
+// The step's pointwise combinations (src/qg/TwoLayerQGEqn.cpp:186-232,
+// 264-323): kind 0: out0 = a - b (Helmholtz right-hand side); kind 1:
+// out0 = a + b + dF t - cb y (Poisson right-hand side); kind 2: the stream
+// functions and vorticities from t (baroclinic) and c (barotropic):
+// out0 = psi1, out1 = psi2, out2 = omega1, out3 = omega2.
+__global__ void qg_combine_kernel(const MeshDev m, int kind, const double* __restrict__ a,
+                                  const double* __restrict__ b, const double* __restrict__ t,
+                                  const double* __restrict__ c, double F1, double F2, double cb,
+                                  double* out0, double* out1, double* out2, double* out3) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= m.nVerts[0]) return;
+  const int v = j * m.nVerts[0] + i;
+  const double y = vertex_coord(m, 1, j);
+  if (kind == 0) {
+    out0[v] = a[v] - b[v];
+  } else if (kind == 1) {
+    out0[v] = a[v] + b[v] + (F1 - F2) * t[v] - cb * y;
+  } else {
+    const double p1 = 0.5 * (t[v] + c[v]), p2 = 0.5 * (c[v] - t[v]);
+    out0[v] = p1;
+    out1[v] = p2;
+    out2[v] = a[v] - F1 * (p2 - p1) - cb * y;
+    out3[v] = b[v] - F2 * (p1 - p2) - cb * y;
+  }
+}
+
+// Element options of a vertex along one direction: (element, node) pairs in
+// ascending element order (a shared vertex belongs to two elements; the
+// periodic seam joins the last element's node N to vertex 0).
+__device__ __forceinline__ int vertex_elements(const MeshDev& m, int d, int g, int* e, int* a) {
+  const int N = m.N, nE = m.nEls[d];
+  int k = 0;
+  const int eo = g / N, ao = g - eo * N;
+  if (ao == 0) {
+    if (eo > 0) {
+      e[k] = eo - 1;
+      a[k++] = N;
+    } else if (m.periodic[d]) {
+      e[k] = nE - 1;  // sorted below
+      a[k++] = N;
+    }
+  }
+  if (eo < nE) {
+    e[k] = eo;
+    a[k++] = ao;
+  }
+  if (k == 2 && e[0] > e[1]) {  // periodic seam: keep ascending element order
+    int te = e[0], ta = a[0];
+    e[0] = e[1];
+    a[0] = a[1];
+    e[1] = te;
+    a[1] = ta;
+  }
+  return k;
+}
+
+// TwoLayerQGEqn::SolveQ (src/qg/TwoLayerQGEqn.cpp:396-418) with the
+// DissipationRHS vector (:435-463) of one layer, per unknown: gathers the
+// element contributions at the unknown's vertex in element order,
+//   detJ w (q + dt rF t - dt Ei omegaHat - dt rF tau_e)
+//   - dt nu detJ sum_pt w_pt grad N_k(pt) . grad omegaHat(pt),
+// with grad omegaHat at a point taken as at its vertex in the element GetEl
+// picks (grad: omegaHat's GenVel field, (-d/dy, d/dx) at every vertex);
+// divides by the assembled PV mass a detJ w (the GLL mass matrix is
+// diagonal) and writes the unknown's vertex and its periodic copies
+// (Vector::UpdateField).
+__global__ void qg_solve_q_kernel(const MeshDev m, Dir dxd, Dir dyd, int G0, double dt,
+                                  const double* __restrict__ q, const double* __restrict__ tau,
+                                  const double* __restrict__ omh, const double2* __restrict__ grad,
+                                  const double* __restrict__ tau_e, double rF, double Ei, double nu,
+                                  double a, double* __restrict__ alpha) {
+  const int ux = blockIdx.x * blockDim.x + threadIdx.x, uy = blockIdx.y;
+  if (ux >= G0) return;
+  const int N = m.N, n = N + 1, nvx = m.nVerts[0], nvy = m.nVerts[1];
+  const int gx = ux + dxd.lo, gy = uy + dyd.lo;
+  const int v = gy * nvx + gx;
+  const double det = (0.5 * m.dx[0]) * (0.5 * m.dx[1]);
+  const double sx = 2.0 / m.dx[0], sy = 2.0 / m.dx[1];
+  int ex[2], ax[2], ey[2], ay[2];
+  const int kx = vertex_elements(m, 0, gx, ex, ax), ky = vertex_elements(m, 1, gy, ey, ay);
+  const double own = q[v] + dt * rF * tau[v] - dt * Ei * omh[v] - dt * rF * tau_e[v];
+  double f = 0.0, dsum = 0.0;
+  for (int jy = 0; jy < ky; jy++)      // element rows ascending ...
+    for (int jx = 0; jx < kx; jx++) {  // ... then columns: ascending element index
+      const int ex_ = ex[jx], ax_ = ax[jx], ey_ = ey[jy], ay_ = ay[jy];
+      const double wk = m.w[ax_] * m.w[ay_];
+      double gsum = 0.0;
+      // d/dx of cardinal ax_ along the node's row, d/dy along its column
+      for (int p = 0; p < n; p++) {
+        const int vx = (ey_ * N + ay_) * nvx + ex_ * N + p;
+        gsum += sx * m.w[ay_] * m.w[p] * m.dC[p * n + ax_] * grad[vx].y;   // d/dx
+        const int vy = (ey_ * N + p) * nvx + ex_ * N + ax_;
+        gsum -= sy * m.w[ax_] * m.w[p] * m.dC[p * n + ay_] * grad[vy].x;   // d/dy = -(.x)
+      }
+      f += det * wk * own - dt * nu * det * gsum;
+      dsum += a * det * wk;
+    }
+  const double x = f / dsum;
+  alpha[v] = x;
+  const bool cx = m.periodic[0] && gx == 0, cy = m.periodic[1] && gy == 0;
+  if (cx) alpha[gy * nvx + nvx - 1] = x;
+  if (cy) alpha[(nvy - 1) * nvx + gx] = x;
+  if (cx && cy) alpha[nvy * nvx - 1] = x;
+}
+
 }  // namespace
 
 // Dispatch a runtime polynomial order onto the compile-time one (NN).
@@ -559,6 +677,35 @@ cudaError_t launch_sl(const MeshDev& m, int ndofs, const double* field, const do
   if (m.N < 3) return cudaErrorInvalidValue;
   SE_DISPATCH_N(m.N, return launch_sl_n<NN>(m, ndofs, field, vel, field_prev, vel_prev, dt, out,
                                             dep_el, dep_xy, err, s));
+}
+
+cudaError_t launch_gen_pv(const MeshDev& m, const double* omega, const double* psi_i,
+                          const double* psi_j, double F, double beta, double* alpha, cudaStream_t s) {
+  const dim3 grid((m.nVerts[0] + 255) / 256, m.nVerts[1]);
+  gen_pv_kernel<<<grid, 256, 0, s>>>(m, omega, psi_i, psi_j, F, beta, alpha);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_qg_combine(const MeshDev& m, int kind, const double* a, const double* b,
+                              const double* t, const double* c, double F1, double F2, double cb,
+                              double* out0, double* out1, double* out2, double* out3,
+                              cudaStream_t s) {
+  const dim3 grid((m.nVerts[0] + 255) / 256, m.nVerts[1]);
+  qg_combine_kernel<<<grid, 256, 0, s>>>(m, kind, a, b, t, c, F1, F2, cb, out0, out1, out2, out3);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_qg_solve_q(const MeshDev& m, const Dir& dx, const Dir& dy, double dt,
+                              const double* q, const double* tau, const double* omh,
+                              const double* grad, const double* tau_e, double rF, double Ei,
+                              double nu, double a, double* alpha, cudaStream_t s) {
+  const int G0 = dx.hi - dx.lo, G1 = dy.hi - dy.lo;
+  if (G0 <= 0 || G1 <= 0) return cudaSuccess;
+  const dim3 grid((G0 + 127) / 128, G1);
+  qg_solve_q_kernel<<<grid, 128, 0, s>>>(m, dx, dy, G0, dt, q, tau, omh,
+                                         reinterpret_cast<const double2*>(grad), tau_e, rF, Ei, nu,
+                                         a, alpha);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_gen_vel(const MeshDev& m, const double* psi, double* vel, unsigned* err,

@@ -138,6 +138,9 @@ SIGNATURES = {
     "se_server_submit": [_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_longlong)],
     "se_server_wait": [_vp, ctypes.c_longlong, ctypes.POINTER(Result)],
     "se_server_destroy": [_vp],
+    "se_qg2_create": [_vp, _vp, _vp, _vp] + [ctypes.c_double] * 6 +
+                     [_vp, ctypes.c_double, ctypes.POINTER(SolverOpts), ctypes.POINTER(_vp)],
+    "se_qg2_solve": [_vp, _vp, _vp, _vp, _vp], "se_qg2_destroy": [_vp],
     "se_helmholtz_solve_noalloc": [_I, ctypes.c_int, _D, _D, _I, _I, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.POINTER(SolverOpts), ctypes.c_int, _vp, _vp,
@@ -563,6 +566,34 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+class TwoLayerQGEqn:
+    """TwoLayerQGEqn(psi1, omega1, psi2, omega2, F1, F2, beta, E2, r, nu,
+    tau_e, dt) (src/qg/TwoLayerQGEqn.h) over se_qg2_*: Solve() advances the
+    four fields one step in place (second order when the previous fields are
+    given, which are then replaced by the fields before the step)."""
+
+    def __init__(self, psi1: Field, omega1: Field, psi2: Field, omega2: Field, F1, F2, beta, E2,
+                 r, nu, tau_e: Field, dt, opts: SolverOpts | None = None):
+        self.fields = (psi1, omega1, psi2, omega2, tau_e)
+        self.opts = opts if opts is not None else solver_opts()
+        h = _vp()
+        _check(load_library().se_qg2_create(psi1._h, omega1._h, psi2._h, omega2._h, float(F1),
+                                            float(F2), float(beta), float(E2), float(r),
+                                            float(nu), tau_e._h, float(dt),
+                                            ctypes.byref(self.opts), ctypes.byref(h)))
+        self._h = h
+
+    def Solve(self, psi1Prev: Field | None = None, omega1Prev: Field | None = None,
+              psi2Prev: Field | None = None, omega2Prev: Field | None = None):
+        prev = (psi1Prev, omega1Prev, psi2Prev, omega2Prev)
+        _check(_lib.se_qg2_solve(self._h, *[f._h if f is not None else None for f in prev]))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.se_qg2_destroy(self._h)
+            self._h = None
 
 
 def GenVel(psi: Field, name: str = "vel") -> Field:
