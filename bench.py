@@ -541,6 +541,71 @@ def run_config1(steps=200, seed=11):
             "sl_ms_per_step": sl_ms / steps}
 
 
+def run_config2(steps=20, seed=5):
+    """Config 2: the two-layer QG baroclinic channel, 128 x 64 elements, p=6,
+    domain [0,2] x [0,1] periodic in x with walls in y, F1 = F2 = 400
+    (deformation radius 0.05), beta = 0.5; initial zonal jet in the upper
+    layer, psi1 = -U L tanh((y - 1/2) / L) (U = 1, L = 0.1), omega1 its
+    Laplacian plus a seeded 1e-3 perturbation, lower layer at rest; dt at
+    Courant 0.5. One first-order step, then `steps` timed second-order steps
+    (TwoLayerQGEqn::Solve) per inversion variant, CUDA events on the
+    library's stream. DOF-updates: both layers' unknowns per step."""
+    import torch
+    import se_b200 as S
+    rng = np.random.default_rng(seed)
+    nx, ny, p = 128, 64, 6
+    m = S.Mesh("m", [nx, ny], "legendre", p, [0.0, 0.0], [2.0, 1.0], [True, False])
+    X = m.verts
+    y = X[:, 1]
+    U, L = 1.0, 0.1
+    s = (y - 0.5) / L
+    psi1 = -U * L * np.tanh(s)
+    om1 = 2.0 * U * np.tanh(s) / np.cosh(s) ** 2 / L
+    wall = (np.abs(y) < 1e-12) | (np.abs(y - 1.0) < 1e-12)
+    om1 = om1 + 1e-3 * np.where(wall, 0.0, rng.standard_normal(len(y)))
+    nvx = nx * p + 1
+    om1 = om1.reshape(-1, nvx)
+    om1[:, -1] = om1[:, 0]  # periodic duplicates
+    om1 = om1.ravel()
+    zeros = np.zeros(len(y))
+    bc = S.BCs(True, True, False, False, m)
+    ng = (nx * p) * (ny * p - 1)
+    vel = S.Field("v", m, 2, None)
+    vel.vals = np.stack([U / np.cosh(s) ** 2, zeros], 1)
+    dt = S.CalcTimeStep(vel, 0.5)
+    out = {"workload": f"two-layer QG channel, {nx}x{ny} elements p={p}, F1=F2=400, jet + 1e-3 "
+                       f"perturbation, dt={dt:.5f} (Courant 0.5), {steps} second-order steps",
+           "unknowns_per_layer": ng}
+    stream = torch.cuda.Stream()
+    S.set_stream(stream.cuda_stream)
+    for name, method, prec, n in (("fdm_fp64", S.METHOD_FDM, S.PREC_FP64, steps),
+                                  ("fdm_tf32_refined_fp64", S.METHOD_FDM, S.PREC_MIXED, steps),
+                                  ("cg_fp64", S.METHOD_CG, S.PREC_FP64, max(2, steps // 10))):
+        f = [S.Field(nm, m, 1, bc if nm.startswith("psi") else None)
+             for nm in ("psi1", "omega1", "psi2", "omega2", "tau_e")]
+        for fi, v in zip(f, (psi1, om1, zeros, zeros, zeros)):
+            fi.vals = v
+        prev = [S.Field("p", m, 1, None) for _ in range(4)]
+        for fi, v in zip(prev, (psi1, om1, zeros, zeros)):
+            fi.vals = v
+        opts = S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=method, precision=prec)
+        qg = S.TwoLayerQGEqn(*f[:4], 400.0, 400.0, 0.5, 0.01, 0.001, 1e-5, f[4], dt, opts)
+        qg.Solve()
+        qg.Solve(*prev)  # warm-up (graphs, eigendecompositions)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            qg.Solve(*prev)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / n
+        psi = f[0].vals
+        out[name] = {"steps": n, "ms_per_step": ms, "dof_updates_per_s": 2 * ng / (ms * 1e-3),
+                     "finite": bool(np.all(np.isfinite(psi))), "max_abs_psi1": float(np.abs(psi).max())}
+        del qg
+    return out
+
+
 # ------------------------------------------------------ ensemble (config 3) --
 def run_ensemble(count=256, seed=2024):
     """256 independent Helmholtz solves, mesh n x n elements with n uniform in
@@ -828,6 +893,8 @@ def main():
         log("configs 0 and 1")
         extras["config0"] = run_config0()
         extras["config1"] = run_config1()
+        log("config 2")
+        extras["config2"] = run_config2()
         log("apply roofline")
         extras["apply_roofline"] = run_apply_roofline()
         log("ensemble")
