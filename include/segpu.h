@@ -111,6 +111,17 @@ int se_field_integrate(const se_field* field, int dof, int average, double* out)
  * out is double[npts][ndofs]. */
 int se_field_interp_global(const se_field* field, const double* pts, int npts, double* out);
 
+/* Field::Save(timeStep) / Field::Read(timeStep) (src/base/Field.cpp:256-368)
+ * with a raw-binary file in place of HDF5: "<name>.<timeStep, 5 digits>.seb"
+ * holds, in the HDF5 file's order, the magic "SEFIELD1", the dimensions
+ * (int32, 2), the mesh resolution (int32 nVerts[0]-1, nVerts[1]-1), the rows
+ * (int64 nVertsTotal) and columns (int32 nDofs), then the /data dataset as
+ * double[rows][columns] in the reference's vertex order; little-endian.
+ * Read checks the header against the field and fails with SE_ERR_ARG on a
+ * mismatch, a missing or a truncated file. */
+int se_field_save(const se_field* field, const char* name, int time_step);
+int se_field_read(se_field* field, const char* name, int time_step);
+
 /* TwoLayerQGEqn::GenVel / QuasiGeostrophicEqn::GenVel
  * (src/qg/TwoLayerQGEqn.cpp:335-352, src/qg/QuasiGeostrophicEqn.cpp:207-223):
  * vel (ndofs 2) = (-d psi/dy, d psi/dx) at every vertex, each derivative by

@@ -1389,6 +1389,73 @@ int se_field_integrate(const se_field* field, int dof, int average, double* out)
   *out = average ? r[0] / ((m.max[0] - m.min[0]) * (m.max[1] - m.min[1])) : r[0];
   return SE_OK;
 }
+// Field::Save / Field::Read (src/base/Field.cpp:256-368) in raw binary:
+// file "<name>.<time step, 5 digits>.seb" holding the HDF5 file's content
+// in order: magic "SEFIELD1", dimensions (int32, 2), mesh resolution (int32
+// nVerts[0]-1, nVerts[1]-1), rows (int64 nVertsTotal), columns (int32
+// nDofs), then the /data dataset as double[rows][columns]; little-endian.
+namespace {
+const char kFieldMagic[8] = {'S', 'E', 'F', 'I', 'E', 'L', 'D', '1'};
+std::string field_file(const char* name, int step) {
+  char buf[32];
+  snprintf(buf, sizeof(buf), ".%.5u.seb", (unsigned)step);
+  return std::string(name) + buf;
+}
+}  // namespace
+
+int se_field_save(const se_field* field, const char* name, int time_step) {
+  if (int rc = check_field(field)) return rc;
+  if (!name || time_step < 0) return fail(SE_ERR_ARG, "bad name or time step");
+  const se_mesh* me = field->mesh;
+  const size_t nv = (size_t)me->nVertsTotal, nd = (size_t)field->ndofs;
+  std::vector<double> h(nv * nd);
+  CK(cudaMemcpyAsync(h.data(), field->vals, sizeof(double) * h.size(), cudaMemcpyDeviceToHost,
+                     g_stream));
+  CK(cudaStreamSynchronize(g_stream));
+  const std::string fn = field_file(name, time_step);
+  FILE* f = std::fopen(fn.c_str(), "wb");
+  if (!f) return fail(SE_ERR_ARG, "cannot create %s", fn.c_str());
+  const int32_t dims = 2;
+  const int32_t res[2] = {me->dev.nVerts[0] - 1, me->dev.nVerts[1] - 1};
+  const int64_t rows = (int64_t)nv;
+  const int32_t cols = (int32_t)nd;
+  bool ok = std::fwrite(kFieldMagic, 1, 8, f) == 8 && std::fwrite(&dims, 4, 1, f) == 1 &&
+            std::fwrite(res, 4, 2, f) == 2 && std::fwrite(&rows, 8, 1, f) == 1 &&
+            std::fwrite(&cols, 4, 1, f) == 1 &&
+            std::fwrite(h.data(), sizeof(double), h.size(), f) == h.size();
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return fail(SE_ERR_ARG, "writing %s failed", fn.c_str());
+  return SE_OK;
+}
+
+int se_field_read(se_field* field, const char* name, int time_step) {
+  if (int rc = check_field(field)) return rc;
+  if (!name || time_step < 0) return fail(SE_ERR_ARG, "bad name or time step");
+  const se_mesh* me = field->mesh;
+  const std::string fn = field_file(name, time_step);
+  FILE* f = std::fopen(fn.c_str(), "rb");
+  if (!f) return fail(SE_ERR_ARG, "cannot open %s", fn.c_str());
+  char magic[8];
+  int32_t dims = 0, res[2] = {0, 0}, cols = 0;
+  int64_t rows = 0;
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kFieldMagic, 8) == 0 &&
+            std::fread(&dims, 4, 1, f) == 1 && std::fread(res, 4, 2, f) == 2 &&
+            std::fread(&rows, 8, 1, f) == 1 && std::fread(&cols, 4, 1, f) == 1;
+  if (!ok || dims != 2 || res[0] != me->dev.nVerts[0] - 1 || res[1] != me->dev.nVerts[1] - 1 ||
+      rows != (int64_t)me->nVertsTotal || cols != field->ndofs) {
+    std::fclose(f);
+    return fail(SE_ERR_ARG, "%s does not hold a field of this mesh and size", fn.c_str());
+  }
+  std::vector<double> h((size_t)rows * cols);
+  ok = std::fread(h.data(), sizeof(double), h.size(), f) == h.size();
+  std::fclose(f);
+  if (!ok) return fail(SE_ERR_ARG, "%s is truncated", fn.c_str());
+  CK(cudaMemcpyAsync(field->vals, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice,
+                     g_stream));
+  CK(cudaStreamSynchronize(g_stream));
+  return SE_OK;
+}
+
 int se_field_gen_vel(const se_field* psi, se_field* vel) {
   if (int rc = check_field(psi)) return rc;
   if (int rc = check_field(vel)) return rc;

@@ -130,7 +130,7 @@ SIGNATURES = {
                               ctypes.POINTER(SolveStats)],
     "se_linsys_solve_async": [_vp, ctypes.c_int],
     "se_linsys_solve_finish": [_vp, ctypes.POINTER(SolveStats)],
-    "se_linsys_apply": [_vp, _vp, _vp], "se_field_gen_vel": [_vp, _vp], "se_linsys_fdm_apply": [_vp, _vp, _vp], "se_linsys_apply_low": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
+    "se_linsys_apply": [_vp, _vp, _vp], "se_field_gen_vel": [_vp, _vp], "se_field_save": [_vp, ctypes.c_char_p, ctypes.c_int], "se_field_read": [_vp, ctypes.c_char_p, ctypes.c_int], "se_linsys_fdm_apply": [_vp, _vp, _vp], "se_linsys_apply_low": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
     "se_linsys_vec_size": [_vp, _I],
     "se_calc_time_step": [_vp, ctypes.c_double, _D],
     "se_field_error": [_vp, _vp, ctypes.c_int, ctypes.c_int, _D],
@@ -311,6 +311,14 @@ class Field:
 
     def Copy(self, field: "Field"):
         _check(_lib.se_field_copy(self._h, field._h))
+
+    def Save(self, timeStep: int, name: str | None = None):
+        """Field::Save: writes "<name>.<timeStep:05>.seb" (raw binary; see se_field_save)."""
+        _check(_lib.se_field_save(self._h, (name or self.name).encode(), int(timeStep)))
+
+    def Read(self, timeStep: int, name: str | None = None):
+        """Field::Read of a file written by Save."""
+        _check(_lib.se_field_read(self._h, (name or self.name).encode(), int(timeStep)))
 
     def PeriodicUpdate(self):
         _check(_lib.se_field_periodic_update(self._h))
