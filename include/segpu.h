@@ -221,6 +221,14 @@ int se_linsys_assemble(se_linsys* ls);
  * (src/linsys/HelmholtzEqn.cpp:127-158, src/linsys/PoissonEqn.cpp:102-134):
  * f = Mass*rhs + lifting, CG + Jacobi with zero initial guess, solution
  * copied into sol's unknowns and periodic copies. stats may be NULL.
+ * remove_null_space: 0 none; 1 the constant null space projected out of
+ * every preconditioned residual, as PETSc does (a right-hand side off the
+ * operator's range then stagnates and ends with
+ * SE_KSP_DIVERGED_INDEFINITE_PC, as in the reference); 2 the same after
+ * replacing f by f - (sum f / sum d) d, d the operator diagonal: the
+ * consistent system that iteration approaches, which converges (no
+ * counterpart in the reference). The FDM method always solves that
+ * consistent system when the null space is removed.
  * Returns SE_ERR_NOT_CONVERGED if the reason is negative. */
 int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats);
 /* Several solves in one call (the batched ensemble; no counterpart in the
@@ -353,10 +361,48 @@ int se_qg2_create(se_field* psi1, se_field* omega1, se_field* psi2, se_field* om
                   double dt, const se_solver_opts* opts, se_qg2** out);
 /* TwoLayerQGEqn::Solve(psi1Prev, omega1Prev, psi2Prev, omega2Prev): second
  * order when all four previous fields are given (they are then replaced by
- * the fields as they were before this step), first order when all are NULL. */
+ * the fields as they were before this step), first order when all are NULL.
+ * A solve that does not converge leaves its last iterate and the step goes
+ * on (the reference never checks); the call then returns
+ * SE_ERR_NOT_CONVERGED with the step complete. */
 int se_qg2_solve(se_qg2* qg, se_field* psi1_prev, se_field* omega1_prev, se_field* psi2_prev,
                  se_field* omega2_prev);
 int se_qg2_destroy(se_qg2* qg);
+
+/* ------------------------------------------- Navier-Stokes splitting step --
+ * Replaces NavierStokesEqn(velocity, pressure, dt) and its Solve
+ * (src/ns/NavierStokesEqn.h, .cpp:23-147): one step of the incompressible
+ * splitting scheme on the device: SL advection of the velocity by itself
+ * (first order, or second order with the previous velocity), the divergence
+ * of the advected velocity at every vertex (times 1.5 times 10.0 in the
+ * second-order step, as the reference writes it), the pressure Poisson solve
+ * (c = -dt, constant null space removed), the pressure-gradient correction
+ * and the viscous Helmholtz solve (c = 1.0, then 1.5 from the first
+ * second-order step on; nu and dt) into the velocity in place.
+ * velocity has 2 components; pressure 1 component on a mesh of the same
+ * geometry (the same object or the same parameters). The reference's
+ * per-component velocity BCs (BCs(bool*, bool*, bool*, bool*),
+ * src/base/BCs.cpp:175-) are given as one scalar se_bcs per component on the
+ * velocity's mesh (NULL: no Dirichlet sides); the velocity's own bcs are not
+ * used. The component systems are block-diagonal in the reference's
+ * interleaved matrix (src/base/Operator.cpp:67-79, :161-172) and are solved
+ * as two scalar systems. The fields must outlive the object. */
+typedef struct se_ns se_ns;
+int se_ns_create(se_field* velocity, se_field* pressure, se_bcs* bcs_u, se_bcs* bcs_v, double dt,
+                 const se_solver_opts* opts, se_ns** out);
+/* NavierStokesEqn::Solve(velocity, pressure, prevVel, nu, svvCutoff):
+ * velocity and pressure must be the fields the object was made with; prevVel
+ * NULL for the first-order step (it is read, not changed); nu is taken when
+ * the viscous systems are made (first call of each order); svvCutoff must be
+ * 0 (SE_ERR_UNSUPPORTED otherwise). A solve that does not converge leaves
+ * its last iterate and the step goes on, as in the reference; the call then
+ * returns SE_ERR_NOT_CONVERGED with the step complete (se_ns_stats shows
+ * which). */
+int se_ns_solve(se_ns* ns, se_field* velocity, se_field* pressure, se_field* prev_vel, double nu,
+                int svvCutoff);
+/* Solver statistics of the last step: [0] pressure, [1] u, [2] v. */
+int se_ns_stats(const se_ns* ns, se_solve_stats stats[3]);
+int se_ns_destroy(se_ns* ns);
 
 /* CalcTimeStep(velocity, courantNo) (src/base/Utils.cpp:23-40). */
 int se_calc_time_step(const se_field* velocity, double courant, double* dt);

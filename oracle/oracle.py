@@ -351,10 +351,15 @@ def update_field(mesh: Mesh, v2f, x, vals):
 
 def helmholtz_solve(mesh: Mesh, sol_vals, rhs_vals, c, nu, dt, bcs=(False, False, False, False),
                     quirk=True, rtol=1e-10, atol=1e-50, max_it=10000, norm_type=0,
-                    remove_null_space=False, nthreads=1, poisson=False):
+                    remove_null_space=False, nthreads=1, poisson=False, project_rhs=False):
     """HelmholtzEqn (src/linsys/HelmholtzEqn.cpp:43-158) or, with poisson=True,
     PoissonEqn(c) (src/linsys/PoissonEqn.cpp:30-134), solved by the restated
-    Jacobi-PCG. Returns the updated solution field and the solver stats."""
+    Jacobi-PCG. project_rhs (with remove_null_space) first replaces the
+    assembled right-hand side b by b - (sum b / sum d) d, d the matrix
+    diagonal: the consistent system that Jacobi CG with the null space
+    projected out of its preconditioned residuals approaches when b is off
+    the operator's range. Returns the updated solution field and the solver
+    stats."""
     f2v, v2f = mesh.bcs_maps(*bcs)
     ng = len(v2f)
     if poisson:
@@ -362,8 +367,14 @@ def helmholtz_solve(mesh: Mesh, sol_vals, rhs_vals, c, nu, dt, bcs=(False, False
     else:
         A = CSR(mesh, f2v, ng, c, nu * dt, quirk, sol_vals)
     f = assemble_rhs(mesh, f2v, ng, rhs_vals)
-    _, _, _, lift = A.arrays()
+    rowptr, col, val, lift = A.arrays()
     f = f + lift
+    if project_rhs and remove_null_space:
+        d = np.zeros(ng)
+        for k in range(ng):
+            row = slice(rowptr[k], rowptr[k + 1])
+            d[k] = val[row][col[row] == k].sum()
+        f = f - (f.sum() / d.sum()) * d
     x, stats = A.pcg(f, rtol=rtol, atol=atol, max_it=max_it, norm_type=norm_type,
                      remove_null_space=remove_null_space, nthreads=nthreads)
     out = update_field(mesh, v2f, x, sol_vals)
@@ -470,3 +481,56 @@ class QG2:
         (self.tau2, self.chi2, self.psi1, self.psi2, self.omega1,
          self.omega2) = self.invert(self.alpha1, self.alpha2, self.tau2, self.chi2, 2.0 * b, b)
         return saved
+
+
+class NS:
+    """NavierStokesEqn (src/ns/NavierStokesEqn.cpp:23-147) restated over the
+    oracle's pieces: SL advection of the velocity by itself, the divergence of
+    the advected velocity and the pressure gradient by InterpDerivsGlobal at
+    the vertices, the pressure PoissonEqn(-dt) with the constant null space
+    removed (its right-hand side projected onto the operator's range first,
+    see helmholtz_solve's project_rhs) and the viscous HelmholtzEqn(c, nu,
+    dt) per velocity component
+    (the reference's interleaved 2-component matrix is block diagonal per
+    component: src/base/Operator.cpp:67-79, :161-172), all by the restated
+    CSR + Jacobi-PCG. The second-order step scales the divergence by 1.5 and
+    10.0 and uses c = 1.5, as the reference writes it. bcs_u, bcs_v are the
+    (bottom, top, left, right) Dirichlet flags of each velocity component;
+    the pressure has none. TEST INFRASTRUCTURE ONLY."""
+
+    def __init__(self, mesh: Mesh, bcs_u, bcs_v, dt, quirk=False, rtol=1e-12):
+        self.m, self.dt, self.quirk, self.rtol = mesh, dt, quirk, rtol
+        self.bcs = (tuple(bcs_u), tuple(bcs_v))
+        self.X = mesh.verts()
+
+    def derivs(self, vals):
+        return self.m.interp_derivs_global(vals, self.X)
+
+    def step(self, vel, pres, prev_vel, nu):
+        """One Solve; returns (velocity, pressure, stats) after the step."""
+        m, dt = self.m, self.dt
+        vel, pres = _f64(vel).copy(), _f64(pres).copy()
+        second = prev_vel is not None
+        if second:
+            sl = m.advect(vel, vel, dt, _f64(prev_vel), _f64(prev_vel))
+        else:
+            sl = m.advect(vel, vel, dt)
+        div = self.derivs(np.ascontiguousarray(sl[:, 0]))[:, 0] + \
+            self.derivs(np.ascontiguousarray(sl[:, 1]))[:, 1]
+        if second:
+            div = div * 1.5 * 10.0
+        # the vertex divergence is off the Neumann operator's range by a little:
+        # solve the consistent system the reference's CG approaches
+        pres, sp = helmholtz_solve(m, pres, div, -dt, 0.0, 0.0, quirk=self.quirk, rtol=self.rtol,
+                                   remove_null_space=True, poisson=True, project_rhs=True)
+        dp = self.derivs(pres)
+        step2 = sl - dt * dp
+        c = 1.5 if second else 1.0
+        stats = [sp]
+        for d in range(2):
+            col, st = helmholtz_solve(m, np.ascontiguousarray(vel[:, d]),
+                                      np.ascontiguousarray(step2[:, d]), c, nu, dt, self.bcs[d],
+                                      quirk=self.quirk, rtol=self.rtol)
+            vel[:, d] = col
+            stats.append(st)
+        return vel, pres, stats

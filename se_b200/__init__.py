@@ -6,11 +6,13 @@ built in-tree by :mod:`se_b200.build`. :mod:`se_b200.segpu` mirrors the
 reference's classes (Mesh, BCs, Field, Advector, HelmholtzEqn, PoissonEqn)
 over that C-ABI.
 """
-from .segpu import (BCs, Advector, Server, REQ_ADVECT, REQ_HELMHOLTZ, CalcTimeStep, Field, FieldError, GenVel, HelmholtzEqn, Mesh, TwoLayerQGEqn,  # noqa: F401
+from .segpu import (BCs, Advector, Server, REQ_ADVECT, REQ_HELMHOLTZ, CalcTimeStep, Field, FieldError, GenVel, HelmholtzEqn, Mesh, NavierStokesEqn,  # noqa: F401
+                    TwoLayerQGEqn,
                     PoissonEqn, SEError, load_library, set_stream, solver_opts, synchronize, solve_batch,
                     MODE_EXACT, MODE_REFERENCE, PREC_FP64, PREC_MIXED, PREC_BF16, PREC_FP16, METHOD_CG,
                     METHOD_FDM, NORM_NATURAL,
                     NORM_PRECONDITIONED, NORM_UNPRECONDITIONED)
 
-__all__ = ["Mesh", "BCs", "Field", "Advector", "HelmholtzEqn", "PoissonEqn", "CalcTimeStep",
+__all__ = ["Mesh", "BCs", "Field", "Advector", "HelmholtzEqn", "PoissonEqn", "NavierStokesEqn",
+           "TwoLayerQGEqn", "GenVel", "CalcTimeStep",
            "FieldError", "SEError", "load_library", "set_stream", "synchronize", "solver_opts"]

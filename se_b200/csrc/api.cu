@@ -879,6 +879,11 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
               cudaGraphConditionalHandleCreate(&hc, cg, 0, 0) == cudaSuccess;
     // prologue
     ok = ok && launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, cs) == cudaSuccess;
+    // a right-hand side off the range of a singular operator: solve for the
+    // one Jacobi CG with the null space removed converges to
+    if (remove_null)
+      ok = ok && launch_project_null(ls->f, ls->dinv, n, ls->fpart, kFdmPartials,
+                                     ls->fpart + 2 * ls->fpart_n + 4, cs) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(ls->r, ls->f, sizeof(double) * n, cudaMemcpyDeviceToDevice, cs) == cudaSuccess;
     ok = ok && cudaMemsetAsync(ls->x, 0, sizeof(double) * n, cs) == cudaSuccess;
     ok = ok && launch_norms(ls->f, wv, n, nt == SE_NORM_NATURAL, ls->fpart, kFdmPartials, res, cs) == cudaSuccess;
@@ -1729,6 +1734,10 @@ int se_linsys_set_opts(se_linsys* ls, const se_solver_opts* opts) {
   if (opts->mode != old_mode) {
     fill_op(ls);
     ls->assembled = false;
+    if (ls->X1) {  // the FDM's Jacobi inverse follows the operator
+      CK(launch_op_diag(ls->op, ls->dinv, g_stream));
+      CK(launch_invert(ls->dinv, ls->n, g_stream));
+    }
   }
   return SE_OK;
 }
@@ -1740,6 +1749,8 @@ int se_linsys_assemble(se_linsys* ls) {
 }
 int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats) {
   if (!ls) return fail(SE_ERR_ARG, "null system");
+  if (remove_null_space < 0 || remove_null_space > 2)
+    return fail(SE_ERR_ARG, "remove_null_space must be 0, 1 or 2");
   if (!ls->assembled)
     if (int rc = se_linsys_assemble(ls)) return rc;
   const MeshDev& m = ls->sol->mesh->dev;
@@ -1771,6 +1782,8 @@ int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats)
 }
 int se_linsys_solve_batch(se_linsys** systems, int n, int remove_null_space, se_solve_stats* stats) {
   if (!systems || n < 0) return fail(SE_ERR_ARG, "bad argument");
+  if (remove_null_space < 0 || remove_null_space > 2)
+    return fail(SE_ERR_ARG, "remove_null_space must be 0, 1 or 2");
   for (int i = 0; i < n; i++)
     if (!systems[i]) return fail(SE_ERR_ARG, "null system %d", i);
   for (int i = 0; i < n; i++)
@@ -1858,6 +1871,8 @@ int se_linsys_solve_batch(se_linsys** systems, int n, int remove_null_space, se_
 }
 int se_linsys_solve_async(se_linsys* ls, int remove_null_space) {
   if (!ls) return fail(SE_ERR_ARG, "null system");
+  if (remove_null_space < 0 || remove_null_space > 2)
+    return fail(SE_ERR_ARG, "remove_null_space must be 0, 1 or 2");
   if (!ls->assembled)
     if (int rc = se_linsys_assemble(ls)) return rc;
   if (ls->opts.method != SE_METHOD_FDM) {
@@ -2014,6 +2029,8 @@ extern "C" int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double
     return fail(SE_ERR_UNSUPPORTED, "polynomial order %d outside [2, %d]", N, SE_MAXN);
   if (nEls[0] < 1 || nEls[1] < 1) return fail(SE_ERR_ARG, "element counts must be positive");
   if (!(max[0] > min[0]) || !(max[1] > min[1])) return fail(SE_ERR_ARG, "empty domain");
+  if (remove_null_space < 0 || remove_null_space > 2)
+    return fail(SE_ERR_ARG, "remove_null_space must be 0, 1 or 2");
   const bool b = bcs[0] != 0, t = bcs[1] != 0, l = bcs[2] != 0, r = bcs[3] != 0;
   const int perx = periodic[0] != 0, pery = periodic[1] != 0;
   if ((b || t) && pery) return fail(SE_ERR_ARG, "both periodic and non-periodic conditions in y");
@@ -2196,6 +2213,7 @@ struct se_qg2 {
   se_field *tmp[4];
   se_linsys *helm1, *helm2, *fish1, *fish2;
   se_advector *adv1, *adv2, *adv1s, *adv2s;
+  int nc;  // solves of the current step that did not converge
 };
 
 namespace {
@@ -2221,6 +2239,18 @@ int qg_release(se_qg2* q) {
     if (int rc_ = (call)) return rc_; \
   } while (0)
 
+// One solve of a composed step; a solve that stops without converging leaves
+// its last iterate in the field (as PETSc's KSPSolve does, whose callers in
+// the reference never check) and is counted, and the step goes on.
+int solve_counting(se_linsys* ls, int null, se_solve_stats* st, int* nc) {
+  const int rc = se_linsys_solve(ls, null, st);
+  if (rc == SE_ERR_NOT_CONVERGED) {
+    ++*nc;
+    return SE_OK;
+  }
+  return rc;
+}
+
 // PV advection of one layer into alpha_hat (first order: prev == nullptr).
 int qg_advect(se_qg2* q, se_advector** adv, se_field* alpha, se_field* vel, se_field* alpha_p,
               se_field* vel_p, se_field* alpha_hat) {
@@ -2237,12 +2267,17 @@ int qg_invert(se_qg2* q, se_field* a1, se_field* a2, se_linsys* helm, se_field* 
   const MeshDev& m = q->psi1->mesh->dev;
   CK(launch_qg_combine(m, 0, a1->vals, a2->vals, nullptr, nullptr, 0, 0, 0, hrhs->vals, nullptr,
                        nullptr, nullptr, g_stream));
-  QK(se_linsys_solve(helm, 0, nullptr));
+  QK(solve_counting(helm, 0, nullptr, &q->nc));
   CK(launch_qg_combine(m, 1, a1->vals, a2->vals, t->vals, nullptr, q->F1, q->F2, cb_fish,
                        frhs->vals, nullptr, nullptr, nullptr, g_stream));
-  QK(se_linsys_solve(fish, 0, nullptr));
+  QK(solve_counting(fish, 0, nullptr, &q->nc));
   CK(launch_qg_combine(m, 2, a1->vals, a2->vals, t->vals, c->vals, q->F1, q->F2, cb_update,
                        p1->vals, p2->vals, o1->vals, o2->vals, g_stream));
+  return SE_OK;
+}
+
+int qg_status(const se_qg2* q) {
+  if (q->nc) return fail(SE_ERR_NOT_CONVERGED, "%d of the step's solves did not converge", q->nc);
   return SE_OK;
 }
 
@@ -2344,6 +2379,7 @@ int se_qg2_solve(se_qg2* q, se_field* psi1p, se_field* omega1p, se_field* psi2p,
   if (!q) return fail(SE_ERR_ARG, "null QG system");
   const MeshDev& m = q->psi1->mesh->dev;
   const bool second = psi1p && omega1p && psi2p && omega2p;
+  q->nc = 0;
   if (second) {
     se_field* pv[] = {psi1p, omega1p, psi2p, omega2p};
     for (se_field* f : pv) {
@@ -2366,7 +2402,7 @@ int se_qg2_solve(se_qg2* q, se_field* psi1p, se_field* omega1p, se_field* psi2p,
     QK(qg_solve_q(q, q->alpha1h, q->om1h, q->r * q->F1, 0.0, q->alpha1));
     QK(qg_invert(q, q->alpha1, q->alpha2, q->helm2, q->hrhs2, q->tau2, q->fish2, q->frhs2,
                  q->chi2, 2.0 * q->beta, q->beta, q->psi1, q->psi2, q->omega1, q->omega2));
-    return SE_OK;
+    return qg_status(q);
   }
   // TwoLayerQGEqn::Solve with previous fields (src/qg/TwoLayerQGEqn.cpp:123-172)
   if (!q->second_assembled) {
@@ -2403,7 +2439,179 @@ int se_qg2_solve(se_qg2* q, se_field* psi1p, se_field* omega1p, se_field* psi2p,
   QK(se_field_copy(psi2p, q->tmp[1]));
   QK(se_field_copy(omega1p, q->tmp[2]));
   QK(se_field_copy(omega2p, q->tmp[3]));
+  return qg_status(q);
+}
+
+}  // extern "C"
+
+// ------------------------------------------- Navier-Stokes splitting step --
+// NavierStokesEqn (src/ns/NavierStokesEqn.cpp:23-147) composed from this
+// library's objects: the SL advector (velocity by itself), the divergence and
+// pressure-gradient kernels (sl.cu), the pressure PoissonEqn(pressure,
+// divVelStep1, -dt) solved with the constant null space removed, and the
+// viscous HelmholtzEqn(velocity, velStep2, c, nu, dt) as one scalar system
+// per velocity component (the reference's interleaved system is block
+// diagonal per component). As in the reference, the viscous systems are made
+// (and their Dirichlet values taken from the velocity) on the first
+// first-order step with c = 1.0 and again on the first second-order step with
+// c = 1.5; the pressure system is made once.
+struct se_ns {
+  se_field *velocity, *pressure;  // the caller's
+  se_bcs *bcs_u, *bcs_v;          // the caller's (may be null)
+  double dt;
+  se_solver_opts opts;
+  bool second_done;
+  se_field *div, *step2;     // divVelStep1 (1 component), velStep2 (2 components)
+  se_field *u, *v, *ru, *rv; // velocity components and their right-hand sides
+  se_linsys *poisson, *hu, *hv;
+  se_advector *adv1, *adv2;  // first order; second order (previous velocity set per call)
+  unsigned* err;
+  se_solve_stats st[3];
+};
+
+namespace {
+bool same_geometry(const se_mesh* a, const se_mesh* b) {
+  if (a == b) return true;
+  const MeshDev &x = a->dev, &y = b->dev;
+  return x.N == y.N && x.nEls[0] == y.nEls[0] && x.nEls[1] == y.nEls[1] &&
+         x.periodic[0] == y.periodic[0] && x.periodic[1] == y.periodic[1] &&
+         x.min[0] == y.min[0] && x.min[1] == y.min[1] && x.max[0] == y.max[0] &&
+         x.max[1] == y.max[1];
+}
+
+int ns_release(se_ns* n) {
+  se_advector* as[] = {n->adv1, n->adv2};
+  for (se_advector* a : as)
+    if (a) se_advector_destroy(a);
+  se_linsys* ls[] = {n->poisson, n->hu, n->hv};
+  for (se_linsys* l : ls)
+    if (l) se_linsys_destroy(l);
+  se_field* fs[] = {n->div, n->step2, n->u, n->v, n->ru, n->rv};
+  for (se_field* f : fs)
+    if (f) se_field_destroy(f);
+  dfree(n->err);
+  delete n;
   return SE_OK;
+}
+
+// (Re)make the two viscous systems with mass coefficient c.
+int ns_make_viscous(se_ns* n, double c, double nu) {
+  if (n->hu) se_linsys_destroy(n->hu);
+  if (n->hv) se_linsys_destroy(n->hv);
+  n->hu = n->hv = nullptr;
+  QK(se_helmholtz_create(n->u, n->ru, c, nu, n->dt, 0, &n->opts, &n->hu));
+  return se_helmholtz_create(n->v, n->rv, c, nu, n->dt, 0, &n->opts, &n->hv);
+}
+}  // namespace
+
+extern "C" {
+
+int se_ns_create(se_field* velocity, se_field* pressure, se_bcs* bcs_u, se_bcs* bcs_v, double dt,
+                 const se_solver_opts* opts, se_ns** out) {
+  if (!out) return fail(SE_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (int rc = check_field(velocity)) return rc;
+  if (int rc = check_field(pressure)) return rc;
+  if (velocity->ndofs != 2 || pressure->ndofs != 1)
+    return fail(SE_ERR_ARG, "velocity needs 2 components and pressure 1");
+  if (!same_geometry(velocity->mesh, pressure->mesh))
+    return fail(SE_ERR_UNSUPPORTED, "pressure mesh of another geometry is not built");
+  se_bcs* bs[] = {bcs_u, bcs_v};
+  for (se_bcs* b : bs)
+    if (b && b->mesh != velocity->mesh) return fail(SE_ERR_ARG, "component BCs on another mesh");
+  if (velocity->mesh->dev.N < 3) return fail(SE_ERR_UNSUPPORTED, "N < 3 SL is not built");
+  se_solver_opts o;
+  if (opts) {
+    if (int rc = check_opts(opts)) return rc;
+    o = *opts;
+  } else {
+    se_solver_opts_default(&o);
+  }
+  se_ns* n = new se_ns();
+  std::memset((void*)n, 0, sizeof(*n));
+  n->velocity = velocity;
+  n->pressure = pressure;
+  n->bcs_u = bcs_u;
+  n->bcs_v = bcs_v;
+  n->dt = dt;
+  n->opts = o;
+  se_mesh* me = velocity->mesh;
+  int rc = dalloc(&n->err, 1);
+  if (!rc) rc = se_field_create(pressure->mesh, 1, nullptr, &n->div);
+  if (!rc) rc = se_field_create(me, 2, nullptr, &n->step2);
+  if (!rc) rc = se_field_create(me, 1, bcs_u, &n->u);
+  if (!rc) rc = se_field_create(me, 1, bcs_v, &n->v);
+  if (!rc) rc = se_field_create(me, 1, nullptr, &n->ru);
+  if (!rc) rc = se_field_create(me, 1, nullptr, &n->rv);
+  if (!rc) rc = se_poisson_create(pressure, n->div, -dt, &n->opts, &n->poisson);
+  if (rc) {
+    ns_release(n);
+    return rc;
+  }
+  *out = n;
+  return SE_OK;
+}
+
+int se_ns_solve(se_ns* n, se_field* velocity, se_field* pressure, se_field* prev_vel, double nu,
+                int svvCutoff) {
+  if (!n) return fail(SE_ERR_ARG, "null Navier-Stokes system");
+  if (velocity != n->velocity || pressure != n->pressure)
+    return fail(SE_ERR_ARG, "velocity and pressure must be the fields the system was made with");
+  if (svvCutoff != 0) return fail(SE_ERR_UNSUPPORTED, "spectral vanishing viscosity not built");
+  const bool second = prev_vel != nullptr;
+  if (second) {
+    if (int rc = check_field(prev_vel)) return rc;
+    if (prev_vel->ndofs != 2 || prev_vel->mesh != velocity->mesh)
+      return fail(SE_ERR_ARG, "previous velocity does not match");
+  }
+  const se_mesh* me = velocity->mesh;
+  const MeshDev& m = me->dev;
+  const int nv = me->nVertsTotal;
+  // advective step: the velocity advected by itself (a new Advector per step
+  // in the reference; here one per order, the previous velocity set per call)
+  se_advector** adv = second ? &n->adv2 : &n->adv1;
+  if (!*adv) QK(se_advector_create(velocity, velocity, prev_vel, prev_vel, adv));
+  (*adv)->field_prev = prev_vel;
+  (*adv)->vel_prev = prev_vel;
+  QK(se_advect(*adv, n->dt));
+  const double* sl = (*adv)->sl->vals;
+  // pressure step
+  CK(cudaMemsetAsync(n->err, 0, sizeof(unsigned), g_stream));
+  CK(launch_ns_pressure(m, second ? 2 : 0, sl, nullptr, 0.0, n->div->vals, n->err, g_stream));
+  int nc = 0;  // solves that stopped without converging (the step goes on, as in the reference)
+  QK(solve_counting(n->poisson, 2, &n->st[0], &nc));
+  CK(launch_ns_pressure(m, 1, sl, pressure->vals, n->dt, n->step2->vals, n->err, g_stream));
+  // viscous step
+  if (!second && !n->hu) QK(ns_make_viscous(n, 1.0, nu));
+  if (second && !n->second_done) QK(ns_make_viscous(n, 1.5, nu));
+  CK(launch_component(nv, 1, 0, velocity->vals, n->u->vals, g_stream));
+  CK(launch_component(nv, 1, 1, velocity->vals, n->v->vals, g_stream));
+  CK(launch_component(nv, 1, 0, n->step2->vals, n->ru->vals, g_stream));
+  CK(launch_component(nv, 1, 1, n->step2->vals, n->rv->vals, g_stream));
+  QK(solve_counting(n->hu, 0, &n->st[1], &nc));
+  QK(solve_counting(n->hv, 0, &n->st[2], &nc));
+  CK(launch_component(nv, 0, 0, velocity->vals, n->u->vals, g_stream));
+  CK(launch_component(nv, 0, 1, velocity->vals, n->v->vals, g_stream));
+  if (second) n->second_done = true;
+  unsigned herr = 0;
+  CK(cudaMemcpyAsync(&herr, n->err, sizeof(unsigned), cudaMemcpyDeviceToHost, g_stream));
+  CK(cudaStreamSynchronize(g_stream));
+  if (herr) return fail(SE_ERR_CUDA, "Navier-Stokes derivative kernel error bits 0x%x", herr);
+  if (nc)
+    return fail(SE_ERR_NOT_CONVERGED, "%d of the step's solves did not converge (reasons %d %d %d)",
+                nc, n->st[0].reason, n->st[1].reason, n->st[2].reason);
+  return SE_OK;
+}
+
+int se_ns_stats(const se_ns* n, se_solve_stats stats[3]) {
+  if (!n || !stats) return fail(SE_ERR_ARG, "null argument");
+  for (int k = 0; k < 3; k++) stats[k] = n->st[k];
+  return SE_OK;
+}
+
+int se_ns_destroy(se_ns* n) {
+  if (!n) return SE_OK;
+  return ns_release(n);
 }
 
 }  // extern "C"

@@ -28,7 +28,13 @@
 // 141-150): zero initial guess, preconditioned/unpreconditioned/natural
 // norm, RTOL/ATOL/DTOL/ITS, and the sign checks for an indefinite matrix
 // or preconditioner; a constant null space is projected out of every
-// preconditioned residual.
+// preconditioned residual. With remove_null == 2 the right-hand side b is
+// first replaced by b - (sum b / sum d) d (d the operator diagonal): the
+// system whose solution that iteration approaches. On a b already in the
+// operator's range this changes nothing beyond rounding; on a b off it (a
+// divergence formed at the vertices, say) PETSc's iteration (remove_null ==
+// 1) stagnates at the size of the off-range part and ends on an indefinite
+// inner product, where this one converges.
 #include "common.cuh"
 #include "fdm_ctl.cuh"
 
@@ -36,7 +42,7 @@ namespace seg {
 namespace {
 
 struct SolveState {
-  double beta, betaold, dpi, bcoef, a, rnorm0, ttol, dp, zmean;
+  double beta, betaold, dpi, bcoef, a, rnorm0, ttol, dp, zmean, cproj;
   int its, done, reason, pbuf;
 };
 struct SolveMeta {
@@ -272,12 +278,11 @@ __device__ __forceinline__ double apply_n(const OpSm& o, const double* P, int tx
 }
 
 template <int N>
-__device__ __forceinline__ double dinv_n(const OpSm& o, int gx, int gy) {
+__device__ __forceinline__ double diag_n(const OpSm& o, int gx, int gy) {
   const int ex = gx / N, ax = gx - ex * N, ey = gy / N, ay = gy - ey * N;
   const double wx = wsum_n<N>(o.dx, o.w, ex, ax), wy = wsum_n<N>(o.dy, o.w, ey, ay);
-  const double d = o.alpha * wx * wy + o.beta0 * kdiag_n<N>(o.dx, o.Kh, ex, ax) * wy +
-                   o.beta1 * wx * kdiag_n<N>(o.dy, o.Kh, ey, ay);
-  return 1.0 / d;
+  return o.alpha * wx * wy + o.beta0 * kdiag_n<N>(o.dx, o.Kh, ex, ax) * wy +
+         o.beta1 * wx * kdiag_n<N>(o.dy, o.Kh, ey, ay);
 }
 
 // --------------------------------------------------------------- scalars --
@@ -304,7 +309,7 @@ __device__ __forceinline__ double norm_of(const SolveMeta& m, double zz, double 
   return m.norm_type == 0 ? sqrt(zz) : (m.norm_type == 1 ? sqrt(rr) : sqrt(fabs(zr)));
 }
 
-enum Step { ST_MEAN = 0, ST_START, ST_APPLY, ST_UPDATE };
+enum Step { ST_PROJ = 0, ST_MEAN, ST_START, ST_APPLY, ST_UPDATE };
 
 // After a barrier: every block updates every solve's state from the partial
 // sums, warp w taking solves w, w + nwarps, ...; then counts active solves.
@@ -318,11 +323,13 @@ __device__ __forceinline__ int update_states(const CgBatch& B, const double* par
   for (int s = w; s < B.nsolves; s += nw) {
     SolveState& S = st[s];
     const SolveMeta& M = mt[s];
-    if (STEP != ST_MEAN && S.done) continue;
+    if (STEP != ST_MEAN && STEP != ST_PROJ && S.done) continue;
     double v[4];
     seg_sum4(part, M.seg_begin, M.seg_end, v);
     if (l != 0) continue;
-    if (STEP == ST_MEAN) {
+    if (STEP == ST_PROJ) {
+      S.cproj = M.remove_null == 2 ? v[0] / v[1] : 0.0;
+    } else if (STEP == ST_MEAN) {
       S.zmean = M.remove_null ? v[3] / M.n : 0.0;
     } else if (STEP == ST_START) {
       const double dp = norm_of(M, v[0], v[1], v[2]);
@@ -379,7 +386,7 @@ __device__ __forceinline__ int update_states(const CgBatch& B, const double* par
   return s_active;
 }
 
-enum Pass { PS_INIT = 0, PS_NULL, PS_APPLY, PS_UPDATE };
+enum Pass { PS_PROJ = 0, PS_INIT, PS_NULL, PS_APPLY, PS_UPDATE };
 
 template <int N, int K>
 struct Regs {
@@ -412,7 +419,7 @@ __device__ __forceinline__ void pass(const CgBatch& B, double* part, const Solve
       for (int q = 0; q < 4; q++) acc[q] = 0.0;
     }
     const SolveState& S = st[T.solve];
-    if (S.done && PASS != PS_INIT) return;
+    if (S.done && PASS != PS_INIT && PASS != PS_PROJ) return;
     load_op(o, B.solves[T.solve], T.solve);
     const int ux = T.x0 + tx, uy = T.y0 + ty;
     const bool in = ux < o.G0 && uy < o.G1;
@@ -438,9 +445,13 @@ __device__ __forceinline__ void pass(const CgBatch& B, double* part, const Solve
       return;
     }
     if (!in) return;
-    if (PASS == PS_INIT) {
-      const double r = o.b[k];
-      const double di = dinv_n<N>(o, gx, gy);
+    if (PASS == PS_PROJ) {  // sums of b and of the diagonal
+      acc[0] += o.b[k];
+      acc[1] += diag_n<N>(o, gx, gy);
+    } else if (PASS == PS_INIT) {
+      const double d = diag_n<N>(o, gx, gy);
+      const double r = o.b[k] - S.cproj * d;
+      const double di = 1.0 / d;
       const double z = r * di;
       if (K > 0) {
         R.x[kk] = 0.0;
@@ -521,7 +532,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) cg_n_kernel(const CgBatch B) {
   if (threadIdx.x == 0) o.solve = -1;
   for (int t = t0 + threadIdx.x; t < t1 && t - t0 < kTileCache; t += kCgThreads)
     tcache[t - t0] = B.tiles[t];
-  bool any_null = false;
+  bool any_null = false, any_proj = false;
   for (int s = threadIdx.x; s < B.nsolves; s += kCgThreads) {
     const CgSolve& C = B.solves[s];
     SolveMeta& M = mt[s];
@@ -535,11 +546,15 @@ __global__ void __launch_bounds__(kCgThreads, 1) cg_n_kernel(const CgBatch B) {
     M.atol = C.atol;
     M.dtol = C.dtol;
     SolveState& S = st[s];
-    S.beta = S.betaold = S.dpi = S.bcoef = S.a = S.rnorm0 = S.ttol = S.dp = S.zmean = 0.0;
+    S.beta = S.betaold = S.dpi = S.bcoef = S.a = S.rnorm0 = S.ttol = S.dp = S.zmean = S.cproj =
+        0.0;
     S.its = S.done = S.reason = S.pbuf = 0;
   }
   __syncthreads();
-  for (int s = 0; s < B.nsolves; s++) any_null |= mt[s].remove_null != 0;
+  for (int s = 0; s < B.nsolves; s++) {
+    any_null |= mt[s].remove_null != 0;
+    any_proj |= mt[s].remove_null == 2;
+  }
 
   // Partial sums alternate between two buffers pass by pass: a block that
   // has passed barrier k may write pass k+1's sums while a slower block still
@@ -547,6 +562,12 @@ __global__ void __launch_bounds__(kCgThreads, 1) cg_n_kernel(const CgBatch B) {
   // arrived at barrier k+1, i.e. finished reading pass k's.
   int pc = 0;
   auto part = [&]() { return B.partials + (size_t)(pc & 1) * B.nseg * 4; };
+  if (any_proj) {
+    pass<N, K, PS_PROJ>(B, part(), st, o, P, red, R, t0, t1, tcache);
+    if (!grid_sync(B.bar_count, B.err)) return;
+    update_states<ST_PROJ>(B, part(), st, mt);
+    ++pc;
+  }
   pass<N, K, PS_INIT>(B, part(), st, o, P, red, R, t0, t1, tcache);
   if (!grid_sync(B.bar_count, B.err)) return;
   update_states<ST_MEAN>(B, part(), st, mt);

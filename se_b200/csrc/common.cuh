@@ -85,6 +85,15 @@ cudaError_t launch_global_to_local(const MeshDev& m, const double* pts, int npts
 // Field::InterpGlobal at points (device arrays).
 cudaError_t launch_interp_global(const MeshDev& m, int ndofs, const double* vals,
                                  const double* pts, int npts, double* out, cudaStream_t s);
+// NavierStokesEqn pressure step (sl.cu): kind 0 out = div(a) (a 2
+// components), kind 2 out = div(a) * 1.5 * 10.0, kind 1 out = a - dt grad p;
+// derivatives as InterpDerivsGlobal at the vertices. err (may be null) gets
+// KERR_BAD_CONFIG if a vertex does not snap to an element's nodes.
+cudaError_t launch_ns_pressure(const MeshDev& m, int kind, const double* a, const double* p,
+                               double dt, double* out, unsigned* err, cudaStream_t s);
+// Component dof of a 2-component field to (to_scalar) or from a scalar field.
+cudaError_t launch_component(int nv, int to_scalar, int dof, double* two, double* one,
+                             cudaStream_t s);
 // Two-layer QG step pieces (sl.cu): GenPV; pointwise combinations (kind 0
 // Helmholtz rhs, 1 Poisson rhs, 2 stream functions and vorticities); SolveQ
 // with the dissipation rhs over the unknowns of (dx, dy). grad is
@@ -247,6 +256,11 @@ cudaError_t launch_maxabs(const double* x, size_t n, double* partial, int npart,
                           cudaStream_t s);
 cudaError_t launch_sub(const double* b, const double* y, double* r, size_t n, cudaStream_t s);
 cudaError_t launch_invert(double* x, size_t n, cudaStream_t s);
+// f -= (sum f / sum d) d with d = 1 / dinv: the right-hand side that Jacobi
+// CG with the constant null space projected out of every preconditioned
+// residual converges to (its limit solves A x = f - c d, c = sum f / sum d).
+cudaError_t launch_project_null(double* f, const double* dinv, size_t n, double* partial,
+                                int npart, double* sum2, cudaStream_t s);
 cudaError_t launch_remove_mean(double* x, size_t n, double* partial, int npart, double* sum2,
                                cudaStream_t s);
 

@@ -189,6 +189,33 @@ __global__ void __launch_bounds__(256) sum_partials_kernel(const double* __restr
   if (threadIdx.x == 0) partial[2 * blockIdx.x] = s, partial[2 * blockIdx.x + 1] = 0.0;
 }
 
+// Per-block partial sums of f and of d = 1 / dinv (the Jacobi diagonal).
+__global__ void __launch_bounds__(256) null_partials_kernel(const double* __restrict__ f,
+                                                            const double* __restrict__ dinv,
+                                                            size_t n, double* __restrict__ partial) {
+  double s0 = 0.0, s1 = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x) {
+    s0 += f[k];
+    s1 += 1.0 / dinv[k];
+  }
+  s0 = block_sum(s0);
+  __syncthreads();
+  s1 = block_sum(s1);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = s0;
+    partial[2 * blockIdx.x + 1] = s1;
+  }
+}
+// f -= (sum f / sum d) d
+__global__ void null_project_kernel(double* __restrict__ f, const double* __restrict__ dinv,
+                                    size_t n, const double* __restrict__ sum2) {
+  const double c = sum2[0] / sum2[1];
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x)
+    f[k] -= c / dinv[k];
+}
+
 __global__ void invert_kernel(double* __restrict__ x, size_t n) {
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
        k += (size_t)gridDim.x * blockDim.x)
@@ -288,6 +315,16 @@ cudaError_t launch_remove_mean(double* x, size_t n, double* partial, int npart, 
   sum_partials_kernel<<<b, 256, 0, s>>>(x, n, partial);
   norm_final_kernel<<<1, 256, 0, s>>>(partial, b, sum2);
   sub_mean_kernel<<<blocks_for(n), 256, 0, s>>>(x, n, sum2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_project_null(double* f, const double* dinv, size_t n, double* partial,
+                                int npart, double* sum2, cudaStream_t s) {
+  int b = blocks_for(n);
+  if (b > npart) b = npart;
+  null_partials_kernel<<<b, 256, 0, s>>>(f, dinv, n, partial);
+  norm_final_kernel<<<1, 256, 0, s>>>(partial, b, sum2);
+  null_project_kernel<<<blocks_for(n), 256, 0, s>>>(f, dinv, n, sum2);
   return cudaGetLastError();
 }
 

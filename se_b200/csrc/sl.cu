@@ -472,22 +472,19 @@ __global__ void max_partials_kernel(const double* partial, int np, double* out) 
 // the Jacobian, its inverse and the sums are formed in the reference's order
 // over the row and column entries (the zero products leave the sums as they
 // are), with exactly rounded operations.
+// d/dx, d/dy of component `dof` of an ndofs-component field at vertex (i, j)
+// (returns false if the vertex's local coordinates did not snap to nodes).
 template <int N>
-__global__ void gen_vel_kernel(const MeshDev m, const double* __restrict__ psi,
-                               double2* __restrict__ vel, unsigned* err) {
+__device__ __forceinline__ bool vertex_derivs(const MeshDev& m, const double* __restrict__ vals,
+                                              int ndofs, int dof, int i, int j, double& dx,
+                                              double& dy, unsigned* err) {
   constexpr int n = N + 1;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = blockIdx.y * blockDim.y + threadIdx.y;
-  const int nvx = m.nVerts[0], nvy = m.nVerts[1];
-  if (i >= nvx || j >= nvy) return;
+  const int nvx = m.nVerts[0];
   const double gx = vertex_coord(m, 0, i), gy = vertex_coord(m, 1, j);
   const int tx = get_topo(m, 0, gx, err), ty = get_topo(m, 1, gy, err);
   const int xi = snap_node<N>(m, local_coord(m, 0, gx, tx));
   const int yi = snap_node<N>(m, local_coord(m, 1, gy, ty));
-  if (xi < 0 || yi < 0) {  // a vertex always lies on a node
-    if (err) atomicOr(err, (unsigned)KERR_BAD_CONFIG);
-    return;
-  }
+  if (xi < 0 || yi < 0) return false;
   const int base = ty * N * nvx + tx * N;
   const double* rowd = m.dC + xi * n;  // d/dxi of the cardinals along the row
   const double* cold = m.dC + yi * n;  // d/deta along the column
@@ -509,29 +506,98 @@ __global__ void gen_vel_kernel(const MeshDev m, const double* __restrict__ psi,
   const double det = xsub(xmul(J00, J11), xmul(J01, J10));
   const double I00 = xdiv(J11, det), I11 = xdiv(J00, det);
   const double I01 = xdiv(-J01, det), I10 = xdiv(-J10, det);
-  // d psi/dx, d psi/dy: sums over the element's nodes in node order (row
-  // yj, column xj); only the node's row and column contribute
-  double dx = 0.0, dy = 0.0;
+  // sums over the element's nodes in node order (row yj, column xj); only
+  // the node's row and column contribute
+  double sx = 0.0, sy = 0.0;
 #pragma unroll
   for (int yj = 0; yj < n; yj++) {
     if (yj == yi) {
 #pragma unroll
       for (int xj = 0; xj < n; xj++) {
         const double g0 = rowd[xj], g1 = xj == xi ? cold[yj] : 0.0;
-        const double p = __ldg(psi + base + yj * nvx + xj);
+        const double p = __ldg(vals + (size_t)(base + yj * nvx + xj) * ndofs + dof);
         const double tx_ = xadd(xmul(g0, I00), xmul(g1, I01));
         const double ty_ = xadd(xmul(g0, I10), xmul(g1, I11));
-        dx = xadd(dx, xmul(tx_, p));
-        dy = xadd(dy, xmul(ty_, p));
+        sx = xadd(sx, xmul(tx_, p));
+        sy = xadd(sy, xmul(ty_, p));
       }
     } else {
       const double g1 = cold[yj];
-      const double p = __ldg(psi + base + yj * nvx + xi);
-      dx = xadd(dx, xmul(xmul(g1, I01), p));
-      dy = xadd(dy, xmul(xmul(g1, I11), p));
+      const double p = __ldg(vals + (size_t)(base + yj * nvx + xi) * ndofs + dof);
+      sx = xadd(sx, xmul(xmul(g1, I01), p));
+      sy = xadd(sy, xmul(xmul(g1, I11), p));
     }
   }
-  vel[j * nvx + i] = make_double2(-dy, dx);
+  dx = sx;
+  dy = sy;
+  return true;
+}
+
+// TwoLayerQGEqn::GenVel / QuasiGeostrophicEqn::GenVel
+// (src/qg/TwoLayerQGEqn.cpp:335-352, src/qg/QuasiGeostrophicEqn.cpp:207-223):
+// vel = (-d psi/dy, d psi/dx) at every vertex, each derivative from
+// Field::InterpDerivsGlobal (src/base/Field.cpp:96-118) in the element that
+// GetEl picks for the vertex. A vertex's local coordinates are GLL nodes in
+// both directions, so Mesh::ShapeFuncDerivsAtCoord gives d/dxi = dC[xi][j] on
+// the node's row and d/deta = dC[yi][j] on its column, exact zeros elsewhere;
+// the Jacobian, its inverse and the sums are formed in the reference's order
+// over the row and column entries (the zero products leave the sums as they
+// are), with exactly rounded operations.
+template <int N>
+__global__ void gen_vel_kernel(const MeshDev m, const double* __restrict__ psi,
+                               double2* __restrict__ vel, unsigned* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= m.nVerts[0] || j >= m.nVerts[1]) return;
+  double dx, dy;
+  if (!vertex_derivs<N>(m, psi, 1, 0, i, j, dx, dy, err)) {  // a vertex always lies on a node
+    if (err) atomicOr(err, (unsigned)KERR_BAD_CONFIG);
+    return;
+  }
+  vel[j * m.nVerts[0] + i] = make_double2(-dy, dx);
+}
+
+// NavierStokesEqn's pressure step (src/ns/NavierStokesEqn.cpp:63-85 and
+// :109-131): kind 0: out[v] = du/dx + dv/dy of the 2-component field a;
+// kind 2: the same times 1.5 times 10.0 (the second-order step's factor, as
+// the reference writes it); kind 1: out[v] = a[v] - dt grad p (a 2
+// components, p scalar).
+template <int N>
+__global__ void ns_pressure_kernel(const MeshDev m, int kind, const double* __restrict__ a,
+                                   const double* __restrict__ p, double dt,
+                                   double* __restrict__ out, unsigned* err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  if (i >= m.nVerts[0] || j >= m.nVerts[1]) return;
+  const int v = j * m.nVerts[0] + i;
+  if (kind != 1) {
+    double ux, uy, vx, vy;
+    if (!vertex_derivs<N>(m, a, 2, 0, i, j, ux, uy, err) ||
+        !vertex_derivs<N>(m, a, 2, 1, i, j, vx, vy, err)) {
+      if (err) atomicOr(err, (unsigned)KERR_BAD_CONFIG);
+      return;
+    }
+    out[v] = kind == 2 ? (ux + vy) * 1.5 * 10.0 : ux + vy;
+  } else {
+    double px, py;
+    if (!vertex_derivs<N>(m, p, 1, 0, i, j, px, py, err)) {
+      if (err) atomicOr(err, (unsigned)KERR_BAD_CONFIG);
+      return;
+    }
+    out[2 * v] = a[2 * v] - dt * px;
+    out[2 * v + 1] = a[2 * v + 1] - dt * py;
+  }
+}
+
+// Component `dof` of a 2-component field to / from a scalar field.
+__global__ void component_kernel(int nv, int to_scalar, int dof, double* __restrict__ two,
+                                 double* __restrict__ one) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  if (to_scalar)
+    one[v] = two[2 * v + dof];
+  else
+    two[2 * v + dof] = one[v];
 }
 
 // ------------------------------------------------- two-layer QG pieces ----
@@ -677,6 +743,22 @@ cudaError_t launch_sl(const MeshDev& m, int ndofs, const double* field, const do
   if (m.N < 3) return cudaErrorInvalidValue;
   SE_DISPATCH_N(m.N, return launch_sl_n<NN>(m, ndofs, field, vel, field_prev, vel_prev, dt, out,
                                             dep_el, dep_xy, err, s));
+}
+
+cudaError_t launch_ns_pressure(const MeshDev& m, int kind, const double* a, const double* p,
+                               double dt, double* out, unsigned* err, cudaStream_t s) {
+  const dim3 block(32, 8);
+  const dim3 grid((m.nVerts[0] + 31) / 32, (m.nVerts[1] + 7) / 8);
+  SE_DISPATCH_N(m.N, {
+    ns_pressure_kernel<NN><<<grid, block, 0, s>>>(m, kind, a, p, dt, out, err);
+    return cudaGetLastError();
+  });
+}
+
+cudaError_t launch_component(int nv, int to_scalar, int dof, double* two, double* one,
+                             cudaStream_t s) {
+  component_kernel<<<(nv + 255) / 256, 256, 0, s>>>(nv, to_scalar, dof, two, one);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_gen_pv(const MeshDev& m, const double* omega, const double* psi_i,

@@ -141,6 +141,10 @@ SIGNATURES = {
     "se_qg2_create": [_vp, _vp, _vp, _vp] + [ctypes.c_double] * 6 +
                      [_vp, ctypes.c_double, ctypes.POINTER(SolverOpts), ctypes.POINTER(_vp)],
     "se_qg2_solve": [_vp, _vp, _vp, _vp, _vp], "se_qg2_destroy": [_vp],
+    "se_ns_create": [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.POINTER(SolverOpts),
+                     ctypes.POINTER(_vp)],
+    "se_ns_solve": [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int],
+    "se_ns_stats": [_vp, ctypes.POINTER(SolveStats)], "se_ns_destroy": [_vp],
     "se_helmholtz_solve_noalloc": [_I, ctypes.c_int, _D, _D, _I, _I, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.POINTER(SolverOpts), ctypes.c_int, _vp, _vp,
@@ -241,11 +245,27 @@ class Mesh:
 
 
 class BCs:
-    """BCs(bottom, top, left, right, mesh, 0) for a scalar field (src/base/BCs.h:3)."""
+    """BCs(bottom, top, left, right, mesh, 0) (src/base/BCs.h:3). With one
+    flag per side it is the scalar constructor (src/base/BCs.cpp:14-); with a
+    pair of flags per side it is the 2-component constructor
+    (src/base/BCs.cpp:175-), held as one scalar BCs per component in
+    ``components`` (used by NavierStokesEqn's viscous step)."""
 
     def __init__(self, bcBottom, bcTop, bcLeft, bcRight, mesh: Mesh, vecOffset=0):
         if vecOffset != 0:
             raise SEError(SE_ERR_UNSUPPORTED, "vecOffset != 0 (block systems) is not built")
+        sides = (bcBottom, bcTop, bcLeft, bcRight)
+        self.components = None
+        if any(isinstance(b, (list, tuple, np.ndarray)) for b in sides):
+            pairs = [tuple(b) if isinstance(b, (list, tuple, np.ndarray)) else (b, b)
+                     for b in sides]
+            if any(len(p) != 2 for p in pairs):
+                raise SEError(SE_ERR_ARG, "per-component BCs need two flags per side")
+            self.components = tuple(BCs(*(bool(p[d]) for p in pairs), mesh) for d in range(2))
+            self._h, self.mesh = None, mesh
+            self.size = [c.vecSize for c in self.components]
+            self.vecSize = sum(self.size)
+            return
         h = _vp()
         _check(load_library().se_bcs_create(mesh._h, int(bcBottom), int(bcTop), int(bcLeft),
                                             int(bcRight), ctypes.byref(h)))
@@ -255,6 +275,8 @@ class BCs:
         self.vecSize = n.value
 
     def maps(self):
+        if self.components is not None:
+            raise SEError(SE_ERR_UNSUPPORTED, "maps of per-component BCs: use components[d]")
         f2v = np.zeros(self.mesh.nVertsTotal, dtype=np.int32)
         v2f = np.zeros(self.vecSize, dtype=np.int32)
         _check(_lib.se_bcs_maps(self._h, _pi(f2v), _pi(v2f)))
@@ -415,9 +437,10 @@ class _LinSys:
         self.opts = opts
         _check(_lib.se_linsys_set_opts(self._h, ctypes.byref(opts)))
 
-    def _solve(self, removeNullSpace: bool, raise_on_diverge: bool):
+    def _solve(self, removeNullSpace: bool, raise_on_diverge: bool, projectRHS: bool = False):
         st = SolveStats()
-        rc = _lib.se_linsys_solve(self._h, int(bool(removeNullSpace)), ctypes.byref(st))
+        null = (2 if projectRHS else 1) if removeNullSpace else 0
+        rc = _lib.se_linsys_solve(self._h, null, ctypes.byref(st))
         if rc == SE_ERR_NOT_CONVERGED and not raise_on_diverge:
             rc = SE_OK
         _check(rc)
@@ -467,14 +490,15 @@ class HelmholtzEqn(_LinSys):
         self._h = h
 
     def Solve(self, name: str = "helm_", removeNullSpace: bool = False, options: str = "",
-              raise_on_diverge: bool = False):
+              raise_on_diverge: bool = False, projectRHS: bool = False):
         """HelmholtzEqn::Solve(name, removeNullSpace); ``options`` is the PETSc
-        options string consulted under prefix ``name``."""
+        options string consulted under prefix ``name``; projectRHS (with
+        removeNullSpace) solves the consistent system (se_linsys_solve mode 2)."""
         if options:
             o = SolverOpts.from_buffer_copy(self.opts)
             _check(_lib.se_solver_opts_parse(ctypes.byref(o), name.encode(), options.encode()))
             self.set_opts(o)
-        return self._solve(removeNullSpace, raise_on_diverge)
+        return self._solve(removeNullSpace, raise_on_diverge, projectRHS)
 
 
 class PoissonEqn(_LinSys):
@@ -490,13 +514,14 @@ class PoissonEqn(_LinSys):
         self._h = h
 
     def Solve(self, removeNullSpace: bool = False, options: str = "",
-              raise_on_diverge: bool = False):
-        """PoissonEqn::Solve(removeNullSpace) with the options prefix "poisson_"."""
+              raise_on_diverge: bool = False, projectRHS: bool = False):
+        """PoissonEqn::Solve(removeNullSpace) with the options prefix "poisson_";
+        projectRHS as for HelmholtzEqn.Solve."""
         if options:
             o = SolverOpts.from_buffer_copy(self.opts)
             _check(_lib.se_solver_opts_parse(ctypes.byref(o), b"poisson_", options.encode()))
             self.set_opts(o)
-        return self._solve(removeNullSpace, raise_on_diverge)
+        return self._solve(removeNullSpace, raise_on_diverge, projectRHS)
 
 
 def solve_batch(systems, removeNullSpace: bool = False, raise_on_diverge: bool = False):
@@ -594,13 +619,57 @@ class TwoLayerQGEqn:
         self._h = h
 
     def Solve(self, psi1Prev: Field | None = None, omega1Prev: Field | None = None,
-              psi2Prev: Field | None = None, omega2Prev: Field | None = None):
+              psi2Prev: Field | None = None, omega2Prev: Field | None = None,
+              raise_on_diverge: bool = False):
         prev = (psi1Prev, omega1Prev, psi2Prev, omega2Prev)
-        _check(_lib.se_qg2_solve(self._h, *[f._h if f is not None else None for f in prev]))
+        rc = _lib.se_qg2_solve(self._h, *[f._h if f is not None else None for f in prev])
+        if rc == SE_ERR_NOT_CONVERGED and not raise_on_diverge:
+            rc = SE_OK  # the step completed, as the reference's does
+        _check(rc)
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.se_qg2_destroy(self._h)
+            self._h = None
+
+
+class NavierStokesEqn:
+    """NavierStokesEqn(velocity, pressure, dt) (src/ns/NavierStokesEqn.h)
+    over se_ns_*: Solve(velocity, pressure, prevVel, nu, svvCutoff) advances
+    the velocity and pressure one splitting step in place (second order when
+    prevVel is given; prevVel is only read). The velocity's Dirichlet sides
+    are its BCs' (per-component BCs, or one scalar BCs for both components);
+    ``stats`` holds the last step's pressure, u and v solver statistics."""
+
+    def __init__(self, velocity: Field, pressure: Field, dt, opts: SolverOpts | None = None):
+        b = velocity.bcs
+        comps = (None, None) if b is None else (b.components or (b, b))
+        self.fields, self.bcs = (velocity, pressure), comps
+        self.opts = opts if opts is not None else solver_opts()
+        h = _vp()
+        _check(load_library().se_ns_create(velocity._h, pressure._h,
+                                           comps[0]._h if comps[0] else None,
+                                           comps[1]._h if comps[1] else None, float(dt),
+                                           ctypes.byref(self.opts), ctypes.byref(h)))
+        self._h = h
+        self.stats = None
+
+    def Solve(self, velocity: Field, pressure: Field, prevVel: Field | None, nu,
+              svvCutoff: int = 0, raise_on_diverge: bool = False):
+        rc = _lib.se_ns_solve(self._h, velocity._h, pressure._h,
+                              prevVel._h if prevVel is not None else None, float(nu),
+                              int(svvCutoff))
+        if rc == SE_ERR_NOT_CONVERGED and not raise_on_diverge:
+            rc = SE_OK  # the step completed, as the reference's does
+        _check(rc)
+        st = (SolveStats * 3)()
+        _check(_lib.se_ns_stats(self._h, st))
+        self.stats = [x.as_dict() for x in st]
+        return self.stats
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.se_ns_destroy(self._h)
             self._h = None
 
 

@@ -215,7 +215,9 @@ def test_poisson_null_space(segpu, oracle):
     """Doubly periodic Poisson with a constant null space removed, for a
     consistent right-hand side (zero mean): converges like the oracle. With an
     inconsistent one (nonzero mean) the projected Jacobi-CG breaks down and
-    both report KSP_DIVERGED_INDEFINITE_PC at the same iteration."""
+    both report KSP_DIVERGED_INDEFINITE_PC at the same iteration; with the
+    right-hand side projected onto the range (mode 2) CG and FDM converge to
+    the oracle's solution of the consistent system."""
     case = (6, 6, 5, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False))
     om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, case, -1.0, 0, 0, True,
                                                      poisson=True)
@@ -237,6 +239,17 @@ def test_poisson_null_space(segpu, oracle):
     out2 = ls.Solve(removeNullSpace=True)
     assert st2["reason"] == out2["reason"] == -8
     assert abs(st2["its"] - out2["its"]) <= 1
+    # mode 2: the right-hand side projected onto the range first; CG and FDM
+    # both converge to the oracle's solution of that consistent system
+    ref3, st3 = oracle.helmholtz_solve(om, sol, bad, -1.0, 0, 0, quirk=True, rtol=1e-12,
+                                       remove_null_space=True, poisson=True, project_rhs=True)
+    assert st3["reason"] == 2
+    for method in (segpu.METHOD_CG, segpu.METHOD_FDM):
+        ls.set_opts(segpu.solver_opts(rtol=1e-12, method=method))
+        out3 = ls.Solve(removeNullSpace=True, projectRHS=True, raise_on_diverge=True)
+        assert out3["reason"] == 2
+        assert np.abs(fs.vals - ref3).max() <= 1e-9 * np.abs(ref3).max()
+    assert segpu.load_library().se_linsys_solve(ls._h, 3, None) == segpu.SE_ERR_ARG
 
 
 def test_solver_reasons(segpu, oracle):
