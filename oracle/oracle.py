@@ -83,6 +83,9 @@ def lib():
         L.or_field_rhs_element.argtypes = [_vp, _D, _int, _D]
         L.or_assemble.restype = _vp
         L.or_assemble.argtypes = [_vp, _I, _int, _dbl, _dbl, _int, _D]
+        L.or_assemble_svv.restype = _vp
+        L.or_assemble_svv.argtypes = [_vp, _I, _int, _dbl, _dbl, _int, _D, _dbl, _int]
+        L.or_svv_element.argtypes = [_vp, _int, _dbl, _int, _D]
         L.or_csr_destroy.argtypes = [_vp]
         L.or_csr_matvec.argtypes = [_vp, _D, _D, _int]
         L.or_assemble_rhs.argtypes = [_vp, _I, _int, _D, _D]
@@ -128,6 +131,7 @@ def ref():
         R.ref_bcs_vecsize.argtypes = [_vp]
         R.ref_bcs_maps.argtypes = [_vp, _I, _I]
         R.ref_element_matrix.argtypes = [_vp, _int, _dbl, _dbl, _D]
+        R.ref_svv_element.argtypes = [_vp, _int, _dbl, _int, _D]
         R.ref_field_rhs_element.argtypes = [_vp, _D, _int, _D]
         R.ref_advect.argtypes = [_vp, _int, _D, _D, _D, _D, _dbl, _D]
         R.ref_departure_first.argtypes = [_vp, _D, _dbl, _D, _I]
@@ -246,6 +250,16 @@ class Mesh:
             self.L.or_element_matrix(self.h, el, c_mass, c_lap, int(bool(quirk)), _pd(M))
         return M.reshape(nn, nn)
 
+    def svv_element(self, el, constant, cutoff):
+        """SVV(constant, cutoff)'s element matrix (SVV::AssembleElement)."""
+        nn = (self.N + 1) ** 2
+        M = np.zeros(nn * nn)
+        if self.use_ref:
+            self.L.ref_svv_element(self.h, el, constant, cutoff, _pd(M))
+        elif self.L.or_svv_element(self.h, el, constant, cutoff, _pd(M)) != 0:
+            raise ValueError("singular dense matrix in the SVV element")
+        return M.reshape(nn, nn)
+
     def field_rhs_element(self, vals, el):
         vals = _f64(vals)
         out = np.zeros((self.N + 1) ** 2)
@@ -286,13 +300,17 @@ class Mesh:
 
 
 class CSR:
-    def __init__(self, mesh: Mesh, f2v, ng, c_mass, c_lap, quirk=True, sol_vals=None):
+    """The assembled operator (or_assemble): c_mass*Mass + c_lap*Laplacian,
+    plus SVV(constant, cutoff) when svv = (constant, cutoff) is given."""
+
+    def __init__(self, mesh: Mesh, f2v, ng, c_mass, c_lap, quirk=True, sol_vals=None, svv=None):
         assert not mesh.use_ref
         self.mesh, self.L = mesh, mesh.L
         self.f2v = np.ascontiguousarray(f2v, dtype=np.int32)
         sv = None if sol_vals is None else _f64(sol_vals)
-        self.h = self.L.or_assemble(mesh.h, _pi(self.f2v), ng, c_mass, c_lap, int(bool(quirk)),
-                                    _pd(sv))
+        svc, svn = (0.0, 0) if svv is None else (float(svv[0]), int(svv[1]))
+        self.h = self.L.or_assemble_svv(mesh.h, _pi(self.f2v), ng, c_mass, c_lap,
+                                        int(bool(quirk)), _pd(sv), svc, svn)
         self.n = ng
 
     class _View(ctypes.Structure):
@@ -351,10 +369,13 @@ def update_field(mesh: Mesh, v2f, x, vals):
 
 def helmholtz_solve(mesh: Mesh, sol_vals, rhs_vals, c, nu, dt, bcs=(False, False, False, False),
                     quirk=True, rtol=1e-10, atol=1e-50, max_it=10000, norm_type=0,
-                    remove_null_space=False, nthreads=1, poisson=False, project_rhs=False):
+                    remove_null_space=False, nthreads=1, poisson=False, project_rhs=False,
+                    svv_cutoff=0):
     """HelmholtzEqn (src/linsys/HelmholtzEqn.cpp:43-158) or, with poisson=True,
     PoissonEqn(c) (src/linsys/PoissonEqn.cpp:30-134), solved by the restated
-    Jacobi-PCG. project_rhs (with remove_null_space) first replaces the
+    Jacobi-PCG; a Helmholtz system with svv_cutoff != 0 adds the SVV
+    operator SVV(dt, svv_cutoff) as HelmholtzEqn does (src/linsys/
+    HelmholtzEqn.cpp:71). project_rhs (with remove_null_space) first replaces the
     assembled right-hand side b by b - (sum b / sum d) d, d the matrix
     diagonal: the consistent system that Jacobi CG with the null space
     projected out of its preconditioned residuals approaches when b is off
@@ -365,7 +386,8 @@ def helmholtz_solve(mesh: Mesh, sol_vals, rhs_vals, c, nu, dt, bcs=(False, False
     if poisson:
         A = CSR(mesh, f2v, ng, 0.0, c, quirk, sol_vals)
     else:
-        A = CSR(mesh, f2v, ng, c, nu * dt, quirk, sol_vals)
+        A = CSR(mesh, f2v, ng, c, nu * dt, quirk, sol_vals,
+                svv=(dt, svv_cutoff) if svv_cutoff else None)
     f = assemble_rhs(mesh, f2v, ng, rhs_vals)
     rowptr, col, val, lift = A.arrays()
     f = f + lift
@@ -506,8 +528,9 @@ class NS:
     def derivs(self, vals):
         return self.m.interp_derivs_global(vals, self.X)
 
-    def step(self, vel, pres, prev_vel, nu):
-        """One Solve; returns (velocity, pressure, stats) after the step."""
+    def step(self, vel, pres, prev_vel, nu, svv_cutoff=0):
+        """One Solve(velocity, pressure, prevVel, nu, svvCutoff); returns
+        (velocity, pressure, stats) after the step."""
         m, dt = self.m, self.dt
         vel, pres = _f64(vel).copy(), _f64(pres).copy()
         second = prev_vel is not None
@@ -530,7 +553,7 @@ class NS:
         for d in range(2):
             col, st = helmholtz_solve(m, np.ascontiguousarray(vel[:, d]),
                                       np.ascontiguousarray(step2[:, d]), c, nu, dt, self.bcs[d],
-                                      quirk=self.quirk, rtol=self.rtol)
+                                      quirk=self.quirk, rtol=self.rtol, svv_cutoff=svv_cutoff)
             vel[:, d] = col
             stats.append(st)
         return vel, pres, stats

@@ -10,7 +10,8 @@
 //   Legendre tables     src/base/Legendre.cpp:15-125
 //   Mesh / GetEl        src/base/Mesh.cpp:17-84, 109-176
 //   BCs maps            src/base/BCs.cpp:14-195
-//   element matrices    src/base/Operator.cpp:63-84 (Laplacian), 157-177 (MassMatrix)
+//   element matrices    src/base/Operator.cpp:63-84 (Laplacian), 157-177 (MassMatrix),
+//                       src/base/SVV.cpp:50-176 (SVV)
 //   FieldRHS            src/base/RHSOp.cpp:31-50
 //   Advector            src/base/Advector.cpp:136-274
 //   InterpDerivsGlobal  src/base/Field.cpp:96-118
@@ -37,6 +38,7 @@
 #include "Operator.h"
 #include "RHSOp.h"
 #include "Advector.h"
+#include "SVV.h"
 #undef private
 
 namespace {
@@ -138,6 +140,17 @@ void ref_element_matrix(void* m, int el, double cMass, double cLap, double* M) {
   Laplacian lap("l", &f, &f, cLap);
   if (cMass != 0.0) mass.AssembleElement(el, M);
   if (cLap != 0.0) lap.AssembleElement(el, M);
+}
+
+// SVV(constant, mN) element matrix for element el of a scalar field (the
+// operator HelmholtzEqn adds when svvCutoff != 0, src/linsys/HelmholtzEqn.cpp:71).
+void ref_svv_element(void* m, int el, double constant, int mN, double* M) {
+  Mesh* mesh = (Mesh*)m;
+  Field f("f", mesh, 1, NULL);
+  int nn = mesh->el->nNodes;
+  std::memset(M, 0, sizeof(double) * nn * nn);
+  SVV svv("s", &f, &f, constant, mN);
+  svv.AssembleElement(el, M);
 }
 
 // FieldRHS (constant 1) element vector for element el of a scalar field.

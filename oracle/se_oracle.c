@@ -720,6 +720,152 @@ void or_element_matrix(const or_mesh* m, int el, double cMass, double cLap,
   }
 }
 
+/* ------------------------------------------------------------------ SVV --
+ * Spectral vanishing viscosity element matrix, restated literally from
+ * src/base/SVV.cpp:120-176 (AssembleElement) with the modal basis of
+ * src/base/Legendre.cpp:307-335 (ModalBasis: (1+x)/2, (1-x)/2, then
+ * (1-x^2)/4 P_{i-2}^{(1,1)}) and the dense helpers of src/base/LinAlg.cpp
+ * (Tran, Mult, Inv; the inverse here is Gauss-Jordan with partial pivoting,
+ * equal to the reference's full-pivoting one up to rounding). Adds
+ * constant*(Lxx + Lyy) to M; Lyy is formed from MinvQMDx exactly as the
+ * reference forms it. */
+static void svv_mult(const double* A, const double* B, double* C, int n) {
+  for (int i = 0; i < n * n; i++) C[i] = 0.0;
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++)
+      for (int k = 0; k < n; k++) C[i * n + j] += A[i * n + k] * B[k * n + j];
+}
+static void svv_tran(const double* A, double* At, int n) {
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) At[j * n + i] = A[i * n + j];
+}
+static int svv_inv(const double* A, double* Ainv, int n) {
+  double* a = (double*)malloc(sizeof(double) * n * n);
+  memcpy(a, A, sizeof(double) * n * n);
+  for (int i = 0; i < n * n; i++) Ainv[i] = 0.0;
+  for (int i = 0; i < n; i++) Ainv[i * n + i] = 1.0;
+  for (int c = 0; c < n; c++) {
+    int p = c;
+    for (int r = c + 1; r < n; r++)
+      if (fabs(a[r * n + c]) > fabs(a[p * n + c])) p = r;
+    if (a[p * n + c] == 0.0) {
+      free(a);
+      return -1;
+    }
+    if (p != c)
+      for (int k = 0; k < n; k++) {
+        double t = a[c * n + k];
+        a[c * n + k] = a[p * n + k];
+        a[p * n + k] = t;
+        t = Ainv[c * n + k];
+        Ainv[c * n + k] = Ainv[p * n + k];
+        Ainv[p * n + k] = t;
+      }
+    const double inv = 1.0 / a[c * n + c];
+    for (int k = 0; k < n; k++) {
+      a[c * n + k] *= inv;
+      Ainv[c * n + k] *= inv;
+    }
+    for (int r = 0; r < n; r++) {
+      if (r == c) continue;
+      const double f = a[r * n + c];
+      if (f == 0.0) continue;
+      for (int k = 0; k < n; k++) {
+        a[r * n + k] -= f * a[c * n + k];
+        Ainv[r * n + k] -= f * Ainv[c * n + k];
+      }
+    }
+  }
+  free(a);
+  return 0;
+}
+/* modal[i][0..N]: monomial coefficients of modal basis function i. */
+static void svv_modal_basis(int N, double* modal) {
+  double Pn[MAXN + 1][MAXN + 2];
+  memset(Pn, 0, sizeof(Pn));
+  memset(modal, 0, sizeof(double) * (N + 1) * (N + 1));
+  Pn[0][0] = 1.0;
+  if (N >= 1) Pn[1][1] = 2.0;
+  for (int i = 2; i <= N; i++) jac_gen(i, 1.0, Pn[i - 1], i - 1, Pn[i - 2], i - 2, Pn[i]);
+  modal[0 * (N + 1) + 0] = +0.5;
+  modal[0 * (N + 1) + 1] = +0.5;
+  modal[1 * (N + 1) + 0] = +0.5;
+  modal[1 * (N + 1) + 1] = -0.5;
+  for (int i = 2; i <= N; i++)
+    for (int j = 0; j < i - 1; j++) {
+      modal[i * (N + 1) + j] += 0.25 * Pn[i - 2][j];
+      modal[i * (N + 1) + j + 2] -= 0.25 * Pn[i - 2][j];
+    }
+}
+/* Jacobi::EvalTotal of a degree-n coefficient array. */
+static double svv_eval_total(int n, const double* c, double x) {
+  double p = 0.0;
+  for (int i = n; i >= 0; i--) p += c[i] * pow(x, i);
+  return p;
+}
+int or_svv_element(const or_mesh* m, int el, double constant, int mN, double* M) {
+  const int N = m->N, nn = m->nn, n1 = N + 1;
+  const size_t sz = sizeof(double) * nn * nn;
+  double *Q = calloc(1, sz), *W = calloc(1, sz), *Lxx = calloc(1, sz), *Lyy = calloc(1, sz),
+         *B = calloc(1, sz), *Bt = calloc(1, sz), *BtW = calloc(1, sz), *BtWB = calloc(1, sz),
+         *BtWBinv = calloc(1, sz), *Mm = calloc(1, sz), *Minv = calloc(1, sz),
+         *Dx = calloc(1, sz), *Dy = calloc(1, sz), *MinvQ = calloc(1, sz), *MinvQM = calloc(1, sz),
+         *MinvQMDx = calloc(1, sz), *MinvQMDy = calloc(1, sz), *MinvQMDxt = calloc(1, sz),
+         *MinvQMDyt = calloc(1, sz), *MinvQMDxtW = calloc(1, sz), *MinvQMDytW = calloc(1, sz);
+  double modal[(MAXN + 1) * (MAXN + 1)];
+  double g0[(MAXN + 1) * (MAXN + 1)], g1[(MAXN + 1) * (MAXN + 1)];
+  svv_modal_basis(N, modal);
+  int rc = 0;
+  for (int i = 0; i < nn; i++) {
+    const int ix = i / n1, iy = i % n1; /* GetRowCol(i, &ix, &iy, N+1) */
+    const double weight = m->weights[i % n1] * m->weights[i / n1];
+    double J[2][2], detJac;
+    ref_derivs_at_pt(m, i, g0, g1); /* el->ShapeFuncDerivs(i) */
+    jac_from_derivs(m, el, g0, g1, J, &detJac);
+    for (int j = 0; j < nn; j++) {
+      const int jx = j / n1, jy = j % n1;
+      const int djx = jx < 2 ? 1 : jx, djy = jy < 2 ? 1 : jy; /* modal degree */
+      B[i * nn + j] = svv_eval_total(djx, modal + jx * n1, m->abcissa[ix]) *
+                      svv_eval_total(djy, modal + jy * n1, m->abcissa[iy]);
+      W[i * nn + j] = Q[i * nn + j] = 0.0;
+      if (i == j) {
+        W[i * nn + j] = detJac * weight;
+        if (jx > mN && jy > mN) {
+          double qExpX = -1.0 * ((double)(N - jx) * (N - jx)) / ((mN - jx) * (mN - jx));
+          double qExpY = -1.0 * ((double)(N - jy) * (N - jy)) / ((mN - jy) * (mN - jy));
+          Q[i * nn + j] = sqrt(exp(qExpX + qExpY));
+        }
+      }
+      Dx[i * nn + j] = g0[j];
+      Dy[i * nn + j] = g1[j];
+    }
+  }
+  svv_tran(B, Bt, nn); /* (the reference's Dxt, Dyt are never used) */
+  svv_mult(Bt, W, BtW, nn);
+  svv_mult(BtW, B, BtWB, nn);
+  if (svv_inv(BtWB, BtWBinv, nn)) rc = -1;
+  svv_mult(BtWBinv, BtW, Mm, nn);
+  if (!rc && svv_inv(Mm, Minv, nn)) rc = -1;
+  if (!rc) {
+    svv_mult(Minv, Q, MinvQ, nn);
+    svv_mult(MinvQ, Mm, MinvQM, nn);
+    svv_mult(MinvQM, Dx, MinvQMDx, nn);
+    svv_mult(MinvQM, Dy, MinvQMDy, nn);
+    svv_tran(MinvQMDx, MinvQMDxt, nn);
+    svv_tran(MinvQMDy, MinvQMDyt, nn);
+    svv_mult(MinvQMDxt, W, MinvQMDxtW, nn);
+    svv_mult(MinvQMDyt, W, MinvQMDytW, nn);
+    svv_mult(MinvQMDxtW, MinvQMDx, Lxx, nn);
+    svv_mult(MinvQMDxtW, MinvQMDx, Lyy, nn); /* as the reference: from MinvQMDx */
+    for (int r = 0; r < nn; r++)
+      for (int c = 0; c < nn; c++) M[r * nn + c] += constant * (Lxx[r * nn + c] + Lyy[r * nn + c]);
+  }
+  double* all[] = {Q, W, Lxx, Lyy, B, Bt, BtW, BtWB, BtWBinv, Mm, Minv, Dx, Dy, MinvQ, MinvQM,
+                   MinvQMDx, MinvQMDy, MinvQMDxt, MinvQMDyt, MinvQMDxtW, MinvQMDytW};
+  for (size_t k = 0; k < sizeof(all) / sizeof(all[0]); k++) free(all[k]);
+  return rc;
+}
+
 /* src/base/RHSOp.cpp:31-50 (FieldRHS, constant 1): at GLL points the
  * interpolation snaps to the nodal value and the shape functions are a
  * Kronecker delta, so each node gets detJ*w*f plus zeros. */
@@ -751,6 +897,13 @@ static int cmp_int(const void* a, const void* b) {
 }
 or_csr* or_assemble(const or_mesh* m, const int* f2v, int ng, double cMass,
                     double cLap, int quirk, const double* sol_vals) {
+  return or_assemble_svv(m, f2v, ng, cMass, cLap, quirk, sol_vals, 0.0, 0);
+}
+/* HelmholtzEqn's operators in its order (src/linsys/HelmholtzEqn.cpp:74-76):
+ * mass, Laplacian, then SVV(svvConstant, svvCutoff) when svvCutoff != 0. */
+or_csr* or_assemble_svv(const or_mesh* m, const int* f2v, int ng, double cMass,
+                        double cLap, int quirk, const double* sol_vals, double svvConstant,
+                        int svvCutoff) {
   int nn = m->nn;
   int nodes[(MAXN + 1) * (MAXN + 1)], rows[(MAXN + 1) * (MAXN + 1)];
   /* pattern: for each row the set of columns reached by any element */
@@ -807,6 +960,7 @@ or_csr* or_assemble(const or_mesh* m, const int* f2v, int ng, double cMass,
   double* rhs = (double*)malloc(sizeof(double) * nn);
   for (int el = 0; el < m->nElsTotal; el++) {
     or_element_matrix(m, el, cMass, cLap, quirk, M);
+    if (svvCutoff) or_svv_element(m, el, svvConstant, svvCutoff, M);
     el_nodes(m, el, nodes);
     for (int r = 0; r < nn; r++) rows[r] = f2v[nodes[r]];
     for (int r = 0; r < nn; r++) {

@@ -78,6 +78,14 @@ typedef struct {
 } or_csr;
 or_csr* or_assemble(const or_mesh* m, const int* field_to_vec, int ng,
                     double cMass, double cLap, int quirk, const double* sol_vals);
+/* The same with HelmholtzEqn's SVV operator (constant svvConstant, cutoff
+ * svvCutoff; none when svvCutoff == 0) added to every element matrix. */
+or_csr* or_assemble_svv(const or_mesh* m, const int* field_to_vec, int ng, double cMass,
+                        double cLap, int quirk, const double* sol_vals, double svvConstant,
+                        int svvCutoff);
+/* SVV::AssembleElement (src/base/SVV.cpp:120-176): M += constant*(Lxx+Lyy).
+ * Returns -1 if a dense inverse fails. */
+int or_svv_element(const or_mesh* m, int el, double constant, int mN, double* M);
 void or_csr_destroy(or_csr* A);
 void or_csr_matvec(const or_csr* A, const double* x, double* y, int nthreads);
 /* Vector::Assemble of FieldRHS(1.0) over rhs_vals into f[ng] (zeroed first). */

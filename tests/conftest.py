@@ -49,4 +49,4 @@ def segpu():
 def golden():
     import numpy as np
     d = os.path.join(ROOT, "tests", "golden")
-    return {k: np.load(os.path.join(d, f"{k}.npz")) for k in ("gll", "mesh", "sl")}
+    return {k: np.load(os.path.join(d, f"{k}.npz")) for k in ("gll", "mesh", "sl", "svv")}

@@ -142,7 +142,16 @@ def main():
     s["second_vel"], s["second_vel_prev"] = vel2, vel2p
     s["second_out"] = m2.advect(psi, vel2, dt2, field_prev=psip, vel_prev=vel2p)
     np.savez_compressed(os.path.join(OUT, "sl.npz"), **s)
-    for f in ("gll.npz", "mesh.npz", "sl.npz"):
+
+    # SVV element matrices (src/base/SVV.cpp:50-176) at the cutoffs the
+    # reference's models use (N/2), one element of a non-square mesh each
+    v = {}
+    for N in (4, 6, 8):
+        m = O.Mesh(3, 2, N, (0.0, -0.5), (1.5, 0.3), (False, False), use_ref=True)
+        v[f"elmat_{N}"] = m.svv_element(4, 0.7, N // 2)
+    v["params"] = np.array([3, 2, 0.0, -0.5, 1.5, 0.3, 4, 0.7])
+    np.savez_compressed(os.path.join(OUT, "svv.npz"), **v)
+    for f in ("gll.npz", "mesh.npz", "sl.npz", "svv.npz"):
         print(f, os.path.getsize(os.path.join(OUT, f)))
 
 
