@@ -201,9 +201,13 @@ int se_solver_opts_parse(se_solver_opts* opts, const char* prefix, const char* o
 
 /* Replaces HelmholtzEqn(sol, rhs, c, nu, dt, svvCutoff)
  * (src/linsys/HelmholtzEqn.h:3, src/linsys/HelmholtzEqn.cpp:43-104):
- * A = c*Mass + nu*dt*Laplacian on sol's mesh and boundary conditions.
- * rhs may be NULL (right-hand side = Dirichlet lifting only).
- * svvCutoff must be 0 (spectral vanishing viscosity is not built). */
+ * A = c*Mass + nu*dt*Laplacian on sol's mesh and boundary conditions, plus
+ * with 0 < svvCutoff <= N the spectral vanishing viscosity operator
+ * SVV(dt, svvCutoff) (src/base/SVV.cpp:50-176) as the reference builds it
+ * (its y term formed from the x derivative, as the reference forms it; the
+ * true Jacobian in either mode). rhs may be NULL (right-hand side = Dirichlet
+ * lifting only). An SVV system is solved by CG (SE_METHOD_FDM, the FDM
+ * inverse and the low-precision apply return SE_ERR_UNSUPPORTED for it). */
 int se_helmholtz_create(se_field* sol, se_field* rhs, double c, double nu, double dt,
                         int svvCutoff, const se_solver_opts* opts, se_linsys** out);
 /* Replaces PoissonEqn(sol, rhs, c) (src/linsys/PoissonEqn.cpp:30-80):
@@ -392,9 +396,11 @@ int se_ns_create(se_field* velocity, se_field* pressure, se_bcs* bcs_u, se_bcs* 
                  const se_solver_opts* opts, se_ns** out);
 /* NavierStokesEqn::Solve(velocity, pressure, prevVel, nu, svvCutoff):
  * velocity and pressure must be the fields the object was made with; prevVel
- * NULL for the first-order step (it is read, not changed); nu is taken when
- * the viscous systems are made (first call of each order); svvCutoff must be
- * 0 (SE_ERR_UNSUPPORTED otherwise). A solve that does not converge leaves
+ * NULL for the first-order step (it is read, not changed); nu and svvCutoff
+ * (0 <= svvCutoff <= N) are taken when the viscous systems are made (first
+ * call of each order), as in the reference; with svvCutoff != 0 those
+ * systems carry the SVV operator and are solved by CG whatever the options'
+ * method (no fast diagonalization holds for them). A solve that does not converge leaves
  * its last iterate and the step goes on, as in the reference; the call then
  * returns SE_ERR_NOT_CONVERGED with the step complete (se_ns_stats shows
  * which). */

@@ -239,6 +239,7 @@ struct se_linsys {
   se_field *sol, *rhs;
   bool poisson;
   double c, nu, dt;
+  int svv;  // svvCutoff of a HelmholtzEqn with the SVV operator (0: none)
   se_solver_opts opts;
   se_bcs* own_bcs;  // when sol has no BCs: natural boundaries, all vertices unknown
   OpDev op;
@@ -295,6 +296,96 @@ Dir make_dir(const MeshDev& m, int d, bool lo_bc, bool hi_bc) {
   return r;
 }
 
+// 1-D factors of SVV(constant, mN)'s element matrix (src/base/SVV.cpp:
+// 120-176) on SE's rectangles, where it equals
+//     2 constant detJ (T along y (x) S along x),
+// S = (F D)^T diag(w) (F D), T = F^T diag(w) F, with F = B diag(q) B^-1 the
+// nodal form of the modal filter: B[a][k] the modal basis of
+// src/base/Legendre.cpp:307-335 ((1+x)/2, (1-x)/2, (1-x^2)/4 P_{k-2}^(1,1))
+// at the GLL node a, q(k) = sqrt(exp(-(N-k)^2/(mN-k)^2)) for k > mN, else
+// 0, D the cardinal derivatives. (The reference's Lyy is formed from the x
+// derivative again, so both of its terms are this same matrix.) Computed in
+// long double.
+void svv_factors(const Gll& g, int mN, double* S, double* T) {
+  typedef long double L;
+  const int N = g.N, n = N + 1;
+  // Jacobi P^(1,1) coefficients by the reference's recurrence (src/base/Jacobi.cpp:21-36)
+  L P[SE_MAXN1][SE_MAXN1 + 1] = {};
+  P[0][0] = 1.0L;
+  if (N >= 1) P[1][1] = 2.0L;
+  for (int k = 2; k <= N; k++) {
+    const L a = 1.0L;
+    const L c1 = 2 * k * (2 * a + k) * (2 * a + 2 * k - 2);
+    const L c2 = (2 * a + 2 * k - 1) * (2 * a + 2 * k) * (2 * a + 2 * k - 2) / c1;
+    const L c3 = 2 * (a + k - 1) * (a + k - 1) * (2 * a + 2 * k) / c1;
+    for (int i = 0; i < k; i++) P[k][i + 1] += c2 * P[k - 1][i];
+    for (int i = 0; i <= k - 2; i++) P[k][i] -= c3 * P[k - 2][i];
+  }
+  L modal[SE_MAXN1][SE_MAXN1 + 1] = {};
+  modal[0][0] = 0.5L, modal[0][1] = 0.5L;
+  modal[1][0] = 0.5L, modal[1][1] = -0.5L;
+  for (int k = 2; k <= N; k++)
+    for (int j = 0; j < k - 1; j++) {
+      modal[k][j] += 0.25L * P[k - 2][j];
+      modal[k][j + 2] -= 0.25L * P[k - 2][j];
+    }
+  L B[SE_MAXN1][SE_MAXN1], Bi[SE_MAXN1][SE_MAXN1], A[SE_MAXN1][SE_MAXN1];
+  for (int a = 0; a < n; a++)
+    for (int k = 0; k < n; k++) {
+      L v = 0.0L;
+      for (int i = N; i >= 0; i--) v = v * (L)g.x[a] + modal[k][i];
+      B[a][k] = v;
+      A[a][k] = v;
+      Bi[a][k] = a == k ? 1.0L : 0.0L;
+    }
+  for (int c = 0; c < n; c++) {  // Gauss-Jordan, partial pivoting
+    int p = c;
+    for (int r = c + 1; r < n; r++)
+      if (fabsl(A[r][c]) > fabsl(A[p][c])) p = r;
+    for (int k = 0; k < n; k++) {
+      std::swap(A[c][k], A[p][k]);
+      std::swap(Bi[c][k], Bi[p][k]);
+    }
+    const L inv = 1.0L / A[c][c];
+    for (int k = 0; k < n; k++) A[c][k] *= inv, Bi[c][k] *= inv;
+    for (int r = 0; r < n; r++) {
+      if (r == c) continue;
+      const L f = A[r][c];
+      for (int k = 0; k < n; k++) A[r][k] -= f * A[c][k], Bi[r][k] -= f * Bi[c][k];
+    }
+  }
+  L q[SE_MAXN1], F[SE_MAXN1][SE_MAXN1], FD[SE_MAXN1][SE_MAXN1];
+  for (int k = 0; k < n; k++) {
+    q[k] = 0.0L;
+    if (k > mN) {
+      const L e = -((L)(N - k) * (N - k)) / ((L)(mN - k) * (mN - k));
+      q[k] = sqrtl(expl(e));
+    }
+  }
+  for (int a = 0; a < n; a++)
+    for (int b = 0; b < n; b++) {
+      L v = 0.0L;
+      for (int k = 0; k < n; k++) v += B[a][k] * q[k] * Bi[k][b];
+      F[a][b] = v;
+    }
+  for (int a = 0; a < n; a++)
+    for (int b = 0; b < n; b++) {
+      L v = 0.0L;
+      for (int c = 0; c < n; c++) v += F[a][c] * (L)g.dC[c * n + b];
+      FD[a][b] = v;
+    }
+  for (int b = 0; b < n; b++)
+    for (int c = 0; c < n; c++) {
+      L s = 0.0L, t = 0.0L;
+      for (int a = 0; a < n; a++) {
+        s += FD[a][b] * (L)g.w[a] * FD[a][c];
+        t += F[a][b] * (L)g.w[a] * F[a][c];
+      }
+      S[b * n + c] = (double)s;
+      T[b * n + c] = (double)t;
+    }
+}
+
 void fill_op(se_linsys* ls) {
   const se_mesh* me = ls->sol->mesh;
   const MeshDev& m = me->dev;
@@ -320,6 +411,12 @@ void fill_op(se_linsys* ls) {
   const int n = m.N + 1;
   for (int a = 0; a < n * n; a++) op.Kh[a] = me->gll.Kh[a];
   for (int a = 0; a < n; a++) op.w[a] = me->gll.w[a];
+  if (ls->svv && !ls->poisson) {
+    // SVV(dt, svvCutoff) (src/linsys/HelmholtzEqn.cpp:71) with the true
+    // Jacobian in either mode (SVV.cpp:132 uses Mesh::DetJac)
+    svv_factors(me->gll, ls->svv, op.Sv, op.Tv);
+    op.gamma = 2.0 * ls->dt * ((0.5 * hx) * (0.5 * hy));
+  }
 }
 
 // Static schedule for one cooperative launch over several solves: tiles of
@@ -692,6 +789,8 @@ int eig_get(const Dir& d, const double* Kh, const double* w, int prec, Eig1D** o
 }
 
 int fdm_setup(se_linsys* ls, int prec) {
+  if (ls->svv)
+    return fail(SE_ERR_UNSUPPORTED, "the SVV operator needs SE_METHOD_CG (no fast diagonalization)");
   if (ls->fdm_ready && ls->fdm_prec == prec) return SE_OK;
   const OpDev& op = ls->op;
   const size_t n = (size_t)ls->n;
@@ -1670,7 +1769,7 @@ int check_opts(const se_solver_opts* o) {
 }
 
 int linsys_create(se_field* sol, se_field* rhs, bool poisson, double c, double nu, double dt,
-                  const se_solver_opts* opts, se_linsys** out) {
+                  int svv, const se_solver_opts* opts, se_linsys** out) {
   if (!out) return fail(SE_ERR_ARG, "null argument");
   *out = nullptr;
   if (opts)
@@ -1685,6 +1784,9 @@ int linsys_create(se_field* sol, se_field* rhs, bool poisson, double c, double n
   for (int k = 0; k < 2; k++)
     if (m.periodic[k] && m.nEls[k] < 2)
       return fail(SE_ERR_UNSUPPORTED, "a periodic direction needs at least 2 elements");
+  if (svv < 0 || svv > m.N) return fail(SE_ERR_ARG, "svvCutoff %d outside [0, N = %d]", svv, m.N);
+  if (svv && opts && opts->method == SE_METHOD_FDM)
+    return fail(SE_ERR_UNSUPPORTED, "the SVV operator needs SE_METHOD_CG (no fast diagonalization)");
   se_linsys* ls = new se_linsys();
   std::memset((void*)ls, 0, sizeof(*ls));
   ls->sol = sol;
@@ -1693,6 +1795,7 @@ int linsys_create(se_field* sol, se_field* rhs, bool poisson, double c, double n
   ls->c = c;
   ls->nu = nu;
   ls->dt = dt;
+  ls->svv = svv;
   if (opts) ls->opts = *opts; else se_solver_opts_default(&ls->opts);
   if (!sol->bcs) {
     int rc = se_bcs_create(sol->mesh, 0, 0, 0, 0, &ls->own_bcs);
@@ -1715,12 +1818,11 @@ int linsys_create(se_field* sol, se_field* rhs, bool poisson, double c, double n
 
 int se_helmholtz_create(se_field* sol, se_field* rhs, double c, double nu, double dt,
                         int svvCutoff, const se_solver_opts* opts, se_linsys** out) {
-  if (svvCutoff != 0) return fail(SE_ERR_UNSUPPORTED, "spectral vanishing viscosity not built");
-  return linsys_create(sol, rhs, false, c, nu, dt, opts, out);
+  return linsys_create(sol, rhs, false, c, nu, dt, svvCutoff, opts, out);
 }
 int se_poisson_create(se_field* sol, se_field* rhs, double c, const se_solver_opts* opts,
                       se_linsys** out) {
-  return linsys_create(sol, rhs, true, c, 0.0, 0.0, opts, out);
+  return linsys_create(sol, rhs, true, c, 0.0, 0.0, 0, opts, out);
 }
 int se_linsys_destroy(se_linsys* ls) {
   if (ls) linsys_free(ls);
@@ -1729,6 +1831,8 @@ int se_linsys_destroy(se_linsys* ls) {
 int se_linsys_set_opts(se_linsys* ls, const se_solver_opts* opts) {
   if (!ls || !opts) return fail(SE_ERR_ARG, "null argument");
   if (int rc = check_opts(opts)) return rc;
+  if (ls->svv && opts->method == SE_METHOD_FDM)
+    return fail(SE_ERR_UNSUPPORTED, "the SVV operator needs SE_METHOD_CG (no fast diagonalization)");
   int old_mode = ls->opts.mode;
   ls->opts = *opts;
   if (opts->mode != old_mode) {
@@ -1923,6 +2027,7 @@ int se_linsys_apply_low(se_linsys* ls, int precision, const void* x_dev, float* 
   if (!ls || !x_dev || !y_dev) return fail(SE_ERR_ARG, "null argument");
   if (precision != SE_PREC_BF16 && precision != SE_PREC_FP16)
     return fail(SE_ERR_ARG, "precision must be SE_PREC_BF16 or SE_PREC_FP16");
+  if (ls->svv) return fail(SE_ERR_UNSUPPORTED, "the low-precision apply has no SVV term");
   CK(launch_op_apply_low(ls->op, precision == SE_PREC_FP16, x_dev, y_dev, g_stream));
   return SE_OK;
 }
@@ -2494,13 +2599,17 @@ int ns_release(se_ns* n) {
   return SE_OK;
 }
 
-// (Re)make the two viscous systems with mass coefficient c.
-int ns_make_viscous(se_ns* n, double c, double nu) {
+// (Re)make the two viscous systems with mass coefficient c (and the SVV
+// operator when svv != 0, which only CG solves: the fast diagonalization does
+// not hold for it, so those two systems use CG whatever the options' method).
+int ns_make_viscous(se_ns* n, double c, double nu, int svv) {
   if (n->hu) se_linsys_destroy(n->hu);
   if (n->hv) se_linsys_destroy(n->hv);
   n->hu = n->hv = nullptr;
-  QK(se_helmholtz_create(n->u, n->ru, c, nu, n->dt, 0, &n->opts, &n->hu));
-  return se_helmholtz_create(n->v, n->rv, c, nu, n->dt, 0, &n->opts, &n->hv);
+  se_solver_opts o = n->opts;
+  if (svv) o.method = SE_METHOD_CG, o.precision = SE_PREC_FP64;
+  QK(se_helmholtz_create(n->u, n->ru, c, nu, n->dt, svv, &o, &n->hu));
+  return se_helmholtz_create(n->v, n->rv, c, nu, n->dt, svv, &o, &n->hv);
 }
 }  // namespace
 
@@ -2557,7 +2666,8 @@ int se_ns_solve(se_ns* n, se_field* velocity, se_field* pressure, se_field* prev
   if (!n) return fail(SE_ERR_ARG, "null Navier-Stokes system");
   if (velocity != n->velocity || pressure != n->pressure)
     return fail(SE_ERR_ARG, "velocity and pressure must be the fields the system was made with");
-  if (svvCutoff != 0) return fail(SE_ERR_UNSUPPORTED, "spectral vanishing viscosity not built");
+  if (svvCutoff < 0 || svvCutoff > velocity->mesh->dev.N)
+    return fail(SE_ERR_ARG, "svvCutoff %d outside [0, N]", svvCutoff);
   const bool second = prev_vel != nullptr;
   if (second) {
     if (int rc = check_field(prev_vel)) return rc;
@@ -2582,8 +2692,8 @@ int se_ns_solve(se_ns* n, se_field* velocity, se_field* pressure, se_field* prev
   QK(solve_counting(n->poisson, 2, &n->st[0], &nc));
   CK(launch_ns_pressure(m, 1, sl, pressure->vals, n->dt, n->step2->vals, n->err, g_stream));
   // viscous step
-  if (!second && !n->hu) QK(ns_make_viscous(n, 1.0, nu));
-  if (second && !n->second_done) QK(ns_make_viscous(n, 1.5, nu));
+  if (!second && !n->hu) QK(ns_make_viscous(n, 1.0, nu, svvCutoff));
+  if (second && !n->second_done) QK(ns_make_viscous(n, 1.5, nu, svvCutoff));
   CK(launch_component(nv, 1, 0, velocity->vals, n->u->vals, g_stream));
   CK(launch_component(nv, 1, 1, velocity->vals, n->v->vals, g_stream));
   CK(launch_component(nv, 1, 0, n->step2->vals, n->ru->vals, g_stream));

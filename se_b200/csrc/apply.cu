@@ -856,6 +856,9 @@ cudaError_t launch_n8(const OpDev& od, const double* x, double* y, unsigned* err
     return launch_mma<n>(op, x, y, err, s);
 cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, unsigned* err,
                             cudaStream_t s) {
+  // an SVV term (dense element blocks) is applied by the CG kernel's staged
+  // per-unknown form, which carries it
+  if (op.gamma != 0.0) return launch_residual(op, x, nullptr, y, nullptr, 0, nullptr, s);
   switch (op.d[0].N) {
     SE_APPLY_N(2) SE_APPLY_N(3) SE_APPLY_N(4) SE_APPLY_N(5) SE_APPLY_N(6) SE_APPLY_N(7)
     SE_APPLY_N(9) SE_APPLY_N(10) SE_APPLY_N(11) SE_APPLY_N(12)
@@ -872,6 +875,7 @@ cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, unsigne
     return fp16 ? launch_tile<n, __half, float, float>(op, (const __half*)x, y, s)         \
                 : launch_tile<n, __nv_bfloat16, float, float>(op, (const __nv_bfloat16*)x, y, s);
 cudaError_t launch_op_apply_low(const OpDev& op, int fp16, const void* x, float* y, cudaStream_t s) {
+  if (op.gamma != 0.0) return cudaErrorNotSupported;  // no SVV term in the low-precision apply
   switch (op.d[0].N) {
     SE_APPLY_LOW_N(2) SE_APPLY_LOW_N(3) SE_APPLY_LOW_N(4) SE_APPLY_LOW_N(5) SE_APPLY_LOW_N(6)
     SE_APPLY_LOW_N(7) SE_APPLY_LOW_N(8) SE_APPLY_LOW_N(9) SE_APPLY_LOW_N(10) SE_APPLY_LOW_N(11)

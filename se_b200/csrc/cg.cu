@@ -135,11 +135,11 @@ __device__ __forceinline__ void seg_sum4(const double* partials, int b, int e, d
 // ---------------------------------------------------------------- operator --
 template <int N>
 struct Geo {
-  static constexpr int n = N + 1;
   static constexpr int W = kCgTileX + 2 * N;
   static constexpr int H = kCgTileY + 2 * N;
   static constexpr int kRows = kCgTileY * W;       // tile rows, full width
   static constexpr int kCols = 2 * N * kCgTileX;   // tile columns, y-halo only
+  static constexpr int kCorners = 4 * N * N;       // the halo's corners
 };
 
 // Unknown index of unwrapped vertex g along d (-1: Dirichlet or outside).
@@ -199,8 +199,9 @@ __device__ __forceinline__ double krow_n(const Dir& d, const double* Kh, int e, 
 // Per-block copy of one solve's operator coefficients.
 struct OpSm {
   double Kh[SE_MAXN1 * SE_MAXN1];
+  double Sv[SE_MAXN1 * SE_MAXN1], Tv[SE_MAXN1 * SE_MAXN1];  // SVV factors (gamma != 0)
   double w[SE_MAXN1];
-  double alpha, beta0, beta1;
+  double alpha, beta0, beta1, gamma;
   Dir dx, dy;
   int G0, G1;
   int solve;
@@ -214,11 +215,17 @@ __device__ __forceinline__ void load_op(OpSm& o, const CgSolve& S, int solve) {
   const OpDev& op = S.op;
   const int n = op.d[0].N + 1;
   for (int k = threadIdx.x; k < n * n; k += blockDim.x) o.Kh[k] = op.Kh[k];
+  if (op.gamma != 0.0)
+    for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+      o.Sv[k] = op.Sv[k];
+      o.Tv[k] = op.Tv[k];
+    }
   if (threadIdx.x < n) o.w[threadIdx.x] = op.w[threadIdx.x];
   if (threadIdx.x == 0) {
     o.alpha = op.alpha;
     o.beta0 = op.beta[0];
     o.beta1 = op.beta[1];
+    o.gamma = op.gamma;
     o.dx = op.d[0];
     o.dy = op.d[1];
     o.G0 = op.G[0];
@@ -236,22 +243,31 @@ __device__ __forceinline__ void load_op(OpSm& o, const CgSolve& S, int solve) {
   __syncthreads();
 }
 
-// Stage p = z + bc*p_old (p = z when first) for the tile and its halo.
+// Stage p = z + bc*p_old (p = z when first) for the tile and its halo: the
+// cross the Kronecker-sum terms read (the tile's rows at full width, its
+// columns at full height), and with an SVV term also the four N x N corners,
+// which its element blocks reach.
 template <int N>
 __device__ __forceinline__ void stage_p(const OpSm& o, int x0, int y0, const double* z,
                                         const double* po, bool first, double bc, double* P) {
   typedef Geo<N> G;
   const int gx0 = x0 + o.dx.lo - N, gy0 = y0 + o.dy.lo - N;
-  for (int k = threadIdx.x; k < G::kRows + G::kCols; k += kCgThreads) {
+  const int total = G::kRows + G::kCols + (o.gamma != 0.0 ? G::kCorners : 0);
+  for (int k = threadIdx.x; k < total; k += kCgThreads) {
     int i, j;
     if (k < G::kRows) {
       j = N + k / G::W;
       i = k - (j - N) * G::W;
-    } else {
+    } else if (k < G::kRows + G::kCols) {
       const int q = k - G::kRows;
       const int jj = q / kCgTileX;
       i = N + (q - jj * kCgTileX);
       j = jj < N ? jj : jj + kCgTileY;
+    } else {
+      const int q = k - G::kRows - G::kCols;
+      const int cj = q / (2 * N), ci = q - cj * (2 * N);
+      i = ci < N ? ci : ci + kCgTileX;
+      j = cj < N ? cj : cj + kCgTileY;
     }
     double v = 0.0;
     const int ux = unknown_1d(o.dx, gx0 + i), uy = unknown_1d(o.dy, gy0 + j);
@@ -264,6 +280,42 @@ __device__ __forceinline__ void stage_p(const OpSm& o, int x0, int y0, const dou
   __syncthreads();
 }
 
+// SVV term (Sv along x (x) Tv along y) at the unknown staged at c (vertex
+// (ex, ax), (ey, ay)): over the up to four elements holding the vertex, the
+// vertex's row of each element block applied to that element's staged
+// values, x contraction first.
+template <int N>
+__device__ __forceinline__ double svv_n(const OpSm& o, const double* c, int ex, int ax, int ey,
+                                        int ay) {
+  typedef Geo<N> G;
+  constexpr int n = N + 1;
+  auto elem = [&](int lx, int ly) {
+    const double* srow = o.Sv + lx * n;
+    const double* trow = o.Tv + ly * n;
+    const double* q = c - ly * G::W - lx;
+    double t = 0.0;
+#pragma unroll
+    for (int b = 0; b < n; b++) {
+      double r = 0.0;
+#pragma unroll
+      for (int a = 0; a < n; a++) r = fma(srow[a], q[b * G::W + a], r);
+      t = fma(trow[b], r, t);
+    }
+    return t;
+  };
+  // the element to the right/above (local index ax, ay) exists unless the
+  // vertex ends a non-periodic mesh; the one to the left/below (local index
+  // N) when the vertex starts an element other than a non-periodic first
+  const bool xr = ax != 0 || ex < o.dx.nE, xl = ax == 0 && (ex > 0 || o.dx.periodic);
+  const bool yr = ay != 0 || ey < o.dy.nE, yl = ay == 0 && (ey > 0 || o.dy.periodic);
+  double s = 0.0;
+  if (xr && yr) s += elem(ax, ay);
+  if (xl && yr) s += elem(N, ay);
+  if (xr && yl) s += elem(ax, N);
+  if (xl && yl) s += elem(N, N);
+  return s;
+}
+
 // (A p) at the thread's unknown (tile coordinates tx, ty; vertex gx, gy).
 template <int N>
 __device__ __forceinline__ double apply_n(const OpSm& o, const double* P, int tx, int ty, int gx,
@@ -274,15 +326,18 @@ __device__ __forceinline__ double apply_n(const OpSm& o, const double* P, int tx
   const double wx = wsum_n<N>(o.dx, o.w, ex, ax), wy = wsum_n<N>(o.dy, o.w, ey, ay);
   const double kx = krow_n<N, 1>(o.dx, o.Kh, ex, ax, c);
   const double ky = krow_n<N, G::W>(o.dy, o.Kh, ey, ay, c);
-  return o.alpha * wx * wy * c[0] + o.beta0 * wy * kx + o.beta1 * wx * ky;
+  const double a = o.alpha * wx * wy * c[0] + o.beta0 * wy * kx + o.beta1 * wx * ky;
+  return o.gamma != 0.0 ? a + o.gamma * svv_n<N>(o, c, ex, ax, ey, ay) : a;
 }
 
 template <int N>
 __device__ __forceinline__ double diag_n(const OpSm& o, int gx, int gy) {
   const int ex = gx / N, ax = gx - ex * N, ey = gy / N, ay = gy - ey * N;
   const double wx = wsum_n<N>(o.dx, o.w, ex, ax), wy = wsum_n<N>(o.dy, o.w, ey, ay);
-  return o.alpha * wx * wy + o.beta0 * kdiag_n<N>(o.dx, o.Kh, ex, ax) * wy +
-         o.beta1 * wx * kdiag_n<N>(o.dy, o.Kh, ey, ay);
+  const double d = o.alpha * wx * wy + o.beta0 * kdiag_n<N>(o.dx, o.Kh, ex, ax) * wy +
+                   o.beta1 * wx * kdiag_n<N>(o.dy, o.Kh, ey, ay);
+  if (o.gamma == 0.0) return d;
+  return d + o.gamma * kdiag_n<N>(o.dx, o.Sv, ex, ax) * kdiag_n<N>(o.dy, o.Tv, ey, ay);
 }
 
 // --------------------------------------------------------------- scalars --
@@ -716,11 +771,17 @@ __global__ void __launch_bounds__(kCgThreads) apply_kernel(const OpDev op, const
   {
     const int n = N + 1;
     for (int k = threadIdx.x; k < n * n; k += kCgThreads) o.Kh[k] = op.Kh[k];
+    if (op.gamma != 0.0)
+      for (int k = threadIdx.x; k < n * n; k += kCgThreads) {
+        o.Sv[k] = op.Sv[k];
+        o.Tv[k] = op.Tv[k];
+      }
     if (threadIdx.x < n) o.w[threadIdx.x] = op.w[threadIdx.x];
     if (threadIdx.x == 0) {
       o.alpha = op.alpha;
       o.beta0 = op.beta[0];
       o.beta1 = op.beta[1];
+      o.gamma = op.gamma;
       o.dx = op.d[0];
       o.dy = op.d[1];
       o.G0 = op.G[0];

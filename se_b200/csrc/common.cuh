@@ -53,6 +53,13 @@ struct OpDev {
   double beta[2];
   double Kh[SE_MAXN1 * SE_MAXN1];
   double w[SE_MAXN1];
+  // Spectral vanishing viscosity (HelmholtzEqn with svvCutoff != 0):
+  // + gamma (Sv along x (x) Tv along y), the assembled 1-D element matrices
+  // S = (F D)^T diag(w) (F D) and T = F^T diag(w) F of the modal filter F;
+  // gamma == 0: no such term (and Sv, Tv unused).
+  double gamma;
+  double Sv[SE_MAXN1 * SE_MAXN1];
+  double Tv[SE_MAXN1 * SE_MAXN1];
 };
 
 // Device-side error bits (a single unsigned word per library instance).

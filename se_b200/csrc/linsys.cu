@@ -36,13 +36,13 @@ __device__ __forceinline__ double wsum(const OpDev& op, const Dir& d, int g) {
   if (a == 0 && (e > 0 || d.periodic)) s += op.w[d.N];
   return s;
 }
-// Assembled 1-D stiffness diagonal of vertex g.
-__device__ __forceinline__ double kdiag(const OpDev& op, const Dir& d, int g) {
+// Assembled 1-D diagonal of vertex g for the element matrix M (Kh, Sv, Tv).
+__device__ __forceinline__ double kdiag(const double* M, const Dir& d, int g) {
   const int n = d.N + 1;
   int e = g / d.N, a = g - e * d.N;
   double s = 0.0;
-  if (e < d.nE) s += op.Kh[a * n + a];
-  if (a == 0 && (e > 0 || d.periodic)) s += op.Kh[d.N * n + d.N];
+  if (e < d.nE) s += M[a * n + a];
+  if (a == 0 && (e > 0 || d.periodic)) s += M[d.N * n + d.N];
   return s;
 }
 // Row g of the assembled 1-D stiffness applied to val(vertex): the row of
@@ -69,98 +69,25 @@ __device__ __forceinline__ double krow(const OpDev& op, const Dir& d, int g, con
 
 __device__ __forceinline__ double diag_at(const OpDev& op, int gx, int gy) {
   const double wx = wsum(op, op.d[0], gx), wy = wsum(op, op.d[1], gy);
-  return op.alpha * wx * wy + op.beta[0] * kdiag(op, op.d[0], gx) * wy +
-         op.beta[1] * wx * kdiag(op, op.d[1], gy);
+  const double d = op.alpha * wx * wy + op.beta[0] * kdiag(op.Kh, op.d[0], gx) * wy +
+                   op.beta[1] * wx * kdiag(op.Kh, op.d[1], gy);
+  if (op.gamma == 0.0) return d;
+  return d + op.gamma * kdiag(op.Sv, op.d[0], gx) * kdiag(op.Tv, op.d[1], gy);
 }
-
-// y(gx, gy) = (A x) for unknown vertex (gx, gy), x given by xv(ux, uy) on
-// unknown coordinates.
-template <class X>
-__device__ __forceinline__ double apply_at(const OpDev& op, int gx, int gy, const X& xv) {
-  const Dir &dx = op.d[0], &dy = op.d[1];
-  const double wx = wsum(op, dx, gx), wy = wsum(op, dy, gy);
-  const int ux = gx - dx.lo, uy = gy - dy.lo;
-  double self = xv(ux, uy);
-  double kx = krow(op, dx, gx, [&](int g) { return unknown(dx, g) ? xv(g - dx.lo, uy) : 0.0; });
-  double ky = krow(op, dy, gy, [&](int g) { return unknown(dy, g) ? xv(ux, g - dy.lo) : 0.0; });
-  return op.alpha * wx * wy * self + op.beta[0] * wy * kx + op.beta[1] * wx * ky;
-}
-
-// ------------------------------------------------ shared-memory tiles ----
-// A tile of kCgTileX x kCgTileY unknowns plus a halo of N vertices on every
-// side, in unwrapped vertex coordinates: the halo of a periodic boundary
-// vertex holds the wrapped-around vertices, and halo entries that are not
-// unknowns (Dirichlet, outside a non-periodic mesh) hold 0. Loading it is one
-// batch of independent coalesced loads; the stencil taps then read shared
-// memory instead of chaining one L2 round trip per tap.
-__device__ __forceinline__ int tile_w(int N) { return kCgTileX + 2 * N; }
-__device__ __forceinline__ int tile_h(int N) { return kCgTileY + 2 * N; }
-
-// Unknown index along one direction of unwrapped vertex g, or -1.
-__device__ __forceinline__ int unknown_of(const Dir& d, int g) {
-  if (d.periodic) {
-    const int L = d.nV - 1;
-    g %= L;
-    if (g < 0) g += L;
-  } else if (g < 0 || g >= d.nV) {
-    return -1;
-  }
-  return (g >= d.lo && g < d.hi) ? g - d.lo : -1;
-}
-
-// Row of the assembled 1-D stiffness at (unwrapped) vertex g applied to the
-// tile values around p (stride between neighbouring vertices).
-__device__ __forceinline__ double krow_tile(const OpDev& op, const Dir& d, int g, const double* p,
-                                            int stride) {
-  const int N = d.N, n = N + 1;
-  const int e = g / N, a = g - e * N;
-  double s = 0.0;
-  if (a != 0) {
-    const double* k = op.Kh + a * n;
-    const double* q = p - a * stride;
-    for (int b = 0; b < n; b++) s = fma(k[b], q[b * stride], s);
-    return s;
-  }
-  if (e > 0 || d.periodic) {
-    const double* k = op.Kh + N * n;
-    const double* q = p - N * stride;
-    for (int b = 0; b < n; b++) s = fma(k[b], q[b * stride], s);
-  }
+// The elements holding vertex g along d: their first vertex and the vertex's
+// local index in each (at most two).
+__device__ __forceinline__ int elems_of(const Dir& d, int g, int* g0, int* loc) {
+  const int N = d.N, e = g / N, a = g - e * N;
+  int k = 0;
   if (e < d.nE) {
-    const double* k = op.Kh;
-    for (int b = 0; b < n; b++) s = fma(k[b], p[b * stride], s);
+    g0[k] = e * N;
+    loc[k++] = a;
   }
-  return s;
-}
-
-// Fill the tile at unknown origin (x0, y0) with val(ux, uy) (only the cross
-// the stencil reads: the tile's rows at full width, its columns at full
-// height), then __syncthreads.
-template <class F>
-__device__ __forceinline__ void load_tile(const OpDev& op, int x0, int y0, double* P, const F& val) {
-  const int N = op.d[0].N, W = tile_w(N), H = tile_h(N);
-  const int gx0 = x0 + op.d[0].lo - N, gy0 = y0 + op.d[1].lo - N;
-  for (int k = threadIdx.x; k < W * H; k += blockDim.x) {
-    const int i = k % W, j = k / W;
-    double v = 0.0;
-    if ((j >= N && j < N + kCgTileY) || (i >= N && i < N + kCgTileX)) {
-      const int ux = unknown_of(op.d[0], gx0 + i), uy = unknown_of(op.d[1], gy0 + j);
-      if (ux >= 0 && uy >= 0) v = val(ux, uy);
-    }
-    P[k] = v;
+  if (a == 0 && (e > 0 || d.periodic)) {
+    g0[k] = (e > 0 ? e - 1 : d.nE - 1) * N;
+    loc[k++] = N;
   }
-  __syncthreads();
-}
-
-// (A p) at this thread's unknown of the tile, from the staged tile.
-__device__ __forceinline__ double apply_tile(const OpDev& op, int gx, int gy, const double* P,
-                                             int tx, int ty) {
-  const int N = op.d[0].N, W = tile_w(N);
-  const double* c = P + (ty + N) * W + (tx + N);
-  const double wx = wsum(op, op.d[0], gx), wy = wsum(op, op.d[1], gy);
-  const double kx = krow_tile(op, op.d[0], gx, c, 1);
-  const double ky = krow_tile(op, op.d[1], gy, c, W);
-  return op.alpha * wx * wy * c[0] + op.beta[0] * wy * kx + op.beta[1] * wx * ky;
+  return k;
 }
 
 __global__ void op_diag_kernel(const OpDev op, double* __restrict__ d) {
@@ -232,7 +159,29 @@ __global__ void lift_kernel(const OpDev op, const MeshDev m, const double* __res
   const double wx = wsum(op, dx, gx), wy = wsum(op, dy, gy);
   double kx = krow(op, dx, gx, [&](int g) { return unknown(dx, g) ? 0.0 : sol[(size_t)gy * nvx + g]; });
   double ky = krow(op, dy, gy, [&](int g) { return unknown(dy, g) ? 0.0 : sol[(size_t)g * nvx + gx]; });
-  lift[(size_t)uy * op.G[0] + ux] = -(op.beta[0] * wy * kx + op.beta[1] * wx * ky);
+  double v = op.beta[0] * wy * kx + op.beta[1] * wx * ky;
+  if (op.gamma != 0.0) {
+    // the SVV element blocks reach every vertex of the elements holding the
+    // unknown: the Dirichlet ones (not unknowns after the periodic fold) lift
+    const int n = dx.N + 1;
+    int x0[2], lx[2], y0[2], ly[2];
+    const int nx = elems_of(dx, gx, x0, lx), ny = elems_of(dy, gy, y0, ly);
+    double sv = 0.0;
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+        for (int b = 0; b < n; b++) {
+          const int vy = fold(dy, y0[j] + b);
+          double r = 0.0;
+          for (int a = 0; a < n; a++) {
+            const int vx = fold(dx, x0[i] + a);
+            if (unknown(dx, vx) && unknown(dy, vy)) continue;
+            r = fma(op.Sv[lx[i] * n + a], sol[(size_t)vy * nvx + vx], r);
+          }
+          sv = fma(op.Tv[ly[j] * n + b], r, sv);
+        }
+    v += op.gamma * sv;
+  }
+  lift[(size_t)uy * op.G[0] + ux] = -v;
 }
 
 // Vector::UpdateField (src/base/Vector.cpp:40-61) with the periodic copies.

@@ -266,8 +266,8 @@ def test_solver_reasons(segpu, oracle):
     st = ls.Solve("helm_")
     assert st["its"] == 0 and st["reason"] in (2, 3)
     with pytest.raises(segpu.SEError) as e:
-        segpu.HelmholtzEqn(fs, fr, 1.0, 1.0, 1.0, 4)
-    assert e.value.code == segpu.SE_ERR_UNSUPPORTED
+        segpu.HelmholtzEqn(fs, fr, 1.0, 1.0, 1.0, 5)  # svvCutoff above N = 4
+    assert e.value.code == segpu.SE_ERR_ARG
 
 
 def test_field_error_calc_time_step(segpu, oracle):

@@ -82,7 +82,8 @@ def setup(segpu, oracle, name, method, mode):
                              method=segpu.METHOD_FDM if method == "fdm" else segpu.METHOD_CG)
     ns = segpu.NavierStokesEqn(velocity, pressure, dt, opts)
     return dict(ref=ref, ns=ns, velocity=velocity, prevVel=prevVel, pressure=pressure,
-                vel=vel, prev=prev, pres=pres, nu=nu, dt=dt, X=X, init=init, tol=1000 * rtol)
+                vel=vel, prev=prev, pres=pres, nu=nu, dt=dt, X=X, init=init, tol=1000 * rtol,
+                om=om)
 
 
 @pytest.mark.parametrize("name", ["taylor", "channel"])
@@ -121,6 +122,34 @@ def test_ns_first_order_taylor_vortex_accuracy(segpu, oracle):
     assert np.abs(c["velocity"].vals - ua).max() < 1e-4
 
 
+@pytest.mark.parametrize("method", ["cg", "fdm"])
+def test_ns_svv_matches_oracle(segpu, oracle, method):
+    """The step with the SVV operator in the viscous systems (svvCutoff =
+    N/2, as the reference's cavity-flow and Kelvin-Helmholtz models pass);
+    the viscous systems are solved by CG with either method, the pressure by
+    the chosen one."""
+    c = setup(segpu, oracle, "channel", method, segpu.MODE_EXACT)
+    ns, ref, nu, TOL = c["ns"], c["ref"], c["nu"], c["tol"]
+    svv = CASES["channel"][1] // 2
+    # seeded noise gives the velocity the high modes the filter acts on
+    noise = 0.02 * np.random.default_rng(7).standard_normal(c["vel"].shape)
+    c["vel"] = np.stack([c["om"].periodic_update(c["vel"][:, d] + noise[:, d])
+                         for d in range(2)], 1)
+    c["velocity"].vals = c["vel"]
+    st = ns.Solve(c["velocity"], c["pressure"], None, nu, svv, raise_on_diverge=True)
+    assert all(s["reason"] > 0 for s in st)
+    vel, pres, _ = ref.step(c["vel"], c["pres"], None, nu, svv_cutoff=svv)
+    assert rel(c["velocity"].vals, vel) < TOL
+    assert rel(c["pressure"].vals, pres) < TOL
+    ns.Solve(c["velocity"], c["pressure"], c["prevVel"], nu, svv, raise_on_diverge=True)
+    vel2, pres2, _ = ref.step(vel, pres, c["prevVel"].vals, nu, svv_cutoff=svv)
+    assert rel(c["velocity"].vals, vel2) < TOL
+    assert rel(c["pressure"].vals, pres2) < TOL
+    # SVV changes the result (the filter acts on this field)
+    vel_plain, _, _ = ref.step(c["vel"], c["pres"], None, nu)
+    assert rel(vel, vel_plain) > 1e-6
+
+
 def test_ns_reference_laplacian_mode(segpu, oracle):
     """The reference's Laplacian (detJ dropped) through the whole step."""
     c = setup(segpu, oracle, "channel", "cg", segpu.MODE_REFERENCE)
@@ -141,7 +170,7 @@ def test_ns_rejections(segpu):
         segpu.NavierStokesEqn(vel, segpu.Field("q", other, 1, None), 0.01)  # pressure geometry
     ns = segpu.NavierStokesEqn(vel, pres, 0.01)
     with pytest.raises(segpu.SEError):
-        ns.Solve(vel, pres, None, 1.0, 2)  # spectral vanishing viscosity
+        ns.Solve(vel, pres, None, 1.0, 5)  # svvCutoff above N = 4
     with pytest.raises(segpu.SEError):
         ns.Solve(segpu.Field("w", m, 2, None), pres, None, 1.0, 0)  # not the system's field
     with pytest.raises(segpu.SEError):
