@@ -99,6 +99,11 @@ int se_field_create(se_mesh* mesh, int ndofs, se_bcs* bcs, se_field** out);
 int se_field_destroy(se_field* field);
 int se_field_upload(se_field* field, const double* vals);
 int se_field_download(const se_field* field, double* vals);
+/* se_field_download queued on the library's stream without waiting (no
+ * counterpart in the reference): vals must stay valid, and is complete after
+ * se_synchronize or a wait on that stream; page-locked vals make the copy
+ * overlap other streams' work. */
+int se_field_download_async(const se_field* field, double* vals);
 /* Device pointer to the values (double[nVertsTotal][ndofs]). */
 int se_field_device_ptr(se_field* field, double** dptr);
 /* Field::Copy (src/base/Field.cpp:49-55), device to device. */

@@ -256,7 +256,7 @@ struct se_linsys {
   int* d_active;
   unsigned* d_err;
   int grid, nseg, seg_begin, seg_end;
-  cudaEvent_t ev[2];
+  cudaEvent_t ev[3];  // FDM solve: graph start, graph end, state copied to the host
   // fast diagonalization (built on the first FDM solve)
   bool fdm_ready;
   int fdm_prec;
@@ -517,8 +517,8 @@ void linsys_free(se_linsys* ls) {
   dfree(ls->d_fparams);
   dfree(ls->d_fstate);
   if (ls->h_fparams) cudaFreeHost(ls->h_fparams);
-  if (ls->ev[0]) cudaEventDestroy(ls->ev[0]);
-  if (ls->ev[1]) cudaEventDestroy(ls->ev[1]);
+  for (cudaEvent_t e : ls->ev)
+    if (e) cudaEventDestroy(e);
   delete ls->own_bcs;
   delete ls;
 }
@@ -1063,9 +1063,9 @@ int fdm_launch(se_linsys* ls, int remove_null) {
     ls->h_fparams = static_cast<FdmParams*>(p);
     ls->h_fstate = reinterpret_cast<FdmState*>(ls->h_fparams + 1);
   }
-  if (!ls->ev[0]) {
-    CK(cudaEventCreate(&ls->ev[0]));
-    CK(cudaEventCreate(&ls->ev[1]));
+  if (!ls->ev[2]) {
+    for (cudaEvent_t& e : ls->ev)
+      if (!e) CK(cudaEventCreate(&e));
   }
   FdmParams& p = *ls->h_fparams;
   p.rtol = ls->opts.rtol;
@@ -1078,10 +1078,11 @@ int fdm_launch(se_linsys* ls, int remove_null) {
   CK(cudaGraphLaunch(ls->fdm_exec, g_stream));
   CK(cudaEventRecord(ls->ev[1], g_stream));
   CK(cudaMemcpyAsync(ls->h_fstate, ls->d_fstate, sizeof(FdmState), cudaMemcpyDeviceToHost, g_stream));
+  CK(cudaEventRecord(ls->ev[2], g_stream));
   return SE_OK;
 }
 int fdm_finish(se_linsys* ls, CgSolve* st, float* kernel_ms) {
-  CK(cudaEventSynchronize(ls->ev[1]));
+  CK(cudaEventSynchronize(ls->ev[2]));  // the state has reached the host
   if (kernel_ms) CK(cudaEventElapsedTime(kernel_ms, ls->ev[0], ls->ev[1]));
   std::memset(st, 0, sizeof(*st));
   st->its = ls->h_fstate->its;
@@ -1458,6 +1459,13 @@ int se_field_download(const se_field* field, double* vals) {
   CK(cudaMemcpyAsync(vals, field->vals, sizeof(double) * field->mesh->nVertsTotal * field->ndofs,
                      cudaMemcpyDeviceToHost, g_stream));
   CK(cudaStreamSynchronize(g_stream));
+  return SE_OK;
+}
+int se_field_download_async(const se_field* field, double* vals) {
+  if (int rc = check_field(field)) return rc;
+  if (!vals) return fail(SE_ERR_ARG, "null host array");
+  CK(cudaMemcpyAsync(vals, field->vals, sizeof(double) * field->mesh->nVertsTotal * field->ndofs,
+                     cudaMemcpyDeviceToHost, g_stream));
   return SE_OK;
 }
 int se_field_device_ptr(se_field* field, double** dptr) {

@@ -430,15 +430,15 @@ cudaError_t run_d(const GemmArgs<double, double, double>& g, cudaStream_t s) {
 }
 
 // FP64 products split over K inside the block: a 32 x 32 output tile per
-// block of W warps; stage i holds a 32-wide slice of K and warp w multiplies
-// its w-th 8-wide part, so every warp keeps the whole tile's 8 accumulator
-// fragments (8 independent MMA chains). At the end the W partial tiles are
-// summed through shared memory in warp order (deterministic) and the
-// epilogue is applied.
-template <int W_, int ST_>
+// block of W warps; stage i holds a (8 W KW)-wide slice of K and warp w
+// multiplies its w-th (8 KW)-wide part, so every warp keeps the whole tile's
+// 8 accumulator fragments (8 independent MMA chains) and runs 8 KW MMAs
+// between barriers. At the end the W partial tiles are summed through shared
+// memory in warp order (deterministic) and the epilogue is applied.
+template <int W_, int ST_, int KW_ = 1>
 struct KCfg {
-  static constexpr int W = W_, ST = ST_;
-  static constexpr int BM = 32, BN = 32, BK = 8 * W;
+  static constexpr int W = W_, ST = ST_, KW = KW_;
+  static constexpr int BM = 32, BN = 32, BK = 8 * W * KW;
   static constexpr int AS = BK + 4, BS = BN + 4, RS = BN + 1;
   static constexpr int THREADS = 32 * W;
   static constexpr int A_ELEMS = BM * AS, B_ELEMS = BK * BS;
@@ -490,7 +490,6 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_ksplit_kernel(
     if (s < nkt) issue(s);
     cp_async_commit();
   }
-  const int kk = warp * 8;
   for (int i = 0; i < nkt; i++) {
     cp_async_wait<C::ST - 2>();
     __syncthreads();
@@ -498,25 +497,29 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_ksplit_kernel(
     cp_async_commit();
     const double* as = As + (i % C::ST) * C::A_ELEMS;
     const double* bs = Bs + (i % C::ST) * C::B_ELEMS;
-    double a[2][4], b[4][2];
 #pragma unroll
-    for (int mt = 0; mt < 2; mt++) {
-      const int r0 = mt * 16 + gq;
-      a[mt][0] = as[r0 * C::AS + kk + tq];
-      a[mt][1] = as[(r0 + 8) * C::AS + kk + tq];
-      a[mt][2] = as[r0 * C::AS + kk + tq + 4];
-      a[mt][3] = as[(r0 + 8) * C::AS + kk + tq + 4];
+    for (int ks = 0; ks < C::KW; ks++) {
+      const int kk = (warp * C::KW + ks) * 8;
+      double a[2][4], b[4][2];
+#pragma unroll
+      for (int mt = 0; mt < 2; mt++) {
+        const int r0 = mt * 16 + gq;
+        a[mt][0] = as[r0 * C::AS + kk + tq];
+        a[mt][1] = as[(r0 + 8) * C::AS + kk + tq];
+        a[mt][2] = as[r0 * C::AS + kk + tq + 4];
+        a[mt][3] = as[(r0 + 8) * C::AS + kk + tq + 4];
+      }
+#pragma unroll
+      for (int nt = 0; nt < 4; nt++) {
+        const int c0 = nt * 8 + gq;
+        b[nt][0] = bs[(kk + tq) * C::BS + c0];
+        b[nt][1] = bs[(kk + tq + 4) * C::BS + c0];
+      }
+#pragma unroll
+      for (int mt = 0; mt < 2; mt++)
+#pragma unroll
+        for (int nt = 0; nt < 4; nt++) mma_f64(acc[mt][nt], a[mt], b[nt]);
     }
-#pragma unroll
-    for (int nt = 0; nt < 4; nt++) {
-      const int c0 = nt * 8 + gq;
-      b[nt][0] = bs[(kk + tq) * C::BS + c0];
-      b[nt][1] = bs[(kk + tq + 4) * C::BS + c0];
-    }
-#pragma unroll
-    for (int mt = 0; mt < 2; mt++)
-#pragma unroll
-      for (int nt = 0; nt < 4; nt++) mma_f64(acc[mt][nt], a[mt], b[nt]);
   }
   cp_async_wait<0>();
   __syncthreads();

@@ -145,6 +145,7 @@ SIGNATURES = {
                      ctypes.POINTER(_vp)],
     "se_ns_solve": [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int],
     "se_ns_stats": [_vp, ctypes.POINTER(SolveStats)], "se_ns_destroy": [_vp],
+    "se_field_download_async": [_vp, _D],
     "se_helmholtz_solve_noalloc": [_I, ctypes.c_int, _D, _D, _I, _I, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.POINTER(SolverOpts), ctypes.c_int, _vp, _vp,
@@ -441,6 +442,22 @@ class _LinSys:
         st = SolveStats()
         null = (2 if projectRHS else 1) if removeNullSpace else 0
         rc = _lib.se_linsys_solve(self._h, null, ctypes.byref(st))
+        if rc == SE_ERR_NOT_CONVERGED and not raise_on_diverge:
+            rc = SE_OK
+        _check(rc)
+        self.stats = st.as_dict()
+        return self.stats
+
+    def solve_async(self, removeNullSpace: bool = False, projectRHS: bool = False):
+        """Queue the solve on the library's stream (se_linsys_solve_async); FDM
+        solves return at once, CG solves complete before returning."""
+        null = (2 if projectRHS else 1) if removeNullSpace else 0
+        _check(_lib.se_linsys_solve_async(self._h, null))
+
+    def solve_finish(self, raise_on_diverge: bool = False):
+        """Wait for a queued solve and return its statistics."""
+        st = SolveStats()
+        rc = _lib.se_linsys_solve_finish(self._h, ctypes.byref(st))
         if rc == SE_ERR_NOT_CONVERGED and not raise_on_diverge:
             rc = SE_OK
         _check(rc)

@@ -346,3 +346,29 @@ def test_fdm_config0_exact_modal_and_null_space(segpu, oracle):
 def test_fdm_options_string(segpu):
     o = segpu.solver_opts("helm_", "-helm_ksp_type preonly -helm_pc_type fdm -helm_ksp_rtol 1e-9")
     assert o.method == segpu.METHOD_FDM and o.rtol == 1e-9
+
+
+def test_async_solve_and_download(segpu, oracle):
+    """se_linsys_solve_async/finish report the solve's own statistics (the
+    state copy has reached the host when finish returns), and
+    se_field_download_async matches the synchronous download after a
+    synchronize."""
+    import ctypes
+    om, m, fs, fr, ls, *_ = build(segpu, oracle, CASES[1], -1.0, -1.0, 1.0, False)
+    ls.set_opts(segpu.solver_opts(rtol=1e-12, mode=segpu.MODE_EXACT, method=segpu.METHOD_FDM))
+    ref = ls.Solve("helm_")
+    want = fs.vals
+    assert ref["reason"] == 2 and ref["its"] >= 1
+    for k in range(3):
+        ls.solve_async()
+        st = ls.solve_finish()
+        assert (st["reason"], st["its"]) == (ref["reason"], ref["its"])
+        assert st["rnorm0"] == ref["rnorm0"]
+    ls.set_opts(segpu.solver_opts(rtol=1e-6, mode=segpu.MODE_EXACT, method=segpu.METHOD_FDM))
+    ls.solve_async()
+    assert ls.solve_finish()["its"] <= ref["its"]
+    out = torch.full((len(want),), float("nan"), dtype=torch.float64).pin_memory()
+    ptr = ctypes.cast(out.data_ptr(), ctypes.POINTER(ctypes.c_double))
+    assert segpu.load_library().se_field_download_async(fs._h, ptr) == 0
+    segpu.synchronize()
+    assert np.array_equal(out.numpy(), fs.vals)
