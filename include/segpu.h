@@ -127,6 +127,30 @@ int se_field_interp_global(const se_field* field, const double* pts, int npts, d
 int se_field_save(const se_field* field, const char* name, int time_step);
 int se_field_read(se_field* field, const char* name, int time_step);
 
+/* Mesh::Save (src/base/Mesh.cpp:366-489) with a raw-binary file in place of
+ * HDF5: "<name>.seb" holds, in the HDF5 file's order, the magic "SEMESH01",
+ * the dimensions (int32 2, int32 0), the mesh resolution (int32 nVerts-1 per
+ * direction), /min and /max (double[2] each), int64 nVertsTotal, int64 linear
+ * quads, /vertices (double[nVertsTotal][2]) and /connectivity
+ * (int32[quads][4], the reference's linear quads); little-endian, 72-byte
+ * header. */
+int se_mesh_save(const se_mesh* mesh, const char* name);
+
+/* WriteXDMFHeader / WriteXDMF / WriteXDMFFooter / WriteXDMFTemporal
+ * (src/base/Utils.cpp:53-229): the same files in the working directory
+ * ("XDMF.<step>.xmf", "time.<step>.ts", "XDMF.temporalAll.xmf",
+ * "XDMF.temporalFields.xmf", "XDMF.FilesField.xdmf") and the same grid,
+ * topology, geometry and attribute structure, with Binary DataItems (byte
+ * offset Seek, little-endian) into the mesh's and the fields' ".seb" files in
+ * place of the HDF5 datasets. se_write_xdmf saves each field
+ * (se_field_save(fields[i], names[i], time_step)); mesh_name names the file
+ * se_mesh_save wrote. */
+int se_write_xdmf_header(int time_step);
+int se_write_xdmf(const se_field* const* fields, const char* const* names, int nfields,
+                  const char* mesh_name, int time_step, double time, double dt);
+int se_write_xdmf_footer(int time_step);
+int se_write_xdmf_temporal(int n_time_steps, int dump_every);
+
 /* TwoLayerQGEqn::GenVel / QuasiGeostrophicEqn::GenVel
  * (src/qg/TwoLayerQGEqn.cpp:335-352, src/qg/QuasiGeostrophicEqn.cpp:207-223):
  * vel (ndofs 2) = (-d psi/dy, d psi/dx) at every vertex, each derivative by

@@ -1568,6 +1568,184 @@ int se_field_read(se_field* field, const char* name, int time_step) {
   return SE_OK;
 }
 
+// ------------------------------------------------------ mesh and XDMF ----
+// Mesh::Save (src/base/Mesh.cpp:366-489) and the XDMF writers
+// (src/base/Utils.cpp:53-229) with raw little-endian binary in place of
+// HDF5. "<name>.seb" holds, in the HDF5 file's order: the magic "SEMESH01",
+// the dimensions (int32 2, int32 pad), the mesh resolution (int32
+// nVerts-1 per direction), /min and /max (double[2] each), the counts
+// (int64 nVertsTotal, int64 linear quads), /vertices (double[nVertsTotal][2])
+// and /connectivity (int32[quads][4], the reference's linear quads). The XDMF
+// files reference these and the fields' ".seb" files as Binary DataItems
+// with their byte offsets (Seek) past the headers.
+namespace {
+const char kMeshMagic[8] = {'S', 'E', 'M', 'E', 'S', 'H', '0', '1'};
+constexpr long kMeshHeaderBytes = 72;
+constexpr long kFieldHeaderBytes = 32;  // "SEFIELD1", dims, resolution, rows, columns
+std::string step_tag(int step) {
+  char buf[16];
+  snprintf(buf, sizeof(buf), "%.5u", (unsigned)step);
+  return buf;
+}
+// operator<< of a double on a default std::ostream (6 significant digits)
+std::string fmt_double(double v) {
+  char buf[64];
+  snprintf(buf, sizeof(buf), "%g", v);
+  return buf;
+}
+bool write_text(const std::string& fn, const std::string& text, const char* mode) {
+  FILE* f = std::fopen(fn.c_str(), mode);
+  if (!f) return false;
+  const bool ok = std::fwrite(text.data(), 1, text.size(), f) == text.size();
+  return (std::fclose(f) == 0) && ok;
+}
+const char* kXdmfHead =
+    "<?xml version=\"1.0\" ?>\n<!DOCTYPE Xdmf SYSTEM \"Xdmf.dtd\" []>\n"
+    "<Xdmf xmlns:xi=\"http://www.w3.org/2001/XInclude\" Version=\"2.0\">\n\n<Domain>\n\n";
+const char* kXdmfFoot = "</Domain>\n\n</Xdmf>\n\n";
+}  // namespace
+
+int se_mesh_save(const se_mesh* mesh, const char* name) {
+  if (!mesh || !name) return fail(SE_ERR_ARG, "null argument");
+  const MeshDev& d = mesh->dev;
+  const int64_t nv = mesh->nVertsTotal;
+  const int32_t nl[2] = {d.nVerts[0] - 1, d.nVerts[1] - 1};
+  const int64_t nq = (int64_t)nl[0] * nl[1];
+  std::vector<double> verts(2 * (size_t)nv);
+  if (int rc = se_mesh_verts(mesh, verts.data())) return rc;
+  std::vector<int32_t> conn(4 * (size_t)nq);
+  for (int64_t e = 0; e < nq; e++) {
+    const int32_t j = (int32_t)(e / nl[0]);
+    int32_t* c = conn.data() + 4 * e;
+    c[0] = (int32_t)e + j;
+    c[1] = c[0] + 1;
+    c[2] = c[1] + d.nVerts[0];
+    c[3] = c[2] - 1;
+  }
+  const std::string fn = std::string(name) + ".seb";
+  FILE* f = std::fopen(fn.c_str(), "wb");
+  if (!f) return fail(SE_ERR_ARG, "cannot create %s", fn.c_str());
+  const int32_t dims[2] = {2, 0};
+  bool ok = std::fwrite(kMeshMagic, 1, 8, f) == 8 && std::fwrite(dims, 4, 2, f) == 2 &&
+            std::fwrite(nl, 4, 2, f) == 2 && std::fwrite(d.min, 8, 2, f) == 2 &&
+            std::fwrite(d.max, 8, 2, f) == 2 && std::fwrite(&nv, 8, 1, f) == 1 &&
+            std::fwrite(&nq, 8, 1, f) == 1 &&
+            std::fwrite(verts.data(), sizeof(double), verts.size(), f) == verts.size() &&
+            std::fwrite(conn.data(), sizeof(int32_t), conn.size(), f) == conn.size();
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return fail(SE_ERR_ARG, "writing %s failed", fn.c_str());
+  return SE_OK;
+}
+
+int se_write_xdmf_header(int time_step) {
+  if (time_step < 0) return fail(SE_ERR_ARG, "bad time step");
+  if (!write_text("XDMF." + step_tag(time_step) + ".xmf", kXdmfHead, "w"))
+    return fail(SE_ERR_ARG, "cannot write the XDMF header");
+  return SE_OK;
+}
+int se_write_xdmf_footer(int time_step) {
+  if (time_step < 0) return fail(SE_ERR_ARG, "bad time step");
+  if (!write_text("XDMF." + step_tag(time_step) + ".xmf", kXdmfFoot, "a"))
+    return fail(SE_ERR_ARG, "cannot write the XDMF footer");
+  return SE_OK;
+}
+
+int se_write_xdmf(const se_field* const* fields, const char* const* names, int nfields,
+                  const char* mesh_name, int time_step, double time, double dt) {
+  if (!fields || !names || nfields < 1 || !mesh_name || time_step < 0)
+    return fail(SE_ERR_ARG, "bad argument");
+  for (int i = 0; i < nfields; i++) {
+    if (int rc = check_field(fields[i])) return rc;
+    if (!names[i]) return fail(SE_ERR_ARG, "null field name");
+    if (fields[i]->mesh != fields[0]->mesh) return fail(SE_ERR_ARG, "fields on different meshes");
+  }
+  const std::string ts = step_tag(time_step);
+  if (!write_text("time." + ts + ".ts", "time step:\t" + std::to_string(time_step) + "\ttime:\t" +
+                                             fmt_double(time) + "\tdt:\t" + fmt_double(dt) + "\n",
+                  "w"))
+    return fail(SE_ERR_ARG, "cannot write time.%s.ts", ts.c_str());
+  for (int i = 0; i < nfields; i++)
+    if (int rc = se_field_save(fields[i], names[i], time_step)) return rc;
+  const MeshDev& d = fields[0]->mesh->dev;
+  const long nv = fields[0]->mesh->nVertsTotal;
+  const long nq = (long)(d.nVerts[0] - 1) * (d.nVerts[1] - 1);
+  const std::string N = std::to_string(nv), M = mesh_name;
+  const std::string fl = "NumberType=\"Float\" Precision=\"8\" Endian=\"Little\"";
+  auto bin = [&](const std::string& dims, long seek, const std::string& file,
+                 const std::string& type) {
+    return "<DataItem Format=\"Binary\" " + type + " Seek=\"" + std::to_string(seek) +
+           "\" Dimensions=\"" + dims + "\">" + file + "</DataItem>\n";
+  };
+  auto slab = [&](int col, int width, const std::string& file, long seek, const char* nm,
+                  const std::string& ind) {
+    std::string t = ind + "<DataItem ItemType=\"HyperSlab\" Dimensions=\"" + N + " 1\"" +
+                    (nm ? std::string(" Name=\"") + nm + "\"" : "") + ">\n";
+    t += ind + "   <DataItem Dimensions=\"3 2\" Format=\"XML\"> 0 " + std::to_string(col) +
+         " 1 1 " + N + " 1 </DataItem>\n";
+    t += ind + "   " + bin(N + " " + std::to_string(width), seek, file, fl);
+    t += ind + "</DataItem>\n";
+    return t;
+  };
+  std::string x;
+  x += "   <Grid Name=\"FEM_Grid_" + M + "\">\n\n";
+  x += "      <Time Value=\"" + fmt_double(time) + "\" />\n\n";
+  x += "         <Topology Type=\"Quadrilateral\" NumberOfElements=\"" + std::to_string(nq) +
+       "\"> \n";
+  x += "            " +
+       bin(std::to_string(nq) + " 4", kMeshHeaderBytes + 16 * nv, M + ".seb",
+           "NumberType=\"Int\" Precision=\"4\" Endian=\"Little\"");
+  x += "         </Topology>\n\n";
+  x += "         <Geometry Type=\"XYZ\">\n";
+  x += "            <DataItem ItemType=\"Function\"  Dimensions=\"" + N +
+       " 3\" Function=\"JOIN($0, $1, 0*$1)\">\n";
+  x += slab(0, 2, M + ".seb", kMeshHeaderBytes, "XCoords", "               ");
+  x += slab(1, 2, M + ".seb", kMeshHeaderBytes, "YCoords", "               ");
+  x += "            </DataItem>\n";
+  x += "         </Geometry>\n\n";
+  for (int i = 0; i < nfields; i++) {
+    const std::string fn = std::string(names[i]) + "." + ts + ".seb";
+    if (fields[i]->ndofs == 1) {
+      x += std::string("         <Attribute Type=\"Scalar\" Center=\"Node\" Name=\"") + names[i] +
+           "\">\n";
+      x += slab(0, 1, fn, kFieldHeaderBytes, nullptr, "            ");
+      x += "         </Attribute>\n\n";
+    } else {
+      x += std::string("         <Attribute Type=\"Vector\" Center=\"Node\" Name=\"") + names[i] +
+           "\">\n";
+      x += "            <DataItem ItemType=\"Function\"  Dimensions=\"" + N +
+           " 3\" Function=\"JOIN($0, $1, 0*$1)\">\n";
+      x += slab(0, 2, fn, kFieldHeaderBytes, "XValue", "               ");
+      x += slab(1, 2, fn, kFieldHeaderBytes, "YValue", "               ");
+      x += "            </DataItem>\n";
+      x += "         </Attribute>\n\n";
+    }
+  }
+  x += "   </Grid>\n\n";
+  if (!write_text("XDMF." + ts + ".xmf", x, "a")) return fail(SE_ERR_ARG, "cannot append XDMF.%s.xmf", ts.c_str());
+  return SE_OK;
+}
+
+int se_write_xdmf_temporal(int n_time_steps, int dump_every) {
+  if (n_time_steps < 0 || dump_every < 1) return fail(SE_ERR_ARG, "bad step counts");
+  const std::string inc =
+      "   <xi:include href=\"XDMF.FilesField.xdmf\" xpointer=\"xpointer(//Xdmf/Grid)\"/>\n\n";
+  const std::string body = std::string(kXdmfHead) + inc + kXdmfFoot;
+  if (!write_text("XDMF.temporalAll.xmf", body, "w") ||
+      !write_text("XDMF.temporalFields.xmf", body, "w"))
+    return fail(SE_ERR_ARG, "cannot write the temporal XDMF files");
+  std::string c =
+      "<?xml version=\"1.0\" ?>\n<Xdmf xmlns:xi=\"http://www.w3.org/2001/XInclude\" "
+      "Version=\"2.0\">\n<Grid GridType=\"Collection\" CollectionType=\"Temporal\" "
+      "Name=\"FEM_Mesh_Fields\">\n";
+  for (int s = 0; s <= n_time_steps; s += dump_every)
+    c += "    <xi:include href=\"XDMF." + step_tag(s) +
+         ".xmf\" xpointer=\"xpointer(//Xdmf/Domain/Grid[1])\"/>\n";
+  c += "</Grid>\n</Xdmf>\n";
+  if (!write_text("XDMF.FilesField.xdmf", c, "w"))
+    return fail(SE_ERR_ARG, "cannot write XDMF.FilesField.xdmf");
+  return SE_OK;
+}
+
 int se_field_gen_vel(const se_field* psi, se_field* vel) {
   if (int rc = check_field(psi)) return rc;
   if (int rc = check_field(vel)) return rc;

@@ -146,6 +146,10 @@ SIGNATURES = {
     "se_ns_solve": [_vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int],
     "se_ns_stats": [_vp, ctypes.POINTER(SolveStats)], "se_ns_destroy": [_vp],
     "se_field_download_async": [_vp, _D],
+    "se_mesh_save": [_vp, ctypes.c_char_p], "se_write_xdmf_header": [ctypes.c_int],
+    "se_write_xdmf_footer": [ctypes.c_int], "se_write_xdmf_temporal": [ctypes.c_int, ctypes.c_int],
+    "se_write_xdmf": [ctypes.POINTER(_vp), ctypes.POINTER(ctypes.c_char_p), ctypes.c_int,
+                      ctypes.c_char_p, ctypes.c_int, ctypes.c_double, ctypes.c_double],
     "se_helmholtz_solve_noalloc": [_I, ctypes.c_int, _D, _D, _I, _I, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                    ctypes.POINTER(SolverOpts), ctypes.c_int, _vp, _vp,
@@ -225,6 +229,11 @@ class Mesh:
         v = np.zeros((self.nVertsTotal, 2))
         _check(_lib.se_mesh_verts(self._h, _pd(v)))
         return v
+
+    def Save(self):
+        """Mesh::Save (src/base/Mesh.cpp:366-489): <name>.seb in the working
+        directory (raw binary in place of <name>.h5)."""
+        _check(_lib.se_mesh_save(self._h, self.name.encode()))
 
     def gll(self):
         n = self.N + 1
@@ -688,6 +697,31 @@ class NavierStokesEqn:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.se_ns_destroy(self._h)
             self._h = None
+
+
+def WriteXDMFHeader(timeStep: int):
+    """WriteXDMFHeader (src/base/Utils.cpp:53-71): starts XDMF.<step>.xmf."""
+    _check(load_library().se_write_xdmf_header(int(timeStep)))
+
+
+def WriteXDMF(fields, nFields: int, timeStep: int, time: float, dt: float):
+    """WriteXDMF (src/base/Utils.cpp:91-168): time.<step>.ts, each field saved
+    as <name>.<step>.seb, and the grid appended to XDMF.<step>.xmf; the mesh
+    file is the one Mesh.Save wrote under the first field's mesh name."""
+    fs = list(fields)[:nFields]
+    hs = (_vp * len(fs))(*[f._h for f in fs])
+    names = (ctypes.c_char_p * len(fs))(*[f.name.encode() for f in fs])
+    _check(load_library().se_write_xdmf(hs, names, len(fs), fs[0].mesh.name.encode(),
+                                        int(timeStep), float(time), float(dt)))
+
+
+def WriteXDMFFooter(timeStep: int):
+    _check(load_library().se_write_xdmf_footer(int(timeStep)))
+
+
+def WriteXDMFTemporal(nTimeSteps: int, dumpEvery: int):
+    """WriteXDMFTemporal (src/base/Utils.cpp:170-229)."""
+    _check(load_library().se_write_xdmf_temporal(int(nTimeSteps), int(dumpEvery)))
 
 
 def GenVel(psi: Field, name: str = "vel") -> Field:
