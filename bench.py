@@ -517,7 +517,8 @@ def run_apply_roofline(ne=768, p=8, reps=20):
             stream.synchronize()
             ms = e0.elapsed_time(e1) / reps
             gbs = bpd * n / (ms * 1e-3) / 1e9
-            out[name] = {"kernel": ("apply_tile_kernel<8, double>" if name == "fp64"
+            out[name] = {"kernel": ("apply_ef8_kernel (element-factored FP64 FMA, cp.async "
+                                    "staging)" if name == "fp64"
                                     else "apply_tile_kernel<8, bf16 -> float>"),
                          "launch_ms": ms, "bytes_per_unknown": bpd, "achieved_gbs": gbs,
                          "peak_gbs": hbm, "frac": gbs / hbm,

@@ -849,6 +849,160 @@ cudaError_t launch_n8(const OpDev& od, const double* x, double* y, unsigned* err
   return cudaGetLastError();
 }
 
+// ------------------------------------------------ order 8, CUDA cores ----
+// Element-factored FP64 apply for N = 8 on the FP64 FMA pipes. A block
+// stages a 64 x 32 vertex tile and an 8-vertex halo to the left and below
+// (zero where a vertex is no unknown), then
+//   x pass: thread (element e, row r) reads the 17 values of its element row
+//           and of the left element's row and forms the 8 outputs of its
+//           element's nodes a = 0..7 with the 9 x 9 stiffness block and, at
+//           a = 0, the left element's last row: 81 FMAs, all coefficients
+//           compile-time offsets into the kernel's parameters;
+//   y pass: thread (element e, column c) does the same along the column and
+//           combines alpha wx wy x + beta_x wy (Kx x) + beta_y wx (Ky x).
+// About 21 FMAs and 3 shared-memory loads per unknown, no padding work, and
+// the staging costs a few instructions per value (each lane maps its staged
+// columns once; a staged row's unknown index is the same for the whole warp):
+// the FP64 pipes out-run HBM, so the kernel is bound by its 16 bytes per
+// unknown.
+constexpr int kEfTX = 64, kEfW = kEfTX + 9, kEfOX = kEfTX + 1;
+
+template <int TY, int MINB>
+__global__ void __launch_bounds__(8 * TY, MINB) apply_ef8_kernel(const OpDev op,
+                                                                  const double* __restrict__ x,
+                                                                  double* __restrict__ y) {
+  constexpr int N = 8, kEfTY = TY, kEfH = TY + 9, kWarps = TY / 4;
+  extern __shared__ __align__(16) double efsm[];
+  double* X = efsm;                   // vertices (gx0-8 .. gx0+64) x (gy0-8 .. gy0+TY)
+  double* OX = X + kEfH * kEfW;       // x-pass results of the tile's vertices
+  double* sw = OX + kEfTY * kEfOX;
+  const Dir& dx = op.d[0];
+  const Dir& dy = op.d[1];
+  const int gx0 = blockIdx.x * kEfTX, gy0 = blockIdx.y * kEfTY;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid <= N) sw[tid] = op.w[tid];
+  {  // staging: warp w takes rows w, w + kWarps, ...; lane l columns l, l + 32, l + 64
+    int cu[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      const int i = lane + 32 * q;
+      cu[q] = i < kEfW ? unk(dx, gx0 - N + i) : -1;
+    }
+#pragma unroll
+    for (int r = 0; r < (kEfH + kWarps - 1) / kWarps; r++) {
+      const int j = warp + kWarps * r;
+      if (j < kEfH) {
+        const int uy = unk(dy, gy0 - N + j);
+        const double* rowp = x + (size_t)(uy < 0 ? 0 : uy) * op.G[0];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+          const int i = lane + 32 * q;
+          if (i < kEfW) {
+            const bool ok = uy >= 0 && cu[q] >= 0;
+            const double* src = ok ? rowp + cu[q] : x;
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(X + j * kEfW + i);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src),
+                         "r"(ok ? 8 : 0));
+          }
+        }
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 0;\n" ::);
+  }
+  __syncthreads();
+  {  // x pass: warp = one element, 32 rows (row stride 73: conflict-free)
+    constexpr int n = N + 1;
+    const int r = lane + 32 * (warp >> 3), e = warp & 7;
+    const int ex = (gx0 >> 3) + e;
+    const double* row = X + (r + N) * kEfW + e * N;  // left element's first node
+    double v[2 * N + 1];
+#pragma unroll
+    for (int k = 0; k <= 2 * N; k++) v[k] = row[k];
+    const bool own = ex < dx.nE, left = ex > 0 || dx.periodic;
+    double o[N];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      double t = 0.0;
+      if (own) {
+#pragma unroll
+        for (int b = 0; b < n; b++) t = fma(op.Kh[a * n + b], v[N + b], t);
+      }
+      o[a] = t;
+    }
+    if (left) {
+      double t = 0.0;
+#pragma unroll
+      for (int b = 0; b < n; b++) t = fma(op.Kh[N * n + b], v[b], t);
+      o[0] += t;
+    }
+#pragma unroll
+    for (int a = 0; a < N; a++) OX[r * kEfOX + e * N + a] = o[a];
+  }
+  __syncthreads();
+  {  // y pass: warp = 32 consecutive columns of one element row
+    constexpr int n = N + 1;
+    const int c = tid & 63, e = tid >> 6;
+    const int ey = (gy0 >> 3) + e;
+    const int gx = gx0 + c;
+    const double* col = X + (e * N) * kEfW + c + N;  // lower element's first node
+    double v[2 * N + 1];
+#pragma unroll
+    for (int k = 0; k <= 2 * N; k++) v[k] = col[k * kEfW];
+    const bool own = ey < dy.nE, left = ey > 0 || dy.periodic;
+    double o[N];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      double t = 0.0;
+      if (own) {
+#pragma unroll
+        for (int b = 0; b < n; b++) t = fma(op.Kh[a * n + b], v[N + b], t);
+      }
+      o[a] = t;
+    }
+    if (left) {
+      double t = 0.0;
+#pragma unroll
+      for (int b = 0; b < n; b++) t = fma(op.Kh[N * n + b], v[b], t);
+      o[0] += t;
+    }
+    if (gx >= dx.lo && gx < dx.hi) {
+      const int ux = gx - dx.lo;
+      const double wx = wsum<N>(dx, sw, gx >> 3, gx & 7);
+#pragma unroll
+      for (int a = 0; a < N; a++) {
+        const int gy = gy0 + e * N + a;
+        if (gy < dy.lo || gy >= dy.hi) continue;
+        const double wy = (a == 0 ? (own ? sw[0] : 0.0) + (left ? sw[N] : 0.0) : sw[a]);
+        const double r = op.alpha * wx * wy * v[N + a] +
+                         op.beta[0] * wy * OX[(e * N + a) * kEfOX + c] + op.beta[1] * wx * o[a];
+        y[(size_t)(gy - dy.lo) * op.G[0] + ux] = r;
+      }
+    }
+  }
+}
+
+template <int TY = 32, int MINB = 3>
+cudaError_t launch_ef8(const OpDev& op, const double* x, double* y, cudaStream_t s) {
+  constexpr size_t smem = sizeof(double) * ((size_t)(TY + 9) * kEfW + (size_t)TY * kEfOX + 16);
+  if (smem > 48 * 1024) {
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr[dev]) {
+      e = cudaFuncSetAttribute(apply_ef8_kernel<TY, MINB>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      attr[dev] = true;
+    }
+  }
+  const dim3 grid((op.d[0].hi + kEfTX - 1) / kEfTX, (op.d[1].hi + TY - 1) / TY);
+  apply_ef8_kernel<TY, MINB><<<grid, 8 * TY, smem, s>>>(op, x, y);
+  return cudaGetLastError();
+}
+
 }  // namespace
 
 #define SE_APPLY_N(n) \
@@ -863,7 +1017,7 @@ cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, unsigne
     SE_APPLY_N(2) SE_APPLY_N(3) SE_APPLY_N(4) SE_APPLY_N(5) SE_APPLY_N(6) SE_APPLY_N(7)
     SE_APPLY_N(9) SE_APPLY_N(10) SE_APPLY_N(11) SE_APPLY_N(12)
     case 8:
-      return launch_n8(op, x, y, err, s);
+      return launch_ef8<32, 3>(op, x, y, s);
     default:
       return cudaErrorInvalidValue;
   }
