@@ -25,7 +25,9 @@
 //
 // Instantiated for FP64 (x, arithmetic and y in FP64) and for the reduced-
 // precision apply (x in BF16 or FP16, operator and arithmetic in FP32, y in
-// FP32).
+// FP32). In FP64, order 8 runs the element-factored kernel on the FP64 FMA
+// pipes (apply_ef8_kernel, at the end of this file) and the other orders the
+// same element products on the FP64 tensor cores (apply_mma_kernel).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -524,212 +526,6 @@ __global__ void __launch_bounds__(kThreads) apply_mma_kernel(const __grid_consta
   }
 }
 
-// ---------------------------------------------------------------------------
-// Order N = 8: both directions in the same MMA fragments. A warp task is two
-// vertically stacked elements (16 grid rows x 8 columns of outputs):
-//   x: Zx (16 x 8) = W (16 rows x 24 window columns) * B (24 x 8), B the
-//      window matrix above, held as fragments;
-//   y: Zy (16 x 8) = A (16 x 32) * V (32 window rows x 8 columns), with the
-//      constant A = [[B^T 0]; [0 B^T]] (lower element: window rows 0..23,
-//      upper element: rows 8..31), also held as fragments.
-// Both accumulators have the same layout (row g / g+8, columns 2t, 2t+1), so
-// y = alpha wx wy u + beta_x wy Zx + beta_y wx Zy is formed in registers and
-// stored to global memory: no output buffer in shared memory. A warp takes
-// three consecutive elements of one 16-row block, sliding the x window's
-// fragments from one element to the next. Tiles are 12 x 4 elements, staged
-// by TMA as above.
-struct N8 {
-  static constexpr int N = 8, TEX = 12, TEY = 4, TW = 96, TH = 32;
-  static constexpr int UW = (TEX - 1) * N + 24;  // 112 staged columns read
-  static constexpr int UH = TH + 16;             // 48 staged rows read
-  static constexpr int UP = ((UW + 1 + 11) / 16) * 16 + 4;  // 116: shift column, 4 mod 16
-  static constexpr int NU = ((UH * UP * 8 + 127) / 128) * 16;
-  static constexpr unsigned BOX_BYTES = (unsigned)(UP * UH * 8);
-  static constexpr int REAL_UW = TW + N + 1, REAL_UH = TH + N + 1;  // staged vertices
-  static constexpr int GROUP = 3;                                   // elements per warp task
-  static constexpr size_t SMEM = 128 + 16 + sizeof(double) * (size_t)(2 * NU);
-};
-
-__device__ __forceinline__ bool tile_tma8(const ApplyOp<double>& op, int tma, int tiles_x, int t,
-                                          int& xs, int& ys) {
-  const int gx0 = (t % tiles_x) * N8::TW, gy0 = (t / tiles_x) * N8::TH;
-  xs = gx0 - N8::N - op.dx.lo;
-  ys = gy0 - N8::N - op.dy.lo;
-  if (!tma) return false;
-  if (op.dx.periodic && (xs < 0 || xs + N8::REAL_UW > op.G0)) return false;
-  if (op.dy.periodic && (ys < 0 || ys + N8::REAL_UH > op.G1)) return false;
-  return true;
-}
-
-// Assembled 1-D weight of node a of element e (e may lie outside the mesh
-// for vertices that are not outputs).
-__device__ __forceinline__ double wnode(const Dir& d, const double* w, int e, int a) {
-  if (a != 0) return w[a];
-  double s = 0.0;
-  if (e < d.nE) s += w[0];
-  if (e > 0 || d.periodic) s += w[8];
-  return s;
-}
-
-__global__ void __launch_bounds__(kThreads, 2) apply_n8_kernel(const __grid_constant__ CUtensorMap map,
-                                                               const ApplyOp<double> op,
-                                                               const double* __restrict__ x,
-                                                               double* __restrict__ y, int tiles_x,
-                                                               int ntiles, int tma, unsigned* err) {
-  constexpr int N = 8, n = 9;
-  typedef N8 T;
-  extern __shared__ unsigned char smem_raw[];
-  unsigned char* base = smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);
-  double* Ubuf = reinterpret_cast<double*>(base);  // [2][NU]
-  uint64_t* bar = reinterpret_cast<uint64_t*>(Ubuf + 2 * T::NU);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int g = lane >> 2, tq = lane & 3;
-  if (blockIdx.x >= ntiles) return;
-
-  // x: B fragments (3 k-steps); y: A fragments of [[B^T 0]; [0 B^T]] (4 k-steps)
-  double bx[3][2], ay[4][4];
-#pragma unroll
-  for (int ks = 0; ks < 3; ks++) {
-    bx[ks][0] = bwin<N>(op, ks * 8 + tq, g);
-    bx[ks][1] = bwin<N>(op, ks * 8 + tq + 4, g);
-  }
-#pragma unroll
-  for (int ks = 0; ks < 4; ks++) {
-    const int k0 = ks * 8 + tq, k1 = k0 + 4;
-    ay[ks][0] = k0 < 24 ? bwin<N>(op, k0, g) : 0.0;           // (m = g,     k0)
-    ay[ks][1] = k0 >= 8 ? bwin<N>(op, k0 - 8, g) : 0.0;       // (m = g + 8, k0)
-    ay[ks][2] = k1 < 24 ? bwin<N>(op, k1, g) : 0.0;           // (m = g,     k1)
-    ay[ks][3] = k1 >= 8 ? bwin<N>(op, k1 - 8, g) : 0.0;       // (m = g + 8, k1)
-  }
-
-  if (threadIdx.x == 0) {
-    mbar_init(&bar[0], 1);
-    mbar_init(&bar[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int xs, ys;
-    if (tile_tma8(op, tma, tiles_x, blockIdx.x, xs, ys)) {
-      mbar_expect_tx(&bar[0], T::BOX_BYTES);
-      tma_load_2d(Ubuf, &map, xs & ~1, ys, &bar[0]);
-    }
-  }
-
-  const bool nat_x = !op.dx.periodic, nat_y = !op.dy.periodic;
-  const int lastx = op.dx.nV - 1, lasty = op.dy.nV - 1;
-  const int rb = (warp & 1) * 16;              // the warp's 16-row block
-  const int e0 = (warp >> 1) * T::GROUP;       // its first element column
-  unsigned phase = 0;
-  int i = 0;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x, i++) {
-    const int s = i & 1;
-    double* U = Ubuf + s * T::NU;
-    const int gx0 = (t % tiles_x) * T::TW, gy0 = (t / tiles_x) * T::TH;
-    int xs, ys, off = 0;
-    if (tile_tma8(op, tma, tiles_x, t, xs, ys)) {
-      mbar_wait_bounded(&bar[s], (phase >> s) & 1u, err);
-      phase ^= 1u << s;
-      off = xs & 1;
-    } else {
-      const int vx0 = gx0 - N, vy0 = gy0 - N;
-      for (int j = warp; j < T::UH; j += kThreads / 32)
-        for (int c = lane; c < T::UP; c += 32) {
-          double v = 0.0;
-          if (j < T::REAL_UH && c < T::REAL_UW) {
-            const int ux = unk(op.dx, vx0 + c), uy = unk(op.dy, vy0 + j);
-            if (ux >= 0 && uy >= 0) v = x[(size_t)uy * op.G0 + ux];
-          }
-          U[j * T::UP + c] = v;
-        }
-      __syncthreads();
-    }
-
-    // prefetch the next tile into the other stage (last read one iteration ago)
-    const int tn = t + gridDim.x;
-    if (threadIdx.x == 0 && tn < ntiles) {
-      int xn, yn;
-      if (tile_tma8(op, tma, tiles_x, tn, xn, yn)) {
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        mbar_expect_tx(&bar[s ^ 1], T::BOX_BYTES);
-        tma_load_2d(Ubuf + (s ^ 1) * T::NU, &map, xn & ~1, yn, &bar[s ^ 1]);
-      }
-    }
-
-    const double* Us = U + off;  // staged (row j, column c) at Us[j * UP + c]
-    const int ey0 = gy0 / N + rb / N;  // element row of the warp's lower element
-    // x window fragments of k-steps e0 .. e0 + GROUP + 1 (sliding)
-    double af[3][4];
-    const double* xr = Us + (rb + N + g) * T::UP + e0 * N + tq;
-#pragma unroll
-    for (int ks = 0; ks < 2; ks++) {
-      af[ks][0] = xr[ks * 8];
-      af[ks][1] = xr[8 * T::UP + ks * 8];
-      af[ks][2] = xr[ks * 8 + 4];
-      af[ks][3] = xr[8 * T::UP + ks * 8 + 4];
-    }
-#pragma unroll
-    for (int el = 0; el < T::GROUP; el++) {
-      const int k = e0 + el;  // element column within the tile
-      {
-        const int ks = el + 2;
-        af[2][0] = xr[ks * 8];
-        af[2][1] = xr[8 * T::UP + ks * 8];
-        af[2][2] = xr[ks * 8 + 4];
-        af[2][3] = xr[8 * T::UP + ks * 8 + 4];
-      }
-      double cx[4] = {0.0, 0.0, 0.0, 0.0}, cy[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-      for (int ks = 0; ks < 3; ks++) dmma(cx, af[ks][0], af[ks][1], af[ks][2], af[ks][3], bx[ks][0], bx[ks][1]);
-      // y: V[k][n] = staged (row rb + k, column k*N + N + n)
-      const double* yc = Us + (rb + tq) * T::UP + k * N + N + g;
-#pragma unroll
-      for (int ks = 0; ks < 4; ks++)
-        dmma(cy, ay[ks][0], ay[ks][1], ay[ks][2], ay[ks][3], yc[(ks * 8) * T::UP],
-             yc[(ks * 8 + 4) * T::UP]);
-#pragma unroll
-      for (int af_s = 0; af_s < 2; af_s++)
-#pragma unroll
-        for (int q = 0; q < 4; q++) af[af_s][q] = af[af_s + 1][q];
-
-      // outputs: rows rb + g (+8), columns k*N + 2tq (+1)
-      const int cx0 = k * N + 2 * tq;
-      const int exk = gx0 / N + k;
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        const int r = rb + g + 8 * h;
-        const int gy = gy0 + r;
-        if (gy < op.dy.lo || gy >= op.dy.hi) continue;
-        const int ay_node = g;  // r mod N
-        const double wy = wnode(op.dy, op.w, ey0 + h, ay_node);
-        const double* up = Us + (r + N) * T::UP + cx0 + N;  // may be 8-byte aligned only
-        const double u0 = up[0], u1 = up[1];
-#pragma unroll
-        for (int qq = 0; qq < 2; qq++) {
-          const int cc = cx0 + qq, gx = gx0 + cc;
-          if (gx < op.dx.lo || gx >= op.dx.hi) continue;
-          const double uval = qq ? u1 : u0;
-          double zx = cx[2 * h + qq], zy = cy[2 * h + qq];
-          if (nat_x && cc % N == 0) {
-            if (gx == 0) zx = fma(-op.Kh[N * n + N], uval, zx);
-            if (gx == lastx) zx = fma(-op.Kh[0], uval, zx);
-          }
-          if (nat_y && ay_node == 0) {
-            if (gy == 0) zy = fma(-op.Kh[N * n + N], uval, zy);
-            if (gy == lasty) zy = fma(-op.Kh[0], uval, zy);
-          }
-          const double wx = wnode(op.dx, op.w, exk, 2 * tq + qq);
-          double v = op.alpha * wx * wy * uval;
-          v = fma(op.bx * wy, zx, v);
-          v = fma(op.by * wx, zy, v);
-          y[(size_t)(gy - op.dy.lo) * op.G0 + (gx - op.dx.lo)] = v;
-        }
-      }
-    }
-    __syncthreads();
-  }
-}
-
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
 // against the driver library).
 PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -796,56 +592,6 @@ cudaError_t launch_mma(const OpDev& od, const double* x, double* y, unsigned* er
   const int ntiles = tiles_x * tiles_y;
   const int grid = ntiles < per_sm[dev] * sms[dev] ? ntiles : per_sm[dev] * sms[dev];
   apply_mma_kernel<N><<<grid, kThreads, T::SMEM, s>>>(map, op, x, y, tiles_x, ntiles, tma, err);
-  return cudaGetLastError();
-}
-
-// Launch of the order-8 kernel (same set-up as launch_mma).
-cudaError_t launch_n8(const OpDev& od, const double* x, double* y, unsigned* err, cudaStream_t s) {
-  typedef N8 T;
-  ApplyOp<double> op;
-  for (int k = 0; k < 81; k++) op.Kh[k] = od.Kh[k];
-  for (int k = 0; k <= 8; k++) op.w[k] = od.w[k];
-  op.alpha = od.alpha;
-  op.bx = od.beta[0];
-  op.by = od.beta[1];
-  op.dx = od.d[0];
-  op.dy = od.d[1];
-  op.G0 = od.G[0];
-  op.G1 = od.G[1];
-  static int per_sm[64] = {};
-  static int sms[64] = {};
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  if (!per_sm[dev]) {
-    e = cudaFuncSetAttribute(apply_n8_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)T::SMEM);
-    if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return e;
-    int b = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, apply_n8_kernel, kThreads, T::SMEM);
-    if (e != cudaSuccess) return e;
-    per_sm[dev] = b > 0 ? b : 1;
-  }
-  CUtensorMap map;
-  std::memset(&map, 0, sizeof(map));
-  int tma = 0;
-  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (enc && (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (od.G[0] % 2) == 0) {
-    const cuuint64_t dims[2] = {(cuuint64_t)od.G[0], (cuuint64_t)od.G[1]};
-    const cuuint64_t strides[1] = {(cuuint64_t)od.G[0] * sizeof(double)};
-    const cuuint32_t box[2] = {(cuuint32_t)T::UP, (cuuint32_t)T::UH};
-    const cuuint32_t estr[2] = {1, 1};
-    tma = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(x), dims, strides, box,
-              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-  }
-  const int tiles_x = (od.d[0].hi + T::TW - 1) / T::TW;
-  const int tiles_y = (od.d[1].hi + T::TH - 1) / T::TH;
-  const int ntiles = tiles_x * tiles_y;
-  const int grid = ntiles < per_sm[dev] * sms[dev] ? ntiles : per_sm[dev] * sms[dev];
-  apply_n8_kernel<<<grid, kThreads, T::SMEM, s>>>(map, op, x, y, tiles_x, ntiles, tma, err);
   return cudaGetLastError();
 }
 
