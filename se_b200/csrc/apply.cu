@@ -713,16 +713,29 @@ __global__ void __launch_bounds__(8 * TY, MINB) apply_ef8_kernel(const OpDev op,
       o[0] += t;
     }
     if (gx >= dx.lo && gx < dx.hi) {
-      const int ux = gx - dx.lo;
       const double wx = wsum<N>(dx, sw, gx >> 3, gx & 7);
+      const double axw = op.alpha * wx, bxw = op.beta[1] * wx;
+      const double w0 = (own ? op.w[0] : 0.0) + (left ? op.w[N] : 0.0);
+      const int gyb = gy0 + e * N;
+      const size_t ld = (size_t)op.G[0];
+      double* yp = y + (ptrdiff_t)(gyb - dy.lo) * op.G[0] + (gx - dx.lo);
+      const double* oxp = OX + (e * N) * kEfOX + c;
+      // y = wy (alpha wx x + beta_x (Kx x)) + beta_y wx (Ky x), wy the
+      // assembled weight of the row (compile-time parameter offsets)
+      if (gyb >= dy.lo && gyb + N <= dy.hi) {  // the whole strip is unknowns
 #pragma unroll
-      for (int a = 0; a < N; a++) {
-        const int gy = gy0 + e * N + a;
-        if (gy < dy.lo || gy >= dy.hi) continue;
-        const double wy = (a == 0 ? (own ? sw[0] : 0.0) + (left ? sw[N] : 0.0) : sw[a]);
-        const double r = op.alpha * wx * wy * v[N + a] +
-                         op.beta[0] * wy * OX[(e * N + a) * kEfOX + c] + op.beta[1] * wx * o[a];
-        y[(size_t)(gy - dy.lo) * op.G[0] + ux] = r;
+        for (int a = 0; a < N; a++) {
+          const double wy = a == 0 ? w0 : op.w[a];
+          yp[a * ld] = fma(wy, fma(axw, v[N + a], op.beta[0] * oxp[a * kEfOX]), bxw * o[a]);
+        }
+      } else {
+#pragma unroll
+        for (int a = 0; a < N; a++) {
+          const int gy = gyb + a;
+          const double wy = a == 0 ? w0 : op.w[a];
+          const double r = fma(wy, fma(axw, v[N + a], op.beta[0] * oxp[a * kEfOX]), bxw * o[a]);
+          if (gy >= dy.lo && gy < dy.hi) yp[(ptrdiff_t)a * op.G[0]] = r;
+        }
       }
     }
   }
@@ -763,7 +776,7 @@ cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, unsigne
     SE_APPLY_N(2) SE_APPLY_N(3) SE_APPLY_N(4) SE_APPLY_N(5) SE_APPLY_N(6) SE_APPLY_N(7)
     SE_APPLY_N(9) SE_APPLY_N(10) SE_APPLY_N(11) SE_APPLY_N(12)
     case 8:
-      return launch_ef8<32, 3>(op, x, y, s);
+      return launch_ef8<32, 4>(op, x, y, s);
     default:
       return cudaErrorInvalidValue;
   }
