@@ -474,7 +474,16 @@ def read_peaks():
 
 
 # ------------------------------------------------------- operator apply ----
-def run_apply_roofline(ne=768, p=8, reps=20):
+def apply_kernel_name(p, name):
+    """The kernel the library's apply dispatches to for order p."""
+    if name != "fp64":
+        return f"apply_tile_kernel<{p}, bf16 -> float>"
+    if p == 8:
+        return "apply_ef8_kernel (element-factored FP64 FMA, cp.async staging)"
+    return f"apply_mma_kernel<{p}> (FP64 DMMA element products, TMA-staged tiles)"
+
+
+def run_apply_roofline(ne=768, p=8, reps=20, precisions=("fp64", "bf16_in_fp32_out")):
     """The matrix-free Helmholtz apply y = A x on a doubly periodic
     ne x ne element mesh of order p (ne = 768, p = 8: 37.7M unknowns, larger
     than L2 in every precision), timed with CUDA events on the launching
@@ -498,6 +507,8 @@ def run_apply_roofline(ne=768, p=8, reps=20):
            "unknowns": n}
     with torch.cuda.stream(stream):
         for name, bpd in (("fp64", 16), ("bf16_in_fp32_out", 6)):
+            if name not in precisions:
+                continue
             if name == "fp64":
                 x = torch.randn(n, device="cuda", dtype=torch.float64, generator=g)
                 y = torch.empty(n, device="cuda", dtype=torch.float64)
@@ -517,9 +528,7 @@ def run_apply_roofline(ne=768, p=8, reps=20):
             stream.synchronize()
             ms = e0.elapsed_time(e1) / reps
             gbs = bpd * n / (ms * 1e-3) / 1e9
-            out[name] = {"kernel": ("apply_ef8_kernel (element-factored FP64 FMA, cp.async "
-                                    "staging)" if name == "fp64"
-                                    else "apply_tile_kernel<8, bf16 -> float>"),
+            out[name] = {"kernel": apply_kernel_name(p, name),
                          "launch_ms": ms, "bytes_per_unknown": bpd, "achieved_gbs": gbs,
                          "peak_gbs": hbm, "frac": gbs / hbm,
                          "peak_source": src + " (MEASURED_PEAKS.json hbm_gbs)",
@@ -616,6 +625,56 @@ def run_config1(steps=200, seed=11):
             "dt": dt, "mass_drift": float((phi.Integrate(0) - mass0) / mass0),
             "rel_l2_error_return": float(S.FieldError(phi, exact)),
             "sl_ms_per_step": sl_ms / steps}
+
+
+def run_sl_second(reps=20, seed=11):
+    """The second-order SL kernel (Advector::SecondOrder: velocities
+    extrapolated to n+1 and n+1/2, departure points at dt and 2 dt, result
+    2 phi^n(x1) - 1/2 phi^{n-1}(x2)) on the doubly periodic 64 x 64 element,
+    p = 8 mesh: Taylor-Green velocities at two time levels (amplitudes 1 and
+    0.98) and the seeded blobs of config 1 (and the same blobs shifted by
+    0.01 as phi^{n-1}), dt at Courant 2. Timed with CUDA events over `reps`
+    launches after 3 warm-up launches; inputs are L2-resident (8.4 MB).
+    Algorithmic bytes per vertex: phi^n, phi^{n-1}, u^n, u^{n-1} in and
+    the result out = 56."""
+    import torch
+    import se_b200 as S
+    hbm, src = read_peaks()
+    rng = np.random.default_rng(seed)
+    m = S.Mesh("m", [64, 64], "legendre", 8, [0, 0], [1, 1], [True, True])
+    X = m.verts
+    x, y = X[:, 0], X[:, 1]
+    phi0 = np.zeros(len(X))
+    for cx, cy in rng.uniform(0, 1, size=(4, 2)):
+        phi0 += np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / 0.05 ** 2)
+    utg = np.stack([-np.sin(np.pi * x) ** 2 * np.sin(2 * np.pi * y),
+                    np.sin(np.pi * y) ** 2 * np.sin(2 * np.pi * x)], 1)
+    phi, phim = S.Field("phi", m, 1, None), S.Field("phim", m, 1, None)
+    vel, velm = S.Field("vel", m, 2, None), S.Field("velm", m, 2, None)
+    phi.vals, vel.vals, velm.vals = phi0, utg, 0.98 * utg
+    phim.vals = np.roll(phi0, 1)
+    dt = S.CalcTimeStep(vel, 2.0)
+    adv = S.Advector(phi, vel, phim, velm)
+    stream = torch.cuda.Stream()
+    S.set_stream(stream.cuda_stream)  # the events below record on the library's stream
+    for _ in range(3):
+        adv.Advect(dt)
+    stream.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        adv.Advect(dt)
+    e1.record(stream)
+    stream.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    nv = len(X)
+    gbs = 56 * nv / (ms * 1e-3) / 1e9
+    return {"workload": "second-order SL, 64x64 elements p=8, Taylor-Green at two levels, "
+                        "Courant 2", "kernel": "sl_second_kernel<8>", "vertices": nv,
+            "launch_ms": ms, "vertex_updates_per_s": nv / (ms * 1e-3),
+            "bytes_per_vertex": 56, "achieved_gbs": gbs, "peak_gbs": hbm, "frac": gbs / hbm,
+            "peak_source": src + " (MEASURED_PEAKS.json hbm_gbs)",
+            "finite": bool(np.isfinite(adv.fieldSL.vals).all())}
 
 
 def run_config2(steps=20, seed=5):
@@ -974,6 +1033,13 @@ def main():
         extras["config2"] = run_config2()
         log("apply roofline")
         extras["apply_roofline"] = run_apply_roofline()
+        # the other orders of the ensemble and serving meshes, at the same
+        # 37.7M unknowns (6144 x 6144)
+        extras["apply_roofline_p4_p6"] = {
+            f"p{p}": run_apply_roofline(ne=6144 // p, p=p, precisions=("fp64",))
+            for p in (4, 6)}
+        log("second-order SL")
+        extras["sl_second_order"] = run_sl_second()
         log("ensemble")
         extras["ensemble"] = run_ensemble()
         log("serving")

@@ -3,12 +3,13 @@
     python -m se_b200.profile_cases apply [ne]       # FP64 operator apply
     python -m se_b200.profile_cases apply_bf16 [ne]  # BF16-in, FP32 operator apply
     python -m se_b200.profile_cases sl [ne]          # first-order SL advection
+    python -m se_b200.profile_cases sl2 [ne]         # second-order SL advection
     python -m se_b200.profile_cases cg [ne]          # persistent Jacobi-PCG solve
     python -m se_b200.profile_cases fdm [ne]         # one FDM solve (a CUDA graph)
     python -m se_b200.profile_cases fdm_apply [ne]   # the FDM transform: 4 product kernels
 
-Each case builds an ne x ne element (default 64, the bench's mesh), p=8,
-doubly periodic mesh and the bench's fields and launches the kernel a few
+Each case builds an ne x ne element (default 64, the bench's mesh), order p
+(third argument, default 8), doubly periodic mesh and the bench's fields and launches the kernel a few
 times directly (not inside a graph), so that ncu can capture individual
 launches. Prints one line with the mean device time of the launches (CUDA
 events).
@@ -20,14 +21,14 @@ import sys
 import numpy as np
 
 
-def main(case: str, ne: int = 64, reps: int = 3) -> None:
+def main(case: str, ne: int = 64, p: int = 8, reps: int = 3) -> None:
     import torch
 
     from . import segpu as S
 
     S.load_library()
     torch.cuda.init()
-    nx, p = ne, 8
+    nx = ne
     m = S.Mesh("m", [nx, nx], "legendre", p, [0.0, 0.0], [1.0, 1.0], [True, True])
     X = m.verts
     x, y = X[:, 0], X[:, 1]
@@ -39,8 +40,13 @@ def main(case: str, ne: int = 64, reps: int = 3) -> None:
     phi.vals, v.vals = phi0, vel
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(reps)]
-    if case == "sl":
-        adv = S.Advector(phi, v)
+    if case in ("sl", "sl2"):
+        if case == "sl":
+            adv = S.Advector(phi, v)
+        else:  # second order: previous level = the same fields, shifted / scaled
+            phim, vm = S.Field("phim", m, 1, bc), S.Field("vm", m, 2, None)
+            phim.vals, vm.vals = np.roll(phi0, 1), 0.98 * vel
+            adv = S.Advector(phi, v, phim, vm)
         dt = S.CalcTimeStep(v, 2.0)
         for a, b in ev:
             a.record()
@@ -74,4 +80,5 @@ def main(case: str, ne: int = 64, reps: int = 3) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "apply", int(sys.argv[2]) if len(sys.argv) > 2 else 64)
+    main(sys.argv[1] if len(sys.argv) > 1 else "apply", int(sys.argv[2]) if len(sys.argv) > 2 else 64,
+         int(sys.argv[3]) if len(sys.argv) > 3 else 8)
