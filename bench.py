@@ -478,8 +478,8 @@ def apply_kernel_name(p, name):
     """The kernel the library's apply dispatches to for order p."""
     if name != "fp64":
         return f"apply_tile_kernel<{p}, bf16 -> float>"
-    if p == 8:
-        return "apply_ef8_kernel (element-factored FP64 FMA, cp.async staging)"
+    if p in (4, 6, 8):
+        return f"apply_ef_kernel<{p}> (element-factored FP64 FMA, cp.async staging)"
     return f"apply_mma_kernel<{p}> (FP64 DMMA element products, TMA-staged tiles)"
 
 
@@ -1033,7 +1033,7 @@ def main():
         extras["config2"] = run_config2()
         log("apply roofline")
         extras["apply_roofline"] = run_apply_roofline()
-        # the other orders of the ensemble and serving meshes, at the same
+        # orders 4 and 6 of the ensemble and serving meshes, at the same
         # 37.7M unknowns (6144 x 6144)
         extras["apply_roofline_p4_p6"] = {
             f"p{p}": run_apply_roofline(ne=6144 // p, p=p, precisions=("fp64",))

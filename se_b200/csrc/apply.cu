@@ -25,9 +25,10 @@
 //
 // Instantiated for FP64 (x, arithmetic and y in FP64) and for the reduced-
 // precision apply (x in BF16 or FP16, operator and arithmetic in FP32, y in
-// FP32). In FP64, order 8 runs the element-factored kernel on the FP64 FMA
-// pipes (apply_ef8_kernel, at the end of this file) and the other orders the
-// same element products on the FP64 tensor cores (apply_mma_kernel).
+// FP32). In FP64, orders 4, 6 and 8 run the element-factored kernel on the
+// FP64 FMA pipes (apply_ef_kernel, at the end of this file) and the other
+// orders the same element products on the FP64 tensor cores
+// (apply_mma_kernel).
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -595,58 +596,72 @@ cudaError_t launch_mma(const OpDev& od, const double* x, double* y, unsigned* er
   return cudaGetLastError();
 }
 
-// ------------------------------------------------ order 8, CUDA cores ----
-// Element-factored FP64 apply for N = 8 on the FP64 FMA pipes. A block
-// stages a 64 x 32 vertex tile and an 8-vertex halo to the left and below
-// (zero where a vertex is no unknown), then
-//   x pass: thread (element e, row r) reads the 17 values of its element row
-//           and of the left element's row and forms the 8 outputs of its
-//           element's nodes a = 0..7 with the 9 x 9 stiffness block and, at
-//           a = 0, the left element's last row: 81 FMAs, all coefficients
+// ------------------------------------------- orders 4, 6, 8, CUDA cores ----
+// Element-factored FP64 apply on the FP64 FMA pipes for N = 4, 6, 8. A block
+// of 256 threads stages a TX x TY vertex tile (TX = N * (64 / N): 64, 60, 64;
+// TY a multiple of N) and an N-vertex halo to the left and below (zero where
+// a vertex is no unknown), then
+//   x pass: thread (element e, row r) reads the 2N+1 values of its element
+//           row and of the left element's row and forms the N outputs of its
+//           element's nodes a = 0..N-1 with the (N+1) x (N+1) stiffness block
+//           and, at a = 0, the left element's last row: all coefficients
 //           compile-time offsets into the kernel's parameters;
 //   y pass: thread (element e, column c) does the same along the column and
 //           combines alpha wx wy x + beta_x wy (Kx x) + beta_y wx (Ky x).
-// About 21 FMAs and 3 shared-memory loads per unknown, no padding work, and
-// the staging costs a few instructions per value (each lane maps its staged
-// columns once; a staged row's unknown index is the same for the whole warp):
-// the FP64 pipes out-run HBM, so the kernel is bound by its 16 bytes per
-// unknown.
-constexpr int kEfTX = 64, kEfW = kEfTX + 9, kEfOX = kEfTX + 1;
+// About 2.6 N FMAs and 3 shared-memory loads per unknown, no padding work,
+// and the staging costs a few instructions per value (each lane maps its
+// staged columns once; a staged row's unknown index is the same for the
+// whole warp). The staged row pitch TX + N + 1 and the x-pass output pitch
+// TX + 1 are odd, so a warp's column-wise reads are conflict-free.
+template <int N>
+struct EfTile {
+  static constexpr int EX = 64 / N;      // elements per tile row
+  static constexpr int TX = EX * N;      // output vertices per tile row
+  static constexpr int W = TX + N + 1;   // staged row pitch (odd)
+  static constexpr int OXP = TX + 1;     // x-pass output pitch (odd)
+  static constexpr int TY = N == 8 ? 32 : (N == 6 ? 24 : 16);  // output rows per tile
+  static constexpr int H = TY + N + 1;   // staged rows
+  static constexpr int ITEMS = EX * TY;  // x-pass (= y-pass) items, one per thread
+  static constexpr int MINB = N == 8 ? 4 : (N == 6 ? 5 : 6);  // blocks per SM
+  static_assert(ITEMS <= 256 && TX * (TY / N) == ITEMS && TY % N == 0, "tile shape");
+  static_assert(W <= 96 && (W & 1) && (OXP & 1), "staging columns and pitches");
+};
+constexpr int kEfThreads = 256, kEfWarps = kEfThreads / 32;
 
-template <int TY, int MINB>
-__global__ void __launch_bounds__(8 * TY, MINB) apply_ef8_kernel(const OpDev op,
-                                                                  const double* __restrict__ x,
-                                                                  double* __restrict__ y) {
-  constexpr int N = 8, kEfTY = TY, kEfH = TY + 9, kWarps = TY / 4;
+template <int N>
+__global__ void __launch_bounds__(kEfThreads, EfTile<N>::MINB)
+    apply_ef_kernel(const OpDev op, const double* __restrict__ x, double* __restrict__ y) {
+  typedef EfTile<N> T;
+  constexpr int W = T::W, OXP = T::OXP, TX = T::TX, TY = T::TY, H = T::H;
   extern __shared__ __align__(16) double efsm[];
-  double* X = efsm;                   // vertices (gx0-8 .. gx0+64) x (gy0-8 .. gy0+TY)
-  double* OX = X + kEfH * kEfW;       // x-pass results of the tile's vertices
-  double* sw = OX + kEfTY * kEfOX;
+  double* X = efsm;            // vertices (gx0-N .. gx0+TX) x (gy0-N .. gy0+TY)
+  double* OX = X + H * W;      // x-pass results of the tile's vertices
+  double* sw = OX + TY * OXP;
   const Dir& dx = op.d[0];
   const Dir& dy = op.d[1];
-  const int gx0 = blockIdx.x * kEfTX, gy0 = blockIdx.y * kEfTY;
+  const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid <= N) sw[tid] = op.w[tid];
-  {  // staging: warp w takes rows w, w + kWarps, ...; lane l columns l, l + 32, l + 64
+  {  // staging: warp w takes rows w, w + 8, ...; lane l columns l, l + 32, l + 64
     int cu[3];
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       const int i = lane + 32 * q;
-      cu[q] = i < kEfW ? unk(dx, gx0 - N + i) : -1;
+      cu[q] = i < W ? unk(dx, gx0 - N + i) : -1;
     }
 #pragma unroll
-    for (int r = 0; r < (kEfH + kWarps - 1) / kWarps; r++) {
-      const int j = warp + kWarps * r;
-      if (j < kEfH) {
+    for (int r = 0; r < (H + kEfWarps - 1) / kEfWarps; r++) {
+      const int j = warp + kEfWarps * r;
+      if (j < H) {
         const int uy = unk(dy, gy0 - N + j);
         const double* rowp = x + (size_t)(uy < 0 ? 0 : uy) * op.G[0];
 #pragma unroll
         for (int q = 0; q < 3; q++) {
           const int i = lane + 32 * q;
-          if (i < kEfW) {
+          if (i < W) {
             const bool ok = uy >= 0 && cu[q] >= 0;
             const double* src = ok ? rowp + cu[q] : x;
-            const unsigned dst = (unsigned)__cvta_generic_to_shared(X + j * kEfW + i);
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(X + j * W + i);
             asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src),
                          "r"(ok ? 8 : 0));
           }
@@ -657,11 +672,11 @@ __global__ void __launch_bounds__(8 * TY, MINB) apply_ef8_kernel(const OpDev op,
     asm volatile("cp.async.wait_group 0;\n" ::);
   }
   __syncthreads();
-  {  // x pass: warp = one element, 32 rows (row stride 73: conflict-free)
-    constexpr int n = N + 1;
-    const int r = lane + 32 * (warp >> 3), e = warp & 7;
-    const int ex = (gx0 >> 3) + e;
-    const double* row = X + (r + N) * kEfW + e * N;  // left element's first node
+  constexpr int n = N + 1;
+  if (tid < T::ITEMS) {  // x pass: thread = (element e, row r), rows of one element per warp run
+    const int r = tid % TY, e = tid / TY;
+    const int ex = gx0 / N + e;
+    const double* row = X + (r + N) * W + e * N;  // left element's first node
     double v[2 * N + 1];
 #pragma unroll
     for (int k = 0; k <= 2 * N; k++) v[k] = row[k];
@@ -683,18 +698,17 @@ __global__ void __launch_bounds__(8 * TY, MINB) apply_ef8_kernel(const OpDev op,
       o[0] += t;
     }
 #pragma unroll
-    for (int a = 0; a < N; a++) OX[r * kEfOX + e * N + a] = o[a];
+    for (int a = 0; a < N; a++) OX[r * OXP + e * N + a] = o[a];
   }
   __syncthreads();
-  {  // y pass: warp = 32 consecutive columns of one element row
-    constexpr int n = N + 1;
-    const int c = tid & 63, e = tid >> 6;
-    const int ey = (gy0 >> 3) + e;
+  if (tid < T::ITEMS) {  // y pass: thread = (element row e, column c), consecutive columns per warp
+    const int c = tid % TX, e = tid / TX;
+    const int ey = gy0 / N + e;
     const int gx = gx0 + c;
-    const double* col = X + (e * N) * kEfW + c + N;  // lower element's first node
+    const double* col = X + (e * N) * W + c + N;  // lower element's first node
     double v[2 * N + 1];
 #pragma unroll
-    for (int k = 0; k <= 2 * N; k++) v[k] = col[k * kEfW];
+    for (int k = 0; k <= 2 * N; k++) v[k] = col[k * W];
     const bool own = ey < dy.nE, left = ey > 0 || dy.periodic;
     double o[N];
 #pragma unroll
@@ -713,27 +727,27 @@ __global__ void __launch_bounds__(8 * TY, MINB) apply_ef8_kernel(const OpDev op,
       o[0] += t;
     }
     if (gx >= dx.lo && gx < dx.hi) {
-      const double wx = wsum<N>(dx, sw, gx >> 3, gx & 7);
+      const double wx = wsum<N>(dx, sw, gx / N, gx % N);
       const double axw = op.alpha * wx, bxw = op.beta[1] * wx;
       const double w0 = (own ? op.w[0] : 0.0) + (left ? op.w[N] : 0.0);
       const int gyb = gy0 + e * N;
       const size_t ld = (size_t)op.G[0];
       double* yp = y + (ptrdiff_t)(gyb - dy.lo) * op.G[0] + (gx - dx.lo);
-      const double* oxp = OX + (e * N) * kEfOX + c;
+      const double* oxp = OX + (e * N) * OXP + c;
       // y = wy (alpha wx x + beta_x (Kx x)) + beta_y wx (Ky x), wy the
       // assembled weight of the row (compile-time parameter offsets)
       if (gyb >= dy.lo && gyb + N <= dy.hi) {  // the whole strip is unknowns
 #pragma unroll
         for (int a = 0; a < N; a++) {
           const double wy = a == 0 ? w0 : op.w[a];
-          yp[a * ld] = fma(wy, fma(axw, v[N + a], op.beta[0] * oxp[a * kEfOX]), bxw * o[a]);
+          yp[a * ld] = fma(wy, fma(axw, v[N + a], op.beta[0] * oxp[a * OXP]), bxw * o[a]);
         }
       } else {
 #pragma unroll
         for (int a = 0; a < N; a++) {
           const int gy = gyb + a;
           const double wy = a == 0 ? w0 : op.w[a];
-          const double r = fma(wy, fma(axw, v[N + a], op.beta[0] * oxp[a * kEfOX]), bxw * o[a]);
+          const double r = fma(wy, fma(axw, v[N + a], op.beta[0] * oxp[a * OXP]), bxw * o[a]);
           if (gy >= dy.lo && gy < dy.hi) yp[(ptrdiff_t)a * op.G[0]] = r;
         }
       }
@@ -741,9 +755,10 @@ __global__ void __launch_bounds__(8 * TY, MINB) apply_ef8_kernel(const OpDev op,
   }
 }
 
-template <int TY = 32, int MINB = 3>
-cudaError_t launch_ef8(const OpDev& op, const double* x, double* y, cudaStream_t s) {
-  constexpr size_t smem = sizeof(double) * ((size_t)(TY + 9) * kEfW + (size_t)TY * kEfOX + 16);
+template <int N>
+cudaError_t launch_ef(const OpDev& op, const double* x, double* y, cudaStream_t s) {
+  typedef EfTile<N> T;
+  constexpr size_t smem = sizeof(double) * ((size_t)T::H * T::W + (size_t)T::TY * T::OXP + 16);
   if (smem > 48 * 1024) {
     static bool attr[64] = {};
     int dev = 0;
@@ -751,14 +766,14 @@ cudaError_t launch_ef8(const OpDev& op, const double* x, double* y, cudaStream_t
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
     if (!attr[dev]) {
-      e = cudaFuncSetAttribute(apply_ef8_kernel<TY, MINB>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      e = cudaFuncSetAttribute(apply_ef_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem);
       if (e != cudaSuccess) return e;
       attr[dev] = true;
     }
   }
-  const dim3 grid((op.d[0].hi + kEfTX - 1) / kEfTX, (op.d[1].hi + TY - 1) / TY);
-  apply_ef8_kernel<TY, MINB><<<grid, 8 * TY, smem, s>>>(op, x, y);
+  const dim3 grid((op.d[0].hi + T::TX - 1) / T::TX, (op.d[1].hi + T::TY - 1) / T::TY);
+  apply_ef_kernel<N><<<grid, kEfThreads, smem, s>>>(op, x, y);
   return cudaGetLastError();
 }
 
@@ -773,10 +788,14 @@ cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, unsigne
   // per-unknown form, which carries it
   if (op.gamma != 0.0) return launch_residual(op, x, nullptr, y, nullptr, 0, nullptr, s);
   switch (op.d[0].N) {
-    SE_APPLY_N(2) SE_APPLY_N(3) SE_APPLY_N(4) SE_APPLY_N(5) SE_APPLY_N(6) SE_APPLY_N(7)
-    SE_APPLY_N(9) SE_APPLY_N(10) SE_APPLY_N(11) SE_APPLY_N(12)
+    SE_APPLY_N(2) SE_APPLY_N(3) SE_APPLY_N(5) SE_APPLY_N(7) SE_APPLY_N(9) SE_APPLY_N(10)
+    SE_APPLY_N(11) SE_APPLY_N(12)
+    case 4:
+      return launch_ef<4>(op, x, y, s);
+    case 6:
+      return launch_ef<6>(op, x, y, s);
     case 8:
-      return launch_ef8<32, 4>(op, x, y, s);
+      return launch_ef<8>(op, x, y, s);
     default:
       return cudaErrorInvalidValue;
   }

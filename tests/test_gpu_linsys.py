@@ -39,6 +39,17 @@ CASES8 = [
     (20, 17, 8, (0.0, 0.0), (1.0, 1.0), (True, False), (True, True, False, False)),
 ]
 
+# Order-4 and order-6 meshes of several element-factored tiles (64 x 16 and
+# 60 x 24 vertices) with partial tiles at the far ends: doubly periodic, a
+# channel, Dirichlet top and left, natural ends everywhere.
+CASES46 = [
+    (37, 9, 4, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False)),
+    (35, 10, 4, (0.0, 0.0), (2.0, 1.0), (False, False), (False, True, True, False)),
+    (23, 11, 6, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False)),
+    (21, 9, 6, (0.0, 0.0), (1.0, 1.0), (True, False), (True, True, False, False)),
+    (22, 7, 6, (-1.0, 0.0), (1.0, 1.0), (False, False), (False, False, False, False)),
+]
+
 
 def build(S, O, case, c, nu, dt, quirk, poisson=False, seed=0):
     nx, ny, N, lo, hi, per, bc = case
@@ -85,10 +96,14 @@ def test_apply_matches_assembled_operator(segpu, oracle, case, quirk):
     assert np.abs(d.cpu().numpy() - diag).max() <= 2e-11 * np.abs(diag).max()
 
 
-@pytest.mark.parametrize("case", range(len(CASES8)))
-def test_apply_order8_tiles(segpu, oracle, case):
-    om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, CASES8[case], -2.0, -1.0, 0.5,
-                                                     False)
+@pytest.mark.parametrize("case", [("o8", k) for k in range(len(CASES8))]
+                         + [("o46", k) for k in range(len(CASES46))])
+def test_apply_factored_tiles(segpu, oracle, case):
+    """The element-factored FP64 apply (orders 4, 6, 8) over meshes of several
+    tiles, against the oracle's assembled CSR operator."""
+    spec = (CASES8 if case[0] == "o8" else CASES46)[case[1]]
+    case = case[1] + (0 if case[0] == "o8" else 10)
+    om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, spec, -2.0, -1.0, 0.5, False)
     n = ls.vecSize
     x = np.random.default_rng(100 + case).standard_normal(n)
     ref = A.matvec(x)
