@@ -478,7 +478,7 @@ def apply_kernel_name(p, name):
     """The kernel the library's apply dispatches to for order p."""
     if name != "fp64":
         return f"apply_tile_kernel<{p}, bf16 -> float>"
-    if p in (4, 6, 8):
+    if 4 <= p <= 8:
         return f"apply_ef_kernel<{p}> (element-factored FP64 FMA, cp.async staging)"
     return f"apply_mma_kernel<{p}> (FP64 DMMA element products, TMA-staged tiles)"
 
@@ -1033,11 +1033,11 @@ def main():
         extras["config2"] = run_config2()
         log("apply roofline")
         extras["apply_roofline"] = run_apply_roofline()
-        # orders 4 and 6 of the ensemble and serving meshes, at the same
-        # 37.7M unknowns (6144 x 6144)
-        extras["apply_roofline_p4_p6"] = {
+        # orders 4 to 7 of the ensemble and serving meshes, at about the
+        # same 37.7M unknowns ((6144 // p) * p squared)
+        extras["apply_roofline_p4_p7"] = {
             f"p{p}": run_apply_roofline(ne=6144 // p, p=p, precisions=("fp64",))
-            for p in (4, 6)}
+            for p in (4, 5, 6, 7)}
         log("second-order SL")
         extras["sl_second_order"] = run_sl_second()
         log("ensemble")

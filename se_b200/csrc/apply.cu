@@ -25,7 +25,7 @@
 //
 // Instantiated for FP64 (x, arithmetic and y in FP64) and for the reduced-
 // precision apply (x in BF16 or FP16, operator and arithmetic in FP32, y in
-// FP32). In FP64, orders 4, 6 and 8 run the element-factored kernel on the
+// FP32). In FP64, orders 4 to 8 run the element-factored kernel on the
 // FP64 FMA pipes (apply_ef_kernel, at the end of this file) and the other
 // orders the same element products on the FP64 tensor cores
 // (apply_mma_kernel).
@@ -596,11 +596,11 @@ cudaError_t launch_mma(const OpDev& od, const double* x, double* y, unsigned* er
   return cudaGetLastError();
 }
 
-// ------------------------------------------- orders 4, 6, 8, CUDA cores ----
-// Element-factored FP64 apply on the FP64 FMA pipes for N = 4, 6, 8. A block
-// of 256 threads stages a TX x TY vertex tile (TX = N * (64 / N): 64, 60, 64;
-// TY a multiple of N) and an N-vertex halo to the left and below (zero where
-// a vertex is no unknown), then
+// ---------------------------------------- orders 4 to 8, CUDA cores ----
+// Element-factored FP64 apply on the FP64 FMA pipes for N = 4..8. A block of
+// 256 threads stages a TX x TY vertex tile (TX = N * (64 / N): 64, 60, 60,
+// 63, 64; TY a multiple of N) and an N-vertex halo to the left and below
+// (zero where a vertex is no unknown), then
 //   x pass: thread (element e, row r) reads the 2N+1 values of its element
 //           row and of the left element's row and forms the N outputs of its
 //           element's nodes a = 0..N-1 with the (N+1) x (N+1) stiffness block
@@ -611,20 +611,23 @@ cudaError_t launch_mma(const OpDev& od, const double* x, double* y, unsigned* er
 // About 2.6 N FMAs and 3 shared-memory loads per unknown, no padding work,
 // and the staging costs a few instructions per value (each lane maps its
 // staged columns once; a staged row's unknown index is the same for the
-// whole warp). The staged row pitch TX + N + 1 and the x-pass output pitch
-// TX + 1 are odd, so a warp's column-wise reads are conflict-free.
+// whole warp). The staged row pitch (TX + N + 1, or one more) and the x-pass
+// output pitch (TX + 1, or one more) are odd, so a warp's column-wise reads
+// are conflict-free.
 template <int N>
 struct EfTile {
   static constexpr int EX = 64 / N;      // elements per tile row
   static constexpr int TX = EX * N;      // output vertices per tile row
-  static constexpr int W = TX + N + 1;   // staged row pitch (odd)
-  static constexpr int OXP = TX + 1;     // x-pass output pitch (odd)
-  static constexpr int TY = N == 8 ? 32 : (N == 6 ? 24 : 16);  // output rows per tile
+  static constexpr int SW = TX + N + 1;  // staged vertices per row
+  static constexpr int W = SW | 1;       // staged row pitch (odd)
+  static constexpr int OXP = (TX + 1) | 1;  // x-pass output pitch (odd)
+  // output rows per tile: 32, 28, 24, 20, 16 for N = 8, 7, 6, 5, 4
+  static constexpr int TY = N == 8 ? 32 : 4 * N;
   static constexpr int H = TY + N + 1;   // staged rows
   static constexpr int ITEMS = EX * TY;  // x-pass (= y-pass) items, one per thread
-  static constexpr int MINB = N == 8 ? 4 : (N == 6 ? 5 : 6);  // blocks per SM
+  static constexpr int MINB = N >= 7 ? 4 : (N == 6 ? 5 : 6);  // blocks per SM
   static_assert(ITEMS <= 256 && TX * (TY / N) == ITEMS && TY % N == 0, "tile shape");
-  static_assert(W <= 96 && (W & 1) && (OXP & 1), "staging columns and pitches");
+  static_assert(SW <= 96, "staging columns");
 };
 constexpr int kEfThreads = 256, kEfWarps = kEfThreads / 32;
 
@@ -632,7 +635,7 @@ template <int N>
 __global__ void __launch_bounds__(kEfThreads, EfTile<N>::MINB)
     apply_ef_kernel(const OpDev op, const double* __restrict__ x, double* __restrict__ y) {
   typedef EfTile<N> T;
-  constexpr int W = T::W, OXP = T::OXP, TX = T::TX, TY = T::TY, H = T::H;
+  constexpr int SW = T::SW, W = T::W, OXP = T::OXP, TX = T::TX, TY = T::TY, H = T::H;
   extern __shared__ __align__(16) double efsm[];
   double* X = efsm;            // vertices (gx0-N .. gx0+TX) x (gy0-N .. gy0+TY)
   double* OX = X + H * W;      // x-pass results of the tile's vertices
@@ -647,7 +650,7 @@ __global__ void __launch_bounds__(kEfThreads, EfTile<N>::MINB)
 #pragma unroll
     for (int q = 0; q < 3; q++) {
       const int i = lane + 32 * q;
-      cu[q] = i < W ? unk(dx, gx0 - N + i) : -1;
+      cu[q] = i < SW ? unk(dx, gx0 - N + i) : -1;
     }
 #pragma unroll
     for (int r = 0; r < (H + kEfWarps - 1) / kEfWarps; r++) {
@@ -658,7 +661,7 @@ __global__ void __launch_bounds__(kEfThreads, EfTile<N>::MINB)
 #pragma unroll
         for (int q = 0; q < 3; q++) {
           const int i = lane + 32 * q;
-          if (i < W) {
+          if (i < SW) {
             const bool ok = uy >= 0 && cu[q] >= 0;
             const double* src = ok ? rowp + cu[q] : x;
             const unsigned dst = (unsigned)__cvta_generic_to_shared(X + j * W + i);
@@ -788,12 +791,15 @@ cudaError_t launch_op_apply(const OpDev& op, const double* x, double* y, unsigne
   // per-unknown form, which carries it
   if (op.gamma != 0.0) return launch_residual(op, x, nullptr, y, nullptr, 0, nullptr, s);
   switch (op.d[0].N) {
-    SE_APPLY_N(2) SE_APPLY_N(3) SE_APPLY_N(5) SE_APPLY_N(7) SE_APPLY_N(9) SE_APPLY_N(10)
-    SE_APPLY_N(11) SE_APPLY_N(12)
+    SE_APPLY_N(2) SE_APPLY_N(3) SE_APPLY_N(9) SE_APPLY_N(10) SE_APPLY_N(11) SE_APPLY_N(12)
     case 4:
       return launch_ef<4>(op, x, y, s);
+    case 5:
+      return launch_ef<5>(op, x, y, s);
     case 6:
       return launch_ef<6>(op, x, y, s);
+    case 7:
+      return launch_ef<7>(op, x, y, s);
     case 8:
       return launch_ef<8>(op, x, y, s);
     default:

@@ -39,15 +39,19 @@ CASES8 = [
     (20, 17, 8, (0.0, 0.0), (1.0, 1.0), (True, False), (True, True, False, False)),
 ]
 
-# Order-4 and order-6 meshes of several element-factored tiles (64 x 16 and
-# 60 x 24 vertices) with partial tiles at the far ends: doubly periodic, a
-# channel, Dirichlet top and left, natural ends everywhere.
-CASES46 = [
+# Order-4 to order-7 meshes of several element-factored tiles (64 x 16,
+# 60 x 20, 60 x 24 and 63 x 28 vertices) with partial tiles at the far ends:
+# doubly periodic, channels, Dirichlet ends, natural ends everywhere.
+CASES_EF = [
     (37, 9, 4, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False)),
     (35, 10, 4, (0.0, 0.0), (2.0, 1.0), (False, False), (False, True, True, False)),
     (23, 11, 6, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False)),
     (21, 9, 6, (0.0, 0.0), (1.0, 1.0), (True, False), (True, True, False, False)),
     (22, 7, 6, (-1.0, 0.0), (1.0, 1.0), (False, False), (False, False, False, False)),
+    (27, 9, 5, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False)),
+    (25, 10, 5, (0.0, 0.0), (1.0, 1.0), (False, False), (True, False, False, True)),
+    (20, 9, 7, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False)),
+    (19, 8, 7, (0.0, 0.0), (2.0, 1.0), (True, False), (True, True, False, False)),
 ]
 
 
@@ -97,11 +101,11 @@ def test_apply_matches_assembled_operator(segpu, oracle, case, quirk):
 
 
 @pytest.mark.parametrize("case", [("o8", k) for k in range(len(CASES8))]
-                         + [("o46", k) for k in range(len(CASES46))])
+                         + [("ef", k) for k in range(len(CASES_EF))])
 def test_apply_factored_tiles(segpu, oracle, case):
-    """The element-factored FP64 apply (orders 4, 6, 8) over meshes of several
+    """The element-factored FP64 apply (orders 4 to 8) over meshes of several
     tiles, against the oracle's assembled CSR operator."""
-    spec = (CASES8 if case[0] == "o8" else CASES46)[case[1]]
+    spec = (CASES8 if case[0] == "o8" else CASES_EF)[case[1]]
     case = case[1] + (0 if case[0] == "o8" else 10)
     om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, spec, -2.0, -1.0, 0.5, False)
     n = ls.vecSize
