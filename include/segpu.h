@@ -163,7 +163,7 @@ int se_field_gen_vel(const se_field* psi, se_field* vel);
  * Replaces Advector(field, velocity) (first order) and
  * Advector(field, velocity, fieldMinusOne, velMinusOne) (second order),
  * Advect(dt) and the public fieldSL (src/base/Advector.h:3-15,
- * src/base/Advector.cpp:54-274). velocity fields have ndofs = 2 and share the
+ * src/base/Advector.cpp:51-246). velocity fields have ndofs = 2 and share the
  * field's mesh. N >= 3 (the reference's bicubic path for N < 3 is not built).
  * The advector keeps pointers to the fields; they must outlive it. */
 int se_advector_create(se_field* field, se_field* velocity, se_field* field_prev,
@@ -283,7 +283,11 @@ int se_linsys_solve_batch(se_linsys** systems, int n, int remove_null_space,
  * fills stats (nullable) and returns what se_linsys_solve would have. */
 int se_linsys_solve_async(se_linsys* ls, int remove_null_space);
 int se_linsys_solve_finish(se_linsys* ls, se_solve_stats* stats);
-/* y = A x on vector unknowns (device pointers, vec_size entries each). */
+/* y = A x on vector unknowns (device pointers, vec_size entries each), on
+ * the calling thread's stream. Orders 4 to 8 return once the apply is
+ * queued; orders 2, 3 and 9 to 12 (a TMA-staged kernel with bounded waits)
+ * return after it has finished, with SE_ERR_TIMEOUT if a stage never
+ * arrived. */
 int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev);
 /* No counterpart in the reference: x = A^{-1} r by the fast-diagonalization
  * transforms in FP64 (four tensor-core products; exact up to rounding, the
@@ -309,12 +313,17 @@ int se_linsys_vec_size(const se_linsys* ls, int* n);
  * (bcs = {bottom, top, left, right}); rhs_dev (nullable) and sol_dev are
  * caller-owned device arrays of nVertsTotal doubles in the reference's vertex
  * order; sol_dev holds the Dirichlet values on entry and the solution on
- * return. poisson != 0 selects A = c*Laplacian (nu, dt ignored).
+ * return. poisson != 0 selects A = c*Laplacian (nu, dt ignored). It runs
+ * the drop-in solver only (Jacobi CG in FP64, PETSc KSPCG semantics): options
+ * are checked as se_helmholtz_create checks them, and method != SE_METHOD_CG
+ * or precision != SE_PREC_FP64 returns SE_ERR_UNSUPPORTED.
  * Limit: at most 65536 vector unknowns (e.g. 32x32 elements at N = 8);
  * larger systems return SE_ERR_UNSUPPORTED. All temporaries live in one
  * static device array of about 5 MB that every GPU loading the library
- * holds until exit; every call shares it, so calls whose device work
- * overlaps race and must be serialised by the caller. The first call on a
+ * holds until exit; every call shares it and leaves its contents behind.
+ * Two calls whose device work overlapped would race on it, so the library
+ * serialises them: each call holds a process-wide lock until its device work
+ * has finished (it returns after a stream synchronize). The first call on a
  * device looks the array up (cudaGetSymbolAddress) and should come before
  * any stream capture. */
 int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double min[2],

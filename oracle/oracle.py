@@ -24,7 +24,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libseoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libseref.so")
-REF_SRC = "/root/reference"
+# the reference checkout (its src/base is compiled into _ref/ when given)
+REF_SRC = os.environ.get("SE_REFERENCE_SRC", "")
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I = ctypes.POINTER(ctypes.c_int)
@@ -37,7 +38,7 @@ def build(with_ref: bool | None = None) -> None:
     """Compile the restatement, and the reference library when its sources exist."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     if with_ref is None:
-        with_ref = os.path.isdir(os.path.join(REF_SRC, "src", "base"))
+        with_ref = bool(REF_SRC) and os.path.isdir(os.path.join(REF_SRC, "src", "base"))
     if with_ref:
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True)
 
@@ -417,8 +418,9 @@ class QG2:
     order. TEST INFRASTRUCTURE ONLY."""
 
     def __init__(self, mesh: Mesh, bcs, psi1, omega1, psi2, omega2, F1, F2, beta, E2, r, nu,
-                 tau_e, dt, quirk=False, rtol=1e-12):
+                 tau_e, dt, quirk=False, rtol=1e-12, nthreads=1):
         self.m, self.bcs, self.quirk, self.rtol = mesh, tuple(bcs), quirk, rtol
+        self.nthreads = nthreads
         self.F1, self.F2, self.beta, self.E2, self.r, self.nu, self.dt = F1, F2, beta, E2, r, nu, dt
         self.psi1, self.omega1 = _f64(psi1).copy(), _f64(omega1).copy()
         self.psi2, self.omega2 = _f64(psi2).copy(), _f64(omega2).copy()
@@ -442,11 +444,11 @@ class QG2:
 
     def helm(self, sol, rhs):
         return helmholtz_solve(self.m, sol, rhs, -(self.F1 + self.F2), -1.0, 1.0, self.bcs,
-                               quirk=self.quirk, rtol=self.rtol)[0]
+                               quirk=self.quirk, rtol=self.rtol, nthreads=self.nthreads)[0]
 
     def fish(self, sol, rhs):
         return helmholtz_solve(self.m, sol, rhs, -1.0, 0.0, 0.0, self.bcs, quirk=self.quirk,
-                               rtol=self.rtol, poisson=True)[0]
+                               rtol=self.rtol, poisson=True, nthreads=self.nthreads)[0]
 
     def solve_q(self, alpha_hat, om_hat, rF, Ei, alpha):
         ng = len(self.v2f)
@@ -475,8 +477,8 @@ class QG2:
             vel1, vel2 = self.gen_vel(self.psi1), self.gen_vel(self.psi2)
             self.alpha1 = self.gen_pv(self.omega1, self.psi1, self.psi2, self.F1)
             self.alpha2 = self.gen_pv(self.omega2, self.psi2, self.psi1, self.F2)
-            a1h = m.advect(self.alpha1, vel1, dt)
-            a2h = m.advect(self.alpha2, vel2, dt)
+            a1h = m.advect(self.alpha1, vel1, dt, nthreads=self.nthreads)
+            a2h = m.advect(self.alpha2, vel2, dt, nthreads=self.nthreads)
             self.tau1, self.chi1, _, _, o1h, _ = self.invert(a1h, a2h, self.tau1, self.chi1,
                                                              2.0 * b, b)
             self.alpha1 = self.solve_q(a1h, o1h, self.r * self.F1, 0.0, self.alpha1)
@@ -494,8 +496,8 @@ class QG2:
         self.alpha2 = self.gen_pv(self.omega2, self.psi2, self.psi1, self.F2)
         a1p = self.gen_pv(o1p, p1p, p2p, self.F1)
         a2p = self.gen_pv(o2p, p2p, p1p, self.F2)
-        a1h = m.advect(self.alpha1, vel1, dt, a1p, vel1p)
-        a2h = m.advect(self.alpha2, vel2, dt, a2p, vel2p)
+        a1h = m.advect(self.alpha1, vel1, dt, a1p, vel1p, nthreads=self.nthreads)
+        a2h = m.advect(self.alpha2, vel2, dt, a2p, vel2p, nthreads=self.nthreads)
         self.tau1, self.chi1, _, _, o1h, o2h = self.invert(a1h, a2h, self.tau1, self.chi1,
                                                            a * 2.0 * b, a * b)
         self.alpha1 = self.solve_q(a1h, o1h, self.r * self.F1, 0.0, self.alpha1)

@@ -366,14 +366,14 @@ void or_interp_global(const or_mesh* m, int ndofs, const double* vals,
 }
 
 /* ------------------------------------------------------------- Advector -- */
-/* src/base/Advector.cpp:150-162: one periodic wrap, or a clamp at walls. */
+/* src/base/Advector.cpp:122-134: one periodic wrap, or a clamp at walls. */
 static void sl_periodic_update(const or_mesh* m, double* c) {
   for (int d = 0; d < 2; d++) {
     if (c[d] < m->min[d]) c[d] = m->periodic[d] ? m->max[d] - m->min[d] + c[d] : m->min[d];
     if (c[d] > m->max[d]) c[d] = m->periodic[d] ? m->min[d] - m->max[d] + c[d] : m->max[d];
   }
 }
-/* src/base/Advector.cpp:164-176: midpoint RK2 backward trajectory; the first
+/* src/base/Advector.cpp:136-148: midpoint RK2 backward trajectory; the first
  * stage always uses the current velocity. */
 static void integrate_rk2(const or_mesh* m, double dt, const double* vel,
                           const double* velField, const double* origin, double* coord) {
@@ -402,7 +402,7 @@ void or_periodic_update(const or_mesh* m, int ndofs, double* vals) {
     for (int d = 0; d < ndofs; d++) vals[(size_t)(nx * ny - 1) * ndofs + d] = vals[d];
 }
 
-/* src/base/Advector.cpp:367-377 */
+/* src/base/Advector.cpp:339-349 */
 static void extrapolate(int nv, const double* v, const double* vm, double* p1,
                         double* ph, double* mh) {
   for (int k = 0; k < 2 * nv; k++) {
@@ -411,7 +411,7 @@ static void extrapolate(int nv, const double* v, const double* vm, double* p1,
     mh[k] = 0.5 * v[k] + 0.5 * vm[k];
   }
 }
-/* src/base/Advector.cpp:231-256: second-order two-step trajectory. */
+/* src/base/Advector.cpp:203-228: second-order two-step trajectory. */
 static void trajectory2(const or_mesh* m, double dt, const double* vel,
                         const double* p1, const double* ph, const double* mh,
                         const double* origin, double* x1, double* x2) {
@@ -467,7 +467,7 @@ static void advect_range(void* vctx, long b, long e, int t) {
   }
 }
 
-/* src/base/Advector.cpp:209-274 (FirstOrder / SecondOrder): every vertex,
+/* src/base/Advector.cpp:181-246 (FirstOrder / SecondOrder): every vertex,
  * periodic duplicates included, then Field::PeriodicUpdate. */
 int or_advect(const or_mesh* m, int ndofs, const double* field, const double* vel,
               const double* field_prev, const double* vel_prev, double dt,

@@ -1813,7 +1813,7 @@ int se_advector_create(se_field* field, se_field* velocity, se_field* field_prev
     delete a;
     return rc;
   }
-  // fieldSL starts as a copy of the field (src/base/Advector.cpp:64-65)
+  // fieldSL starts as a copy of the field (src/base/Advector.cpp:63-64)
   if ((rc = se_field_copy(a->sl, field))) {
     se_field_destroy(a->sl);
     dfree(a->err);
@@ -2200,7 +2200,19 @@ int se_linsys_solve_finish(se_linsys* ls, se_solve_stats* stats) {
 }
 int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev) {
   if (!ls || !x_dev || !y_dev) return fail(SE_ERR_ARG, "null argument");
+  // orders 4 to 8 (and SVV systems) run kernels without barrier waits;
+  // the TMA-staged kernel of the other orders reports a barrier that timed
+  // out in the error word, read back here
+  const int N = ls->op.d[0].N;
+  const bool waits = ls->op.gamma == 0.0 && (N < 4 || N > 8);
+  if (waits) CK(cudaMemsetAsync(ls->d_err, 0, sizeof(unsigned), g_stream));
   CK(launch_op_apply(ls->op, x_dev, y_dev, ls->d_err, g_stream));
+  if (waits) {
+    unsigned err = 0;
+    CK(cudaMemcpyAsync(&err, ls->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, g_stream));
+    CK(cudaStreamSynchronize(g_stream));
+    if (err & KERR_BARRIER_TIMEOUT) return fail(SE_ERR_TIMEOUT, "apply: a TMA stage never arrived");
+  }
   return SE_OK;
 }
 int se_linsys_fdm_apply(se_linsys* ls, const double* r_dev, double* x_dev) {
@@ -2274,11 +2286,13 @@ int se_field_error(const se_field* numeric, const se_field* analytic, int dof, i
 //
 // Limits and sharing: at most kNoAllocMaxUnknowns vector unknowns and
 // kNoAllocMaxTiles tiles of 32x16 unknowns per solve; larger systems are
-// rejected with SE_ERR_UNSUPPORTED. The array is held by every GPU that loads
-// the library until the process exits, and every call on a device shares it
-// and leaves its contents behind: calls whose device work overlaps (other
-// streams, other host threads) race on it and must be serialised by the
-// caller. The first call on each device looks up the array's device address
+// rejected with SE_ERR_UNSUPPORTED. Only the drop-in solver runs here
+// (SE_METHOD_CG in SE_PREC_FP64); other methods and precisions are refused
+// with SE_ERR_UNSUPPORTED. The array is held by every GPU that loads the
+// library until the process exits, and every call on a device shares it and
+// leaves its contents behind. Two calls whose device work overlapped would
+// race on it, so each call holds g_noalloc_mu until its stream has finished
+// its work. The first call on each device looks up the array's device address
 // (cudaGetSymbolAddress, with that device current); make that first call
 // before any stream capture.
 namespace {
@@ -2331,8 +2345,17 @@ extern "C" int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double
     return fail(SE_ERR_UNSUPPORTED, "periodic x with a bottom wall only (reference: bc error)");
   if ((perx && nEls[0] < 2) || (pery && nEls[1] < 2))
     return fail(SE_ERR_UNSUPPORTED, "a periodic direction needs at least 2 elements");
+  // the vertex grid must fit an int before any index is formed from it
+  const long nvx = (long)nEls[0] * N + 1, nvy = (long)nEls[1] * N + 1;
+  if (nvx * nvy > (1L << 30)) return fail(SE_ERR_UNSUPPORTED, "mesh too large");
   se_solver_opts o;
   if (opts) o = *opts; else se_solver_opts_default(&o);
+  if (int rc = check_opts(&o)) return rc;
+  // this entry point runs the drop-in solver only: Jacobi CG in FP64
+  if (o.method != SE_METHOD_CG)
+    return fail(SE_ERR_UNSUPPORTED, "the no-allocation solve runs SE_METHOD_CG only");
+  if (o.precision != SE_PREC_FP64)
+    return fail(SE_ERR_UNSUPPORTED, "the no-allocation solve runs SE_PREC_FP64 only");
 
   // host tables on the stack: mesh, boundary ranges, operator
   se_mesh mesh;
@@ -2363,6 +2386,7 @@ extern "C" int se_helmholtz_solve_noalloc(const int nEls[2], int N, const double
   op.G[0] = op.d[0].hi - op.d[0].lo;
   op.G[1] = op.d[1].hi - op.d[1].lo;
   const long n = (long)op.G[0] * op.G[1];
+  if (n <= 0) return fail(SE_ERR_ARG, "the system has no unknowns");
   if (n > kNoAllocMaxUnknowns)
     return fail(SE_ERR_UNSUPPORTED,
                 "%ld unknowns exceed the no-allocation limit of %d; use se_helmholtz_create", n,

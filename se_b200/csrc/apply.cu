@@ -309,11 +309,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
       : "memory");
   return ok != 0;
 }
-// Wait for a barrier phase, at most 2^20 polls.
-__device__ __forceinline__ void mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned* err) {
+// Wait for a barrier phase, at most 2^20 polls; false when the polls ran
+// out (the error bit is then set).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, unsigned* err) {
   for (int it = 0; it < (1 << 20); it++)
-    if (mbar_try_wait(bar, parity)) return;
-  if (err) atomicOr(err, (unsigned)KERR_BARRIER_TIMEOUT);
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicOr(err, (unsigned)KERR_BARRIER_TIMEOUT);
+  return false;
 }
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
                                             uint64_t* bar) {
@@ -414,7 +416,16 @@ __global__ void __launch_bounds__(kThreads) apply_mma_kernel(const __grid_consta
     const int ex0 = gx0 / N, ey0 = gy0 / N;
     int xs, ys, off = 0;
     if (tile_tma<N>(op, tma, tiles_x, t, xs, ys)) {
-      mbar_wait_bounded(&bar[s], (phase >> s) & 1u, err);
+      const bool arrived = mbar_wait_bounded(&bar[s], (phase >> s) & 1u, err);
+      // a stage that never arrived: no thread computes on it or issues
+      // another load; the block waits (bounded) for the copy still in
+      // flight into that stage, so that it does not land after the block
+      // has left, and returns with the error bit set
+      if (__syncthreads_or(!arrived)) {
+        for (int it = 0; it < (1 << 20); it++)
+          if (mbar_try_wait(&bar[s], (phase >> s) & 1u)) break;
+        return;
+      }
       phase ^= 1u << s;
       off = xs & 1;
     } else {
@@ -579,7 +590,8 @@ cudaError_t launch_mma(const OpDev& od, const double* x, double* y, unsigned* er
   std::memset(&map, 0, sizeof(map));
   int tma = 0;
   PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
-  if (enc && (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (od.G[0] % 2) == 0) {
+  // the TMA path's bounded waits report through err, so it needs one
+  if (enc && err && (reinterpret_cast<uintptr_t>(x) & 15) == 0 && (od.G[0] % 2) == 0) {
     const cuuint64_t dims[2] = {(cuuint64_t)od.G[0], (cuuint64_t)od.G[1]};
     const cuuint64_t strides[1] = {(cuuint64_t)od.G[0] * sizeof(double)};
     const cuuint32_t box[2] = {(cuuint32_t)T::UP, (cuuint32_t)T::UH};

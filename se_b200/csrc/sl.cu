@@ -5,7 +5,7 @@
 // reference). Each thread integrates the backward trajectory and gathers the
 // (N+1)^2 element block of the field at every stage.
 //
-// Reference: src/base/Advector.cpp:150-274 (PeriodicUpdate, IntegrateRK2,
+// Reference: src/base/Advector.cpp:122-148,181-246,339-349 (PeriodicUpdate, IntegrateRK2,
 // FirstOrder, SecondOrder, ExtrapolateVelocities), src/base/Mesh.cpp:109-176
 // (GetEl, GlobalToLocal), src/base/Legendre.cpp:145-169 and :293-305
 // (ShapeFuncsAtCoord, IsRoot), src/base/Field.cpp:57-76 (InterpLocal/Global).
@@ -89,7 +89,7 @@ __device__ __forceinline__ void cardinal(const MeshDev& m, double l, double* c) 
   }
 }
 
-// Advector::PeriodicUpdate (src/base/Advector.cpp:150-162).
+// Advector::PeriodicUpdate (src/base/Advector.cpp:122-134).
 __device__ __forceinline__ double wrap(const MeshDev& m, int d, double c) {
   if (c < m.min[d]) c = m.periodic[d] ? xadd(m.span[d], c) : m.min[d];
   if (c > m.max[d]) c = m.periodic[d] ? xadd(m.nspan[d], c) : m.max[d];
@@ -125,7 +125,7 @@ struct Vec2 {
   }
 };
 // c0*v + c1*vm with the reference's rounding (Advector::ExtrapolateVelocities,
-// src/base/Advector.cpp:367-377): each product rounded, then the sum.
+// src/base/Advector.cpp:339-349): each product rounded, then the sum.
 struct Vec2Mix {
   typedef V2 T;
   const double2* __restrict__ v;
@@ -200,7 +200,7 @@ __device__ __forceinline__ void store_with_copies(const MeshDev& m, double* out,
   if (m.periodic[0] && m.periodic[1] && i == 0 && j == 0) store<T>(out, nvy * nvx - 1, v);
 }
 
-// Advector::FirstOrder with IntegrateRK2 (src/base/Advector.cpp:164-229).
+// Advector::FirstOrder with IntegrateRK2 (src/base/Advector.cpp:136-148,181-201).
 template <int N, class FSrc>
 __global__ void __launch_bounds__(256) sl_first_kernel(const MeshDev m, FSrc field,
                                                        const double2* __restrict__ vel,
@@ -231,7 +231,7 @@ __global__ void __launch_bounds__(256) sl_first_kernel(const MeshDev m, FSrc fie
   if (owner) store_with_copies(m, out, i, j, val);
 }
 
-// Advector::SecondOrder (src/base/Advector.cpp:231-274) with the
+// Advector::SecondOrder (src/base/Advector.cpp:203-246) with the
 // extrapolated velocities formed on the fly at each gathered vertex.
 template <int N, class FSrc>
 __global__ void __launch_bounds__(256) sl_second_kernel(const MeshDev m, FSrc field,
@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(256) sl_second_kernel(const MeshDev m, FSrc fi
     }
   }
   if (owner) {
-    // fieldSL = 2 psi(x1) - 0.5 psiPrev(x2) (src/base/Advector.cpp:266-268)
+    // fieldSL = 2 psi(x1) - 0.5 psiPrev(x2) (src/base/Advector.cpp:236-240)
     typename FSrc::T r;
     double* rp = reinterpret_cast<double*>(&r);
     const double* a = reinterpret_cast<const double*>(&p1);

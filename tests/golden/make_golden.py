@@ -1,11 +1,12 @@
 """Generate the golden fixtures in tests/golden/ from the reference itself.
 
 Runs the reference's own src/base code, compiled unmodified into
-oracle/_ref/libseref.so by ``make -C oracle ref`` (needs the SE checkout at
-/root/reference, read-only). The fixtures pin the oracle restatement and
-the product's host tables on machines without the checkout.
+oracle/_ref/libseref.so by ``make -C oracle ref`` (needs the SE checkout,
+read-only, named by the SE_REFERENCE_SRC environment variable). The fixtures
+pin the oracle restatement and the product's host tables on machines
+without the checkout.
 
-    python tests/golden/make_golden.py
+    SE_REFERENCE_SRC=<SE checkout> python tests/golden/make_golden.py
 
 The reference publishes no golden vectors or known-answer tests of its own;
 these are seeded synthetic cases with the shapes the reference runs.

@@ -1,12 +1,12 @@
 """Single-kernel cases for profiling the library with ncu.
 
-    python -m se_b200.profile_cases apply [ne]       # FP64 operator apply
-    python -m se_b200.profile_cases apply_bf16 [ne]  # BF16-in, FP32 operator apply
-    python -m se_b200.profile_cases sl [ne]          # first-order SL advection
-    python -m se_b200.profile_cases sl2 [ne]         # second-order SL advection
-    python -m se_b200.profile_cases cg [ne]          # persistent Jacobi-PCG solve
-    python -m se_b200.profile_cases fdm [ne]         # one FDM solve (a CUDA graph)
-    python -m se_b200.profile_cases fdm_apply [ne]   # the FDM transform: 4 product kernels
+    python tests/profile_cases.py apply [ne]       # FP64 operator apply
+    python tests/profile_cases.py apply_bf16 [ne]  # BF16-in, FP32 operator apply
+    python tests/profile_cases.py sl [ne]          # first-order SL advection
+    python tests/profile_cases.py sl2 [ne]         # second-order SL advection
+    python tests/profile_cases.py cg [ne]          # persistent Jacobi-PCG solve
+    python tests/profile_cases.py fdm [ne]         # one FDM solve (a CUDA graph)
+    python tests/profile_cases.py fdm_apply [ne]   # the FDM transform: 4 product kernels
 
 Each case builds an ne x ne element (default 64, the bench's mesh), order p
 (third argument, default 8), doubly periodic mesh and the bench's fields and launches the kernel a few
@@ -16,15 +16,20 @@ events).
 """
 from __future__ import annotations
 
+import os
 import sys
 
 import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
 
 
 def main(case: str, ne: int = 64, p: int = 8, reps: int = 3) -> None:
     import torch
 
-    from . import segpu as S
+    from se_b200 import segpu as S
 
     S.load_library()
     torch.cuda.init()

@@ -1,0 +1,146 @@
+"""Parity at the sizes the benchmark reports.
+
+1. The bench step (bench.py): 64x64 elements, p=8, doubly periodic, one
+   first-order SL advection of the seeded Gaussian tracer by the Taylor-Green
+   vortex at Courant 2, then (lap - 1) u = tracer_SL with the true Jacobian,
+   262,144 unknowns. The GPU runs the whole step with each solver variant the
+   bench times (FDM FP64, FDM in reduced precision refined in FP64, the CG
+   drop-in) at the bench's rtol 1e-10; the oracle runs the same step (SL with
+   accurate cardinal functions, restated AIJ + Jacobi CG) to rtol 1e-12.
+   Tolerances: advected tracer 1e-12 of its magnitude (the SL parity of the
+   smaller tests); solution 1e-8 of its magnitude for every variant (rtol
+   1e-10 in the preconditioned norm, amplified by the operator's
+   conditioning); the CG drop-in's iteration count within 0.5% (and 2) of the
+   oracle's at the same rtol.
+2. The two-layer QG channel of the QG benchmark: 128x64 elements, p=6,
+   [0,2]x[0,1] periodic in x with walls in y, F1 = F2 = 400, the zonal jet
+   plus a seeded 1e-3 perturbation, dt at Courant 0.5: one first-order step
+   and one second-order step (TwoLayerQGEqn::Solve) on the GPU with CG and
+   FDM inversions against the oracle's restatement, both sides at rtol
+   1e-12; fields within 1e-9 of their magnitude.
+
+The oracle runs on all host threads (it takes tens of seconds per solve at
+these sizes)."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NTH = os.cpu_count() or 1
+
+
+def rel(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+@pytest.fixture(scope="module")
+def bench_step(oracle):
+    import bench as B
+    om = oracle.Mesh(B.NX, B.NY, B.P, accurate=True)
+    X = om.verts()
+    phi, vel = B.workload_fields(X)
+    dt = om.calc_time_step(vel, B.COURANT)
+    sl = om.advect(phi, vel, dt, nthreads=NTH)
+    zero = np.zeros(om.nv)
+    u, st = oracle.helmholtz_solve(om, zero, sl, -B.LAMBDA, -1.0, 1.0, quirk=False, rtol=1e-12,
+                                   nthreads=NTH)
+    _, st10 = oracle.helmholtz_solve(om, zero, sl, -B.LAMBDA, -1.0, 1.0, quirk=False,
+                                     rtol=B.RTOL, nthreads=NTH)
+    return {"B": B, "phi": phi, "vel": vel, "dt": dt, "sl": sl, "u": u, "its10": st10["its"]}
+
+
+@pytest.mark.parametrize("variant", ["fdm_fp64", "fdm_tf32", "cg_fp64"])
+def test_bench_step_matches_oracle(segpu, bench_step, variant):
+    S, h = segpu, bench_step
+    B = h["B"]
+    meth, prec = B.VARIANTS[variant]
+    m = S.Mesh("mesh", [B.NX, B.NY], "legendre", B.P, [0.0, 0.0], [1.0, 1.0], [True, True])
+    bc = S.BCs(False, False, False, False, m)
+    phi, v, u = S.Field("phi", m, 1, bc), S.Field("vel", m, 2, None), S.Field("u", m, 1, bc)
+    phi.vals, v.vals = h["phi"], h["vel"]
+    dt = h["dt"]
+    assert abs(S.CalcTimeStep(v, B.COURANT) - dt) <= 1e-15 * dt
+    adv = S.Advector(phi, v)
+    adv.Advect(dt)
+    assert rel(adv.fieldSL.vals, h["sl"]) < 1e-12
+    opts = S.solver_opts(rtol=B.RTOL, mode=S.MODE_EXACT, method=getattr(S, meth),
+                         precision=getattr(S, prec), max_it=10000)
+    helm = S.HelmholtzEqn(u, adv.fieldSL, -B.LAMBDA, -1.0, 1.0, 0, opts)
+    st = helm.Solve("helm_", raise_on_diverge=True)
+    assert st["reason"] > 0
+    err = rel(u.vals, h["u"])
+    assert err < 1e-8, err
+    if variant == "cg_fp64":
+        its, ref = st["its"], h["its10"]
+        assert abs(its - ref) <= max(2, 0.005 * ref), (its, ref)
+
+
+QG_NX, QG_NY, QG_P = 128, 64, 6
+
+
+def qg_initial(X, seed=5):
+    """The QG benchmark's initial state: upper-layer zonal jet
+    psi1 = -U L tanh((y - 1/2) / L) (U = 1, L = 0.1), omega1 its Laplacian plus
+    a seeded 1e-3 perturbation off the walls, lower layer at rest."""
+    rng = np.random.default_rng(seed)
+    y = X[:, 1]
+    U, L = 1.0, 0.1
+    s = (y - 0.5) / L
+    psi1 = -U * L * np.tanh(s)
+    om1 = 2.0 * U * np.tanh(s) / np.cosh(s) ** 2 / L
+    wall = (np.abs(y) < 1e-12) | (np.abs(y - 1.0) < 1e-12)
+    om1 = om1 + 1e-3 * np.where(wall, 0.0, rng.standard_normal(len(y)))
+    nvx = QG_NX * QG_P + 1
+    om1 = om1.reshape(-1, nvx)
+    om1[:, -1] = om1[:, 0]
+    zeros = np.zeros(len(y))
+    vel = np.stack([U / np.cosh(s) ** 2, zeros], 1)
+    return psi1, om1.ravel(), zeros, zeros, zeros, vel
+
+
+QG_PARAMS = dict(F1=400.0, F2=400.0, beta=0.5, E2=0.01, r=0.001, nu=1e-5)
+
+
+@pytest.fixture(scope="module")
+def qg_ref(oracle):
+    om = oracle.Mesh(QG_NX, QG_NY, QG_P, (0.0, 0.0), (2.0, 1.0), (True, False), accurate=True)
+    X = om.verts()
+    psi1, om1, psi2, om2, tau_e, vel = qg_initial(X)
+    dt = om.calc_time_step(vel, 0.5)
+    ref = oracle.QG2(om, (True, True, False, False), psi1, om1, psi2, om2, tau_e=tau_e, dt=dt,
+                     rtol=1e-12, nthreads=NTH, **QG_PARAMS)
+    ref.step(None)
+    first = (ref.psi1.copy(), ref.omega1.copy(), ref.psi2.copy(), ref.omega2.copy())
+    ref.step((psi1, om1, psi2, om2))
+    second = (ref.psi1.copy(), ref.omega1.copy(), ref.psi2.copy(), ref.omega2.copy())
+    return {"X": X, "dt": dt, "init": (psi1, om1, psi2, om2, tau_e), "first": first,
+            "second": second}
+
+
+@pytest.mark.parametrize("method", ["cg", "fdm"])
+def test_qg_channel_steps_match_oracle(segpu, qg_ref, method):
+    S = segpu
+    m = S.Mesh("m", [QG_NX, QG_NY], "legendre", QG_P, [0.0, 0.0], [2.0, 1.0], [True, False])
+    bc = S.BCs(True, True, False, False, m)
+    names = ("psi1", "omega1", "psi2", "omega2", "tau_e")
+    f = [S.Field(nm, m, 1, bc if nm.startswith("psi") else None) for nm in names]
+    for fi, v in zip(f, qg_ref["init"]):
+        fi.vals = v
+    prev = [S.Field(f"{nm}-prev", m, 1, None) for nm in names[:4]]
+    for fi, v in zip(prev, qg_ref["init"][:4]):
+        fi.vals = v
+    opts = S.solver_opts(rtol=1e-12, mode=S.MODE_EXACT,
+                         method=S.METHOD_FDM if method == "fdm" else S.METHOD_CG)
+    p = QG_PARAMS
+    qg = S.TwoLayerQGEqn(*f[:4], p["F1"], p["F2"], p["beta"], p["E2"], p["r"], p["nu"], f[4],
+                         qg_ref["dt"], opts)
+    qg.Solve()  # first order
+    for fi, v in zip(f[:4], qg_ref["first"]):
+        assert np.all(np.isfinite(fi.vals))
+        assert rel(fi.vals, v) < 1e-9, rel(fi.vals, v)
+    qg.Solve(*prev)  # second order with the initial fields as the previous level
+    for fi, v in zip(f[:4], qg_ref["second"]):
+        assert rel(fi.vals, v) < 1e-9, rel(fi.vals, v)
+    assert rel(f[0].vals, qg_ref["init"][0]) > 1e-6  # the step moved the fields

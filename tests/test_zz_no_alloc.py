@@ -27,20 +27,29 @@ def _arr(t, v):
     return (t * len(v))(*v)
 
 
-def run_noalloc(S, case, rhs, sol, c, nu, dt, poisson=False, rtol=1e-12, null=False):
+def run_noalloc(S, case, rhs, sol, c, nu, dt, poisson=False, rtol=1e-12, null=False, opts=None,
+                free_bytes=None, allow_diverge=False):
     lib = S.load_library()
     nx, ny, N, lo, hi, per, bc = case
     rhs_d = None if rhs is None else torch.tensor(rhs, device="cuda", dtype=torch.float64)
     sol_d = torch.tensor(sol, device="cuda", dtype=torch.float64)
     st = S.SolveStats()
-    opts = S.solver_opts(rtol=rtol)
+    if opts is None:
+        opts = S.solver_opts(rtol=rtol)
     torch.cuda.synchronize()
+    if free_bytes is not None:
+        free_bytes.append(torch.cuda.mem_get_info()[0])
     rc = lib.se_helmholtz_solve_noalloc(
         _arr(ctypes.c_int, [nx, ny]), N, _arr(ctypes.c_double, lo), _arr(ctypes.c_double, hi),
         _arr(ctypes.c_int, [int(per[0]), int(per[1])]), _arr(ctypes.c_int, [int(b) for b in bc]),
         c, nu, dt, int(poisson), ctypes.byref(opts), int(null),
         ctypes.c_void_p(None if rhs_d is None else rhs_d.data_ptr()),
         ctypes.c_void_p(sol_d.data_ptr()), ctypes.byref(st))
+    if free_bytes is not None:
+        torch.cuda.synchronize()
+        free_bytes.append(torch.cuda.mem_get_info()[0])
+    if rc == S.SE_ERR_NOT_CONVERGED and allow_diverge:
+        rc = 0
     if rc != 0:
         raise S.SEError(rc, lib.se_last_error().decode())
     return sol_d.cpu().numpy(), st.as_dict()
@@ -57,10 +66,10 @@ def run_linsys(S, case, rhs, sol, c, nu, dt, poisson=False, rtol=1e-12, null=Fal
     opts = S.solver_opts(rtol=rtol)
     if poisson:
         ls = S.PoissonEqn(fs, fr if rhs is not None else None, c, opts)
-        st = ls.Solve(removeNullSpace=null)
+        st = ls.Solve(removeNullSpace=bool(null), projectRHS=null == 2)
     else:
         ls = S.HelmholtzEqn(fs, fr if rhs is not None else None, c, nu, dt, 0, opts)
-        st = ls.Solve("helm_", removeNullSpace=null)
+        st = ls.Solve("helm_", removeNullSpace=bool(null), projectRHS=null == 2)
     return fs.vals, st
 
 
@@ -113,3 +122,48 @@ def test_noalloc_refuses_systems_beyond_its_limit(segpu):
         run_noalloc(segpu, big, None, np.zeros(nvx * nvx), -1.0, -1.0, 1.0)
     assert e.value.code == segpu.SE_ERR_UNSUPPORTED
     assert "no-allocation limit" in str(e.value)
+
+
+def test_noalloc_allocates_no_device_memory(segpu):
+    # after a first call (which looks the static array up), a call leaves the
+    # device's free memory exactly as it found it
+    rhs, sol = fields(CHANNEL, 3)
+    run_noalloc(segpu, CHANNEL, rhs, sol, -3.0, -1.0, 1.0)
+    free = []
+    run_noalloc(segpu, CHANNEL, rhs, sol, -3.0, -1.0, 1.0, free_bytes=free)
+    assert free[0] == free[1]
+
+
+PERIODIC = (6, 6, 5, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False))
+
+
+def test_noalloc_periodic_poisson_null_space(segpu):
+    # a singular periodic Poisson system with the constant null space removed
+    # (mode 1: projected from every preconditioned residual; mode 2: the
+    # right-hand side projected onto the range first), against the allocating
+    # path: same reason, same iteration count, same solution when converged
+    rhs, sol = fields(PERIODIC, 4)
+    for null in (1, 2):
+        got, st = run_noalloc(segpu, PERIODIC, rhs, sol, -1.0, 0.0, 0.0, poisson=True,
+                              rtol=1e-10, null=null, allow_diverge=True)
+        ref, rs = run_linsys(segpu, PERIODIC, rhs, sol, -1.0, 0.0, 0.0, poisson=True,
+                             rtol=1e-10, null=null)
+        assert st["reason"] == rs["reason"] and st["its"] == rs["its"]
+        if rs["reason"] > 0:
+            assert np.abs(got - ref).max() <= TOL * np.abs(ref).max()
+
+
+def test_noalloc_refuses_other_methods_and_precisions(segpu):
+    rhs, sol = fields(CHANNEL, 5)
+    for kw in ({"method": segpu.METHOD_FDM}, {"precision": segpu.PREC_MIXED},
+               {"precision": segpu.PREC_BF16}):
+        opts = segpu.solver_opts(rtol=1e-10, **kw)
+        with pytest.raises(segpu.SEError) as e:
+            run_noalloc(segpu, CHANNEL, rhs, sol, -3.0, -1.0, 1.0, opts=opts)
+        assert e.value.code == segpu.SE_ERR_UNSUPPORTED
+    # an unknown norm type is an argument error, as in se_helmholtz_create
+    opts = segpu.solver_opts(rtol=1e-10)
+    opts.norm_type = 7
+    with pytest.raises(segpu.SEError) as e:
+        run_noalloc(segpu, CHANNEL, rhs, sol, -3.0, -1.0, 1.0, opts=opts)
+    assert e.value.code == segpu.SE_ERR_ARG
