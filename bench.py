@@ -140,7 +140,7 @@ VARIANTS = {
     # name: (method, precision) -- FDM: fast diagonalization refined in FP64 to
     # rtol; CG: PETSc KSPCG + PCJACOBI semantics (the drop-in)
     "fdm_fp64": ("METHOD_FDM", "PREC_FP64"),
-    "fdm_tf32": ("METHOD_FDM", "PREC_MIXED"),
+    "fdm_tf32x3_tc": ("METHOD_FDM", "PREC_MIXED"),
     "cg_fp64": ("METHOD_CG", "PREC_FP64"),
 }
 HEADLINE = "fdm_fp64"
@@ -716,7 +716,7 @@ def run_config2(steps=20, seed=5):
     stream = torch.cuda.Stream()
     S.set_stream(stream.cuda_stream)
     for name, method, prec, n in (("fdm_fp64", S.METHOD_FDM, S.PREC_FP64, steps),
-                                  ("fdm_tf32_refined_fp64", S.METHOD_FDM, S.PREC_MIXED, steps),
+                                  ("fdm_tf32x3_tc_refined_fp64", S.METHOD_FDM, S.PREC_MIXED, steps),
                                   ("cg_fp64", S.METHOD_CG, S.PREC_FP64, max(2, steps // 10))):
         f = [S.Field(nm, m, 1, bc if nm.startswith("psi") else None)
              for nm in ("psi1", "omega1", "psi2", "omega2", "tau_e")]
@@ -760,7 +760,7 @@ def run_ensemble(count=256, seed=2024):
     out = {"workload": "256 solves, n x n elements n~U{8..64}, p~U{4,6,8}, lambda~logU[1e-2,1e2], "
                        "8-mode RHS, rtol 1e-10"}
     for name, method, prec in (("fdm_fp64", S.METHOD_FDM, S.PREC_FP64),
-                               ("fdm_tf32_refined_fp64", S.METHOD_FDM, S.PREC_MIXED),
+                               ("fdm_tf32x3_tc_refined_fp64", S.METHOD_FDM, S.PREC_MIXED),
                                ("cg_fp64", S.METHOD_CG, S.PREC_FP64)):
         systems = []
         for ne, p, lam, sd in specs:
@@ -907,7 +907,7 @@ def run_serving(seconds=2.0, seed=77, load=0.7):
                        "n in {8,16,32,64,128}, p in 4..8, page-locked client buffers",
            "load": load}
     cap_reqs = stream(4000)
-    for label, prec in (("fp64", S.PREC_FP64), ("tf32_refined_fp64", S.PREC_MIXED)):
+    for label, prec in (("fp64", S.PREC_FP64), ("tf32x3_tc_refined_fp64", S.PREC_MIXED)):
         opts = S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=S.METHOD_FDM, precision=prec)
         srv = S.Server(slots=16, device_gib=60.0)
         cv = threading.Condition()

@@ -296,6 +296,13 @@ int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev);
  * preconditioner for callers that run their own Krylov loop. The first call
  * on a system computes its 1-D eigendecompositions (host work, allocation). */
 int se_linsys_fdm_apply(se_linsys* ls, const double* r_dev, double* x_dev);
+/* No counterpart in the reference: x = A^{-1} r by the fast-diagonalization
+ * transforms in FP64 (precision SE_PREC_FP64, as se_linsys_fdm_apply) or on
+ * the tcgen05 tensor cores (SE_PREC_MIXED: r split into TF32 hi/lo pairs,
+ * three TF32 products per K step with FP32 accumulation, about 1e-6
+ * relative), the inner solve of the mixed-precision refinement; same
+ * arguments and rules as se_linsys_fdm_apply. */
+int se_linsys_fdm_apply_prec(se_linsys* ls, int precision, const double* r_dev, double* x_dev);
 /* No counterpart in the reference: y = A x with x in BF16 or FP16
  * (precision SE_PREC_BF16 / SE_PREC_FP16) and y in FP32, the operator and
  * the arithmetic in FP32 (device pointers, vec_size entries each). */

@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsegpu.so")
-SOURCES = ["api.cu", "sl.cu", "linsys.cu", "cg.cu", "fdm.cu", "gemm.cu", "apply.cu", "server.cu"]
+SOURCES = ["api.cu", "sl.cu", "linsys.cu", "cg.cu", "fdm.cu", "gemm.cu", "tc_gemm.cu", "apply.cu", "server.cu"]
 LIBS = ["-lcusolver"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -41,10 +41,26 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object in parallel (one nvcc per file),
+    then link the shared library."""
     if not force and up_to_date():
         return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    flags = [f for f in NVCC_FLAGS if f != "-shared"]
+    procs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        cmd = [nvcc(), *flags, "-c", "-o", obj, os.path.join(CSRC, src)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((src, obj, subprocess.Popen(cmd, cwd=CSRC)))
+    failed = [src for src, _, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError(f"nvcc failed on {', '.join(failed)}")
     tmp = LIB + ".tmp"
-    cmd = [nvcc(), *NVCC_FLAGS, "-o", tmp, *[os.path.join(CSRC, s) for s in SOURCES], *LIBS]
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", tmp,
+           *[obj for _, obj, _ in procs], *LIBS]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True, cwd=CSRC)

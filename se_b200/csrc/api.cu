@@ -267,6 +267,13 @@ struct se_linsys {
   int fdm_lbuf_prec;          // precision the L2, L3 buffers were sized for
   double *X1, *X2, *ax;       // FP64 work: two transform buffers, A x
   void *L1, *L2, *L3;         // low-precision work (L1 unused)
+  // tcgen05 path (SE_PREC_MIXED): operand pairs of the eigenvector products
+  // (cached per direction) and two work pairs, [G_y][tc_px] and [G_x][tc_py]
+  const float *tcSx[2], *tcSy[2], *tcSxT[2], *tcSyT[2];
+  float *tcY[2], *tcX[2];
+  int tc_px, tc_py, tc_sms;
+  TcPlan* tc_plan;  // the four products' plans (for the output tc_out)
+  double* tc_out;
   double* fpart;              // reduction partials [2*fpart_n] + results [16]
   int fpart_n;
   double lmax[2];  // largest 1-D eigenvalue magnitude per direction
@@ -512,6 +519,11 @@ void linsys_free(se_linsys* ls) {
   if (ls->L1) cudaFree(ls->L1);
   if (ls->L2) cudaFree(ls->L2);
   if (ls->L3) cudaFree(ls->L3);
+  for (int k = 0; k < 2; k++) {
+    dfree(ls->tcY[k]);
+    dfree(ls->tcX[k]);
+  }
+  delete[] ls->tc_plan;
   dfree(ls->fpart);
   if (ls->fdm_exec) cudaGraphExecDestroy(ls->fdm_exec);
   dfree(ls->d_fparams);
@@ -647,6 +659,18 @@ void assemble_1d(const Dir& d, const double* Kh, const double* w, std::vector<do
     }
 }
 
+// Row pitch (in FP32) of a tcgen05 operand with n columns: whole 128-byte
+// rows, so that the TMA strides are multiples of 16 bytes.
+int tc_pitch(int n) { return (n + 31) / 32 * 32; }
+// f rounded to the nearest TF32 number (ties away from zero), as cvt.rna.tf32.
+float tf32_rna(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u = (u + 0x1000u) & 0xFFFFE000u;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
 uint16_t to_bf16(float f) {
   uint32_t u;
   std::memcpy(&u, &f, 4);
@@ -746,6 +770,10 @@ struct Eig1D {
   double lmax = 0.0;
   void* low[3] = {nullptr, nullptr, nullptr};   // [1] FP32, [2] BF16 copies of S
   void* lowT[3] = {nullptr, nullptr, nullptr};  // and of ST
+  // TF32 hi/lo pairs for the tcgen05 products, rows padded to tc_pitch:
+  // tc[0] of S (row-major E^T), tc[1] of ST (row-major E); [.][0] hi, [.][1] lo
+  float* tc[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int tc_pitch = 0;
 };
 typedef std::tuple<int, int, int, int, int, int> EigKey;
 std::mutex g_eig_mu;
@@ -772,7 +800,7 @@ int eig_get(const Dir& d, const double* Kh, const double* w, int prec, Eig1D** o
     for (double v : lam) ne->lmax = std::max(ne->lmax, std::fabs(v));
     e = ne;
   }
-  if (prec != 0 && !e->low[prec]) {
+  if (prec == 2 && !e->low[prec]) {
     if (Sh.empty()) {
       Sh.resize((size_t)e->n * e->n);
       CK(cudaMemcpy(Sh.data(), e->S, sizeof(double) * Sh.size(), cudaMemcpyDeviceToHost));
@@ -783,6 +811,31 @@ int eig_get(const Dir& d, const double* Kh, const double* w, int prec, Eig1D** o
     for (int j = 0; j < n; j++)
       for (int i = 0; i < n; i++) T[(size_t)i * n + j] = Sh[(size_t)j * n + i];
     if (int rc = upload_low(T, prec, &e->lowT[prec])) return rc;
+  }
+  if (prec == 1 && !e->tc[0][0]) {
+    if (Sh.empty()) {
+      Sh.resize((size_t)e->n * e->n);
+      CK(cudaMemcpy(Sh.data(), e->S, sizeof(double) * Sh.size(), cudaMemcpyDeviceToHost));
+    }
+    const int n = e->n, pitch = tc_pitch(n);
+    for (int t = 0; t < 2; t++) {
+      std::vector<float> hi((size_t)n * pitch, 0.0f), lo((size_t)n * pitch, 0.0f);
+      for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) {
+          const double v = t == 0 ? Sh[(size_t)i * n + j] : Sh[(size_t)j * n + i];
+          const float h = tf32_rna((float)v);
+          hi[(size_t)i * pitch + j] = h;
+          lo[(size_t)i * pitch + j] = (float)(v - (double)h);
+        }
+      for (int k = 0; k < 2; k++) {
+        float* d = nullptr;
+        if (int rc = dalloc(&d, hi.size())) return rc;
+        CK(cudaMemcpy(d, k == 0 ? hi.data() : lo.data(), sizeof(float) * hi.size(),
+                      cudaMemcpyHostToDevice));
+        e->tc[t][k] = d;
+      }
+    }
+    e->tc_pitch = pitch;
   }
   *out = e;
   return SE_OK;
@@ -819,7 +872,28 @@ int fdm_setup(se_linsys* ls, int prec) {
     CK(launch_op_diag(op, ls->dinv, g_stream));
     CK(launch_invert(ls->dinv, n, g_stream));
   }
-  if (prec != 0 && ls->fdm_lbuf_prec != prec) {
+  if (prec == 1) {
+    for (int k = 0; k < 2; k++) {
+      ls->tcSx[k] = ex->tc[0][k];
+      ls->tcSxT[k] = ex->tc[1][k];
+      ls->tcSy[k] = ey->tc[0][k];
+      ls->tcSyT[k] = ey->tc[1][k];
+    }
+    ls->tc_px = ex->tc_pitch;
+    ls->tc_py = ey->tc_pitch;
+    if (!ls->tcY[0]) {
+      const size_t ny = (size_t)op.G[1] * ls->tc_px, nx = (size_t)op.G[0] * ls->tc_py;
+      for (int k = 0; k < 2; k++) {
+        if ((rc = dalloc(&ls->tcY[k], ny)) || (rc = dalloc(&ls->tcX[k], nx))) return rc;
+        CK(cudaMemset(ls->tcY[k], 0, sizeof(float) * ny));
+        CK(cudaMemset(ls->tcX[k], 0, sizeof(float) * nx));
+      }
+      int dev = 0;
+      CK(cudaGetDevice(&dev));
+      CK(cudaDeviceGetAttribute(&ls->tc_sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+  }
+  if (prec == 2 && ls->fdm_lbuf_prec != prec) {
     const size_t es = prec == 1 ? sizeof(float) : sizeof(uint16_t);
     if (ls->L1) cudaFree(ls->L1);
     if (ls->L2) cudaFree(ls->L2);
@@ -884,6 +958,47 @@ int fdm_apply_low(se_linsys* ls, const double* in, double* out) {
   return SE_OK;
 }
 
+
+// x += A^{-1} r on the tcgen05 tensor cores (tc_gemm.cu): r split into TF32
+// hi/lo pairs, then four products whose outputs chain without transposes
+//   T1[x'][y] = F Ex,  T2[y'][x'] = (Ey^T T1) / lambda,  T3[x][y'] = T2 Ex^T,
+//   x[y][x] += Ey T3,
+// each product three TF32 MMAs per K step (about 21 operand bits), FP32
+// accumulation; the last adds into the FP64 solution.
+int fdm_apply_tc(se_linsys* ls, const double* in, double* out) {
+  const int gx = ls->op.G[0], gy = ls->op.G[1];
+  if (!ls->tc_plan || ls->tc_out != out) {
+    // plans (tile shapes, tensor maps) of the four products, once per output
+    const int px = ls->tc_px, py = ls->tc_py;
+    const OpDev& op = ls->op;
+    if (!ls->tc_plan) ls->tc_plan = new TcPlan[4];
+    TcEpi e;
+    std::memset(&e, 0, sizeof(e));
+    e.err = &ls->d_fstate->kerr;
+    // P1: M = gy, N = gx, K = gx
+    e.M = gy; e.N = gx; e.K = gx; e.out_hi = ls->tcX[0]; e.out_lo = ls->tcX[1]; e.pitch = py;
+    CK(tc_plan(&ls->tc_plan[0], TC_EPI_SPLIT, ls->tcY[0], ls->tcY[1], px, ls->tcSx[0], ls->tcSx[1],
+               px, e));
+    // P2: M = gx, N = gy, K = gy, spectral divide
+    e.M = gx; e.N = gy; e.K = gy; e.out_hi = ls->tcY[0]; e.out_lo = ls->tcY[1]; e.pitch = px;
+    e.lm = ls->lx; e.ln = ls->ly; e.alpha = op.alpha; e.bm = op.beta[0]; e.bn = op.beta[1];
+    e.null_tol = null_tol(ls);
+    CK(tc_plan(&ls->tc_plan[1], TC_EPI_DIVIDE, ls->tcX[0], ls->tcX[1], py, ls->tcSy[0],
+               ls->tcSy[1], py, e));
+    // P3: M = gy, N = gx, K = gx
+    e.M = gy; e.N = gx; e.K = gx; e.out_hi = ls->tcX[0]; e.out_lo = ls->tcX[1]; e.pitch = py;
+    CK(tc_plan(&ls->tc_plan[2], TC_EPI_SPLIT, ls->tcY[0], ls->tcY[1], px, ls->tcSxT[0],
+               ls->tcSxT[1], px, e));
+    // P4: M = gx, N = gy, K = gy, accumulated into the FP64 solution [gy][gx]
+    e.M = gx; e.N = gy; e.K = gy; e.out_hi = e.out_lo = nullptr; e.out64 = out; e.pitch = gx;
+    CK(tc_plan(&ls->tc_plan[3], TC_EPI_ACC64, ls->tcX[0], ls->tcX[1], py, ls->tcSyT[0],
+               ls->tcSyT[1], py, e));
+    ls->tc_out = out;
+  }
+  CK(launch_tc_split(in, gy, gx, gx, ls->tcY[0], ls->tcY[1], ls->tc_px, g_stream));
+  for (int k = 0; k < 4; k++) CK(launch_tc_plan(ls->tc_plan[k], g_stream));
+  return SE_OK;
+}
 
 // The whole FDM solve as one CUDA graph: right-hand side assembly, r = f,
 // x = 0, the initial norm and test, then a conditional while-node whose body
@@ -1007,7 +1122,9 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
       ok = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
       int brc = SE_OK;
       if (ok) {
-        brc = prec == 0 ? fdm_apply64(ls, ls->r, ls->x, true) : fdm_apply_low(ls, ls->r, ls->x);
+        brc = prec == 0   ? fdm_apply64(ls, ls->r, ls->x, true)
+              : prec == 1 ? fdm_apply_tc(ls, ls->r, ls->x)
+                          : fdm_apply_low(ls, ls->r, ls->x);
         if (!brc && remove_null)
           brc = launch_remove_mean(ls->x, n, ls->fpart, kFdmPartials, ls->fpart + 2 * ls->fpart_n + 4, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
         // r = f - A x with the norm and the convergence test in one launch
@@ -1089,6 +1206,8 @@ int fdm_finish(se_linsys* ls, CgSolve* st, float* kernel_ms) {
   st->reason = ls->h_fstate->reason;
   st->dp = ls->h_fstate->dp;
   st->rnorm0 = ls->h_fstate->rnorm0;
+  if (ls->h_fstate->kerr & KERR_BARRIER_TIMEOUT)
+    return fail(SE_ERR_TIMEOUT, "FDM solve: a tensor-core product's bounded wait gave up");
   return SE_OK;
 }
 int run_fdm(se_linsys* ls, int remove_null, CgSolve* st, float* kernel_ms) {
@@ -2220,6 +2339,24 @@ int se_linsys_fdm_apply(se_linsys* ls, const double* r_dev, double* x_dev) {
   if (r_dev == x_dev) return fail(SE_ERR_ARG, "r and x must not alias");
   if (int rc = fdm_setup(ls, 0)) return rc;
   return fdm_apply64(ls, r_dev, x_dev, false);
+}
+int se_linsys_fdm_apply_prec(se_linsys* ls, int precision, const double* r_dev, double* x_dev) {
+  if (!ls || !r_dev || !x_dev) return fail(SE_ERR_ARG, "null argument");
+  if (r_dev == x_dev) return fail(SE_ERR_ARG, "r and x must not alias");
+  if (precision == SE_PREC_FP64) return se_linsys_fdm_apply(ls, r_dev, x_dev);
+  if (precision != SE_PREC_MIXED)
+    return fail(SE_ERR_UNSUPPORTED, "precision must be SE_PREC_FP64 or SE_PREC_MIXED");
+  if (int rc = fdm_setup(ls, 1)) return rc;
+  if (!ls->d_fparams) {  // the products report through the loop state's error word
+    int rc;
+    if ((rc = dalloc(&ls->d_fparams, 1)) || (rc = dalloc(&ls->d_fstate, 1)) ||
+        (rc = dalloc(&ls->d_rescount, 1)))
+      return rc;
+    CK(cudaMemset(ls->d_rescount, 0, sizeof(unsigned)));
+    CK(cudaMemset(ls->d_fstate, 0, sizeof(FdmState)));
+  }
+  CK(cudaMemsetAsync(x_dev, 0, sizeof(double) * ls->n, g_stream));
+  return fdm_apply_tc(ls, r_dev, x_dev);
 }
 int se_linsys_apply_low(se_linsys* ls, int precision, const void* x_dev, float* y_dev) {
   if (!ls || !x_dev || !y_dev) return fail(SE_ERR_ARG, "null argument");

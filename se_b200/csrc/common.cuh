@@ -10,6 +10,7 @@
 //    vertex grid: rows [lo_y, hi_y), columns [lo_x, hi_x). Dirichlet and
 //    periodic-duplicate vertices are not unknowns.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -219,7 +220,8 @@ struct FdmParams {
 };
 struct FdmState {
   double rnorm0, ttol, dp, best;
-  int its, reason, stalled, pad;
+  int its, reason, stalled;
+  unsigned kerr;  // KERR_* bits of the loop's kernels (zeroed by the loop's set-up)
 };
 // Set up the loop from res = {norm^2 of f, .}: rnorm0, tolerance, the
 // iteration-0 test; sets the while-condition (1 = iterate).
@@ -230,6 +232,40 @@ cudaError_t launch_fdm_init(const FdmParams* p, FdmState* st, const double* res,
 // while-condition.
 cudaError_t launch_fdm_check(const FdmParams* p, FdmState* st, const double* res,
                              cudaGraphConditionalHandle h, cudaStream_t s);
+
+// FDM products on the tcgen05 tensor cores (tc_gemm.cu): D (M x N) = A B with
+// A = (a_hi + a_lo) stored [M][K] (pitch a_pitch) and B stored transposed as
+// (b_hi + b_lo) [N][K] (pitch b_pitch), FP32 pairs whose hi parts are TF32
+// numbers; three kind::tf32 MMAs per K step (Ah Bh + Ah Bl + Al Bh). Element
+// (m, n) of D goes to [n * pitch + m]: kind TC_EPI_SPLIT stores the hi/lo
+// split of D, TC_EPI_DIVIDE that of D / (alpha + bm lm[m] + bn ln[n]) (0 where
+// the divisor is at most null_tol in magnitude), TC_EPI_ACC64 adds D to an
+// FP64 array. Pitches are multiples of 4; bases 16-byte aligned; err must be
+// set (KERR_BARRIER_TIMEOUT when a bounded wait gave up).
+enum { TC_EPI_SPLIT = 0, TC_EPI_DIVIDE = 1, TC_EPI_ACC64 = 2 };
+struct TcEpi {
+  int M, N, K;
+  float *out_hi, *out_lo;  // SPLIT / DIVIDE: the next product's operand pair
+  int pitch;
+  double* out64;           // ACC64
+  const double *lm, *ln;   // DIVIDE
+  double alpha, bm, bn, null_tol;
+  unsigned* err;
+};
+// A product planned once per buffer set (tile shape, tensor maps), launched
+// as often as needed.
+struct TcPlan {
+  CUtensorMap maps[4];
+  TcEpi e;
+  int epi, bn, ck;
+};
+cudaError_t tc_plan(TcPlan* p, int epi, const float* a_hi, const float* a_lo, int a_pitch,
+                    const float* b_hi, const float* b_lo, int b_pitch, const TcEpi& e);
+cudaError_t launch_tc_plan(const TcPlan& p, cudaStream_t s);
+// hi/lo split of an FP64 [rows][cols] array (leading dimension ld) into FP32
+// arrays of the given pitch: hi = x rounded to TF32, lo = x - hi in FP32.
+cudaError_t launch_tc_split(const double* x, int rows, int cols, int ld, float* hi, float* lo,
+                            int pitch, cudaStream_t s);
 
 // C = A B (row-major, leading dimensions lda/ldb/ldc) on the tensor cores
 // (gemm.cu). prec: 0 FP64, 1 TF32 on FP32 data, 2 BF16. epi: 0 store,

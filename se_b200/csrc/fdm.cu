@@ -72,6 +72,7 @@ __global__ void fdm_init_kernel(const FdmParams* __restrict__ p, FdmState* __res
   st->best = dp;
   st->its = 0;
   st->stalled = 0;
+  st->kerr = 0;
   int reason = 0;
   if (!(dp == dp) || isinf(dp)) reason = -9;
   else if (dp <= st->ttol) reason = dp < p->atol ? 3 : 2;

@@ -130,7 +130,7 @@ SIGNATURES = {
                               ctypes.POINTER(SolveStats)],
     "se_linsys_solve_async": [_vp, ctypes.c_int],
     "se_linsys_solve_finish": [_vp, ctypes.POINTER(SolveStats)],
-    "se_linsys_apply": [_vp, _vp, _vp], "se_field_gen_vel": [_vp, _vp], "se_field_save": [_vp, ctypes.c_char_p, ctypes.c_int], "se_field_read": [_vp, ctypes.c_char_p, ctypes.c_int], "se_linsys_fdm_apply": [_vp, _vp, _vp], "se_linsys_apply_low": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
+    "se_linsys_apply": [_vp, _vp, _vp], "se_field_gen_vel": [_vp, _vp], "se_field_save": [_vp, ctypes.c_char_p, ctypes.c_int], "se_field_read": [_vp, ctypes.c_char_p, ctypes.c_int], "se_linsys_fdm_apply": [_vp, _vp, _vp], "se_linsys_fdm_apply_prec": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_apply_low": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
     "se_linsys_vec_size": [_vp, _I],
     "se_calc_time_step": [_vp, ctypes.c_double, _D],
     "se_field_error": [_vp, _vp, ctypes.c_int, ctypes.c_int, _D],
@@ -483,9 +483,13 @@ class _LinSys:
         """y = A x on device pointers of vecSize doubles."""
         _check(_lib.se_linsys_apply(self._h, _vp(x_ptr), _vp(y_ptr)))
 
-    def fdm_apply(self, r_ptr: int, x_ptr: int):
-        """x = A^{-1} r by the FP64 fast-diagonalization transforms (device pointers)."""
-        _check(_lib.se_linsys_fdm_apply(self._h, _vp(r_ptr), _vp(x_ptr)))
+    def fdm_apply(self, r_ptr: int, x_ptr: int, precision: int = PREC_FP64):
+        """x = A^{-1} r by the fast-diagonalization transforms (device pointers):
+        FP64 products, or (PREC_MIXED) TF32 hi/lo products on the tensor cores."""
+        if precision == PREC_FP64:
+            _check(_lib.se_linsys_fdm_apply(self._h, _vp(r_ptr), _vp(x_ptr)))
+        else:
+            _check(_lib.se_linsys_fdm_apply_prec(self._h, int(precision), _vp(r_ptr), _vp(x_ptr)))
 
     def apply_low(self, x_ptr: int, y_ptr: int, precision: int = PREC_BF16):
         """y (FP32) = A x for x of vecSize BF16 (or FP16) values; device pointers."""

@@ -7,6 +7,7 @@
     python tests/profile_cases.py cg [ne]          # persistent Jacobi-PCG solve
     python tests/profile_cases.py fdm [ne]         # one FDM solve (a CUDA graph)
     python tests/profile_cases.py fdm_apply [ne]   # the FDM transform: 4 product kernels
+    python tests/profile_cases.py fdm_apply_tc [ne]  # the same on the tcgen05 tensor cores (TF32 hi/lo)
 
 Each case builds an ne x ne element (default 64, the bench's mesh), order p
 (third argument, default 8), doubly periodic mesh and the bench's fields and launches the kernel a few
@@ -57,8 +58,8 @@ def main(case: str, ne: int = 64, p: int = 8, reps: int = 3) -> None:
             a.record()
             adv.Advect(dt)
             b.record()
-    elif case in ("apply", "apply_bf16", "cg", "fdm", "fdm_apply"):
-        method = S.METHOD_FDM if case in ("fdm", "fdm_apply") else S.METHOD_CG
+    elif case in ("apply", "apply_bf16", "cg", "fdm", "fdm_apply", "fdm_apply_tc"):
+        method = S.METHOD_FDM if case.startswith("fdm") else S.METHOD_CG
         h = S.HelmholtzEqn(u, phi, -1.0, -1.0, 1.0, 0,
                            S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=method))
         n = h.vecSize
@@ -74,6 +75,8 @@ def main(case: str, ne: int = 64, p: int = 8, reps: int = 3) -> None:
                 h.apply_low(xb.data_ptr(), yf.data_ptr(), S.PREC_BF16)
             elif case == "fdm_apply":
                 h.fdm_apply(xin.data_ptr(), yout.data_ptr())
+            elif case == "fdm_apply_tc":
+                h.fdm_apply(xin.data_ptr(), yout.data_ptr(), S.PREC_MIXED)
             else:
                 h.Solve("helm_")
             b.record()
