@@ -141,6 +141,7 @@ VARIANTS = {
     # rtol; CG: PETSc KSPCG + PCJACOBI semantics (the drop-in)
     "fdm_fp64": ("METHOD_FDM", "PREC_FP64"),
     "fdm_tf32x3_tc": ("METHOD_FDM", "PREC_MIXED"),
+    "fdm_fp64_then_tc": ("METHOD_FDM", "PREC_FP64_TC"),
     "cg_fp64": ("METHOD_CG", "PREC_FP64"),
 }
 HEADLINE = "fdm_fp64"

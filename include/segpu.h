@@ -188,12 +188,16 @@ int se_advector_departures(se_advector* adv, int* el, double* xy);
 #define SE_MODE_REFERENCE 0 /* the reference's Laplacian with detJac forced to 1 (src/base/Operator.cpp:72) */
 #define SE_MODE_EXACT 1     /* the Laplacian with its true Jacobian */
 #define SE_PREC_FP64 0      /* every operation in FP64: the drop-in */
-#define SE_PREC_MIXED 1     /* FP32 data, TF32 tensor-core inner solves, FP64 refinement */
+#define SE_PREC_MIXED 1     /* FDM only: every refinement step's inverse on the tcgen05 tensor
+                               cores (TF32 hi/lo operand pairs, FP32 accumulation, about 1e-6
+                               relative); residuals, norms and the solution in FP64 */
 #define SE_PREC_BF16 2      /* BF16 data, FP32-accumulated tensor-core inner solves, FP64 refinement;
                                refinement converges only while 2^-8 times the operator's
                                condition number stays below 1 (small or well-conditioned
                                systems) and otherwise stops with SE_KSP_DIVERGED_BREAKDOWN */
 #define SE_PREC_FP16 3      /* FP16 data, FP32 arithmetic: se_linsys_apply_low only */
+#define SE_PREC_FP64_TC 4   /* FDM only: the first refinement step's inverse in FP64, the
+                               following ones as SE_PREC_MIXED */
 #define SE_METHOD_CG 0      /* PETSc KSPCG + PCJACOBI semantics: the drop-in (FP64 only) */
 #define SE_METHOD_FDM 1     /* fast diagonalization: exact inverse by 1-D eigenvector transforms */
 typedef struct {

@@ -9,7 +9,8 @@ over that C-ABI.
 from .segpu import (BCs, Advector, Server, REQ_ADVECT, REQ_HELMHOLTZ, CalcTimeStep, Field, FieldError, GenVel, HelmholtzEqn, Mesh, NavierStokesEqn,  # noqa: F401
                     TwoLayerQGEqn, WriteXDMF, WriteXDMFHeader, WriteXDMFFooter, WriteXDMFTemporal,
                     PoissonEqn, SEError, load_library, set_stream, solver_opts, synchronize, solve_batch,
-                    MODE_EXACT, MODE_REFERENCE, PREC_FP64, PREC_MIXED, PREC_BF16, PREC_FP16, METHOD_CG,
+                    MODE_EXACT, MODE_REFERENCE, PREC_FP64, PREC_MIXED, PREC_BF16, PREC_FP16, PREC_FP64_TC,
+                    METHOD_CG,
                     METHOD_FDM, NORM_NATURAL,
                     NORM_PRECONDITIONED, NORM_UNPRECONDITIONED)
 

@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <functional>
 #include <mutex>
 #include <tuple>
 #include <string>
@@ -910,6 +911,9 @@ int fdm_setup(se_linsys* ls, int prec) {
   return SE_OK;
 }
 
+int op_gx(const se_linsys* ls) { return ls->op.G[0]; }
+int op_gy(const se_linsys* ls) { return ls->op.G[1]; }
+
 // Spectral entries below this magnitude are a null mode (constant null space
 // of a periodic Poisson operator) and are zeroed.
 double null_tol(const se_linsys* ls) {
@@ -965,7 +969,7 @@ int fdm_apply_low(se_linsys* ls, const double* in, double* out) {
 //   x[y][x] += Ey T3,
 // each product three TF32 MMAs per K step (about 21 operand bits), FP32
 // accumulation; the last adds into the FP64 solution.
-int fdm_apply_tc(se_linsys* ls, const double* in, double* out) {
+int fdm_apply_tc(se_linsys* ls, const double* in, double* out, bool split_done = false) {
   const int gx = ls->op.G[0], gy = ls->op.G[1];
   if (!ls->tc_plan || ls->tc_out != out) {
     // plans (tile shapes, tensor maps) of the four products, once per output
@@ -995,7 +999,8 @@ int fdm_apply_tc(se_linsys* ls, const double* in, double* out) {
                ls->tcSyT[1], py, e));
     ls->tc_out = out;
   }
-  CK(launch_tc_split(in, gy, gx, gx, ls->tcY[0], ls->tcY[1], ls->tc_px, g_stream));
+  // the input's TF32 split (the refinement loop's residual kernel writes it)
+  if (!split_done) CK(launch_tc_split(in, gy, gx, gx, ls->tcY[0], ls->tcY[1], ls->tc_px, g_stream));
   for (int k = 0; k < 4; k++) CK(launch_tc_plan(ls->tc_plan[k], g_stream));
   return SE_OK;
 }
@@ -1088,9 +1093,16 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
     cudaGraph_t cg = nullptr;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
-    cudaGraphConditionalHandle hc;
+    // prec 3 (FP64 first step, tensor-core steps after): an IF node for the
+    // first step (condition hf, set by the initial test) and the while loop
+    // (condition hc, reset to 0 at every launch, set by each step's test);
+    // otherwise the while loop alone, its condition set by the initial test
+    const bool hybrid = prec == 3;
+    cudaGraphConditionalHandle hc, hf = 0;
     bool ok = cudaStreamGetCaptureInfo(cs, &status, nullptr, &cg, &deps, &ndeps) == cudaSuccess &&
-              cudaGraphConditionalHandleCreate(&hc, cg, 0, 0) == cudaSuccess;
+              cudaGraphConditionalHandleCreate(&hc, cg, 0, hybrid ? cudaGraphCondAssignDefault : 0) ==
+                  cudaSuccess;
+    if (hybrid) ok = ok && cudaGraphConditionalHandleCreate(&hf, cg, 0, 0) == cudaSuccess;
     // prologue
     ok = ok && launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, cs) == cudaSuccess;
     // a right-hand side off the range of a singular operator: solve for the
@@ -1099,47 +1111,64 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
       ok = ok && launch_project_null(ls->f, ls->dinv, n, ls->fpart, kFdmPartials,
                                      ls->fpart + 2 * ls->fpart_n + 4, cs) == cudaSuccess;
     ok = ok && cudaMemcpyAsync(ls->r, ls->f, sizeof(double) * n, cudaMemcpyDeviceToDevice, cs) == cudaSuccess;
+    // the tensor-core inverse reads r as TF32 hi/lo pairs: the first from f,
+    // the others from the residual kernel
+    if (prec == 1)
+      ok = ok && launch_tc_split(ls->f, op_gy(ls), op_gx(ls), op_gx(ls), ls->tcY[0], ls->tcY[1],
+                                 ls->tc_px, cs) == cudaSuccess;
     ok = ok && cudaMemsetAsync(ls->x, 0, sizeof(double) * n, cs) == cudaSuccess;
     ok = ok && launch_norms(ls->f, wv, n, nt == SE_NORM_NATURAL, ls->fpart, kFdmPartials, res, cs) == cudaSuccess;
-    ok = ok && launch_fdm_init(ls->d_fparams, ls->d_fstate, res, hc, cs) == cudaSuccess;
-    // the while-node, depending on the prologue
-    cudaGraphNode_t cn = nullptr;
-    cudaGraph_t body = nullptr;
-    if (ok) {
+    ok = ok && launch_fdm_init(ls->d_fparams, ls->d_fstate, res, hybrid ? hf : hc, cs) == cudaSuccess;
+    // a conditional node after what was captured so far, its body captured on
+    // stream bs by `fill`
+    std::vector<cudaGraph_t> bodies;
+    auto add_cond = [&](cudaGraphConditionalHandle h, cudaGraphConditionalNodeType type,
+                        const std::function<int()>& fill) {
+      if (!ok) return;
+      cudaGraphNode_t cn = nullptr;
       ok = cudaStreamGetCaptureInfo(cs, &status, nullptr, &cg, &deps, &ndeps) == cudaSuccess;
       cudaGraphNodeParams cp = {};
       cp.type = cudaGraphNodeTypeConditional;
-      cp.conditional.handle = hc;
-      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.handle = h;
+      cp.conditional.type = type;
       cp.conditional.size = 1;
       ok = ok && cudaGraphAddNode(&cn, cg, deps, ndeps, &cp) == cudaSuccess;
       ok = ok && cudaStreamUpdateCaptureDependencies(cs, &cn, 1, cudaStreamSetCaptureDependencies) == cudaSuccess;
-      if (ok) body = cp.conditional.phGraph_out[0];
-    }
-    // the loop body, captured on its own stream
-    if (ok) {
+      if (!ok) return;
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      bodies.push_back(body);
       g_stream = bs;
       ok = cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-      int brc = SE_OK;
       if (ok) {
-        brc = prec == 0   ? fdm_apply64(ls, ls->r, ls->x, true)
-              : prec == 1 ? fdm_apply_tc(ls, ls->r, ls->x)
-                          : fdm_apply_low(ls, ls->r, ls->x);
-        if (!brc && remove_null)
-          brc = launch_remove_mean(ls->x, n, ls->fpart, kFdmPartials, ls->fpart + 2 * ls->fpart_n + 4, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
-        // r = f - A x with the norm and the convergence test in one launch
-        if (!brc)
-          brc = launch_residual_check(ls->op, ls->x, ls->f, ls->r, wv, nt == SE_NORM_NATURAL,
-                                      ls->fpart, res, ls->d_rescount, ls->d_fparams,
-                                      ls->d_fstate, hc, bs) == cudaSuccess
-                    ? SE_OK
-                    : SE_ERR_CUDA;
+        const int brc = fill();
         cudaGraph_t bodyg = body;
         const bool ended = cudaStreamEndCapture(bs, &bodyg) == cudaSuccess;
         ok = ended && brc == SE_OK;
       }
       g_stream = cs;
-    }
+    };
+    // one refinement step: x += A^{-1} r with the given inverse, then r = f - A x
+    // with the norm and the convergence test (setting hc) in one launch, and
+    // the TF32 split of r when tensor-core steps follow
+    auto step = [&](int inv) -> int {
+      int brc = inv == 0   ? fdm_apply64(ls, ls->r, ls->x, true)
+                : inv == 1 ? fdm_apply_tc(ls, ls->r, ls->x, true)
+                           : fdm_apply_low(ls, ls->r, ls->x);
+      if (!brc && remove_null)
+        brc = launch_remove_mean(ls->x, n, ls->fpart, kFdmPartials, ls->fpart + 2 * ls->fpart_n + 4, bs) == cudaSuccess ? SE_OK : SE_ERR_CUDA;
+      const bool split = prec == 1 || prec == 3;
+      if (!brc)
+        brc = launch_residual_check(ls->op, ls->x, ls->f, ls->r, wv, nt == SE_NORM_NATURAL,
+                                    ls->fpart, res, ls->d_rescount, ls->d_fparams, ls->d_fstate,
+                                    hc, bs, split ? ls->tcY[0] : nullptr,
+                                    split ? ls->tcY[1] : nullptr, ls->tc_px) == cudaSuccess
+                  ? SE_OK
+                  : SE_ERR_CUDA;
+      return brc;
+    };
+    if (hybrid) add_cond(hf, cudaGraphCondTypeIf, [&]() { return step(0); });
+    add_cond(hc, cudaGraphCondTypeWhile, [&]() { return step(prec == 3 ? 1 : prec); });
+    cudaGraph_t body = bodies.empty() ? nullptr : bodies.back();
     // epilogue
     ok = ok && launch_update_field(ls->op, m, ls->x, ls->sol->vals, cs) == cudaSuccess;
     const bool ended = cudaStreamEndCapture(cs, &graph) == cudaSuccess;
@@ -1169,8 +1198,10 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
 // assembly through the field update) and the state read-back into pinned
 // memory. fdm_finish reads the state once the stream is done.
 int fdm_launch(se_linsys* ls, int remove_null) {
-  const int prec = ls->opts.precision == SE_PREC_FP64 ? 0 : (ls->opts.precision == SE_PREC_MIXED ? 1 : 2);
-  if (int rc = fdm_setup(ls, prec)) return rc;
+  // inverse kinds: 0 FP64, 1 TF32x3 tensor cores, 2 BF16, 3 FP64 first then 1
+  const int pr = ls->opts.precision;
+  const int prec = pr == SE_PREC_FP64 ? 0 : pr == SE_PREC_MIXED ? 1 : pr == SE_PREC_FP64_TC ? 3 : 2;
+  if (int rc = fdm_setup(ls, prec == 3 ? 1 : prec)) return rc;
   const int key = prec | ((remove_null != 0) << 2) | (ls->opts.norm_type << 3) | (ls->opts.mode << 6);
   if (!ls->fdm_exec || ls->fdm_key != key)
     if (int rc = fdm_build_graph(ls, prec, remove_null != 0)) return rc;
@@ -2061,7 +2092,8 @@ int check_opts(const se_solver_opts* o) {
     return fail(SE_ERR_ARG, "unknown method %d", o->method);
   if (o->precision == SE_PREC_FP16)
     return fail(SE_ERR_UNSUPPORTED, "SE_PREC_FP16 is an apply precision (se_linsys_apply_low) only");
-  if (o->precision != SE_PREC_FP64 && o->precision != SE_PREC_MIXED && o->precision != SE_PREC_BF16)
+  if (o->precision != SE_PREC_FP64 && o->precision != SE_PREC_MIXED && o->precision != SE_PREC_BF16 &&
+      o->precision != SE_PREC_FP64_TC)
     return fail(SE_ERR_ARG, "unknown precision %d", o->precision);
   if (o->precision != SE_PREC_FP64 && o->method != SE_METHOD_FDM)
     return fail(SE_ERR_UNSUPPORTED, "reduced precision needs SE_METHOD_FDM");

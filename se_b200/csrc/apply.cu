@@ -38,6 +38,7 @@
 #include <cstring>
 
 #include "common.cuh"
+#include "fdm_ctl.cuh"
 
 namespace seg {
 namespace {
@@ -643,11 +644,51 @@ struct EfTile {
 };
 constexpr int kEfThreads = 256, kEfWarps = kEfThreads / 32;
 
+// Stage the tile's vertices and its N-vertex halo to the left and below into
+// X (zero where a vertex is no unknown): warp w takes rows w, w + 8, ...;
+// lane l columns l, l + 32, l + 64; all copies issued before the wait.
+template <int N>
+__device__ __forceinline__ void ef_stage(const OpDev& op, const double* __restrict__ x, double* X,
+                                         int gx0, int gy0) {
+  typedef EfTile<N> T;
+  constexpr int SW = T::SW, W = T::W, H = T::H;
+  const Dir& dx = op.d[0];
+  const Dir& dy = op.d[1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int cu[3];
+#pragma unroll
+  for (int q = 0; q < 3; q++) {
+    const int i = lane + 32 * q;
+    cu[q] = i < SW ? unk(dx, gx0 - N + i) : -1;
+  }
+#pragma unroll
+  for (int r = 0; r < (H + kEfWarps - 1) / kEfWarps; r++) {
+    const int j = warp + kEfWarps * r;
+    if (j < H) {
+      const int uy = unk(dy, gy0 - N + j);
+      const double* rowp = x + (size_t)(uy < 0 ? 0 : uy) * op.G[0];
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const int i = lane + 32 * q;
+        if (i < SW) {
+          const bool ok = uy >= 0 && cu[q] >= 0;
+          const double* src = ok ? rowp + cu[q] : x;
+          const unsigned dst = (unsigned)__cvta_generic_to_shared(X + j * W + i);
+          asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src),
+                       "r"(ok ? 8 : 0));
+        }
+      }
+    }
+  }
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_group 0;\n" ::);
+}
+
 template <int N>
 __global__ void __launch_bounds__(kEfThreads, EfTile<N>::MINB)
     apply_ef_kernel(const OpDev op, const double* __restrict__ x, double* __restrict__ y) {
   typedef EfTile<N> T;
-  constexpr int SW = T::SW, W = T::W, OXP = T::OXP, TX = T::TX, TY = T::TY, H = T::H;
+  constexpr int W = T::W, OXP = T::OXP, TX = T::TX, TY = T::TY, H = T::H;
   extern __shared__ __align__(16) double efsm[];
   double* X = efsm;            // vertices (gx0-N .. gx0+TX) x (gy0-N .. gy0+TY)
   double* OX = X + H * W;      // x-pass results of the tile's vertices
@@ -655,37 +696,9 @@ __global__ void __launch_bounds__(kEfThreads, EfTile<N>::MINB)
   const Dir& dx = op.d[0];
   const Dir& dy = op.d[1];
   const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   if (tid <= N) sw[tid] = op.w[tid];
-  {  // staging: warp w takes rows w, w + 8, ...; lane l columns l, l + 32, l + 64
-    int cu[3];
-#pragma unroll
-    for (int q = 0; q < 3; q++) {
-      const int i = lane + 32 * q;
-      cu[q] = i < SW ? unk(dx, gx0 - N + i) : -1;
-    }
-#pragma unroll
-    for (int r = 0; r < (H + kEfWarps - 1) / kEfWarps; r++) {
-      const int j = warp + kEfWarps * r;
-      if (j < H) {
-        const int uy = unk(dy, gy0 - N + j);
-        const double* rowp = x + (size_t)(uy < 0 ? 0 : uy) * op.G[0];
-#pragma unroll
-        for (int q = 0; q < 3; q++) {
-          const int i = lane + 32 * q;
-          if (i < SW) {
-            const bool ok = uy >= 0 && cu[q] >= 0;
-            const double* src = ok ? rowp + cu[q] : x;
-            const unsigned dst = (unsigned)__cvta_generic_to_shared(X + j * W + i);
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(dst), "l"(src),
-                         "r"(ok ? 8 : 0));
-          }
-        }
-      }
-    }
-    asm volatile("cp.async.commit_group;\n" ::);
-    asm volatile("cp.async.wait_group 0;\n" ::);
-  }
+  ef_stage<N>(op, x, X, gx0, gy0);
   __syncthreads();
   constexpr int n = N + 1;
   if (tid < T::ITEMS) {  // x pass: thread = (element e, row r), rows of one element per warp run
@@ -792,7 +805,237 @@ cudaError_t launch_ef(const OpDev& op, const double* x, double* y, cudaStream_t 
   return cudaGetLastError();
 }
 
+// ------------------------------- refinement residual, orders 4 to 8 ----
+// r = b - A x on apply_ef_kernel's tile: the stiffness sums of both passes,
+// the combination and the subtraction in double-double (the stiffness rows
+// sum to zero, so the taps cancel and a plain FP64 sum loses the digits a
+// 1e-10 residual needs), rounded once. Per-block partial sums of (w r)^2 (or
+// r w r when natural) and r^2; the block that finishes last sums the
+// partials in block order and runs the FDM loop's convergence test (ResTail).
+// Optionally also writes r's TF32 hi/lo split for the tensor-core inverse.
+template <int N>
+__global__ void __launch_bounds__(kEfThreads, 2)
+    residual_ef_kernel(const OpDev op, const double* __restrict__ x, const double* __restrict__ b,
+                       double* __restrict__ rout, const double* __restrict__ wv, int natural,
+                       double* __restrict__ partial, const ResTail tail, float* __restrict__ sp_hi,
+                       float* __restrict__ sp_lo, int sp_pitch) {
+  typedef EfTile<N> T;
+  constexpr int W = T::W, OXP = T::OXP, TX = T::TX, TY = T::TY, H = T::H;
+  extern __shared__ __align__(16) double efsm[];
+  double* X = efsm;              // staged vertices
+  double* OXH = X + H * W;       // x-pass stiffness sums, high parts
+  double* OXL = OXH + TY * OXP;  // and low parts
+  double* sw = OXL + TY * OXP;
+  __shared__ double red[kEfWarps][2];
+  __shared__ unsigned last;
+  const Dir& dx = op.d[0];
+  const Dir& dy = op.d[1];
+  const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
+  const int tid = threadIdx.x;
+  if (tid <= N) sw[tid] = op.w[tid];
+  ef_stage<N>(op, x, X, gx0, gy0);
+  __syncthreads();
+  constexpr int n = N + 1;
+  if (tid < T::ITEMS) {  // x pass
+    const int r = tid % TY, e = tid / TY;
+    const int ex = gx0 / N + e;
+    const double* row = X + (r + N) * W + e * N;
+    double v[2 * N + 1];
+#pragma unroll
+    for (int k = 0; k <= 2 * N; k++) v[k] = row[k];
+    const bool own = ex < dx.nE, left = ex > 0 || dx.periodic;
+    double oh[N], ol[N];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      double hi = 0.0, lo = 0.0;
+      if (own) {
+#pragma unroll
+        for (int q = 0; q < n; q++) dd_fma(hi, lo, op.Kh[a * n + q], v[N + q]);
+      }
+      oh[a] = hi;
+      ol[a] = lo;
+    }
+    if (left) {
+      double hi = 0.0, lo = 0.0;
+#pragma unroll
+      for (int q = 0; q < n; q++) dd_fma(hi, lo, op.Kh[N * n + q], v[q]);
+      dd_add(oh[0], ol[0], hi);
+      ol[0] += lo;
+    }
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      OXH[r * OXP + e * N + a] = oh[a];
+      OXL[r * OXP + e * N + a] = ol[a];
+    }
+  }
+  __syncthreads();
+  double acc0 = 0.0, acc1 = 0.0;
+  if (tid < T::ITEMS) {  // y pass, the combination and the residual
+    const int c = tid % TX, e = tid / TX;
+    const int ey = gy0 / N + e;
+    const int gx = gx0 + c;
+    const double* col = X + (e * N) * W + c + N;
+    double v[2 * N + 1];
+#pragma unroll
+    for (int k = 0; k <= 2 * N; k++) v[k] = col[k * W];
+    const bool own = ey < dy.nE, left = ey > 0 || dy.periodic;
+    double yh[N], yl[N];
+#pragma unroll
+    for (int a = 0; a < N; a++) {
+      double hi = 0.0, lo = 0.0;
+      if (own) {
+#pragma unroll
+        for (int q = 0; q < n; q++) dd_fma(hi, lo, op.Kh[a * n + q], v[N + q]);
+      }
+      yh[a] = hi;
+      yl[a] = lo;
+    }
+    if (left) {
+      double hi = 0.0, lo = 0.0;
+#pragma unroll
+      for (int q = 0; q < n; q++) dd_fma(hi, lo, op.Kh[N * n + q], v[q]);
+      dd_add(yh[0], yl[0], hi);
+      yl[0] += lo;
+    }
+    if (gx >= dx.lo && gx < dx.hi) {
+      const double wx = wsum<N>(dx, sw, gx / N, gx % N);
+      const double w0 = (own ? op.w[0] : 0.0) + (left ? op.w[N] : 0.0);
+      const int gyb = gy0 + e * N;
+      const size_t ux = (size_t)(gx - dx.lo);
+#pragma unroll
+      for (int a = 0; a < N; a++) {
+        const int gy = gyb + a;
+        if (gy < dy.lo || gy >= dy.hi) continue;
+        const double wy = a == 0 ? w0 : op.w[a];
+        const size_t k = (size_t)(gy - dy.lo) * op.G[0] + ux;
+        const double cm = -op.alpha * wx * wy, cx = -op.beta[0] * wy, cy = -op.beta[1] * wx;
+        double hi = b[k], lo = 0.0;
+        dd_fma(hi, lo, cm, v[N + a]);
+        dd_fma(hi, lo, cx, OXH[(e * N + a) * OXP + c]);
+        lo = fma(cx, OXL[(e * N + a) * OXP + c], lo);
+        dd_fma(hi, lo, cy, yh[a]);
+        lo = fma(cy, yl[a], lo);
+        const double rv = hi + lo;
+        rout[k] = rv;
+        const double z = wv ? rv * wv[k] : rv;
+        acc0 += natural ? z * rv : z * z;
+        acc1 += rv * rv;
+        if (sp_hi) {
+          uint32_t h;
+          asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"((float)rv));
+          const float fh = __uint_as_float(h);
+          const size_t o = (size_t)(gy - dy.lo) * sp_pitch + ux;
+          sp_hi[o] = fh;
+          sp_lo[o] = (float)(rv - (double)fh);
+        }
+      }
+    }
+  }
+  // block sums in a fixed order
+  const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    acc0 += __shfl_down_sync(0xffffffffu, acc0, o);
+    acc1 += __shfl_down_sync(0xffffffffu, acc1, o);
+  }
+  if (lane == 0) {
+    red[warp][0] = acc0;
+    red[warp][1] = acc1;
+  }
+  __syncthreads();
+  const unsigned blk = blockIdx.y * gridDim.x + blockIdx.x, nb = gridDim.x * gridDim.y;
+  if (tid == 0) {
+    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+    for (int q = 0; q < kEfWarps; q++) {
+      s0 += red[q][0];
+      s1 += red[q][1];
+    }
+    partial[2 * blk] = s0;
+    partial[2 * blk + 1] = s1;
+  }
+  if (!tail.count) return;
+  // the last block to finish sums the partials in block order and runs the
+  // refinement step's convergence test (no block waits for another)
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) last = atomicAdd(tail.count, 1u) == nb - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double s0 = 0.0, s1 = 0.0;
+  for (unsigned k = tid; k < nb; k += kEfThreads) {
+    s0 += __ldcg(partial + 2 * k);
+    s1 += __ldcg(partial + 2 * k + 1);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_down_sync(0xffffffffu, s0, o);
+    s1 += __shfl_down_sync(0xffffffffu, s1, o);
+  }
+  __syncthreads();
+  if (lane == 0) {
+    red[warp][0] = s0;
+    red[warp][1] = s1;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double t0 = 0.0, t1 = 0.0;
+#pragma unroll
+    for (int q = 0; q < kEfWarps; q++) {
+      t0 += red[q][0];
+      t1 += red[q][1];
+    }
+    tail.res[0] = t0;
+    tail.res[1] = t1;
+    *tail.count = 0u;
+    fdm_check_state(tail.p, tail.st, t0, tail.h);
+  }
+}
+
+template <int N>
+cudaError_t launch_res_ef(const OpDev& op, const double* x, const double* b, double* r,
+                          const double* w, int natural, double* partial, const ResTail& tail,
+                          float* sh, float* sl, int sp, cudaStream_t s) {
+  typedef EfTile<N> T;
+  constexpr size_t smem = sizeof(double) * ((size_t)T::H * T::W + 2 * (size_t)T::TY * T::OXP + 16);
+  if (smem > 48 * 1024) {
+    static bool attr[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (!attr[dev]) {
+      e = cudaFuncSetAttribute(residual_ef_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem);
+      if (e != cudaSuccess) return e;
+      attr[dev] = true;
+    }
+  }
+  const dim3 grid((op.d[0].hi + T::TX - 1) / T::TX, (op.d[1].hi + T::TY - 1) / T::TY);
+  residual_ef_kernel<N><<<grid, kEfThreads, smem, s>>>(op, x, b, r, w, natural, partial, tail, sh,
+                                                       sl, sp);
+  return cudaGetLastError();
+}
+
 }  // namespace
+
+bool residual_ef_supported(const OpDev& op) {
+  return op.gamma == 0.0 && op.d[0].N >= 4 && op.d[0].N <= 8;
+}
+
+cudaError_t launch_residual_ef(const OpDev& op, const double* x, const double* b, double* r,
+                               const double* w, int natural, double* partial, const ResTail& tail,
+                               float* split_hi, float* split_lo, int split_pitch, cudaStream_t s) {
+  if (!residual_ef_supported(op) || !b || !partial) return cudaErrorInvalidValue;
+  switch (op.d[0].N) {
+    case 4: return launch_res_ef<4>(op, x, b, r, w, natural, partial, tail, split_hi, split_lo, split_pitch, s);
+    case 5: return launch_res_ef<5>(op, x, b, r, w, natural, partial, tail, split_hi, split_lo, split_pitch, s);
+    case 6: return launch_res_ef<6>(op, x, b, r, w, natural, partial, tail, split_hi, split_lo, split_pitch, s);
+    case 7: return launch_res_ef<7>(op, x, b, r, w, natural, partial, tail, split_hi, split_lo, split_pitch, s);
+    default: return launch_res_ef<8>(op, x, b, r, w, natural, partial, tail, split_hi, split_lo, split_pitch, s);
+  }
+}
 
 #define SE_APPLY_N(n) \
   case n:             \

@@ -677,27 +677,6 @@ __global__ void __launch_bounds__(kCgThreads, 1) cg_n_kernel(const CgBatch B) {
 
 
 // ------------------------------------------- extended-precision residual --
-// Error-free transformations (Knuth TwoSum; TwoProd with an FMA): the pair
-// (hi, lo) carries a value to about twice double precision.
-// The _rn intrinsics keep each operation a single IEEE operation: the
-// compiler must not fuse a product into a following sum here.
-__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
-  s = __dadd_rn(a, b);
-  const double bb = __dsub_rn(s, a);
-  e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
-}
-__device__ __forceinline__ void dd_add(double& hi, double& lo, double x) {
-  double s, e;
-  two_sum(hi, x, s, e);
-  hi = s;
-  lo += e;
-}
-__device__ __forceinline__ void dd_fma(double& hi, double& lo, double a, double b) {
-  const double p = __dmul_rn(a, b);
-  const double pe = fma(a, b, -p);  // exact: a*b - p
-  dd_add(hi, lo, p);
-  lo += pe;
-}
 // krow_n in double-double: the stiffness rows sum to zero, so the taps cancel
 // and a plain FP64 sum loses the digits a 1e-10 residual needs.
 template <int N, int STRIDE>
@@ -748,15 +727,8 @@ __device__ __forceinline__ double residual_dd(const OpSm& o, const double* P, in
 // ------------------------------------------- standalone apply / residual --
 // y = A x, or with b: r = b - A x (extended precision) with per-block partial sums of
 // (w r)^2 (or r w r when natural) and r^2 (w = Jacobi inverse, nullptr: 1).
-// Tail of the FDM refinement step fused into the residual launch (count ==
-// nullptr: none).
-struct ResTail {
-  double* res;
-  unsigned* count;
-  const FdmParams* p;
-  FdmState* st;
-  cudaGraphConditionalHandle h;
-};
+// Tail of the FDM refinement step fused into the residual launch (ResTail,
+// count == nullptr: none).
 
 template <int N>
 __global__ void __launch_bounds__(kCgThreads) apply_kernel(const OpDev op, const double* __restrict__ x,
@@ -896,9 +868,18 @@ cudaError_t launch_residual(const OpDev& op, const double* x, const double* b, d
 cudaError_t launch_residual_check(const OpDev& op, const double* x, const double* b, double* r,
                                   const double* w, int natural, double* partial, double* res,
                                   unsigned* count, const FdmParams* p, FdmState* st,
-                                  cudaGraphConditionalHandle h, cudaStream_t s) {
+                                  cudaGraphConditionalHandle h, cudaStream_t s, float* split_hi,
+                                  float* split_lo, int split_pitch) {
   if (!partial || !count) return cudaErrorInvalidValue;
   const ResTail tail{res, count, p, st, h};
+  if (residual_ef_supported(op))
+    return launch_residual_ef(op, x, b, r, w, natural, partial, tail, split_hi, split_lo,
+                              split_pitch, s);
+  if (split_hi) {  // the general kernel, then the split
+    cudaError_t e = residual_any(op, x, b, r, w, natural, partial, tail, s);
+    if (e != cudaSuccess) return e;
+    return launch_tc_split(r, op.G[1], op.G[0], op.G[0], split_hi, split_lo, split_pitch, s);
+  }
   return residual_any(op, x, b, r, w, natural, partial, tail, s);
 }
 

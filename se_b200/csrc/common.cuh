@@ -77,6 +77,28 @@ __device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a,
 __device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double xdiv(double a, double b) { return __ddiv_rn(a, b); }
 
+// ---- double-double arithmetic (error-free transformations: Knuth's TwoSum;
+// TwoProd with an FMA): a pair (hi, lo) carries a value to about twice double
+// precision. The _rn intrinsics keep each operation one IEEE operation (the
+// compiler must not fuse a product into a following sum here).
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+}
+__device__ __forceinline__ void dd_add(double& hi, double& lo, double x) {
+  double s, e;
+  two_sum(hi, x, s, e);
+  hi = s;
+  lo += e;
+}
+__device__ __forceinline__ void dd_fma(double& hi, double& lo, double a, double b) {
+  const double p = __dmul_rn(a, b);
+  const double pe = fma(a, b, -p);  // exact: a*b - p
+  dd_add(hi, lo, p);
+  lo += pe;
+}
+
 // ---------------------------------------------------------------------------
 // Host launch wrappers (defined in sl.cu / linsys.cu). All take the stream.
 
@@ -146,12 +168,29 @@ cudaError_t launch_residual(const OpDev& op, const double* x, const double* b, d
 // that finishes last (arrival counter *count, zero between launches) sums
 // the partials in block order into res[0..1], runs the convergence test on
 // the loop state and sets the loop's while-condition h.
+// split_hi/split_lo (nullable): also write r's TF32 hi/lo split, rows of
+// split_pitch FP32 (the tensor-core inverse's input).
 struct FdmParams;
 struct FdmState;
+struct ResTail {
+  double* res;
+  unsigned* count;
+  const FdmParams* p;
+  FdmState* st;
+  cudaGraphConditionalHandle h;
+};
 cudaError_t launch_residual_check(const OpDev& op, const double* x, const double* b, double* r,
                                   const double* w, int natural, double* partial, double* res,
                                   unsigned* count, const FdmParams* p, FdmState* st,
-                                  cudaGraphConditionalHandle h, cudaStream_t s);
+                                  cudaGraphConditionalHandle h, cudaStream_t s,
+                                  float* split_hi = nullptr, float* split_lo = nullptr,
+                                  int split_pitch = 0);
+// The element-factored residual of orders 4 to 8 without an SVV term
+// (apply.cu); false when the operator needs the general kernel.
+bool residual_ef_supported(const OpDev& op);
+cudaError_t launch_residual_ef(const OpDev& op, const double* x, const double* b, double* r,
+                               const double* w, int natural, double* partial, const ResTail& tail,
+                               float* split_hi, float* split_lo, int split_pitch, cudaStream_t s);
 int residual_blocks(const OpDev& op);
 cudaError_t launch_op_diag(const OpDev& op, double* d, cudaStream_t s);
 // f = Mass*rhs over the unknowns (FieldRHS + Vector::Assemble), plus lift.

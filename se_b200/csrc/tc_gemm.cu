@@ -254,10 +254,6 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   tc_fence_before();
-  // every CTA's barriers must be initialised before any peer copies into
-  // them: arrive now, wait just before the exchange (the loads and MMAs run
-  // in between)
-  if (CK > 1) asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
@@ -305,6 +301,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 
   // the partial accumulator into shared memory (over the drained ring)
   const bool ready = mbar_wait(done, 0);
+  // peers may copy into this CTA's receive slots (over its ring) once every
+  // CTA of the cluster has passed this point: arrive now, wait just before
+  // the copies (the arrival also publishes the barrier initialisation)
+  if (CK > 1) asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
   tc_fence_after();
   if (!ready) atomicOr(e.err, (unsigned)KERR_BARRIER_TIMEOUT);
   __syncthreads();  // the issuers' flags are visible past this barrier

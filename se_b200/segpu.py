@@ -42,7 +42,7 @@ SE_ERR_DOMAIN = -7
 
 NORM_PRECONDITIONED, NORM_UNPRECONDITIONED, NORM_NATURAL = 0, 1, 2
 MODE_REFERENCE, MODE_EXACT = 0, 1
-PREC_FP64, PREC_MIXED, PREC_BF16, PREC_FP16 = 0, 1, 2, 3
+PREC_FP64, PREC_MIXED, PREC_BF16, PREC_FP16, PREC_FP64_TC = 0, 1, 2, 3, 4
 METHOD_CG, METHOD_FDM = 0, 1
 
 KSP_REASONS = {2: "CONVERGED_RTOL", 3: "CONVERGED_ATOL", -3: "DIVERGED_ITS",

@@ -4,10 +4,12 @@
 //   shim_main cpu   options parsing and a Mesh (host tables), then a Field,
 //                   which must fail loudly without a CUDA device (no CPU
 //                   fallback)
-//   shim_main gpu   (lap - 1) u = f on an 8x8, p=6 doubly periodic mesh
-//                   through Mesh, BCs, Field, Advector and HelmholtzEqn;
-//                   prints the iteration count and the solution values
-#include <cmath>
+//   shim_main gpu <fields>   (lap - 1) u = f on an 8x8, p=6 doubly periodic
+//                   mesh through Mesh, BCs, Field, Advector and
+//                   HelmholtzEqn, with the tracer and the velocity read from
+//                   <fields> (raw doubles: nVertsTotal tracer values, then
+//                   nVertsTotal velocity pairs); prints the iteration count
+//                   and the solution values
 #include <cstdio>
 #include <cstring>
 
@@ -31,22 +33,20 @@ static int cpu_case() {
   return 0;
 }
 
-static int gpu_case() {
+static int gpu_case(const char* fields) {
   int nEls[2] = {8, 8};
   double lo[2] = {0.0, 0.0}, hi[2] = {1.0, 1.0};
   bool per[2] = {true, true};
   Mesh m("m", nEls, "legendre", 6, lo, hi, per);
-  std::vector<double> xy((size_t)m.nVertsTotal * 2);
-  se_ok(se_mesh_verts(m.h, xy.data()));
   BCs bcs(false, false, false, false, &m);
   Field phi("phi", &m, 1, &bcs), vel("vel", &m, 2, nullptr), u("u", &m, 1, &bcs);
-  const double pi = 3.14159265358979323846;
-  for (int i = 0; i < m.nVertsTotal; i++) {
-    const double x = xy[2 * i], y = xy[2 * i + 1];
-    phi.vals[i][0] = std::exp(-((x - 0.3) * (x - 0.3) + (y - 0.6) * (y - 0.6)) / 0.0025);
-    vel.vals[i][0] = -std::sin(pi * x) * std::sin(pi * x) * std::sin(2 * pi * y);
-    vel.vals[i][1] = std::sin(pi * y) * std::sin(pi * y) * std::sin(2 * pi * x);
-  }
+  std::FILE* fp = std::fopen(fields, "rb");
+  if (!fp) return 2;
+  const size_t nv = (size_t)m.nVertsTotal;
+  const bool got = std::fread(phi.host.data(), sizeof(double), nv, fp) == nv &&
+                   std::fread(vel.host.data(), sizeof(double), 2 * nv, fp) == 2 * nv;
+  std::fclose(fp);
+  if (!got) return 3;
   phi.Upload();
   vel.Upload();
   Advector adv(&phi, &vel);
@@ -62,6 +62,6 @@ static int gpu_case() {
 }
 
 int main(int argc, char** argv) {
-  if (argc > 1 && std::strcmp(argv[1], "gpu") == 0) return gpu_case();
+  if (argc > 2 && std::strcmp(argv[1], "gpu") == 0) return gpu_case(argv[2]);
   return cpu_case();
 }

@@ -52,7 +52,7 @@ def bench_step(oracle):
     return {"B": B, "phi": phi, "vel": vel, "dt": dt, "sl": sl, "u": u, "its10": st10["its"]}
 
 
-@pytest.mark.parametrize("variant", ["fdm_fp64", "fdm_tf32x3_tc", "cg_fp64"])
+@pytest.mark.parametrize("variant", ["fdm_fp64", "fdm_tf32x3_tc", "fdm_fp64_then_tc", "cg_fp64"])
 def test_bench_step_matches_oracle(segpu, bench_step, variant):
     S, h = segpu, bench_step
     B = h["B"]
