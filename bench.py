@@ -717,6 +717,7 @@ def run_config2(steps=20, seed=5):
     stream = torch.cuda.Stream()
     S.set_stream(stream.cuda_stream)
     for name, method, prec, n in (("fdm_fp64", S.METHOD_FDM, S.PREC_FP64, steps),
+                                  ("fdm_fp64_then_tc", S.METHOD_FDM, S.PREC_FP64_TC, steps),
                                   ("fdm_tf32x3_tc_refined_fp64", S.METHOD_FDM, S.PREC_MIXED, steps),
                                   ("cg_fp64", S.METHOD_CG, S.PREC_FP64, max(2, steps // 10))):
         f = [S.Field(nm, m, 1, bc if nm.startswith("psi") else None)
@@ -761,6 +762,7 @@ def run_ensemble(count=256, seed=2024):
     out = {"workload": "256 solves, n x n elements n~U{8..64}, p~U{4,6,8}, lambda~logU[1e-2,1e2], "
                        "8-mode RHS, rtol 1e-10"}
     for name, method, prec in (("fdm_fp64", S.METHOD_FDM, S.PREC_FP64),
+                               ("fdm_fp64_then_tc", S.METHOD_FDM, S.PREC_FP64_TC),
                                ("fdm_tf32x3_tc_refined_fp64", S.METHOD_FDM, S.PREC_MIXED),
                                ("cg_fp64", S.METHOD_CG, S.PREC_FP64)):
         systems = []
@@ -801,19 +803,21 @@ def run_ensemble(count=256, seed=2024):
 
 
 # ------------------------------------------------------- serving (config 4) --
-def run_serving(seconds=2.0, seed=77, load=0.7):
-    """Serving through the continuous-batching server (se_server_*): half
-    Helmholtz solves (lambda = 1, rtol 1e-10, FDM) and half 10-step
+def run_serving(seconds=2.0, seed=77, rate=2000.0):
+    """Serving through the continuous-batching server (se_server_*), the
+    configured workload: a Poisson stream of `rate` requests/s (2,000),
+    half Helmholtz solves (lambda = 1, rtol 1e-10, FDM) and half 10-step
     first-order SL jobs (Courant 1), on n x n element doubly periodic meshes
-    with n in {8, 16, 32, 64, 128} and p uniform in 4..8. Every
-    configuration is warmed once. The client holds page-locked inputs and a
-    pool of page-locked result buffers per configuration (a result buffer is
-    reused once its result was collected; submission waits for a free one).
+    with n in {8, 16, 32, 64, 128} and p uniform in 4..8. Every configuration
+    is warmed once (its 1-D eigendecompositions and solve graph are made
+    then, not on the request path). The client holds page-locked inputs and a
+    pool of page-locked result buffers with prebuilt request structures per
+    configuration (a buffer is reused once its result was collected).
 
-    Two phases per precision: (1) capacity, the whole request stream
+    Two phases per solver precision: (1) capacity, the whole request stream
     submitted as fast as the pools allow; (2) latency, Poisson arrivals at
-    `load` x capacity for `seconds`, with p50/p99 from submission to result.
-    DOF-updates: Helmholtz unknowns; SL vertices x steps."""
+    `rate` for `seconds`, with p50/p99 from submission to result (the
+    server's clock). DOF-updates: Helmholtz unknowns; SL vertices x steps."""
     import queue
     import threading
 
@@ -854,25 +858,26 @@ def run_serving(seconds=2.0, seed=77, load=0.7):
         ps = rng.choice(orders, size=n_req)
         return [(int(k), int(n), int(p)) for k, n, p in zip(kinds, ns, ps)]
 
-    def serve(srv, opts, reqs, gaps, pools, cv):
+    def serve(srv, reqs, gaps, pools, cv):
         """Submit reqs (after gaps; None: back to back) and collect them in
         submission order on a second thread."""
         pending = queue.Queue()
         lat, fails = [], {}
 
         def collect():
+            res = S.segpu.Result()
             while True:
                 item = pending.get()
                 if item is None:
                     return
-                t, key, buf = item
-                _, res = srv.wait(t)
-                lat.append(res["latency_ms"])
-                if res["status"] != 0 or res["reason"] < 0:
-                    tag = f"status={res['status']} reason={res['reason']}: {res['error']}"
+                t, key, slot = item
+                srv.wait_request(t, res)
+                lat.append(res.latency_ms)
+                if res.status != 0 or res.reason < 0:
+                    tag = f"status={res.status} reason={res.reason}: {res.error.decode()}"
                     fails[tag] = fails.get(tag, 0) + 1
                 with cv:
-                    pools[key].append(buf)
+                    pools[key].append(slot)
                     cv.notify_all()
 
         th = threading.Thread(target=collect)
@@ -885,15 +890,12 @@ def run_serving(seconds=2.0, seed=77, load=0.7):
                 due += gaps[i]
                 while time.perf_counter() < due:
                     pass
-            f, aux, dt, d = inp(*key)
             with cv:
                 while not pools[key]:
                     cv.wait()
-                buf = pools[key].pop()
-            t = srv.submit(key[0], (key[1], key[1]), key[2], (0, 0), (1, 1), (1, 1), f, aux,
-                           opts=opts, c=-1.0, nu=-1.0, dt=1.0, steps=10, sl_dt=dt, out=buf.numpy())
-            pending.put((t, key, buf))
-            dofs += d
+                slot = pools[key].pop()
+            pending.put((srv.submit_request(slot[1]), key, slot))
+            dofs += inputs[key][3]
         pending.put(None)
         th.join()
         wall = time.perf_counter() - t0
@@ -904,31 +906,38 @@ def run_serving(seconds=2.0, seed=77, load=0.7):
     keys = sorted({(k, n, p) for k in (0, 1) for n in sizes for p in orders})
     for key in keys:
         inp(*key)
-    out = {"workload": "Helmholtz (FDM, rtol 1e-10) and 10-step SL requests, n x n elements "
-                       "n in {8,16,32,64,128}, p in 4..8, page-locked client buffers",
-           "load": load}
+    out = {"workload": "Poisson arrivals, mean 2,000 req/s: Helmholtz (FDM, rtol 1e-10) and 10-step "
+                       "SL requests, n x n elements n in {8,16,32,64,128}, p in 4..8, page-locked "
+                       "client buffers", "offered_req_per_s": rate}
     cap_reqs = stream(4000)
-    for label, prec in (("fp64", S.PREC_FP64), ("tf32x3_tc_refined_fp64", S.PREC_MIXED)):
+    n_req = int(rate * seconds)
+    lat_reqs = stream(n_req)
+    gaps = rng.exponential(1.0 / rate, size=n_req)
+    for label, prec in (("fp64", S.PREC_FP64), ("fp64_then_tc", S.PREC_FP64_TC),
+                        ("tf32x3_tc", S.PREC_MIXED)):
         opts = S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=S.METHOD_FDM, precision=prec)
         srv = S.Server(slots=16, device_gib=60.0)
         cv = threading.Condition()
-        pools = {key: [torch.empty((key[1] * key[2] + 1) ** 2, dtype=torch.float64, pin_memory=True)
-                       for _ in range(8)] for key in keys}
-        for key in keys:  # warm every configuration
+        pools = {}
+        for key in keys:
             f, aux, dt, _ = inp(*key)
-            srv.wait(srv.submit(key[0], (key[1], key[1]), key[2], (0, 0), (1, 1), (1, 1), f, aux,
-                                opts=opts, c=-1.0, nu=-1.0, dt=1.0, steps=10, sl_dt=dt))
-        cap = serve(srv, opts, cap_reqs, None, pools, cv)
-        rate = load * cap["req_per_s"]
-        n_req = int(rate * seconds)
-        lat_reqs = stream(n_req)
-        gaps = rng.exponential(1.0 / rate, size=n_req)
-        lat = serve(srv, opts, lat_reqs, gaps, pools, cv)
+            pools[key] = []
+            for _ in range(8):
+                buf = torch.empty((key[1] * key[2] + 1) ** 2, dtype=torch.float64, pin_memory=True)
+                req = srv.request(key[0], (key[1], key[1]), key[2], (0, 0), (1, 1), (1, 1), f, aux,
+                                  opts=opts, c=-1.0, nu=-1.0, dt=1.0, steps=10, sl_dt=dt,
+                                  out=buf.numpy())
+                pools[key].append((buf, req))
+            # warm the configuration: instance, eigendecompositions, solve graph
+            srv.wait_request(srv.submit_request(pools[key][0][1]))
+        cap = serve(srv, cap_reqs, None, pools, cv)
+        lat = serve(srv, lat_reqs, gaps, pools, cv)
         srv.close()
         del pools
         out[label] = {"capacity_req_per_s": cap["req_per_s"],
                       "capacity_dof_updates_per_s": cap["dof_updates_per_s"],
                       "offered_req_per_s": rate, "req_per_s": lat["req_per_s"],
+                      "dof_updates_per_s": lat["dof_updates_per_s"],
                       "p50_ms": lat["p50_ms"], "p99_ms": lat["p99_ms"],
                       "failed": cap["failed"] + lat["failed"],
                       "failures": {**cap["failures"], **lat["failures"]}}

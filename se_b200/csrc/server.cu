@@ -25,6 +25,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/segpu.h"
@@ -65,6 +66,7 @@ void release(Instance* in) {
 struct Job {
   long long ticket = 0;
   se_request req;
+  std::string key;  // configuration key, formed by the submitting thread
   double t_submit = 0, t_admit = 0, t_done = 0;
   Instance* inst = nullptr;
   int slot = -1;
@@ -75,13 +77,22 @@ struct Job {
 
 // Page-locked host memory can be the source or destination of an
 // asynchronous copy directly; other memory goes through the slot's staging.
+// The answer is cached per address (clients reuse their buffers); a stale
+// entry only changes the copy path, not the result: pageable memory given to
+// an asynchronous copy is copied synchronously by the runtime.
 bool pinned(const void* p) {
+  static thread_local std::unordered_map<const void*, bool> cache;
+  auto it = cache.find(p);
+  if (it != cache.end()) return it->second;
   cudaPointerAttributes at;
-  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+  bool pin = false;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess)
     cudaGetLastError();
-    return false;
-  }
-  return at.type == cudaMemoryTypeHost;
+  else
+    pin = at.type == cudaMemoryTypeHost;
+  if (cache.size() > 4096) cache.clear();
+  cache[p] = pin;
+  return pin;
 }
 
 struct Slot {
@@ -171,9 +182,9 @@ int create(se_server* S, const se_request& r, Instance** out) {
 // A free instance for the request, creating one (after releasing least
 // recently used free instances) if the budget allows. Returns SE_OK with
 // *out == nullptr when the request must wait for memory.
-int acquire(se_server* S, const se_request& r, Instance** out) {
+int acquire(se_server* S, const se_request& r, const std::string& key, Instance** out) {
   *out = nullptr;
-  auto& lst = S->pool[key_of(r)];
+  auto& lst = S->pool[key];
   for (Instance* in : lst)
     if (!in->busy) {
       *out = in;
@@ -326,7 +337,7 @@ void worker_loop(se_server* S) {
       Job* j = S->queue.front();
       Instance* in = nullptr;
       lk.unlock();
-      int rc = acquire(S, j->req, &in);
+      int rc = acquire(S, j->req, j->key, &in);
       lk.lock();
       if (rc) {
         S->queue.pop_front();
@@ -402,6 +413,7 @@ int se_server_submit(se_server* S, const se_request* req, long long* ticket) {
   if (req->kind == SE_REQ_ADVECT && (!req->aux || req->steps < 0)) return SE_ERR_ARG;
   Job* j = new Job();
   j->req = *req;
+  j->key = key_of(*req);
   std::memset(&j->res, 0, sizeof(j->res));
   j->t_submit = now_ms();
   {

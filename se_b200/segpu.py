@@ -612,6 +612,45 @@ class Server:
         self._keep[t.value] = (fin, fa, out, r)
         return t.value
 
+    def request(self, kind, nEls, N, lo, hi, periodic, field_in, aux=None, bcs=(0, 0, 0, 0),
+                c=-1.0, nu=-1.0, dt=1.0, poisson=False, opts=None, steps=0, sl_dt=0.0, out=None):
+        """A reusable request structure for submit_request(): the arrays are
+        referenced, not copied, and must stay alive (and in place) while any
+        request made from it is in flight."""
+        r = Request()
+        r.kind = kind
+        r.nEls[:] = [int(nEls[0]), int(nEls[1])]
+        r.N = int(N)
+        r.min[:] = [float(lo[0]), float(lo[1])]
+        r.max[:] = [float(hi[0]), float(hi[1])]
+        r.periodic[:] = [int(bool(periodic[0])), int(bool(periodic[1]))]
+        r.bcs[:] = [int(bool(b)) for b in bcs]
+        r.c, r.nu, r.dt, r.poisson = float(c), float(nu), float(dt), int(bool(poisson))
+        r.opts = opts if opts is not None else solver_opts(rtol=1e-10, mode=MODE_EXACT,
+                                                           method=METHOD_FDM)
+        r.steps, r.sl_dt = int(steps), float(sl_dt)
+        r.in_ = field_in.ctypes.data
+        r.aux = None if aux is None else aux.ctypes.data
+        r.out = out.ctypes.data
+        return r
+
+    def submit_request(self, r):
+        """Queue a request made by request(); returns its ticket."""
+        t = ctypes.c_longlong()
+        rc = _lib.se_server_submit(self._h, ctypes.byref(r), ctypes.byref(t))
+        if rc:
+            raise SEError(rc, "se_server_submit failed")
+        return t.value
+
+    def wait_request(self, ticket, res=None):
+        """Wait for a request queued by submit_request(); returns the filled
+        Result structure (res, if given, is reused)."""
+        res = res if res is not None else Result()
+        rc = _lib.se_server_wait(self._h, ctypes.c_longlong(ticket), ctypes.byref(res))
+        if rc:
+            raise SEError(rc, "se_server_wait failed")
+        return res
+
     def wait(self, ticket):
         res = Result()
         rc = _lib.se_server_wait(self._h, ctypes.c_longlong(ticket), ctypes.byref(res))

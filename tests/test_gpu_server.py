@@ -82,3 +82,45 @@ def test_admission_with_few_slots_and_a_tiny_budget(segpu):
     for (a, _), (b, _) in zip(outs[: len(reqs)], outs[len(reqs):]):
         assert np.array_equal(a, b)
     srv.close()
+
+
+@pytest.mark.parametrize("prec", ["PREC_MIXED", "PREC_FP64_TC"])
+def test_mixed_precision_results_same_alone_and_in_mix(segpu, prec):
+    """The tensor-core solve precisions through the lean request path
+    (request / submit_request / wait_request, the serving benchmark's
+    client): each Helmholtz result is bit-identical alone and in a shuffled
+    concurrent mix, and within 1e-9 of the FP64 solve."""
+    S = segpu
+    opts = S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=S.METHOD_FDM,
+                         precision=getattr(S, prec))
+    srv = S.Server(slots=4, device_gib=8.0)
+    reqs = [r for r in requests(S) if r["kind"] == S.REQ_HELMHOLTZ]
+    built = []
+    for r in reqs:
+        f = np.ascontiguousarray(r["field_in"], dtype=np.float64)
+        aux = None if r["aux"] is None else np.ascontiguousarray(r["aux"], dtype=np.float64)
+        outs = [np.zeros(len(f)) for _ in range(4)]
+        reqs_k = [srv.request(r["kind"], r["nEls"], r["N"], r["lo"], r["hi"], r["periodic"], f,
+                              aux, bcs=r["bcs"], c=r["c"], nu=r["nu"], dt=r["dt"], opts=opts,
+                              out=o) for o in outs]
+        built.append((f, aux, outs, reqs_k))
+    alone = []
+    for f, aux, outs, rk in built:
+        res = srv.wait_request(srv.submit_request(rk[0]))
+        assert res.status == 0 and res.reason == 2
+        alone.append(outs[0].copy())
+    order = [(k, c) for k in range(len(built)) for c in range(1, 4)]
+    np.random.default_rng(3).shuffle(order)
+    tickets = [(k, c, srv.submit_request(built[k][3][c])) for k, c in order]
+    for k, c, t in tickets:
+        res = srv.wait_request(t)
+        assert res.status == 0 and res.reason == 2
+        assert np.array_equal(built[k][2][c], alone[k])
+    srv.close()
+    # against the FP64 solve of the same systems
+    fp = S.Server(slots=2, device_gib=8.0)
+    for r, got in zip(reqs, alone):
+        out, res = fp.wait(fp.submit(**r))
+        assert res["status"] == 0
+        assert np.abs(out - got).max() <= 1e-9 * np.abs(out).max()
+    fp.close()
