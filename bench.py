@@ -314,7 +314,27 @@ def run_gpu(args, rank, world):
             e1.record(stream)
             torch.cuda.synchronize()
             fdm_ms.append(e0.elapsed_time(e1))
-        del helm, rr, xx
+        # the same transform on the tcgen05 tensor cores (TF32 hi/lo split of r,
+        # then four tc_product_kernel launches) and the refinement residual
+        # r = b - A x in double-double (residual_ef_kernel), alone
+        bb = torch.randn(ngf, dtype=torch.float64, device="cuda")
+        for _ in range(3):
+            helm.fdm_apply(rr.data_ptr(), xx.data_ptr(), S.PREC_MIXED)
+            helm.residual(rr.data_ptr(), bb.data_ptr(), xx.data_ptr())
+        tc_ms, res_ms = [], []
+        for _ in range(max(5, min(args.steps, 20))):
+            for fn, acc in ((lambda: helm.fdm_apply(rr.data_ptr(), xx.data_ptr(), S.PREC_MIXED),
+                             tc_ms),
+                            (lambda: helm.residual(rr.data_ptr(), bb.data_ptr(), xx.data_ptr()),
+                             res_ms)):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                acc.append(e0.elapsed_time(e1))
+        del helm, rr, xx, bb
         log("FP64 DGEMM reference")
         # FP64 peak of this GPU: a large cuBLAS DGEMM (denominator for the
         # FP64-bound SL kernel)
@@ -337,7 +357,8 @@ def run_gpu(args, rank, world):
     return {"step_ms": step_ms, "e2e_ms": e2e, "e2e_serial_ms": head["e2e_serial_ms"], "ng": ng,
             "nv": m.nVertsTotal, "clocks": clock,
             "variants": results, "sl_ms": float(np.median(sl_ms)), "fp64_tflops": fp64_tflops,
-            "fdm_apply_ms": float(np.median(fdm_ms)), "gx": int(round(ng ** 0.5))}
+            "fdm_apply_ms": float(np.median(fdm_ms)), "gx": int(round(ng ** 0.5)),
+            "tc_apply_ms": float(np.median(tc_ms)), "residual_ms": float(np.median(res_ms))}
 
 
 def e2e_pipelined(S, lib, m, bc, v, phi0, dt, opts, steps, warmup, stream0):
@@ -463,6 +484,46 @@ def sl_roofline(r):
             "traffic": SL_TRAFFIC_BYTES,
             "fp64_tflops_achieved": fp64, "fp64_tflops_peak_measured_dgemm": r["fp64_tflops"],
             "fp64_frac": fp64 / r["fp64_tflops"]}
+
+
+def tc_roofline(r):
+    """The tensor-core FDM inverse (SE_PREC_MIXED's inner solve): one TF32
+    split of r plus four tc_product_kernel launches (M = N = K = 512), each
+    three kind::tf32 MMAs per K step, timed live with CUDA events (L2
+    flushed). Achieved = tensor FLOPs issued (4 x 3 x 2 M N K) / the whole
+    inverse's time, against the TF32 dense rate (half the measured BF16 GEMM
+    rate: kind::tf32 runs at half the kind::f16 rate). Useful FLOPs are a
+    third of those."""
+    d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    bf16 = float(d.get("bf16_tflops", 1590.0))
+    src = "measured" if "bf16_tflops" in d else "fallback"
+    g = r["gx"]
+    flops = 4 * 3 * 2.0 * g ** 3
+    t = r["tc_apply_ms"] * 1e-3
+    achieved = flops / t / 1e12
+    return {"kernel": "tc_split_kernel + 4 x tc_product_kernel<64, 4> (tcgen05 kind::tf32, TMEM, "
+                      "TMA, 4-CTA cluster split-K), M=N=K=512", "bound": "tensor",
+            "achieved": achieved, "peak": bf16 / 2, "unit": "TFLOP/s", "frac": achieved / (bf16 / 2),
+            "peak_source": f"{src} BF16 GEMM rate / 2 (MEASURED_PEAKS.json bf16_tflops)",
+            "inverse_ms": r["tc_apply_ms"], "fp64_inverse_ms": r["fdm_apply_ms"],
+            "speedup_vs_fp64_inverse": r["fdm_apply_ms"] / r["tc_apply_ms"],
+            "tensor_flops_per_inverse": flops, "useful_flops_per_inverse": flops / 3}
+
+
+def residual_roofline(r):
+    """The refinement residual r = b - A x in double-double
+    (residual_ef_kernel<8>): algorithmic bytes 24 per unknown (x and b read,
+    r written) / live launch time against the measured HBM bandwidth; the
+    kernel is bound by its FP64 issue (double-double sums), reported beside."""
+    peaks = read_peaks()
+    n = r["gx"] ** 2
+    t = r["residual_ms"] * 1e-3
+    achieved = 24.0 * n / t / 1e9
+    return {"kernel": "residual_ef_kernel<8> (double-double, element-factored)", "bound": "hbm",
+            "achieved": achieved, "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
+            "peak_source": peaks[1] + " (MEASURED_PEAKS.json hbm_gbs)", "launch_ms": r["residual_ms"],
+            "unknowns": n, "algorithmic_bytes_per_launch": 24.0 * n}
 
 
 def read_peaks():
@@ -1113,6 +1174,7 @@ def main():
     line = {k: extras[k] for k in order if k in extras}
     line.update({
         "variants": variants, "parity_vs_cpu": parity, "vs_cpu": ratios,
+        "tc_roofline": tc_roofline(r), "residual_roofline": residual_roofline(r),
         "sl_roofline": sl_roofline(r), "roofline": roofline(r), "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * r["nv"],
                 "d2h_bytes_per_step": 8 * r["nv"], "ms_per_step": r["e2e_ms"],

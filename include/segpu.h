@@ -300,6 +300,12 @@ int se_linsys_apply(se_linsys* ls, const double* x_dev, double* y_dev);
  * preconditioner for callers that run their own Krylov loop. The first call
  * on a system computes its 1-D eigendecompositions (host work, allocation). */
 int se_linsys_fdm_apply(se_linsys* ls, const double* r_dev, double* x_dev);
+/* No counterpart in the reference: r = b - A x with the operator's sums and
+ * the subtraction in double-double (rounded once), the residual of the
+ * FP64 iterative refinement, for callers that refine themselves; device
+ * pointers, vec_size entries each, r not aliasing x or b; queued on the
+ * calling thread's stream. */
+int se_linsys_residual(se_linsys* ls, const double* x_dev, const double* b_dev, double* r_dev);
 /* No counterpart in the reference: x = A^{-1} r by the fast-diagonalization
  * transforms in FP64 (precision SE_PREC_FP64, as se_linsys_fdm_apply) or on
  * the tcgen05 tensor cores (SE_PREC_MIXED: r split into TF32 hi/lo pairs,

@@ -2372,6 +2372,16 @@ int se_linsys_fdm_apply(se_linsys* ls, const double* r_dev, double* x_dev) {
   if (int rc = fdm_setup(ls, 0)) return rc;
   return fdm_apply64(ls, r_dev, x_dev, false);
 }
+int se_linsys_residual(se_linsys* ls, const double* x_dev, const double* b_dev, double* r_dev) {
+  if (!ls || !x_dev || !b_dev || !r_dev) return fail(SE_ERR_ARG, "null argument");
+  if (r_dev == x_dev || r_dev == b_dev) return fail(SE_ERR_ARG, "r must not alias x or b");
+  if (!ls->fpart) {
+    ls->fpart_n = std::max(kFdmPartials, residual_blocks(ls->op));
+    if (int rc = dalloc(&ls->fpart, 2 * (size_t)ls->fpart_n + 16)) return rc;
+  }
+  CK(launch_residual(ls->op, x_dev, b_dev, r_dev, nullptr, 0, ls->fpart, g_stream));
+  return SE_OK;
+}
 int se_linsys_fdm_apply_prec(se_linsys* ls, int precision, const double* r_dev, double* x_dev) {
   if (!ls || !r_dev || !x_dev) return fail(SE_ERR_ARG, "null argument");
   if (r_dev == x_dev) return fail(SE_ERR_ARG, "r and x must not alias");

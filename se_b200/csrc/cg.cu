@@ -862,6 +862,8 @@ cudaError_t residual_any(const OpDev& op, const double* x, const double* b, doub
 cudaError_t launch_residual(const OpDev& op, const double* x, const double* b, double* y,
                             const double* w, int natural, double* partial, cudaStream_t s) {
   const ResTail none{nullptr, nullptr, nullptr, nullptr, 0};
+  if (b && partial && residual_ef_supported(op))
+    return launch_residual_ef(op, x, b, y, w, natural, partial, none, nullptr, nullptr, 0, s);
   return residual_any(op, x, b, y, w, natural, partial, none, s);
 }
 

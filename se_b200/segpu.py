@@ -130,7 +130,7 @@ SIGNATURES = {
                               ctypes.POINTER(SolveStats)],
     "se_linsys_solve_async": [_vp, ctypes.c_int],
     "se_linsys_solve_finish": [_vp, ctypes.POINTER(SolveStats)],
-    "se_linsys_apply": [_vp, _vp, _vp], "se_field_gen_vel": [_vp, _vp], "se_field_save": [_vp, ctypes.c_char_p, ctypes.c_int], "se_field_read": [_vp, ctypes.c_char_p, ctypes.c_int], "se_linsys_fdm_apply": [_vp, _vp, _vp], "se_linsys_fdm_apply_prec": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_apply_low": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
+    "se_linsys_apply": [_vp, _vp, _vp], "se_field_gen_vel": [_vp, _vp], "se_field_save": [_vp, ctypes.c_char_p, ctypes.c_int], "se_field_read": [_vp, ctypes.c_char_p, ctypes.c_int], "se_linsys_fdm_apply": [_vp, _vp, _vp], "se_linsys_fdm_apply_prec": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_residual": [_vp, _vp, _vp, _vp], "se_linsys_apply_low": [_vp, ctypes.c_int, _vp, _vp], "se_linsys_diagonal": [_vp, _vp],
     "se_linsys_vec_size": [_vp, _I],
     "se_calc_time_step": [_vp, ctypes.c_double, _D],
     "se_field_error": [_vp, _vp, ctypes.c_int, ctypes.c_int, _D],
@@ -482,6 +482,10 @@ class _LinSys:
     def apply(self, x_ptr: int, y_ptr: int):
         """y = A x on device pointers of vecSize doubles."""
         _check(_lib.se_linsys_apply(self._h, _vp(x_ptr), _vp(y_ptr)))
+
+    def residual(self, x_ptr: int, b_ptr: int, r_ptr: int):
+        """r = b - A x in double-double, rounded once (device pointers)."""
+        _check(_lib.se_linsys_residual(self._h, _vp(x_ptr), _vp(b_ptr), _vp(r_ptr)))
 
     def fdm_apply(self, r_ptr: int, x_ptr: int, precision: int = PREC_FP64):
         """x = A^{-1} r by the fast-diagonalization transforms (device pointers):

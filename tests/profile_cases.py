@@ -8,6 +8,7 @@
     python tests/profile_cases.py fdm [ne]         # one FDM solve (a CUDA graph)
     python tests/profile_cases.py fdm_apply [ne]   # the FDM transform: 4 product kernels
     python tests/profile_cases.py fdm_apply_tc [ne]  # the same on the tcgen05 tensor cores (TF32 hi/lo)
+    python tests/profile_cases.py residual [ne]    # the refinement residual r = b - A x (double-double)
 
 Each case builds an ne x ne element (default 64, the bench's mesh), order p
 (third argument, default 8), doubly periodic mesh and the bench's fields and launches the kernel a few
@@ -58,7 +59,7 @@ def main(case: str, ne: int = 64, p: int = 8, reps: int = 3) -> None:
             a.record()
             adv.Advect(dt)
             b.record()
-    elif case in ("apply", "apply_bf16", "cg", "fdm", "fdm_apply", "fdm_apply_tc"):
+    elif case in ("apply", "apply_bf16", "cg", "fdm", "fdm_apply", "fdm_apply_tc", "residual"):
         method = S.METHOD_FDM if case.startswith("fdm") else S.METHOD_CG
         h = S.HelmholtzEqn(u, phi, -1.0, -1.0, 1.0, 0,
                            S.solver_opts(rtol=1e-10, mode=S.MODE_EXACT, method=method))
@@ -67,6 +68,7 @@ def main(case: str, ne: int = 64, p: int = 8, reps: int = 3) -> None:
         yout = torch.empty_like(xin)
         xb = xin.float().to(torch.bfloat16)
         yf = torch.empty(n, dtype=torch.float32, device="cuda")
+        bres = torch.randn(n, dtype=torch.float64, device="cuda")
         for a, b in ev:
             a.record()
             if case == "apply":
@@ -77,6 +79,8 @@ def main(case: str, ne: int = 64, p: int = 8, reps: int = 3) -> None:
                 h.fdm_apply(xin.data_ptr(), yout.data_ptr())
             elif case == "fdm_apply_tc":
                 h.fdm_apply(xin.data_ptr(), yout.data_ptr(), S.PREC_MIXED)
+            elif case == "residual":
+                h.residual(xin.data_ptr(), bres.data_ptr(), yout.data_ptr())
             else:
                 h.Solve("helm_")
             b.record()

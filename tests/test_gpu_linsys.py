@@ -421,3 +421,36 @@ def test_async_solve_and_download(segpu, oracle):
     assert segpu.load_library().se_field_download_async(fs._h, ptr) == 0
     segpu.synchronize()
     assert np.array_equal(out.numpy(), fs.vals)
+
+
+@pytest.mark.parametrize("case", [0, 1, 2, 4])
+def test_residual_double_double(segpu, oracle, case):
+    """se_linsys_residual: r = b - A x with the sums in double-double equals
+    the oracle's CSR residual to 2e-11 of |A| |x| + |b| (the apply's parity
+    bound: the assembled CSR and the Kronecker form round their coefficients
+    differently), with the element-factored kernel at orders 4 to 8 and the
+    general one otherwise; and when b is the library's own apply of x the
+    residual is only that apply's rounding (the cancellation keeps its
+    digits)."""
+    om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, CASES[case], -2.0, -1.0, 0.5,
+                                                     False)
+    n = ls.vecSize
+    rng = np.random.default_rng(31 + case)
+    x = rng.standard_normal(n)
+    b = rng.standard_normal(n)
+    xd = torch.tensor(x, device="cuda", dtype=torch.float64)
+    bd = torch.tensor(b, device="cuda", dtype=torch.float64)
+    rd = torch.empty_like(xd)
+    ls.residual(xd.data_ptr(), bd.data_ptr(), rd.data_ptr())
+    torch.cuda.synchronize()
+    rowptr, col, val, _ = A.arrays()
+    absA = np.array([np.abs(val[rowptr[i]:rowptr[i + 1]]).sum() for i in range(n)])
+    ref = b - A.matvec(x)
+    assert (np.abs(rd.cpu().numpy() - ref) / (absA * np.abs(x).max() + np.abs(b))).max() < 2e-11
+    # b = the library's own FP64 apply of x: the residual is that apply's
+    # rounding, a few units of |A| |x| in the last place, not more
+    bd2 = torch.empty_like(xd)
+    ls.apply(xd.data_ptr(), bd2.data_ptr())
+    ls.residual(xd.data_ptr(), bd2.data_ptr(), rd.data_ptr())
+    torch.cuda.synchronize()
+    assert np.abs(rd.cpu().numpy()).max() <= 1e-13 * (absA * np.abs(x).max()).max()
