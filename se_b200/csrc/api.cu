@@ -567,7 +567,7 @@ int linsys_alloc(se_linsys* ls) {
       (rc = dalloc(&ls->r, n)) || (rc = dalloc(&ls->z, n)) || (rc = dalloc(&ls->p0, n)) ||
       (rc = dalloc(&ls->p1, n)) || (rc = dalloc(&ls->w, n)) || (rc = dalloc(&ls->dinv, n)))
     return rc;
-  CK(cudaMemset(ls->lift, 0, sizeof(double) * n));
+  CK(cudaMemsetAsync(ls->lift, 0, sizeof(double) * n, g_stream));
   int dev = 0;
   CK(cudaGetDevice(&dev));
   const int grid = cg_plan(dev, ls->op.d[0].N, cg_tiles(ls->op), 1, &ls->resident);
@@ -582,12 +582,16 @@ int linsys_alloc(se_linsys* ls) {
       (rc = dalloc(&ls->d_partials, (size_t)S.nseg * 8)) || (rc = dalloc(&ls->d_bar, 2)) ||
       (rc = dalloc(&ls->d_active, 1)) || (rc = dalloc(&ls->d_err, 1)))
     return rc;
-  CK(cudaMemcpy(ls->d_tiles, S.tiles.data(), sizeof(CgTile) * S.tiles.size(),
-                cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(ls->d_block_begin, S.block_begin.data(), sizeof(int) * S.block_begin.size(),
-                cudaMemcpyHostToDevice));
-  CK(cudaMemset(ls->d_bar, 0, 2 * sizeof(unsigned)));
-  CK(cudaMemset(ls->d_err, 0, sizeof(unsigned)));
+  // on the caller's stream, finished before the system is handed out: the
+  // library's streams are non-blocking, so nothing orders them against the
+  // legacy stream
+  CK(cudaMemcpyAsync(ls->d_tiles, S.tiles.data(), sizeof(CgTile) * S.tiles.size(),
+                     cudaMemcpyHostToDevice, g_stream));
+  CK(cudaMemcpyAsync(ls->d_block_begin, S.block_begin.data(), sizeof(int) * S.block_begin.size(),
+                     cudaMemcpyHostToDevice, g_stream));
+  CK(cudaMemsetAsync(ls->d_bar, 0, 2 * sizeof(unsigned), g_stream));
+  CK(cudaMemsetAsync(ls->d_err, 0, sizeof(unsigned), g_stream));
+  CK(cudaStreamSynchronize(g_stream));
   return SE_OK;
 }
 
@@ -679,6 +683,13 @@ uint16_t to_bf16(float f) {
   return (uint16_t)(u >> 16);
 }
 
+// Host-to-device copy complete on return (set-up data that kernels on any of
+// the library's non-blocking streams read afterwards).
+cudaError_t upload_now(void* dst, const void* src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, g_stream);
+  return e != cudaSuccess ? e : cudaStreamSynchronize(g_stream);
+}
+
 // Generalised eigenvectors S (S^T K S = diag(lam), S^T W S = I) of one
 // direction, on the device: eigenvectors of W^-1/2 K W^-1/2 by cuSOLVER
 // syevd (setup only), then scaled by W^-1/2.
@@ -721,7 +732,7 @@ int eig_1d(const Dir& d, const double* Kh, const double* w, double** S_dev, doub
   for (int j = 0; j < n; j++)
     for (int i = 0; i < n; i++) A[(size_t)j * n + i] /= std::sqrt(W[i]);
   S_host = A;
-  CK(cudaMemcpy(dA, A.data(), sizeof(double) * A.size(), cudaMemcpyHostToDevice));
+  CK(upload_now(dA, A.data(), sizeof(double) * A.size()));
   std::vector<double> T((size_t)n * n);
   for (int j = 0; j < n; j++)
     for (int i = 0; i < n; i++) T[(size_t)i * n + j] = A[(size_t)j * n + i];
@@ -731,7 +742,7 @@ int eig_1d(const Dir& d, const double* Kh, const double* w, double** S_dev, doub
     dfree(dlam);
     return rc2;
   }
-  CK(cudaMemcpy(dT, T.data(), sizeof(double) * T.size(), cudaMemcpyHostToDevice));
+  CK(upload_now(dT, T.data(), sizeof(double) * T.size()));
   *S_dev = dA;
   *ST_dev = dT;
   *lam_dev = dlam;
@@ -745,14 +756,14 @@ int upload_low(const std::vector<double>& S, int prec, void** out) {
     for (size_t k = 0; k < n; k++) v[k] = (float)S[k];
     float* d = nullptr;
     if (int rc = dalloc(&d, n)) return rc;
-    CK(cudaMemcpy(d, v.data(), sizeof(float) * n, cudaMemcpyHostToDevice));
+    CK(upload_now(d, v.data(), sizeof(float) * n));
     *out = d;
   } else {
     std::vector<uint16_t> v(n);
     for (size_t k = 0; k < n; k++) v[k] = to_bf16((float)S[k]);
     uint16_t* d = nullptr;
     if (int rc = dalloc(&d, n)) return rc;
-    CK(cudaMemcpy(d, v.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice));
+    CK(upload_now(d, v.data(), sizeof(uint16_t) * n));
     *out = d;
   }
   return SE_OK;
@@ -831,8 +842,7 @@ int eig_get(const Dir& d, const double* Kh, const double* w, int prec, Eig1D** o
       for (int k = 0; k < 2; k++) {
         float* d = nullptr;
         if (int rc = dalloc(&d, hi.size())) return rc;
-        CK(cudaMemcpy(d, k == 0 ? hi.data() : lo.data(), sizeof(float) * hi.size(),
-                      cudaMemcpyHostToDevice));
+        CK(upload_now(d, k == 0 ? hi.data() : lo.data(), sizeof(float) * hi.size()));
         e->tc[t][k] = d;
       }
     }
@@ -886,8 +896,8 @@ int fdm_setup(se_linsys* ls, int prec) {
       const size_t ny = (size_t)op.G[1] * ls->tc_px, nx = (size_t)op.G[0] * ls->tc_py;
       for (int k = 0; k < 2; k++) {
         if ((rc = dalloc(&ls->tcY[k], ny)) || (rc = dalloc(&ls->tcX[k], nx))) return rc;
-        CK(cudaMemset(ls->tcY[k], 0, sizeof(float) * ny));
-        CK(cudaMemset(ls->tcX[k], 0, sizeof(float) * nx));
+        CK(cudaMemsetAsync(ls->tcY[k], 0, sizeof(float) * ny, g_stream));
+        CK(cudaMemsetAsync(ls->tcX[k], 0, sizeof(float) * nx, g_stream));
       }
       int dev = 0;
       CK(cudaGetDevice(&dev));
@@ -1063,7 +1073,7 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
     if ((rc = dalloc(&ls->d_fparams, 1)) || (rc = dalloc(&ls->d_fstate, 1)) ||
         (rc = dalloc(&ls->d_rescount, 1)))
       return rc;
-    CK(cudaMemset(ls->d_rescount, 0, sizeof(unsigned)));
+    CK(cudaMemsetAsync(ls->d_rescount, 0, sizeof(unsigned), g_stream));
   }
   if (ls->fdm_exec) {
     cudaGraphExecDestroy(ls->fdm_exec);
@@ -2394,8 +2404,8 @@ int se_linsys_fdm_apply_prec(se_linsys* ls, int precision, const double* r_dev, 
     if ((rc = dalloc(&ls->d_fparams, 1)) || (rc = dalloc(&ls->d_fstate, 1)) ||
         (rc = dalloc(&ls->d_rescount, 1)))
       return rc;
-    CK(cudaMemset(ls->d_rescount, 0, sizeof(unsigned)));
-    CK(cudaMemset(ls->d_fstate, 0, sizeof(FdmState)));
+    CK(cudaMemsetAsync(ls->d_rescount, 0, sizeof(unsigned), g_stream));
+    CK(cudaMemsetAsync(ls->d_fstate, 0, sizeof(FdmState), g_stream));
   }
   CK(cudaMemsetAsync(x_dev, 0, sizeof(double) * ls->n, g_stream));
   return fdm_apply_tc(ls, r_dev, x_dev);
