@@ -2090,6 +2090,14 @@ int se_solver_opts_parse(se_solver_opts* o, const char* prefix, const char* opti
       else if (val == "unpreconditioned") o->norm_type = SE_NORM_UNPRECONDITIONED;
       else if (val == "natural") o->norm_type = SE_NORM_NATURAL;
       else return fail(SE_ERR_UNSUPPORTED, "ksp_norm_type %s", val.c_str());
+    } else if (key == "precision") {
+      // Not a PETSc key: the FDM solve's arithmetic (FP64, or the
+      // reduced-precision inverses refined to the same FP64 tolerance).
+      if (val == "fp64") o->precision = SE_PREC_FP64;
+      else if (val == "mixed") o->precision = SE_PREC_MIXED;
+      else if (val == "fp64_tc") o->precision = SE_PREC_FP64_TC;
+      else if (val == "bf16") o->precision = SE_PREC_BF16;
+      else return fail(SE_ERR_UNSUPPORTED, "precision %s (fp64, mixed, fp64_tc, bf16)", val.c_str());
     }
   }
   return SE_OK;

@@ -83,6 +83,13 @@ def test_solver_options_parse(segpu):
     with pytest.raises(segpu.SEError) as e:
         segpu.solver_opts("helm_", "-helm_ksp_type gmres")
     assert e.value.code == segpu.SE_ERR_UNSUPPORTED
+    o = segpu.solver_opts("helm_", "-helm_pc_type fdm -helm_precision fp64_tc")
+    assert o.method == segpu.METHOD_FDM and o.precision == segpu.PREC_FP64_TC
+    o = segpu.solver_opts("helm_", "-helm_pc_type fdm -helm_precision mixed")
+    assert o.precision == segpu.PREC_MIXED
+    with pytest.raises(segpu.SEError) as e:
+        segpu.solver_opts("helm_", "-helm_precision fp8")
+    assert e.value.code == segpu.SE_ERR_UNSUPPORTED
 
 
 def test_no_device_fails_loudly(segpu):
