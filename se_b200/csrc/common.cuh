@@ -312,11 +312,23 @@ cudaError_t launch_tc_split(const double* x, int rows, int cols, int ld, float* 
 // (|divisor| <= null_tol gives 0), 2 accumulate into FP64 C scaled by *cmax
 // (cmax == nullptr: 1). a_fp64: A is FP64 (scaled by 1/*amax when amax is
 // given) whatever prec; c_fp64: C is FP64 (required for epi 2).
+//
+// low (FP64 only, k in 1..8): the lowest k x k block of spectral coefficients
+// carried apart from the backward transform. With epi 1 the block of C
+// (rows and columns < k) is moved into zlow[k][k] and left 0 in C; with
+// epi 0 or 2 the product's outputs get sum_a A[r][a] U[a][c] added, U[a][c] =
+// sum_b zlow[a][b] ex[c * ldex + b], in double-double (with the old value
+// for epi 2), rounded once.
+struct FdmLow {
+  double* zlow;
+  const double* ex;
+  int ldex, k;
+};
 cudaError_t launch_fdm_gemm(int prec, int epi, const void* A, int a_fp64, const void* B, void* C,
                             int c_fp64, int M, int N, int K, int lda, int ldb, int ldc,
                             const double* amax, const double* cmax, const double* lx,
                             const double* ly, double alpha, double bx, double by, double null_tol,
-                            cudaStream_t s);
+                            cudaStream_t s, const FdmLow* low = nullptr);
 
 // Fast-diagonalization pieces (fdm.cu). prec: 0 FP64, 1 FP32, 2 BF16.
 cudaError_t launch_spectral_divide(int prec, void* v, int gx, int gy, const double* lx,
@@ -338,6 +350,13 @@ cudaError_t launch_maxabs(const double* x, size_t n, double* partial, int npart,
                           cudaStream_t s);
 cudaError_t launch_sub(const double* b, const double* y, double* r, size_t n, cudaStream_t s);
 cudaError_t launch_invert(double* x, size_t n, cudaStream_t s);
+// C = A^T (Bh + Bl) in double-double for n x n row-major matrices, returned
+// as Ch + Cl (Bl may be null); set-up only.
+cudaError_t launch_dd_gemm_tn(int n, const double* A, const double* Bh, const double* Bl,
+                              double* Ch, double* Cl, cudaStream_t s);
+// y = a y + b x (a == 0: y = b x, y not read)
+cudaError_t launch_axpby(double* y, double a, double b, const double* x, size_t n,
+                         cudaStream_t s);
 // f -= (sum f / sum d) d with d = 1 / dinv: the right-hand side that Jacobi
 // CG with the constant null space projected out of every preconditioned
 // residual converges to (its limit solves A x = f - c d, c = sum f / sum d).

@@ -223,6 +223,51 @@ __global__ void invert_kernel(double* __restrict__ x, size_t n) {
     x[k] = 1.0 / x[k];
 }
 
+// C = A^T (Bh + Bl) for n x n row-major matrices, every product and sum in
+// double-double (TwoProd by FMA, TwoSum), the result returned as the pair
+// Ch + Cl. Set-up only: the residuals of the eigenvector refinement, whose
+// entries are differences far below the operands' size. Bl may be null.
+__global__ void __launch_bounds__(256) dd_gemm_tn_kernel(int n, const double* __restrict__ A,
+                                                         const double* __restrict__ Bh,
+                                                         const double* __restrict__ Bl,
+                                                         double* __restrict__ Ch,
+                                                         double* __restrict__ Cl) {
+  __shared__ double as[16][17], bh[16][17], bl[16][17];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int i0 = blockIdx.y * 16, j0 = blockIdx.x * 16;
+  const int i = i0 + ty, j = j0 + tx;
+  double sh = 0.0, sl = 0.0;
+  for (int k0 = 0; k0 < n; k0 += 16) {
+    const int k = k0 + ty;
+    const bool kr = k < n;
+    as[ty][tx] = (kr && i0 + tx < n) ? A[(size_t)k * n + i0 + tx] : 0.0;
+    bh[ty][tx] = (kr && j < n) ? Bh[(size_t)k * n + j] : 0.0;
+    bl[ty][tx] = (Bl && kr && j < n) ? Bl[(size_t)k * n + j] : 0.0;
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < 16; kk++) {
+      const double a = as[kk][ty];
+      dd_fma(sh, sl, a, bh[kk][tx]);
+      sl = fma(a, bl[kk][tx], sl);
+    }
+    __syncthreads();
+  }
+  if (i < n && j < n) {
+    double s, e;
+    two_sum(sh, sl, s, e);
+    Ch[(size_t)i * n + j] = s;
+    Cl[(size_t)i * n + j] = e;
+  }
+}
+
+// y = a y + b x (a == 0 does not read y)
+__global__ void axpby_kernel(double* __restrict__ y, double a, double b,
+                             const double* __restrict__ x, size_t n) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x)
+    y[k] = a == 0.0 ? b * x[k] : fma(a, y[k], b * x[k]);
+}
+
 int blocks_for(size_t n) {
   size_t b = (n + 255) / 256;
   return (int)(b < 1184 ? (b < 1 ? 1 : b) : 1184);
@@ -282,6 +327,20 @@ cudaError_t launch_norms(const double* r, const double* w, size_t n, int natural
   if (b > npart) b = npart;
   norm_partials_kernel<<<b, 256, 0, s>>>(r, w, n, natural, partial);
   norm_final_kernel<<<1, 256, 0, s>>>(partial, b, out2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dd_gemm_tn(int n, const double* A, const double* Bh, const double* Bl,
+                              double* Ch, double* Cl, cudaStream_t s) {
+  if (n <= 0) return cudaErrorInvalidValue;
+  const dim3 grid((n + 15) / 16, (n + 15) / 16);
+  dd_gemm_tn_kernel<<<grid, 256, 0, s>>>(n, A, Bh, Bl, Ch, Cl);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_axpby(double* y, double a, double b, const double* x, size_t n,
+                         cudaStream_t s) {
+  axpby_kernel<<<blocks_for(n), 256, 0, s>>>(y, a, b, x, n);
   return cudaGetLastError();
 }
 

@@ -20,7 +20,13 @@
 // Epilogues: store; store after the spectral divide
 // C[l][k] /= alpha + bx lx[k] + by ly[l] (entries whose divisor is below
 // null_tol in magnitude — the null mode — become 0); accumulate into an FP64
-// C with an optional scale read from device memory.
+// C with an optional scale read from device memory. The FP64 products can
+// carry the lowest k x k spectral block (k <= 8) apart from the backward
+// transform: the divide moves it out of C into zlow, and the transform's
+// last product adds sum_a A[r][a] U[a][c], U[a][c] = sum_b zlow[a][b]
+// ex[c][b], to its outputs in double-double (the block holds the largest
+// coefficients of a smooth solution, whose FP64 product rounding would
+// otherwise dominate the solve's first residual).
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -116,6 +122,11 @@ struct GemmArgs {
   const double* cmax;  // accumulate scale, nullptr: 1
   const double *lx, *ly;
   double alpha, bx, by, null_tol;
+  // FP64 only: the low spectral block carried apart (FdmLow, common.cuh);
+  // lowk = 0: none
+  double* zlow;
+  const double* ex;
+  int ldex, lowk;
 };
 
 enum { EPI_STORE = 0, EPI_DIVIDE = 1, EPI_ACCUM = 2 };
@@ -284,6 +295,14 @@ __global__ void __launch_bounds__(kThreads) fdm_gemm_kernel(const GemmArgs<TA, T
 // so any leading dimension and any edge), BM x BN block tile of WM x WN
 // warps, each warp (BM/WM) x (BN/WN) in m16n8 MMA tiles.
 //
+constexpr int kLowMax = 8;
+// Shared-memory doubles of the low block of a BM x BN output tile: zlow
+// (8 x 8), the tile's rows of A's first 8 columns, U (8 x BN) as hi and lo.
+template <int BM, int BN>
+struct LowSm {
+  static constexpr int SIZE = kLowMax * kLowMax + BM * kLowMax + 2 * kLowMax * BN;
+};
+
 template <int BM_, int BN_, int WM_, int WN_, int ST_, int BK_ = 16>
 struct DCfg {
   static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_, ST = ST_;
@@ -292,6 +311,7 @@ struct DCfg {
   static constexpr int MT = BM / WM / 16, NT = BN / WN / 8;
   static constexpr int A_ELEMS = BM * AS, B_ELEMS = BK * BS;
   static constexpr size_t SMEM = (size_t)ST * (A_ELEMS + B_ELEMS) * sizeof(double);
+  static_assert(ST * (A_ELEMS + B_ELEMS) >= LowSm<BM, BN>::SIZE, "low block exceeds the pipeline");
 };
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
@@ -303,6 +323,51 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Stages zlow and A's first k columns of rows m0..m0+BM, then U for columns
+// n0..n0+BN, into sm (LowSm layout). Ends with the block synchronised.
+template <int BM, int BN, int THREADS>
+__device__ __forceinline__ void low_stage(const GemmArgs<double, double, double>& g, double* sm,
+                                          int m0, int n0, int tid) {
+  const int lk = g.lowk;
+  double* zl = sm;
+  double* al = zl + kLowMax * kLowMax;
+  double* uh = al + BM * kLowMax;
+  double* ul = uh + kLowMax * BN;
+  for (int e = tid; e < lk * lk; e += THREADS) zl[e] = g.zlow[e];
+  for (int e = tid; e < BM * kLowMax; e += THREADS) {
+    const int r = e / kLowMax, a = e % kLowMax, gr = m0 + r;
+    al[e] = (a < lk && gr < g.M) ? g.A[(size_t)gr * g.lda + a] : 0.0;
+  }
+  __syncthreads();
+  for (int e = tid; e < kLowMax * BN; e += THREADS) {
+    const int a = e / BN, c = e % BN, gc = n0 + c;
+    double h = 0.0, l = 0.0;
+    if (a < lk && gc < g.N)
+      for (int b = 0; b < lk; b++) dd_fma(h, l, zl[a * lk + b], g.ex[(size_t)gc * g.ldex + b]);
+    uh[e] = h;
+    ul[e] = l;
+  }
+  __syncthreads();
+}
+
+// v (the product's FP64 output at tile row r, column c) plus the low block,
+// plus the old value when accumulating, rounded once.
+template <int BM, int BN, int EPI>
+__device__ __forceinline__ double low_add(const double* sm, int lk, int r, int c, double v,
+                                          const double* dst) {
+  const double* al = sm + kLowMax * kLowMax + r * kLowMax;
+  const double* uh = sm + kLowMax * kLowMax + BM * kLowMax;
+  const double* ul = uh + kLowMax * BN;
+  double h = 0.0, l = 0.0;
+  for (int a = 0; a < lk; a++) {
+    dd_fma(h, l, al[a], uh[a * BN + c]);
+    l = fma(al[a], ul[a * BN + c], l);
+  }
+  dd_add(h, l, v);
+  if constexpr (EPI == EPI_ACCUM) dd_add(h, l, *dst);
+  return h + l;
 }
 
 template <class C, int EPI>
@@ -380,7 +445,13 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_kernel(const GemmArgs<do
     }
   }
   cp_async_wait<0>();
-
+  const int lk = g.lowk;
+  if constexpr (EPI != EPI_DIVIDE) {
+    if (lk) {
+      __syncthreads();  // the pipeline's shared memory is free from here
+      low_stage<C::BM, C::BN, C::THREADS>(g, dsm, m0, n0, tid);
+    }
+  }
 
 #pragma unroll
   for (int mt = 0; mt < C::MT; mt++)
@@ -399,6 +470,15 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_kernel(const GemmArgs<do
           if constexpr (EPI == EPI_DIVIDE) {
             const double d = g.alpha + g.bx * g.lx[c] + g.by * g.ly[r];
             v = fabs(d) <= g.null_tol ? 0.0 : v / d;
+            if (r < lk && c < lk) {
+              g.zlow[r * lk + c] = v;
+              v = 0.0;
+            }
+          } else {
+            if (lk) {
+              *dst = low_add<C::BM, C::BN, EPI>(dsm, lk, r - m0, c - n0, v, dst);
+              continue;
+            }
           }
           if constexpr (EPI == EPI_ACCUM)
             *dst += v;
@@ -443,7 +523,8 @@ struct KCfg {
   static constexpr int THREADS = 32 * W;
   static constexpr int A_ELEMS = BM * AS, B_ELEMS = BK * BS;
   static constexpr int PIPE = ST * (A_ELEMS + B_ELEMS), RED = W * BM * RS;
-  static constexpr size_t SMEM = sizeof(double) * (size_t)(PIPE > RED ? PIPE : RED);
+  static constexpr int LOW = RED + LowSm<BM, BN>::SIZE;  // partial tiles, then the low block
+  static constexpr size_t SMEM = sizeof(double) * (size_t)(PIPE > LOW ? PIPE : LOW);
 };
 
 template <class C, int EPI>
@@ -535,6 +616,10 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_ksplit_kernel(
         const int r = mt * 16 + gq + (q >> 1) * 8, c = nt * 8 + 2 * tq + (q & 1);
         red[(warp * C::BM + r) * C::RS + c] = acc[mt][nt][q];
       }
+  const int lk = g.lowk;
+  if constexpr (EPI != EPI_DIVIDE) {
+    if (lk) low_stage<C::BM, C::BN, C::THREADS>(g, dsm + C::RED, m0, n0, tid);
+  }
   __syncthreads();
   for (int e = tid; e < C::BM * C::BN; e += C::THREADS) {
     const int r = e / C::BN, c = e % C::BN;
@@ -547,6 +632,15 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_ksplit_kernel(
     if constexpr (EPI == EPI_DIVIDE) {
       const double d = g.alpha + g.bx * g.lx[gc] + g.by * g.ly[gr];
       v = fabs(d) <= g.null_tol ? 0.0 : v / d;
+      if (gr < lk && gc < lk) {
+        g.zlow[gr * lk + gc] = v;
+        v = 0.0;
+      }
+    } else {
+      if (lk) {
+        *dst = low_add<C::BM, C::BN, EPI>(dsm + C::RED, lk, r, c, v, dst);
+        continue;
+      }
     }
     if constexpr (EPI == EPI_ACCUM)
       *dst += v;
@@ -608,12 +702,20 @@ cudaError_t launch_fdm_gemm(int prec, int epi, const void* A, int a_fp64, const 
                             int c_fp64, int M, int N, int K, int lda, int ldb, int ldc,
                             const double* amax, const double* cmax, const double* lx,
                             const double* ly, double alpha, double bx, double by, double null_tol,
-                            cudaStream_t s) {
+                            cudaStream_t s, const FdmLow* low) {
 #define SE_GEMM_ARGS(TA, TB, TC)                                                              \
   GemmArgs<TA, TB, TC> g{(const TA*)A, (const TB*)B, (TC*)C, M, N, K, lda, ldb, ldc, amax, cmax, \
-                         lx, ly, alpha, bx, by, null_tol}
+                         lx, ly, alpha, bx, by, null_tol, nullptr, nullptr, 0, 0}
   if (prec == 0) {
     SE_GEMM_ARGS(double, double, double);
+    if (low && low->k > 0) {
+      if (low->k > kLowMax || !low->zlow || (epi != EPI_DIVIDE && !low->ex))
+        return cudaErrorInvalidValue;
+      g.zlow = low->zlow;
+      g.ex = low->ex;
+      g.ldex = low->ldex;
+      g.lowk = low->k;
+    }
     if (epi == EPI_DIVIDE) return run<0, double, double, double, EPI_DIVIDE>(g, s);
     if (epi == EPI_ACCUM) return run<0, double, double, double, EPI_ACCUM>(g, s);
     return run<0, double, double, double, EPI_STORE>(g, s);
