@@ -143,6 +143,10 @@ VARIANTS = {
     "fdm_tf32x3_tc": ("METHOD_FDM", "PREC_MIXED"),
     "fdm_fp64_then_tc": ("METHOD_FDM", "PREC_FP64_TC"),
     "cg_fp64": ("METHOD_CG", "PREC_FP64"),
+    # CG whose apply reads its direction in BF16 / FP16 and computes in FP32,
+    # inside FP64 iterative refinement (double-double residual)
+    "cg_bf16_apply_refined": ("METHOD_CG", "PREC_BF16"),
+    "cg_fp16_apply_refined": ("METHOD_CG", "PREC_FP16"),
 }
 HEADLINE = "fdm_fp64"
 
@@ -203,7 +207,8 @@ def run_gpu(args, rank, world):
         for name in chosen:
             meth, prec = VARIANTS[name]
             opts = S.solver_opts(rtol=RTOL, mode=S.MODE_EXACT, method=getattr(S, meth),
-                                 precision=getattr(S, prec), max_it=10000)
+                                 precision=getattr(S, prec),
+                                 max_it=100000 if prec in ("PREC_BF16", "PREC_FP16") else 10000)
             helm = S.HelmholtzEqn(u, adv.fieldSL, -LAMBDA, -1.0, 1.0, 0, opts)
             ng = helm.vecSize
 

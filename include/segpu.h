@@ -191,14 +191,19 @@ int se_advector_departures(se_advector* adv, int* el, double* xy);
 #define SE_PREC_MIXED 1     /* FDM only: every refinement step's inverse on the tcgen05 tensor
                                cores (TF32 hi/lo operand pairs, FP32 accumulation, about 1e-6
                                relative); residuals, norms and the solution in FP64 */
-#define SE_PREC_BF16 2      /* BF16 data, FP32-accumulated tensor-core inner solves, FP64 refinement;
-                               refinement converges only while 2^-8 times the operator's
-                               condition number stays below 1 (small or well-conditioned
-                               systems) and otherwise stops with SE_KSP_DIVERGED_BREAKDOWN */
-#define SE_PREC_FP16 3      /* FP16 data, FP32 arithmetic: se_linsys_apply_low only */
+#define SE_PREC_BF16 2      /* SE_METHOD_CG: FP64 iterative refinement around a CG whose
+                               operator apply reads its direction vector in BF16 and computes
+                               in FP32 (dots, updates, residuals FP64; orders 4-8, no SVV, no
+                               null-space removal). SE_METHOD_FDM: BF16 data,
+                               FP32-accumulated inner inverses, FP64 refinement; converges only
+                               while 2^-8 times the operator's condition number stays below 1
+                               and otherwise stops with SE_KSP_DIVERGED_BREAKDOWN */
+#define SE_PREC_FP16 3      /* SE_METHOD_CG: as SE_PREC_BF16 with an FP16 direction vector
+                               (each inner solve scaled into FP16's range); also the FP16
+                               input of se_linsys_apply_low */
 #define SE_PREC_FP64_TC 4   /* FDM only: the first refinement step's inverse in FP64, the
                                following ones as SE_PREC_MIXED */
-#define SE_METHOD_CG 0      /* PETSc KSPCG + PCJACOBI semantics: the drop-in (FP64 only) */
+#define SE_METHOD_CG 0      /* PETSc KSPCG + PCJACOBI semantics: the drop-in (FP64; BF16/FP16 as above) */
 #define SE_METHOD_FDM 1     /* fast diagonalization: exact inverse by 1-D eigenvector transforms */
 typedef struct {
   double rtol;    /* default 1e-5 (PETSc) */

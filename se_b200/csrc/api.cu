@@ -269,6 +269,10 @@ struct se_linsys {
   double *X1, *X2, *ax;       // FP64 work: two transform buffers, A x
   double* zlow;               // FP64 inverse: the low spectral block [lowk][lowk]
   int lowk;
+  // CG with the reduced-precision apply in FP64 refinement: outer residual,
+  // inner solution, norm partials [2 * mx_np] + results [16]
+  double *mx_r, *mx_d, *mx_part;
+  int mx_np;
   void *L1, *L2, *L3;         // low-precision work (L1 unused)
   // tcgen05 path (SE_PREC_MIXED): operand pairs of the eigenvector products
   // (cached per direction) and two work pairs, [G_y][tc_px] and [G_x][tc_py]
@@ -520,6 +524,9 @@ void linsys_free(se_linsys* ls) {
   dfree(ls->X2);
   dfree(ls->ax);
   dfree(ls->zlow);
+  dfree(ls->mx_r);
+  dfree(ls->mx_d);
+  dfree(ls->mx_part);
   if (ls->L1) cudaFree(ls->L1);
   if (ls->L2) cudaFree(ls->L2);
   if (ls->L3) cudaFree(ls->L3);
@@ -600,7 +607,7 @@ int linsys_alloc(se_linsys* ls) {
 
 // Run the persistent CG for A x = b on this system's schedule; fills stats.
 int run_cg(se_linsys* ls, const double* b, double* x, double rtol, double atol, double dtol,
-           int max_it, int remove_null, CgSolve* out_state, float* kernel_ms) {
+           int max_it, int remove_null, CgSolve* out_state, float* kernel_ms, int lowp = 0) {
   CgSolve cs = make_solve(ls, b, x, rtol, atol, dtol, max_it, remove_null);
   cudaStream_t s = g_stream;
   CK(cudaMemcpyAsync(ls->d_solve, &cs, sizeof(cs), cudaMemcpyHostToDevice, s));
@@ -622,7 +629,7 @@ int run_cg(se_linsys* ls, const double* b, double* x, double rtol, double atol, 
     CK(cudaEventCreate(&ls->ev[1]));
   }
   CK(cudaEventRecord(ls->ev[0], s));
-  CK(launch_cg(B, ls->grid, ls->op.d[0].N, ls->resident, s));
+  CK(launch_cg(B, ls->grid, ls->op.d[0].N, ls->resident, s, lowp));
   CK(cudaEventRecord(ls->ev[1], s));
   unsigned err = 0;
   CK(cudaMemcpyAsync(out_state, ls->d_solve, sizeof(CgSolve), cudaMemcpyDeviceToHost, s));
@@ -637,12 +644,129 @@ int check_field(const se_field* f) {
   if (!f || !f->mesh || !f->vals) return fail(SE_ERR_ARG, "null field");
   return SE_OK;
 }
+
+// Partial-sum slots of the FDM and refinement norms (at least one per block of
+// any norm or residual launch).
+constexpr int kFdmPartials = 1184;
+
+// Inner relative tolerance of the reduced-precision CG: each refinement step
+// needs only a contraction; tighter inner solves cost more iterations than
+// they save in outer steps.
+constexpr double kMixedInnerRtol = 1e-2;
+constexpr int kMixedMaxOuter = 100;
+
+// SE_METHOD_CG with SE_PREC_BF16 / SE_PREC_FP16: FP64 iterative refinement
+// around the persistent CG whose operator apply reads its direction vector
+// rounded to BF16 / FP16 and computes in FP32. Every outer step:
+//   r = f - A x            (double-double residual, FP64 result)
+//   test ||r|| in the chosen norm against max(rtol ||f||, atol)
+//   s = RMS of D^-1 r;  solve A d = r / s by that CG to kMixedInnerRtol
+//   x += s d               (FP64)
+// The dots, updates and vectors of the inner CG stay FP64; the scaling keeps
+// FP16 directions inside its range. out: its = inner CG iterations summed,
+// dp / rnorm0 the outer residual norms, reason PETSc's code (2 rtol, 3 atol,
+// -3 iterations, -4 dtol, or the inner CG's breakdown).
+int run_mixed_cg(se_linsys* ls, int lowp, CgSolve* out, int* outer, float* kernel_ms) {
+  const OpDev& op = ls->op;
+  const size_t n = (size_t)ls->n;
+  if (op.gamma != 0.0)
+    return fail(SE_ERR_UNSUPPORTED, "the reduced-precision CG apply has no SVV term");
+  if (op.d[0].N < 4 || op.d[0].N > 8)
+    return fail(SE_ERR_UNSUPPORTED, "the reduced-precision CG apply covers orders 4 to 8");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (ls->grid > cg_max_grid(dev, op.d[0].N, ls->resident, 1, lowp))
+    return fail(SE_ERR_UNSUPPORTED, "the reduced-precision CG kernel does not fit the CG grid");
+  cudaStream_t s = g_stream;
+  if (!ls->mx_r) {
+    ls->mx_np = std::max(kFdmPartials, std::max(residual_partial_blocks(op), residual_blocks(op)));
+    int rc;
+    if ((rc = dalloc(&ls->mx_r, n)) || (rc = dalloc(&ls->mx_d, n)) ||
+        (rc = dalloc(&ls->mx_part, 2 * (size_t)ls->mx_np + 16)))
+      return rc;
+  }
+  // Jacobi inverse for the norms (the operator may have changed mode)
+  CK(launch_op_diag(op, ls->dinv, s));
+  CK(launch_invert(ls->dinv, n, s));
+  double* out2 = ls->mx_part + 2 * ls->mx_np;
+  const int nt = ls->opts.norm_type;
+  // h2[0] = sum (D^-1 r)^2, h2[1] = sum r^2, h2[2] = sum r D^-1 r (natural only)
+  double h2[4] = {0.0, 0.0, 0.0, 0.0};
+  auto norms = [&](bool fresh_partials) -> int {
+    if (fresh_partials)
+      CK(launch_norms(ls->mx_r, ls->dinv, n, 0, ls->mx_part, ls->mx_np, out2, s));
+    else
+      CK(launch_norm_final(ls->mx_part, residual_partial_blocks(op), out2, s));
+    CK(cudaMemcpyAsync(h2, out2, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (nt == SE_NORM_NATURAL) {
+      CK(launch_norms(ls->mx_r, ls->dinv, n, 1, ls->mx_part, ls->mx_np, out2 + 2, s));
+      CK(cudaMemcpyAsync(h2 + 2, out2 + 2, sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaStreamSynchronize(s));
+    return SE_OK;
+  };
+  auto norm = [&]() {
+    return std::sqrt(nt == SE_NORM_PRECONDITIONED ? h2[0]
+                     : nt == SE_NORM_UNPRECONDITIONED ? h2[1]
+                                                      : std::fabs(h2[2]));
+  };
+  CK(cudaMemsetAsync(ls->x, 0, sizeof(double) * n, s));
+  CK(cudaMemcpyAsync(ls->mx_r, ls->f, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+  if (int rc = norms(true)) return rc;
+  const double rnorm0 = norm();
+  const double ttol = std::max(ls->opts.rtol * rnorm0, ls->opts.atol);
+  std::memset(out, 0, sizeof(*out));
+  out->rnorm0 = rnorm0;
+  float total_ms = 0.f;
+  int its = 0, k = 0, reason = 0;
+  double dp = rnorm0;
+  for (;; k++) {
+    if (dp <= ttol) {
+      reason = dp <= ls->opts.atol ? 3 : 2;
+      break;
+    }
+    if (!(dp == dp) || dp > ls->opts.dtol * rnorm0) {
+      reason = -4;
+      break;
+    }
+    if (its >= ls->opts.max_it || k >= kMixedMaxOuter) {
+      reason = -3;
+      break;
+    }
+    const double sc = std::sqrt(h2[0] / (double)n);
+    if (!(sc > 0.0)) {
+      reason = 2;
+      break;
+    }
+    CK(launch_axpby(ls->mx_r, 0.0, 1.0 / sc, ls->mx_r, n, s));
+    CgSolve st;
+    float ms = 0.f;
+    if (int rc = run_cg(ls, ls->mx_r, ls->mx_d, kMixedInnerRtol, 0.0, 1e30, ls->opts.max_it - its, 0,
+                        &st, &ms, lowp))
+      return rc;
+    its += st.its;
+    total_ms += ms;
+    if (st.reason < 0 && st.reason != -3) {  // breakdown or indefinite inner system
+      reason = st.reason;
+      break;
+    }
+    CK(launch_axpby(ls->x, 1.0, sc, ls->mx_d, n, s));
+    CK(launch_residual(op, ls->x, ls->f, ls->mx_r, ls->dinv, 0, ls->mx_part, s));
+    if (int rc = norms(false)) return rc;
+    dp = norm();
+  }
+  out->its = its;
+  out->dp = dp;
+  out->reason = reason;
+  *outer = k;
+  if (kernel_ms) *kernel_ms = total_ms;
+  return SE_OK;
+}
 }  // namespace
 
 
 // ------------------------------------------------- fast diagonalization ----
 namespace {
-constexpr int kFdmPartials = 1184;
 // 1-D assembled stiffness (dense, n x n) and weights on one direction's
 // unknowns: element rows of Kh and w added at the vertices they map to
 // (periodic end folded onto the start, Dirichlet vertices dropped).
@@ -2237,13 +2361,14 @@ namespace {
 int check_opts(const se_solver_opts* o) {
   if (o->method != SE_METHOD_CG && o->method != SE_METHOD_FDM)
     return fail(SE_ERR_ARG, "unknown method %d", o->method);
-  if (o->precision == SE_PREC_FP16)
-    return fail(SE_ERR_UNSUPPORTED, "SE_PREC_FP16 is an apply precision (se_linsys_apply_low) only");
   if (o->precision != SE_PREC_FP64 && o->precision != SE_PREC_MIXED && o->precision != SE_PREC_BF16 &&
-      o->precision != SE_PREC_FP64_TC)
+      o->precision != SE_PREC_FP64_TC && o->precision != SE_PREC_FP16)
     return fail(SE_ERR_ARG, "unknown precision %d", o->precision);
-  if (o->precision != SE_PREC_FP64 && o->method != SE_METHOD_FDM)
-    return fail(SE_ERR_UNSUPPORTED, "reduced precision needs SE_METHOD_FDM");
+  if (o->method == SE_METHOD_FDM && o->precision == SE_PREC_FP16)
+    return fail(SE_ERR_UNSUPPORTED, "SE_PREC_FP16 with SE_METHOD_FDM (BF16, MIXED or FP64_TC)");
+  if (o->method == SE_METHOD_CG && o->precision != SE_PREC_FP64 && o->precision != SE_PREC_BF16 &&
+      o->precision != SE_PREC_FP16)
+    return fail(SE_ERR_UNSUPPORTED, "SE_METHOD_CG runs in FP64, BF16 or FP16");
   if (o->norm_type < SE_NORM_PRECONDITIONED || o->norm_type > SE_NORM_NATURAL)
     return fail(SE_ERR_ARG, "unknown norm type %d", o->norm_type);
   if (o->mode != SE_MODE_REFERENCE && o->mode != SE_MODE_EXACT)
@@ -2344,22 +2469,28 @@ int se_linsys_solve(se_linsys* ls, int remove_null_space, se_solve_stats* stats)
   const MeshDev& m = ls->sol->mesh->dev;
   CgSolve st;
   float kms = 0.f;
-  int rc;
+  int rc, outer = 0;
   if (ls->opts.method == SE_METHOD_FDM) {
     // right-hand side assembly and field update are inside the FDM graph
     rc = run_fdm(ls, remove_null_space, &st, &kms);
     if (rc) return rc;
   } else {
     CK(launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, g_stream));
-    rc = run_cg(ls, ls->f, ls->x, ls->opts.rtol, ls->opts.atol, ls->opts.dtol, ls->opts.max_it,
-                remove_null_space, &st, &kms);
+    if (ls->opts.precision == SE_PREC_FP64) {
+      rc = run_cg(ls, ls->f, ls->x, ls->opts.rtol, ls->opts.atol, ls->opts.dtol, ls->opts.max_it,
+                  remove_null_space, &st, &kms);
+    } else {
+      if (remove_null_space)
+        return fail(SE_ERR_UNSUPPORTED, "the reduced-precision CG does not remove a null space");
+      rc = run_mixed_cg(ls, ls->opts.precision == SE_PREC_BF16 ? 1 : 2, &st, &outer, &kms);
+    }
     if (rc) return rc;
     CK(launch_update_field(ls->op, m, ls->x, ls->sol->vals, g_stream));
   }
   if (stats) {
     stats->reason = st.reason;
     stats->its = st.its;
-    stats->outer_its = ls->opts.method == SE_METHOD_FDM ? st.its : 0;
+    stats->outer_its = ls->opts.method == SE_METHOD_FDM ? st.its : outer;
     stats->rnorm = st.dp;
     stats->rnorm0 = st.rnorm0;
     stats->kernel_ms = kms;
@@ -2392,12 +2523,14 @@ int se_linsys_solve_batch(se_linsys** systems, int n, int remove_null_space, se_
   cudaEvent_t ready;
   CK(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
   CK(cudaEventRecord(ready, saved));
-  std::vector<int> fdm_idx;
+  std::vector<int> fdm_idx, mixed_idx;
   std::map<int, std::vector<int>> cg_groups;
   for (int i = 0; i < n; i++) {
     if (systems[i]->opts.method == SE_METHOD_FDM) fdm_idx.push_back(i);
+    else if (systems[i]->opts.precision != SE_PREC_FP64) mixed_idx.push_back(i);  // one by one
     else cg_groups[systems[i]->op.d[0].N].push_back(i);
   }
+  std::vector<se_solve_stats> mixed_stats(mixed_idx.size());
   int rc = SE_OK;
   for (size_t k = 0; k < fdm_idx.size() && !rc; k++) {
     g_stream = pool[k % pool.size()];
@@ -2428,6 +2561,10 @@ int se_linsys_solve_batch(se_linsys** systems, int n, int remove_null_space, se_
       }
     }
   }
+  for (size_t k = 0; k < mixed_idx.size() && !rc; k++) {
+    rc = se_linsys_solve(systems[mixed_idx[k]], remove_null_space, &mixed_stats[k]);
+    if (rc == SE_ERR_NOT_CONVERGED) rc = SE_OK;  // reported with the others below
+  }
   for (size_t k = 0; k < fdm_idx.size() && !rc; k++)
     rc = fdm_finish(systems[fdm_idx[k]], &st[fdm_idx[k]], &kms[fdm_idx[k]]);
   // the caller's stream sees every solve's result
@@ -2442,7 +2579,15 @@ int se_linsys_solve_batch(se_linsys** systems, int n, int remove_null_space, se_
   cudaEventDestroy(ready);
   if (rc) return rc;
   int worst = SE_OK;
+  std::vector<int> mixed_at(n, -1);
+  for (size_t k = 0; k < mixed_idx.size(); k++) mixed_at[mixed_idx[k]] = (int)k;
   for (int i = 0; i < n; i++) {
+    if (mixed_at[i] >= 0) {
+      const se_solve_stats& ms = mixed_stats[mixed_at[i]];
+      if (stats) stats[i] = ms;
+      if (ms.reason < 0) worst = SE_ERR_NOT_CONVERGED;
+      continue;
+    }
     if (stats) {
       se_solve_stats& o = stats[i];
       o.reason = st[i].reason;

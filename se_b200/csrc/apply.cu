@@ -1024,6 +1024,25 @@ bool residual_ef_supported(const OpDev& op) {
   return op.gamma == 0.0 && op.d[0].N >= 4 && op.d[0].N <= 8;
 }
 
+namespace {
+template <int N>
+int res_ef_blocks(const OpDev& op) {
+  typedef EfTile<N> T;
+  return ((op.d[0].hi + T::TX - 1) / T::TX) * ((op.d[1].hi + T::TY - 1) / T::TY);
+}
+}  // namespace
+
+int residual_partial_blocks(const OpDev& op) {
+  if (!residual_ef_supported(op)) return residual_blocks(op);
+  switch (op.d[0].N) {
+    case 4: return res_ef_blocks<4>(op);
+    case 5: return res_ef_blocks<5>(op);
+    case 6: return res_ef_blocks<6>(op);
+    case 7: return res_ef_blocks<7>(op);
+    default: return res_ef_blocks<8>(op);
+  }
+}
+
 cudaError_t launch_residual_ef(const OpDev& op, const double* x, const double* b, double* r,
                                const double* w, int natural, double* partial, const ResTail& tail,
                                float* split_hi, float* split_lo, int split_pitch, cudaStream_t s) {

@@ -35,6 +35,9 @@
 // divergence formed at the vertices, say) PETSc's iteration (remove_null ==
 // 1) stagnates at the size of the off-range part and ends on an indefinite
 // inner product, where this one converges.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 #include "fdm_ctl.cuh"
 
@@ -155,9 +158,9 @@ __device__ __forceinline__ int unknown_1d(const Dir& d, int g) {
 }
 
 // Assembled 1-D GLL weight and stiffness diagonal at vertex g (e = g/N, a).
-template <int N>
-__device__ __forceinline__ double wsum_n(const Dir& d, const double* w, int e, int a) {
-  double s = 0.0;
+template <int N, class T = double>
+__device__ __forceinline__ T wsum_n(const Dir& d, const T* w, int e, int a) {
+  T s = T(0);
   if (e < d.nE) s += w[a];
   if (a == 0 && (e > 0 || d.periodic)) s += w[N];
   return s;
@@ -172,20 +175,19 @@ __device__ __forceinline__ double kdiag_n(const Dir& d, const double* Kh, int e,
 }
 // Row of the assembled 1-D stiffness at vertex (e, a) applied to the staged
 // values around c (stride between neighbouring vertices).
-template <int N, int STRIDE>
-__device__ __forceinline__ double krow_n(const Dir& d, const double* Kh, int e, int a,
-                                         const double* c) {
+template <int N, int STRIDE, class T = double>
+__device__ __forceinline__ T krow_n(const Dir& d, const T* Kh, int e, int a, const T* c) {
   constexpr int n = N + 1;
-  double s = 0.0;
+  T s = T(0);
   if (a != 0) {
-    const double* k = Kh + a * n;
-    const double* q = c - a * STRIDE;
+    const T* k = Kh + a * n;
+    const T* q = c - a * STRIDE;
 #pragma unroll
     for (int b = 0; b < n; b++) s = fma(k[b], q[b * STRIDE], s);
     return s;
   }
   if (e > 0 || d.periodic) {
-    const double* k = Kh + N * n;
+    const T* k = Kh + N * n;
 #pragma unroll
     for (int b = 0; b < n; b++) s = fma(k[b], c[(b - N) * STRIDE], s);
   }
@@ -202,6 +204,9 @@ struct OpSm {
   double Sv[SE_MAXN1 * SE_MAXN1], Tv[SE_MAXN1 * SE_MAXN1];  // SVV factors (gamma != 0)
   double w[SE_MAXN1];
   double alpha, beta0, beta1, gamma;
+  // FP32 copies for the reduced-precision apply
+  float Khf[SE_MAXN1 * SE_MAXN1], wf[SE_MAXN1];
+  float alphaf, beta0f, beta1f;
   Dir dx, dy;
   int G0, G1;
   int solve;
@@ -214,17 +219,26 @@ __device__ __forceinline__ void load_op(OpSm& o, const CgSolve& S, int solve) {
   __syncthreads();
   const OpDev& op = S.op;
   const int n = op.d[0].N + 1;
-  for (int k = threadIdx.x; k < n * n; k += blockDim.x) o.Kh[k] = op.Kh[k];
+  for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
+    o.Kh[k] = op.Kh[k];
+    o.Khf[k] = (float)op.Kh[k];
+  }
   if (op.gamma != 0.0)
     for (int k = threadIdx.x; k < n * n; k += blockDim.x) {
       o.Sv[k] = op.Sv[k];
       o.Tv[k] = op.Tv[k];
     }
-  if (threadIdx.x < n) o.w[threadIdx.x] = op.w[threadIdx.x];
+  if (threadIdx.x < n) {
+    o.w[threadIdx.x] = op.w[threadIdx.x];
+    o.wf[threadIdx.x] = (float)op.w[threadIdx.x];
+  }
   if (threadIdx.x == 0) {
     o.alpha = op.alpha;
     o.beta0 = op.beta[0];
     o.beta1 = op.beta[1];
+    o.alphaf = (float)op.alpha;
+    o.beta0f = (float)op.beta[0];
+    o.beta1f = (float)op.beta[1];
     o.gamma = op.gamma;
     o.dx = op.d[0];
     o.dy = op.d[1];
@@ -247,9 +261,22 @@ __device__ __forceinline__ void load_op(OpSm& o, const CgSolve& S, int solve) {
 // cross the Kronecker-sum terms read (the tile's rows at full width, its
 // columns at full height), and with an SVV term also the four N x N corners,
 // which its element blocks reach.
-template <int N>
+// The value a staged p takes: FP64 (LP 0), or rounded to BF16 (LP 1) or
+// FP16 (LP 2) and held as FP32, the reduced-precision apply's input.
+template <int LP>
+__device__ __forceinline__ auto lp_value(double v) {
+  if constexpr (LP == 0)
+    return v;
+  else if constexpr (LP == 1)
+    return __bfloat162float(__double2bfloat16(v));
+  else
+    return __half2float(__double2half(v));
+}
+
+template <int N, int LP = 0>
 __device__ __forceinline__ void stage_p(const OpSm& o, int x0, int y0, const double* z,
-                                        const double* po, bool first, double bc, double* P) {
+                                        const double* po, bool first, double bc,
+                                        decltype(lp_value<LP>(0.0))* P) {
   typedef Geo<N> G;
   const int gx0 = x0 + o.dx.lo - N, gy0 = y0 + o.dy.lo - N;
   const int total = G::kRows + G::kCols + (o.gamma != 0.0 ? G::kCorners : 0);
@@ -275,7 +302,7 @@ __device__ __forceinline__ void stage_p(const OpSm& o, int x0, int y0, const dou
       const size_t q = (size_t)uy * o.G0 + ux;
       v = first ? z[q] : fma(bc, po[q], z[q]);
     }
-    P[j * G::W + i] = v;
+    P[j * G::W + i] = lp_value<LP>(v);
   }
   __syncthreads();
 }
@@ -328,6 +355,20 @@ __device__ __forceinline__ double apply_n(const OpSm& o, const double* P, int tx
   const double ky = krow_n<N, G::W>(o.dy, o.Kh, ey, ay, c);
   const double a = o.alpha * wx * wy * c[0] + o.beta0 * wy * kx + o.beta1 * wx * ky;
   return o.gamma != 0.0 ? a + o.gamma * svv_n<N>(o, c, ex, ax, ey, ay) : a;
+}
+
+// (A p) in FP32 arithmetic on the staged reduced-precision p (no SVV term):
+// the same sums as apply_n, FP32 coefficients and accumulation.
+template <int N>
+__device__ __forceinline__ float apply_lp(const OpSm& o, const float* P, int tx, int ty, int gx,
+                                          int gy) {
+  typedef Geo<N> G;
+  const float* c = P + (ty + N) * G::W + (tx + N);
+  const int ex = gx / N, ax = gx - ex * N, ey = gy / N, ay = gy - ey * N;
+  const float wx = wsum_n<N, float>(o.dx, o.wf, ex, ax), wy = wsum_n<N, float>(o.dy, o.wf, ey, ay);
+  const float kx = krow_n<N, 1, float>(o.dx, o.Khf, ex, ax, c);
+  const float ky = krow_n<N, G::W, float>(o.dy, o.Khf, ey, ay, c);
+  return o.alphaf * wx * wy * c[0] + o.beta0f * wy * kx + o.beta1f * wx * ky;
 }
 
 template <int N>
@@ -452,7 +493,7 @@ struct Regs {
 // One pass over the block's tiles; writes the block's segment partials.
 constexpr int kTileCache = 64;  // tile descriptors a block keeps in shared memory
 
-template <int N, int K, int PASS>
+template <int N, int K, int PASS, int LP = 0>
 __device__ __forceinline__ void pass(const CgBatch& B, double* part, const SolveState* st, OpSm& o,
                                      double* P, double (*red)[4], Regs<N, K>& R, int t0, int t1,
                                      const CgTile* tcache) {
@@ -483,10 +524,22 @@ __device__ __forceinline__ void pass(const CgBatch& B, double* part, const Solve
     if (PASS == PS_APPLY) {
       const double* po = S.pbuf ? o.p1 : o.p0;
       double* pn = S.pbuf ? o.p0 : o.p1;
-      stage_p<N>(o, T.x0, T.y0, o.z, po, S.its == 0, S.bcoef, P);
+      double p = 0.0, w = 0.0;
+      if constexpr (LP == 0) {
+        stage_p<N>(o, T.x0, T.y0, o.z, po, S.its == 0, S.bcoef, P);
+        if (in) {
+          p = P[(ty + N) * Geo<N>::W + (tx + N)];
+          w = apply_n<N>(o, P, tx, ty, gx, gy);
+        }
+      } else {
+        float* PF = reinterpret_cast<float*>(P);
+        stage_p<N, LP>(o, T.x0, T.y0, o.z, po, S.its == 0, S.bcoef, PF);
+        if (in) {
+          p = S.its == 0 ? o.z[k] : fma(S.bcoef, po[k], o.z[k]);  // the FP64 direction
+          w = (double)apply_lp<N>(o, PF, tx, ty, gx, gy);
+        }
+      }
       if (in) {
-        const double p = P[(ty + N) * Geo<N>::W + (tx + N)];
-        const double w = apply_n<N>(o, P, tx, ty, gx, gy);
         pn[k] = p;
         if (K > 0) {
           R.p[kk] = p;
@@ -572,7 +625,7 @@ __device__ __forceinline__ void pass(const CgBatch& B, double* part, const Solve
   }
 }
 
-template <int N, int K>
+template <int N, int K, int LP = 0>
 __global__ void __launch_bounds__(kCgThreads, 1) cg_n_kernel(const CgBatch B) {
   extern __shared__ double dyn[];
   SolveState* st = reinterpret_cast<SolveState*>(dyn);
@@ -634,7 +687,7 @@ __global__ void __launch_bounds__(kCgThreads, 1) cg_n_kernel(const CgBatch B) {
   int active = update_states<ST_START>(B, part(), st, mt);
   while (active > 0) {
     ++pc;
-    pass<N, K, PS_APPLY>(B, part(), st, o, P, red, R, t0, t1, tcache);
+    pass<N, K, PS_APPLY, LP>(B, part(), st, o, P, red, R, t0, t1, tcache);
     if (!grid_sync(B.bar_count, B.err)) return;
     update_states<ST_APPLY>(B, part(), st, mt);
     ++pc;
@@ -820,15 +873,35 @@ cudaError_t launch_apply_n(const OpDev& op, const double* x, const double* b, do
   return cudaGetLastError();
 }
 
-template <int N, int K>
+template <int N, int K, int LP = 0>
 const void* kernel_ptr() {
-  return (const void*)cg_n_kernel<N, K>;
+  return (const void*)cg_n_kernel<N, K, LP>;
 }
 
-const void* pick(int N, int K) {
+// lp: 0 FP64 apply (every order); 1 BF16, 2 FP16 input with FP32 arithmetic
+// (orders 4 to 8).
+const void* pick(int N, int K, int lp = 0) {
 #define SE_CASE(n)                                         \
   case n:                                                  \
     return K > 0 ? kernel_ptr<n, kCgResidentTiles>() : kernel_ptr<n, 0>();
+#define SE_LP_CASE(n, l)                                                            \
+  case n:                                                                           \
+    return K > 0 ? kernel_ptr<n, kCgResidentTiles, l>() : kernel_ptr<n, 0, l>();
+  if (lp == 1) {
+    switch (N) {
+      SE_LP_CASE(4, 1) SE_LP_CASE(5, 1) SE_LP_CASE(6, 1) SE_LP_CASE(7, 1) SE_LP_CASE(8, 1)
+      default:
+        return nullptr;
+    }
+  }
+  if (lp == 2) {
+    switch (N) {
+      SE_LP_CASE(4, 2) SE_LP_CASE(5, 2) SE_LP_CASE(6, 2) SE_LP_CASE(7, 2) SE_LP_CASE(8, 2)
+      default:
+        return nullptr;
+    }
+  }
+  if (lp != 0) return nullptr;
   switch (N) {
     SE_CASE(2) SE_CASE(3) SE_CASE(4) SE_CASE(5) SE_CASE(6) SE_CASE(7) SE_CASE(8) SE_CASE(9)
     SE_CASE(10) SE_CASE(11) SE_CASE(12)
@@ -836,6 +909,7 @@ const void* pick(int N, int K) {
       return nullptr;
   }
 #undef SE_CASE
+#undef SE_LP_CASE
 }
 
 }  // namespace
@@ -895,8 +969,8 @@ size_t cg_dyn_smem_bytes(int N, int nsolves) {
          sizeof(double) * (size_t)(kCgTileX + 2 * N) * (kCgTileY + 2 * N);
 }
 
-int cg_max_grid(int device, int N, bool resident, int nsolves) {
-  const void* f = pick(N, resident ? 1 : 0);
+int cg_max_grid(int device, int N, bool resident, int nsolves, int lowp) {
+  const void* f = pick(N, resident ? 1 : 0, lowp);
   if (!f) return 0;
   int sms = 0, per_sm = 0;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess)
@@ -907,8 +981,9 @@ int cg_max_grid(int device, int N, bool resident, int nsolves) {
   return sms * per_sm;
 }
 
-cudaError_t launch_cg(const CgBatch& batch, int grid, int N, bool resident, cudaStream_t s) {
-  const void* f = pick(N, resident ? 1 : 0);
+cudaError_t launch_cg(const CgBatch& batch, int grid, int N, bool resident, cudaStream_t s,
+                      int lowp) {
+  const void* f = pick(N, resident ? 1 : 0, lowp);
   if (!f) return cudaErrorInvalidValue;
   const size_t smem = cg_dyn_smem_bytes(N, batch.nsolves);
   if (smem > 48 * 1024) {

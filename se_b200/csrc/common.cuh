@@ -188,6 +188,8 @@ cudaError_t launch_residual_check(const OpDev& op, const double* x, const double
 // The element-factored residual of orders 4 to 8 without an SVV term
 // (apply.cu); false when the operator needs the general kernel.
 bool residual_ef_supported(const OpDev& op);
+// Partial-sum pairs launch_residual (with b and partial given) writes.
+int residual_partial_blocks(const OpDev& op);
 cudaError_t launch_residual_ef(const OpDev& op, const double* x, const double* b, double* r,
                                const double* w, int natural, double* partial, const ResTail& tail,
                                float* split_hi, float* split_lo, int split_pitch, cudaStream_t s);
@@ -247,10 +249,14 @@ constexpr int kCgResidentTiles = 4;
 // Dynamic shared memory of one CG block (order N, nsolves per launch).
 size_t cg_dyn_smem_bytes(int N, int nsolves);
 // Blocks of kCgThreads that can be co-resident for the CG kernel.
-int cg_max_grid(int device, int N, bool resident, int nsolves);
+int cg_max_grid(int device, int N, bool resident, int nsolves, int lowp = 0);
 // Persistent CG over a batch of same-order solves; resident needs every block
 // to own at most kCgResidentTiles tiles.
-cudaError_t launch_cg(const CgBatch& batch, int grid, int N, bool resident, cudaStream_t s);
+// lowp: 0 the FP64 apply; 1 (BF16) or 2 (FP16): the CG's direction vector
+// rounded to that type for the operator apply, computed in FP32 (orders 4 to
+// 8, no SVV term); dots, updates and the other vectors stay FP64.
+cudaError_t launch_cg(const CgBatch& batch, int grid, int N, bool resident, cudaStream_t s,
+                      int lowp = 0);
 
 // Device-resident parameters and state of an FDM refinement loop.
 struct FdmParams {

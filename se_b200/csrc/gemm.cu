@@ -325,43 +325,80 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// Stages zlow and A's first k columns of rows m0..m0+BM, then U for columns
-// n0..n0+BN, into sm (LowSm layout). Ends with the block synchronised.
+// The low block's global operands of one thread, loaded into registers when
+// the kernel starts (they do not depend on the product), so their latency
+// hides behind the main loop: one zlow entry, this thread's share of A's
+// first 8 columns over the tile's rows, and the 8 leading entries of the
+// ex row of the output column whose U entries this thread forms (entries
+// tid, tid + THREADS, ... of the 8 x BN block, all in column tid % BN).
 template <int BM, int BN, int THREADS>
-__device__ __forceinline__ void low_stage(const GemmArgs<double, double, double>& g, double* sm,
-                                          int m0, int n0, int tid) {
+struct LowRegs {
+  static_assert(THREADS % BN == 0 && THREADS >= kLowMax * kLowMax, "low block thread map");
+  static constexpr int AL = (BM * kLowMax + THREADS - 1) / THREADS;
+  static constexpr int UE = kLowMax * BN / THREADS;
+  double z, al[AL], ex[kLowMax];
+};
+
+template <int BM, int BN, int THREADS>
+__device__ __forceinline__ void low_prefetch(const GemmArgs<double, double, double>& g, int m0,
+                                             int n0, int tid, LowRegs<BM, BN, THREADS>& L) {
   const int lk = g.lowk;
+  {
+    const int a = tid / kLowMax, b = tid % kLowMax;  // zlow entry (a, b) as an 8 x 8 block
+    L.z = (tid < kLowMax * kLowMax && a < lk && b < lk) ? g.zlow[a * lk + b] : 0.0;
+  }
+#pragma unroll
+  for (int q = 0; q < LowRegs<BM, BN, THREADS>::AL; q++) {
+    const int e = tid + q * THREADS, r = e / kLowMax, a = e % kLowMax, gr = m0 + r;
+    L.al[q] = (e < BM * kLowMax && a < lk && gr < g.M) ? g.A[(size_t)gr * g.lda + a] : 0.0;
+  }
+  const int gc = n0 + tid % BN;
+#pragma unroll
+  for (int b = 0; b < kLowMax; b++)
+    L.ex[b] = (b < lk && gc < g.N) ? g.ex[(size_t)gc * g.ldex + b] : 0.0;
+}
+
+// Writes the prefetched operands to sm (LowSm layout: zlow as 8 x 8 padded
+// with zeros, A's rows, U hi and lo) and forms U there; ends with the block
+// synchronised.
+template <int BM, int BN, int THREADS>
+__device__ __forceinline__ void low_stage(double* sm, int tid, const LowRegs<BM, BN, THREADS>& L) {
   double* zl = sm;
   double* al = zl + kLowMax * kLowMax;
   double* uh = al + BM * kLowMax;
   double* ul = uh + kLowMax * BN;
-  for (int e = tid; e < lk * lk; e += THREADS) zl[e] = g.zlow[e];
-  for (int e = tid; e < BM * kLowMax; e += THREADS) {
-    const int r = e / kLowMax, a = e % kLowMax, gr = m0 + r;
-    al[e] = (a < lk && gr < g.M) ? g.A[(size_t)gr * g.lda + a] : 0.0;
+  if (tid < kLowMax * kLowMax) zl[tid] = L.z;
+#pragma unroll
+  for (int q = 0; q < LowRegs<BM, BN, THREADS>::AL; q++) {
+    const int e = tid + q * THREADS;
+    if (e < BM * kLowMax) al[e] = L.al[q];
   }
   __syncthreads();
-  for (int e = tid; e < kLowMax * BN; e += THREADS) {
-    const int a = e / BN, c = e % BN, gc = n0 + c;
+  const int c = tid % BN;
+#pragma unroll
+  for (int q = 0; q < LowRegs<BM, BN, THREADS>::UE; q++) {
+    const int a = (tid + q * THREADS) / BN;
     double h = 0.0, l = 0.0;
-    if (a < lk && gc < g.N)
-      for (int b = 0; b < lk; b++) dd_fma(h, l, zl[a * lk + b], g.ex[(size_t)gc * g.ldex + b]);
-    uh[e] = h;
-    ul[e] = l;
+#pragma unroll
+    for (int b = 0; b < kLowMax; b++) dd_fma(h, l, zl[a * kLowMax + b], L.ex[b]);
+    uh[a * BN + c] = h;
+    ul[a * BN + c] = l;
   }
   __syncthreads();
 }
 
 // v (the product's FP64 output at tile row r, column c) plus the low block,
-// plus the old value when accumulating, rounded once.
+// plus the old value when accumulating, rounded once. Entries beyond lowk
+// are zero in sm, so the sums run over all 8.
 template <int BM, int BN, int EPI>
-__device__ __forceinline__ double low_add(const double* sm, int lk, int r, int c, double v,
+__device__ __forceinline__ double low_add(const double* sm, int r, int c, double v,
                                           const double* dst) {
   const double* al = sm + kLowMax * kLowMax + r * kLowMax;
   const double* uh = sm + kLowMax * kLowMax + BM * kLowMax;
   const double* ul = uh + kLowMax * BN;
   double h = 0.0, l = 0.0;
-  for (int a = 0; a < lk; a++) {
+#pragma unroll
+  for (int a = 0; a < kLowMax; a++) {
     dd_fma(h, l, al[a], uh[a * BN + c]);
     l = fma(al[a], ul[a * BN + c], l);
   }
@@ -380,6 +417,10 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_kernel(const GemmArgs<do
   const int wm = (warp / C::WN) * (C::BM / C::WM), wn = (warp % C::WN) * (C::BN / C::WN);
   const int m0 = blockIdx.y * C::BM, n0 = blockIdx.x * C::BN;
   const int nkt = (g.K + C::BK - 1) / C::BK;
+  LowRegs<C::BM, C::BN, C::THREADS> LR;
+  if constexpr (EPI != EPI_DIVIDE) {
+    if (g.lowk) low_prefetch<C::BM, C::BN, C::THREADS>(g, m0, n0, tid, LR);
+  }
 
   auto issue = [&](int i) {
     const int k0 = i * C::BK;
@@ -449,7 +490,7 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_kernel(const GemmArgs<do
   if constexpr (EPI != EPI_DIVIDE) {
     if (lk) {
       __syncthreads();  // the pipeline's shared memory is free from here
-      low_stage<C::BM, C::BN, C::THREADS>(g, dsm, m0, n0, tid);
+      low_stage<C::BM, C::BN, C::THREADS>(dsm, tid, LR);
     }
   }
 
@@ -476,7 +517,7 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_kernel(const GemmArgs<do
             }
           } else {
             if (lk) {
-              *dst = low_add<C::BM, C::BN, EPI>(dsm, lk, r - m0, c - n0, v, dst);
+              *dst = low_add<C::BM, C::BN, EPI>(dsm, r - m0, c - n0, v, dst);
               continue;
             }
           }
@@ -537,6 +578,10 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_ksplit_kernel(
   const int gq = lane >> 2, tq = lane & 3;
   const int m0 = blockIdx.y * C::BM, n0 = blockIdx.x * C::BN;
   const int nkt = (g.K + C::BK - 1) / C::BK;
+  LowRegs<C::BM, C::BN, C::THREADS> LR;
+  if constexpr (EPI != EPI_DIVIDE) {
+    if (g.lowk) low_prefetch<C::BM, C::BN, C::THREADS>(g, m0, n0, tid, LR);
+  }
 
   auto issue = [&](int i) {
     const int k0 = i * C::BK;
@@ -618,7 +663,7 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_ksplit_kernel(
       }
   const int lk = g.lowk;
   if constexpr (EPI != EPI_DIVIDE) {
-    if (lk) low_stage<C::BM, C::BN, C::THREADS>(g, dsm + C::RED, m0, n0, tid);
+    if (lk) low_stage<C::BM, C::BN, C::THREADS>(dsm + C::RED, tid, LR);
   }
   __syncthreads();
   for (int e = tid; e < C::BM * C::BN; e += C::THREADS) {
@@ -638,7 +683,7 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_ksplit_kernel(
       }
     } else {
       if (lk) {
-        *dst = low_add<C::BM, C::BN, EPI>(dsm + C::RED, lk, r, c, v, dst);
+        *dst = low_add<C::BM, C::BN, EPI>(dsm + C::RED, r, c, v, dst);
         continue;
       }
     }

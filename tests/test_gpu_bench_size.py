@@ -52,7 +52,8 @@ def bench_step(oracle):
     return {"B": B, "phi": phi, "vel": vel, "dt": dt, "sl": sl, "u": u, "its10": st10["its"]}
 
 
-@pytest.mark.parametrize("variant", ["fdm_fp64", "fdm_tf32x3_tc", "fdm_fp64_then_tc", "cg_fp64"])
+@pytest.mark.parametrize("variant", ["fdm_fp64", "fdm_tf32x3_tc", "fdm_fp64_then_tc", "cg_fp64",
+                                     "cg_bf16_apply_refined", "cg_fp16_apply_refined"])
 def test_bench_step_matches_oracle(segpu, bench_step, variant):
     S, h = segpu, bench_step
     B = h["B"]
@@ -67,7 +68,8 @@ def test_bench_step_matches_oracle(segpu, bench_step, variant):
     adv.Advect(dt)
     assert rel(adv.fieldSL.vals, h["sl"]) < 1e-12
     opts = S.solver_opts(rtol=B.RTOL, mode=S.MODE_EXACT, method=getattr(S, meth),
-                         precision=getattr(S, prec), max_it=10000)
+                         precision=getattr(S, prec),
+                         max_it=100000 if prec in ("PREC_BF16", "PREC_FP16") else 10000)
     helm = S.HelmholtzEqn(u, adv.fieldSL, -B.LAMBDA, -1.0, 1.0, 0, opts)
     st = helm.Solve("helm_", raise_on_diverge=True)
     assert st["reason"] > 0

@@ -193,7 +193,8 @@ def test_option_checks(segpu):
     b = segpu.BCs(False, False, False, False, m)
     u, r = segpu.Field("u", m, 1, b), segpu.Field("r", m, 1, b)
     for bad in (dict(precision=segpu.PREC_FP16, method=segpu.METHOD_FDM),
-                dict(precision=segpu.PREC_BF16, method=segpu.METHOD_CG),
+                dict(precision=segpu.PREC_MIXED, method=segpu.METHOD_CG),
+                dict(precision=segpu.PREC_FP64_TC, method=segpu.METHOD_CG),
                 dict(method=7), dict(norm_type=5)):
         with pytest.raises(segpu.SEError):
             segpu.HelmholtzEqn(u, r, -1.0, -1.0, 1.0, 0, segpu.solver_opts(**bad))
@@ -356,6 +357,53 @@ def test_fdm_solve_matches_oracle(segpu, oracle, case, prec):
     got = fs.vals
     assert np.abs(got - ref_sol).max() <= 1e-8 * np.abs(ref_sol).max()
     assert np.array_equal(got[f2v < 0], sol[f2v < 0])
+
+
+@pytest.mark.parametrize("case", [CASES_EF[0], CASES_EF[1], CASES_EF[3], CASES_EF[6], CASES_EF[8],
+                                  CASES8[0], CASES8[1]])
+@pytest.mark.parametrize("prec", ["bf16", "fp16"])
+def test_cg_reduced_precision_apply_refined(segpu, oracle, case, prec):
+    """CG whose operator apply reads its direction vector in BF16 / FP16 and
+    computes in FP32, inside FP64 iterative refinement with the double-double
+    residual, to rtol 1e-10: the oracle's CG solution at rtol 1e-14 within
+    1e-8 of its magnitude, reached over several refinement steps; Dirichlet
+    values untouched."""
+    om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, case, -3.0, -1.0, 1.0, True,
+                                                     seed=7)
+    ref_sol, st = oracle.helmholtz_solve(om, sol, rhs, -3.0, -1.0, 1.0, bcs=case[6], quirk=True,
+                                         rtol=1e-14)
+    p = segpu.PREC_BF16 if prec == "bf16" else segpu.PREC_FP16
+    ls.set_opts(segpu.solver_opts(rtol=1e-10, method=segpu.METHOD_CG, precision=p,
+                                  max_it=100000))
+    out = ls.Solve("helm_")
+    assert out["reason"] == 2, out
+    assert out["outer_its"] >= 2 and out["rnorm"] <= 1e-10 * out["rnorm0"], out
+    got = fs.vals
+    assert np.abs(got - ref_sol).max() <= 1e-8 * np.abs(ref_sol).max()
+    assert np.array_equal(got[f2v < 0], sol[f2v < 0])
+    # deterministic: the same solve again gives the same bits
+    again = ls.Solve("helm_")
+    assert again["its"] == out["its"] and np.array_equal(fs.vals, got)
+
+
+def test_cg_reduced_precision_refusals(segpu):
+    """The reduced-precision CG covers orders 4-8 without SVV or null-space
+    removal; the rest is refused, not run in another precision."""
+    o = segpu.solver_opts(rtol=1e-10, method=segpu.METHOD_CG, precision=segpu.PREC_BF16)
+    m = segpu.Mesh("m", [4, 4], "legendre", 3, [0, 0], [1, 1], [True, True])
+    b = segpu.BCs(False, False, False, False, m)
+    u, r = segpu.Field("u", m, 1, b), segpu.Field("r", m, 1, b)
+    r.vals = np.cos(2 * np.pi * m.verts[:, 0])
+    with pytest.raises(segpu.SEError) as e:
+        segpu.HelmholtzEqn(u, r, -1.0, -1.0, 1.0, 0, o).Solve("helm_")
+    assert e.value.code == segpu.SE_ERR_UNSUPPORTED
+    m6 = segpu.Mesh("m6", [4, 4], "legendre", 6, [0, 0], [1, 1], [True, True])
+    b6 = segpu.BCs(False, False, False, False, m6)
+    u6, r6 = segpu.Field("u", m6, 1, b6), segpu.Field("r", m6, 1, b6)
+    r6.vals = np.cos(2 * np.pi * m6.verts[:, 0])
+    with pytest.raises(segpu.SEError) as e:
+        segpu.PoissonEqn(u6, r6, 1.0, o).Solve(removeNullSpace=True)
+    assert e.value.code == segpu.SE_ERR_UNSUPPORTED
 
 
 def test_fdm_config0_exact_modal_and_null_space(segpu, oracle):
