@@ -663,9 +663,14 @@ constexpr int kMixedMaxOuter = 100;
 //   s = RMS of D^-1 r;  solve A d = r / s by that CG to kMixedInnerRtol
 //   x += s d               (FP64)
 // The dots, updates and vectors of the inner CG stay FP64; the scaling keeps
-// FP16 directions inside its range. out: its = inner CG iterations summed,
-// dp / rnorm0 the outer residual norms, reason PETSc's code (2 rtol, 3 atol,
-// -3 iterations, -4 dtol, or the inner CG's breakdown).
+// FP16 directions inside its range. The apply's rounding perturbs the
+// operator by about 2^-9 (BF16) or 2^-12 (FP16) of the direction, so the
+// inner solves converge only while that times the system's condition number
+// stays well below 1; past it the outer residual stops falling and the solve
+// ends with SE_KSP_DIVERGED_BREAKDOWN (the FDM refinement's rule: no 10% gain
+// in three steps). out: its = inner CG iterations summed, dp / rnorm0 the
+// outer residual norms, reason PETSc's code (2 rtol, 3 atol, -3 iterations,
+// -4 dtol, -5 stalled, or the inner CG's breakdown).
 int run_mixed_cg(se_linsys* ls, int lowp, CgSolve* out, int* outer, float* kernel_ms) {
   const OpDev& op = ls->op;
   const size_t n = (size_t)ls->n;
@@ -718,8 +723,8 @@ int run_mixed_cg(se_linsys* ls, int lowp, CgSolve* out, int* outer, float* kerne
   std::memset(out, 0, sizeof(*out));
   out->rnorm0 = rnorm0;
   float total_ms = 0.f;
-  int its = 0, k = 0, reason = 0;
-  double dp = rnorm0;
+  int its = 0, k = 0, reason = 0, stalled = 0;
+  double dp = rnorm0, prev = rnorm0;
   for (;; k++) {
     if (dp <= ttol) {
       reason = dp <= ls->opts.atol ? 3 : 2;
@@ -729,6 +734,14 @@ int run_mixed_cg(se_linsys* ls, int lowp, CgSolve* out, int* outer, float* kerne
       reason = -4;
       break;
     }
+    if (k > 0) {  // the FDM refinement's rule: no 10% gain in three steps
+      stalled = dp > 0.9 * prev ? stalled + 1 : 0;
+      if (stalled >= 3) {
+        reason = SE_KSP_DIVERGED_BREAKDOWN;
+        break;
+      }
+    }
+    prev = dp;
     if (its >= ls->opts.max_it || k >= kMixedMaxOuter) {
       reason = -3;
       break;
@@ -741,8 +754,12 @@ int run_mixed_cg(se_linsys* ls, int lowp, CgSolve* out, int* outer, float* kerne
     CK(launch_axpby(ls->mx_r, 0.0, 1.0 / sc, ls->mx_r, n, s));
     CgSolve st;
     float ms = 0.f;
-    if (int rc = run_cg(ls, ls->mx_r, ls->mx_d, kMixedInnerRtol, 0.0, 1e30, ls->opts.max_it - its, 0,
-                        &st, &ms, lowp))
+    // an inner solve ends at its tolerance or after n iterations (where CG
+    // in exact arithmetic is done; one that stalls on the reduced-precision
+    // apply hands the refinement what it has)
+    const int inner_max = (int)std::min<long>(ls->opts.max_it - its, std::max<long>(100, (long)n));
+    if (int rc = run_cg(ls, ls->mx_r, ls->mx_d, kMixedInnerRtol, 0.0, 1e30, inner_max, 0, &st, &ms,
+                        lowp))
       return rc;
     its += st.its;
     total_ms += ms;

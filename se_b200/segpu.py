@@ -46,7 +46,7 @@ PREC_FP64, PREC_MIXED, PREC_BF16, PREC_FP16, PREC_FP64_TC = 0, 1, 2, 3, 4
 METHOD_CG, METHOD_FDM = 0, 1
 
 KSP_REASONS = {2: "CONVERGED_RTOL", 3: "CONVERGED_ATOL", -3: "DIVERGED_ITS",
-               -4: "DIVERGED_DTOL", -8: "DIVERGED_INDEFINITE_PC",
+               -4: "DIVERGED_DTOL", -5: "DIVERGED_BREAKDOWN", -8: "DIVERGED_INDEFINITE_PC",
                -9: "DIVERGED_NANORINF", -10: "DIVERGED_INDEFINITE_MAT"}
 
 
