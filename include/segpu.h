@@ -235,7 +235,7 @@ int se_solver_opts_default(se_solver_opts* opts);
  * "-helm_ksp_rtol 1e-10 -helm_ksp_max_it 500", into opts. Unknown options
  * and other prefixes are ignored; a ksp_type other than cg or preonly, or a
  * pc_type other than jacobi or fdm, returns SE_ERR_UNSUPPORTED. One key is
- * this library's own: -<prefix>precision fp64|mixed|fp64_tc|bf16 sets
+ * this library's own: -<prefix>precision fp64|mixed|fp64_tc|bf16|fp16 sets
  * opts->precision. */
 int se_solver_opts_parse(se_solver_opts* opts, const char* prefix, const char* options);
 

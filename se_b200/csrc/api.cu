@@ -2367,7 +2367,8 @@ int se_solver_opts_parse(se_solver_opts* o, const char* prefix, const char* opti
       else if (val == "mixed") o->precision = SE_PREC_MIXED;
       else if (val == "fp64_tc") o->precision = SE_PREC_FP64_TC;
       else if (val == "bf16") o->precision = SE_PREC_BF16;
-      else return fail(SE_ERR_UNSUPPORTED, "precision %s (fp64, mixed, fp64_tc, bf16)", val.c_str());
+      else if (val == "fp16") o->precision = SE_PREC_FP16;
+      else return fail(SE_ERR_UNSUPPORTED, "precision %s (fp64, mixed, fp64_tc, bf16, fp16)", val.c_str());
     }
   }
   return SE_OK;

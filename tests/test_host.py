@@ -87,6 +87,8 @@ def test_solver_options_parse(segpu):
     assert o.method == segpu.METHOD_FDM and o.precision == segpu.PREC_FP64_TC
     o = segpu.solver_opts("helm_", "-helm_pc_type fdm -helm_precision mixed")
     assert o.precision == segpu.PREC_MIXED
+    o = segpu.solver_opts("helm_", "-helm_ksp_type cg -helm_precision fp16")
+    assert o.method == segpu.METHOD_CG and o.precision == segpu.PREC_FP16
     with pytest.raises(segpu.SEError) as e:
         segpu.solver_opts("helm_", "-helm_precision fp8")
     assert e.value.code == segpu.SE_ERR_UNSUPPORTED
