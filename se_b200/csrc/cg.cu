@@ -280,7 +280,23 @@ __device__ __forceinline__ void stage_p(const OpSm& o, int x0, int y0, const dou
   typedef Geo<N> G;
   const int gx0 = x0 + o.dx.lo - N, gy0 = y0 + o.dy.lo - N;
   const int total = G::kRows + G::kCols + (o.gamma != 0.0 ? G::kCorners : 0);
-  for (int k = threadIdx.x; k < total; k += kCgThreads) {
+  // A tile whose staged window lies inside the unknown range of both
+  // directions (no periodic wrap, no Dirichlet or outside vertex) indexes its
+  // unknowns affinely; the others map each vertex (unknown_1d).
+  const bool interior = gx0 >= o.dx.lo && gx0 + G::W <= o.dx.hi && gy0 >= o.dy.lo &&
+                        gy0 + G::H <= o.dy.hi;
+  const size_t base = interior ? (size_t)(gy0 - o.dy.lo) * o.G0 + (gx0 - o.dx.lo) : 0;
+  // every load of the thread issued before any is used (one memory round
+  // trip per tile instead of one per staged value)
+  constexpr int MAXK = (G::kRows + G::kCols + G::kCorners + kCgThreads - 1) / kCgThreads;
+  double v[MAXK];
+  int pos[MAXK];
+#pragma unroll
+  for (int t = 0; t < MAXK; t++) {
+    const int k = threadIdx.x + t * kCgThreads;
+    v[t] = 0.0;
+    pos[t] = -1;
+    if (k >= total) continue;
     int i, j;
     if (k < G::kRows) {
       j = N + k / G::W;
@@ -296,14 +312,19 @@ __device__ __forceinline__ void stage_p(const OpSm& o, int x0, int y0, const dou
       i = ci < N ? ci : ci + kCgTileX;
       j = cj < N ? cj : cj + kCgTileY;
     }
-    double v = 0.0;
-    const int ux = unknown_1d(o.dx, gx0 + i), uy = unknown_1d(o.dy, gy0 + j);
-    if (ux >= 0 && uy >= 0) {
-      const size_t q = (size_t)uy * o.G0 + ux;
-      v = first ? z[q] : fma(bc, po[q], z[q]);
+    pos[t] = j * G::W + i;
+    long q = -1;
+    if (interior) {
+      q = (long)(base + (size_t)j * o.G0 + i);
+    } else {
+      const int ux = unknown_1d(o.dx, gx0 + i), uy = unknown_1d(o.dy, gy0 + j);
+      if (ux >= 0 && uy >= 0) q = (long)uy * o.G0 + ux;
     }
-    P[j * G::W + i] = lp_value<LP>(v);
+    if (q >= 0) v[t] = first ? z[q] : fma(bc, po[q], z[q]);
   }
+#pragma unroll
+  for (int t = 0; t < MAXK; t++)
+    if (pos[t] >= 0) P[pos[t]] = lp_value<LP>(v[t]);
   __syncthreads();
 }
 
