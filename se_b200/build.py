@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsegpu.so")
-SOURCES = ["api.cu", "sl.cu", "linsys.cu", "cg.cu", "fdm.cu", "gemm.cu", "tc_gemm.cu", "apply.cu", "server.cu"]
+SOURCES = ["api.cu", "sl.cu", "linsys.cu", "cg.cu", "fdm.cu", "gemm.cu", "tc_gemm.cu", "apply.cu", "server.cu", "bloch.cu"]
 LIBS = ["-lcusolver"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -269,6 +270,11 @@ struct se_linsys {
   double *X1, *X2, *ax;       // FP64 work: two transform buffers, A x
   double* zlow;               // FP64 inverse: the low spectral block [lowk][lowk]
   int lowk;
+  // FP64 inverse of a doubly periodic system with 2^k elements per
+  // direction: Bloch form (bloch.cu) with its complex spectral work array
+  bool bloch;
+  BlochDir bdx, bdy;
+  double2* xh;
   // CG with the reduced-precision apply in FP64 refinement: outer residual,
   // inner solution, norm partials [2 * mx_np] + results [16]
   double *mx_r, *mx_d, *mx_part;
@@ -524,6 +530,7 @@ void linsys_free(se_linsys* ls) {
   dfree(ls->X2);
   dfree(ls->ax);
   dfree(ls->zlow);
+  dfree(ls->xh);
   dfree(ls->mx_r);
   dfree(ls->mx_d);
   dfree(ls->mx_part);
@@ -1113,6 +1120,140 @@ int eig_get(const Dir& d, const double* Kh, const double* w, int prec, Eig1D** o
   return SE_OK;
 }
 
+// ---- Bloch form of a periodic direction (bloch.cu) ----
+typedef std::complex<long double> cld;
+
+// Eigenvalues and eigenvectors of a Hermitian n x n matrix (row-major, long
+// double) by cyclic complex Jacobi rotations: each pivot's phase is moved
+// into column q, then a real rotation (Numerical Recipes' tan formula)
+// zeroes it. A is overwritten; U's columns are the eigenvectors. Jacobi in
+// extended precision gives eigenvectors accurate to the FP64 rounding even
+// for the small eigenvalues of these blocks, whose spread is about 1e5.
+void herm_jacobi(int n, std::vector<cld>& A, std::vector<cld>& U, std::vector<long double>& ev) {
+  U.assign((size_t)n * n, cld(0));
+  for (int i = 0; i < n; i++) U[(size_t)i * n + i] = 1;
+  for (int sweep = 0; sweep < 100; sweep++) {
+    long double off = 0, dg = 0;
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++)
+        (i == j ? dg : off) += std::norm(A[(size_t)i * n + j]);
+    if (off <= 1e-36L * dg) break;
+    for (int p = 0; p < n - 1; p++)
+      for (int q = p + 1; q < n; q++) {
+        const cld apq = A[(size_t)p * n + q];
+        const long double r = std::abs(apq);
+        if (r == 0) continue;
+        const cld ph = apq / r, phc = std::conj(ph);
+        for (int k = 0; k < n; k++) {
+          A[(size_t)k * n + q] *= phc;  // column q by e^{-i phi}
+          U[(size_t)k * n + q] *= phc;
+        }
+        for (int k = 0; k < n; k++) A[(size_t)q * n + k] *= ph;  // row q by e^{i phi}
+        const long double app = A[(size_t)p * n + p].real(), aqq = A[(size_t)q * n + q].real();
+        const long double th = (aqq - app) / (2 * r);
+        const long double t = (th >= 0 ? 1 : -1) / (std::fabs(th) + std::sqrt(th * th + 1));
+        const long double c = 1 / std::sqrt(t * t + 1), sn = t * c;
+        for (int k = 0; k < n; k++) {
+          const cld akp = A[(size_t)k * n + p], akq = A[(size_t)k * n + q];
+          A[(size_t)k * n + p] = c * akp - sn * akq;
+          A[(size_t)k * n + q] = sn * akp + c * akq;
+          const cld ukp = U[(size_t)k * n + p], ukq = U[(size_t)k * n + q];
+          U[(size_t)k * n + p] = c * ukp - sn * ukq;
+          U[(size_t)k * n + q] = sn * ukp + c * ukq;
+        }
+        for (int k = 0; k < n; k++) {
+          const cld apk = A[(size_t)p * n + k], aqk = A[(size_t)q * n + k];
+          A[(size_t)p * n + k] = c * apk - sn * aqk;
+          A[(size_t)q * n + k] = sn * apk + c * aqk;
+        }
+      }
+  }
+  ev.resize(n);
+  for (int i = 0; i < n; i++) ev[i] = A[(size_t)i * n + i].real();
+}
+
+struct Bloch1D {
+  BlochDir d;
+  double2 *V = nullptr, *tw = nullptr;
+  double* mu = nullptr;
+};
+std::mutex g_bloch_mu;
+std::map<std::pair<int, int>, Bloch1D*> g_bloch[64];
+
+// A periodic direction of 2^k >= 2 elements qualifies for the Bloch form
+// when its transforms fit the kernels' 48 KB of shared memory (the y pass
+// holds two complex copies of a column and the twiddles).
+bool bloch_ok(const Dir& d) {
+  return d.periodic && d.lo == 0 && d.nE >= 2 && (d.nE & (d.nE - 1)) == 0 &&
+         16L * (2L * d.N * d.nE + d.nE / 2 + 1) <= 48L * 1024;
+}
+
+// The nel wavenumber blocks of one periodic direction (cached per device,
+// element count and order): K_m and W_m from the reference element's
+// stiffness Kh and weights w (the operator's coefficients scale them),
+// W_m^{-1/2} K_m W_m^{-1/2} = U diag(mu) U^H by herm_jacobi, V = W^{-1/2} U.
+int bloch_get(const Dir& d, const double* Kh, const double* w, Bloch1D** out) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(SE_ERR_UNSUPPORTED, "device index %d", dev);
+  std::lock_guard<std::mutex> lk(g_bloch_mu);
+  Bloch1D*& b = g_bloch[dev][std::make_pair(d.nE, d.N)];
+  if (b) {
+    *out = b;
+    return SE_OK;
+  }
+  const int nel = d.nE, p = d.N, n1 = p + 1;
+  int logn = 0;
+  while ((1 << logn) < nel) logn++;
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  std::vector<double2> V((size_t)nel * p * p), tw(std::max(1, nel / 2));
+  std::vector<double> mu((size_t)nel * p);
+  std::vector<long double> ws(p);
+  for (int i = 0; i < p; i++) ws[i] = 1 / std::sqrt((long double)w[i] + (i == 0 ? w[p] : 0.0));
+  std::vector<cld> A((size_t)p * p), U;
+  std::vector<long double> ev;
+  for (int m = 0; m < nel; m++) {
+    const long double th = two_pi * m / nel;
+    const cld eth(std::cos(th), std::sin(th));
+    for (int i = 0; i < p; i++)
+      for (int j = 0; j < p; j++) {
+        cld v = (long double)Kh[i * n1 + j];
+        if (i == 0 && j == 0) v += (long double)Kh[p * n1 + p];
+        if (j == 0) v += (long double)Kh[i * n1 + p] * eth;
+        if (i == 0) v += (long double)Kh[p * n1 + j] * std::conj(eth);
+        A[(size_t)i * p + j] = ws[i] * v * ws[j];
+      }
+    herm_jacobi(p, A, U, ev);
+    for (int i = 0; i < p; i++)
+      for (int k = 0; k < p; k++) {
+        const cld v = ws[i] * U[(size_t)i * p + k];
+        V[((size_t)m * p + i) * p + k] = make_double2((double)v.real(), (double)v.imag());
+      }
+    for (int k = 0; k < p; k++) mu[(size_t)m * p + k] = (double)ev[k];
+  }
+  for (int j = 0; j < nel / 2; j++) {
+    const long double a = two_pi * j / nel;
+    tw[j] = make_double2((double)std::cos(a), (double)-std::sin(a));
+  }
+  Bloch1D* nb = new Bloch1D();
+  int rc;
+  if ((rc = dalloc(&nb->V, V.size())) || (rc = dalloc(&nb->tw, tw.size())) ||
+      (rc = dalloc(&nb->mu, mu.size()))) {
+    dfree(nb->V);
+    dfree(nb->tw);
+    dfree(nb->mu);
+    delete nb;
+    return rc;
+  }
+  CK(upload_now(nb->V, V.data(), sizeof(double2) * V.size()));
+  CK(upload_now(nb->tw, tw.data(), sizeof(double2) * tw.size()));
+  CK(upload_now(nb->mu, mu.data(), sizeof(double) * mu.size()));
+  nb->d = BlochDir{nel, p, logn, nb->V, nb->mu, nb->tw};
+  b = nb;
+  *out = b;
+  return SE_OK;
+}
+
 int fdm_setup(se_linsys* ls, int prec) {
   if (ls->svv)
     return fail(SE_ERR_UNSUPPORTED, "the SVV operator needs SE_METHOD_CG (no fast diagonalization)");
@@ -1141,6 +1282,15 @@ int fdm_setup(se_linsys* ls, int prec) {
         (rc = dalloc(&ls->zlow, 64)) || (rc = dalloc(&ls->fpart, 2 * (size_t)ls->fpart_n + 16)))
       return rc;
     ls->lowk = std::min(8, std::min(op.G[0], op.G[1]));
+    if (bloch_ok(op.d[0]) && bloch_ok(op.d[1])) {
+      Bloch1D *bx = nullptr, *by = nullptr;
+      if ((rc = bloch_get(op.d[0], op.Kh, op.w, &bx)) || (rc = bloch_get(op.d[1], op.Kh, op.w, &by)))
+        return rc;
+      ls->bdx = bx->d;
+      ls->bdy = by->d;
+      if ((rc = dalloc(&ls->xh, bloch_spectrum_elems(ls->bdx, ls->bdy)))) return rc;
+      ls->bloch = true;
+    }
     // Jacobi inverse for the preconditioned residual norm
     CK(launch_op_diag(op, ls->dinv, g_stream));
     CK(launch_invert(ls->dinv, n, g_stream));
@@ -1208,6 +1358,11 @@ int fdm_apply64(se_linsys* ls, const double* in, double* out, bool accumulate) {
   const int gx = ls->op.G[0], gy = ls->op.G[1];
   const OpDev& op = ls->op;
   const double nt = null_tol(ls);
+  if (ls->bloch) {
+    CK(launch_bloch_inverse(ls->bdx, ls->bdy, op.alpha, op.beta[0], op.beta[1], nt, in, out,
+                            accumulate, ls->xh, g_stream));
+    return SE_OK;
+  }
   const FdmLow low{ls->zlow, ls->SxT, gx, ls->lowk};
   CK(launch_fdm_gemm(0, 0, in, 1, ls->SxT, ls->X1, 1, gy, gx, gx, gx, gx, gx, nullptr, nullptr,
                      nullptr, nullptr, 0, 0, 0, 0, g_stream));

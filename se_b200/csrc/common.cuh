@@ -325,6 +325,24 @@ cudaError_t launch_tc_split(const double* x, int rows, int cols, int ld, float* 
 // epi 0 or 2 the product's outputs get sum_a A[r][a] U[a][c] added, U[a][c] =
 // sum_b zlow[a][b] ex[c * ldex + b], in double-double (with the old value
 // for epi 2), rounded once.
+// One periodic direction of nel = 2^logn equal elements of order p in Bloch
+// form (bloch.cu): V [nel][p][p] complex, row i column k, the W-orthonormal
+// eigenvectors of wavenumber m; mu [nel][p] their eigenvalues; tw [nel/2]
+// the FFT twiddles exp(-2 pi i j / nel).
+struct BlochDir {
+  int nel, p, logn;
+  const double2* V;
+  const double* mu;
+  const double2* tw;
+};
+// x (= or +=) A^{-1} in for a doubly periodic system by Bloch waves (three
+// launches); xh: bloch_spectrum_elems complex work. Shared memory limits:
+// 16 p nel bytes (x direction) and 32 p nel bytes (y) each at most 48 KB.
+cudaError_t launch_bloch_inverse(const BlochDir& bx, const BlochDir& by, double alpha, double cx,
+                                 double cy, double null_tol, const double* in, double* out,
+                                 bool accumulate, double2* xh, cudaStream_t s);
+size_t bloch_spectrum_elems(const BlochDir& bx, const BlochDir& by);
+
 struct FdmLow {
   double* zlow;
   const double* ex;

@@ -161,6 +161,69 @@ def test_fdm_apply_inverts_operator(segpu, oracle, case):
     assert (np.abs(A.matvec(x) - r) / scale).max() < 1e-12
 
 
+# Doubly periodic meshes with 2^k elements per direction: the FP64 inverse
+# takes the Bloch form (an FFT across elements and p x p blocks per
+# wavenumber) instead of dense eigenvector products.
+CASES_BLOCH = [
+    (8, 16, 4, (0.0, 0.0), (1.0, 2.0), (True, True), (False, False, False, False)),
+    (16, 4, 6, (0.0, 0.0), (2.0, 1.0), (True, True), (False, False, False, False)),
+    (32, 32, 8, (0.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False)),
+    (2, 8, 12, (-1.0, 0.0), (1.0, 1.0), (True, True), (False, False, False, False)),
+]
+
+
+@pytest.mark.parametrize("case", CASES_BLOCH)
+@pytest.mark.parametrize("quirk", [False, True])
+def test_fdm_bloch_inverts_operator(segpu, oracle, case, quirk):
+    """The Bloch-form inverse: A (A^{-1} r) = r to FP64 rounding (relative to
+    |A| |x|: 1e-12, 3e-12 at order 12, whose element blocks span a wider
+    range of eigenvalues), for the true-Jacobian and the detJ = 1 operators,
+    square and stretched elements, orders 4 to 12."""
+    om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, case, -2.0, -1.0, 0.5, quirk)
+    n = ls.vecSize
+    r = np.random.default_rng(11).standard_normal(n)
+    rd = torch.tensor(r, device="cuda", dtype=torch.float64)
+    xd = torch.zeros(n, device="cuda", dtype=torch.float64)
+    ls.fdm_apply(rd.data_ptr(), xd.data_ptr())
+    torch.cuda.synchronize()
+    x = xd.cpu().numpy()
+    rowptr, col, val, _ = A.arrays()
+    scale = np.array([np.abs(val[rowptr[i]:rowptr[i + 1]]).sum() for i in range(n)]) * np.abs(x).max()
+    assert (np.abs(A.matvec(x) - r) / scale).max() < (3e-12 if case[2] == 12 else 1e-12)
+
+
+@pytest.mark.parametrize("case", CASES_BLOCH)
+def test_fdm_bloch_solve_matches_oracle(segpu, oracle, case):
+    """FDM solve in Bloch form, refined in FP64 to rtol 1e-10: the oracle's CG
+    solution at rtol 1e-14 within 1e-8 of its magnitude; a periodic Poisson
+    system with its null space removed likewise."""
+    om, m, fs, fr, ls, A, f2v, v2f, sol, rhs = build(segpu, oracle, case, -3.0, -1.0, 1.0, False,
+                                                     seed=21)
+    ref_sol, st = oracle.helmholtz_solve(om, sol, rhs, -3.0, -1.0, 1.0, bcs=case[6], quirk=False,
+                                         rtol=1e-14)
+    ls.set_opts(segpu.solver_opts(rtol=1e-10, method=segpu.METHOD_FDM, mode=segpu.MODE_EXACT))
+    out = ls.Solve("helm_")
+    assert out["reason"] == 2 and out["its"] <= 2, out
+    assert np.abs(fs.vals - ref_sol).max() <= 1e-8 * np.abs(ref_sol).max()
+    # Poisson, constant null space
+    X = om.verts()
+    f = om.periodic_update(np.cos(2 * np.pi * X[:, 0] / (case[4][0] - case[3][0]))
+                           * np.sin(2 * np.pi * X[:, 1] / (case[4][1] - case[3][1])))
+    bc = segpu.BCs(False, False, False, False, m)
+    u, rf = segpu.Field("u", m, 1, bc), segpu.Field("f", m, 1, bc)
+    rf.vals = f
+    ps = segpu.PoissonEqn(u, rf, 1.0, segpu.solver_opts(rtol=1e-10, method=segpu.METHOD_FDM,
+                                                        mode=segpu.MODE_EXACT))
+    out = ps.Solve(removeNullSpace=True)
+    assert out["reason"] == 2, out
+    u_cg = segpu.Field("ucg", m, 1, bc)
+    pc = segpu.PoissonEqn(u_cg, rf, 1.0, segpu.solver_opts(rtol=1e-13, mode=segpu.MODE_EXACT))
+    pc.Solve(removeNullSpace=True)
+    ref = u_cg.vals - u_cg.vals.mean()
+    got = u.vals - u.vals.mean()
+    assert np.abs(got - ref).max() <= 1e-8 * np.abs(ref).max()
+
+
 @pytest.mark.parametrize("case", [0, 1, 4])
 def test_fdm_apply_tensor_cores_inverts_operator(segpu, oracle, case):
     """se_linsys_fdm_apply_prec(SE_PREC_MIXED): the FDM inverse on the tcgen05
