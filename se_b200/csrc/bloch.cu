@@ -22,8 +22,9 @@
 //                     wavenumbers by conjugate symmetry (the result is real),
 //                     inverse FFT, store or accumulate.
 // The passes are latency-bound: one row (mode) per block, at most 32
-// registers a thread (8 blocks per SM) and the twiddles in shared memory,
-// so that a whole pass fits one wave.
+// registers a thread (8 blocks per SM), the order a template parameter (the
+// p-term sums unrolled, their loads issued together) and the twiddles in
+// shared memory.
 // The spectral array is complex, column-major over the x modes
 // ([(m_x, k_x)][y]). Element counts are powers of two (the FFT); the
 // twiddles are tabulated on the host in extended precision. The FFT's
@@ -37,7 +38,6 @@ namespace seg {
 namespace {
 
 constexpr int kBlochThreads = 256;
-constexpr int kBlochMaxP = SE_MAXN;  // the sums over a block's p terms unroll to this
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
@@ -50,18 +50,19 @@ __device__ __forceinline__ int bitrev(int v, int logn) {
   return logn == 0 ? 0 : (int)(__brev((unsigned)v) >> (32 - logn));
 }
 
-// In-place radix-2 FFTs of length n = 2^logn on nseq sequences S[s][0..n)
-// (stride n), input in bit-reversed order, output in natural order.
-// inverse: conjugate twiddles. Unnormalised.
-__device__ void fft_seqs(double2* S, int nseq, int n, int logn, const double2* tw, bool inverse) {
-  const int nb = nseq * (n / 2);
+// In-place radix-2 FFTs of length n = 2^logn on NSEQ sequences S[s][0..n)
+// (stride n), input in bit-reversed order, output in natural order;
+// inverse: conjugate twiddles (tw in shared memory). Unnormalised.
+template <int NSEQ>
+__device__ __forceinline__ void fft_seqs(double2* S, int n, int logn, const double2* tw,
+                                         bool inverse) {
+  const int hn = n >> 1, nb = NSEQ * hn;
   for (int s = 1; s <= logn; s++) {
-    const int m2 = 1 << s, half = m2 >> 1, step = n / m2;
+    const int half = 1 << (s - 1), step = n >> s;
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-      const int q = b / (n / 2), j = b - q * (n / 2);
-      const int grp = j / half, pos = j - grp * half;
+      const int q = b >> (logn - 1), j = b & (hn - 1);
+      const int pos = j & (half - 1), k0 = ((j >> (s - 1)) << s) + pos, k1 = k0 + half;
       double2* x = S + q * n;
-      const int k0 = grp * m2 + pos, k1 = k0 + half;
       double2 w = tw[pos * step];
       if (inverse) w.y = -w.y;
       const double2 u = x[k0], v = cmul(x[k1], w);
@@ -72,161 +73,168 @@ __device__ void fft_seqs(double2* S, int nseq, int n, int logn, const double2* t
   }
 }
 
-// R consecutive rows y0..y0+R-1 of the real G_y x G_x array F (rows past
-// G_y skipped): S[r][i][m] = sum_e F(e, i) e^{-i th_m e}, then
-// xh[(m, k) * gy + y] = sum_i conj(V_m[i][k]) S[r][i][m] for m = 0..nel/2;
-// each V entry is loaded once for the R rows.
-template <int R>
+__device__ __forceinline__ void load_twiddles(double2* tw, const double2* g, int hn) {
+  for (int t = threadIdx.x; t < hn; t += blockDim.x) tw[t] = g[t];
+}
+
+// Row y = blockIdx.x of the real G_y x G_x array F: S[i][m] =
+// sum_e F(e, i) e^{-i th_m e}, then xh[(m, k) * gy + y] =
+// sum_i conj(V_m[i][k]) S[i][m] for m = 0..nel/2.
+template <int P>
 __global__ void __launch_bounds__(kBlochThreads, 8) bloch_x_forward(BlochDir bx, int gy,
-                                                                 const double* __restrict__ F,
-                                                                 double2* __restrict__ xh) {
+                                                                    const double* __restrict__ F,
+                                                                    double2* __restrict__ xh) {
   extern __shared__ double2 bsm[];
-  const int nel = bx.nel, p = bx.p, gx = nel * p, mx = nel / 2 + 1;
-  const int y0 = blockIdx.x * R;
-  double2* S = bsm;  // [R][p][nel]
-  double2* tw = bsm + R * gx;  // [nel/2]
-  for (int t = threadIdx.x; t < nel / 2; t += blockDim.x) tw[t] = bx.tw[t];
-  for (int t = threadIdx.x; t < R * gx; t += blockDim.x) {
-    const int r = t / gx, u = t - r * gx, e = u / p, i = u - e * p;
-    const int y = y0 + r;
-    S[(r * p + i) * nel + bitrev(e, bx.logn)] =
-        make_double2(y < gy ? F[(size_t)y * gx + u] : 0.0, 0.0);
+  const int nel = bx.nel, logn = bx.logn, gx = nel * P, mx = nel / 2 + 1;
+  const int y = blockIdx.x;
+  double2* S = bsm;            // [P][nel]
+  double2* tw = bsm + P * nel;  // [nel/2]
+  load_twiddles(tw, bx.tw, nel >> 1);
+  for (int t = threadIdx.x; t < gx; t += blockDim.x) {
+    const int e = t / P, i = t - e * P;
+    S[i * nel + bitrev(e, logn)] = make_double2(F[(size_t)y * gx + t], 0.0);
   }
   __syncthreads();
-  fft_seqs(S, R * p, nel, bx.logn, tw, false);
-  // one output (m, k, r) per thread and pass, r fastest (contiguous stores);
-  // the p-term sum unrolled to the largest order so that every load is
-  // issued before the arithmetic
-  for (int o = threadIdx.x; o < mx * p * R; o += blockDim.x) {
-    const int c = o / R, r = o - c * R, m = c / p, k = c - m * p;
-    const double2* V = bx.V + (size_t)m * p * p + k;
-    const double2* Sr = S + (r * p) * nel + m;
+  fft_seqs<P>(S, nel, logn, tw, false);
+  for (int o = threadIdx.x; o < mx * P; o += blockDim.x) {
+    const int m = o / P, k = o - m * P;
+    const double2* V = bx.V + (size_t)m * P * P + k;
+    double2 vv[P];
+#pragma unroll
+    for (int i = 0; i < P; i++) vv[i] = V[i * P];
     double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-    for (int i = 0; i < kBlochMaxP; i++) {
-      if (i < p) {
-        const double2 t = cmulc(V[i * p], Sr[i * nel]);
-        acc.x += t.x;
-        acc.y += t.y;
-      }
+    for (int i = 0; i < P; i++) {
+      const double2 t = cmulc(vv[i], S[i * nel + m]);
+      acc.x += t.x;
+      acc.y += t.y;
     }
-    if (y0 + r < gy) xh[(size_t)c * gy + y0 + r] = acc;
+    xh[(size_t)o * gy + y] = acc;
   }
 }
 
-// C consecutive x modes c = (m_x, k_x) (modes past the last skipped): their
-// columns of the spectral array along y.
-template <int C>
-__global__ void __launch_bounds__(kBlochThreads, 8) bloch_y_solve(BlochDir bx, BlochDir by, int cols,
-                                                               double alpha, double cx, double cy,
-                                                               double null_tol, double scale,
-                                                               double2* __restrict__ xh) {
+// x mode c = blockIdx.x = (m_x, k_x): its column of the spectral array along y.
+template <int P>
+__global__ void __launch_bounds__(kBlochThreads, 8) bloch_y_solve(BlochDir bx, BlochDir by,
+                                                                  double alpha, double cx,
+                                                                  double cy, double null_tol,
+                                                                  double scale,
+                                                                  double2* __restrict__ xh) {
   extern __shared__ double2 bsm[];
-  const int nel = by.nel, p = by.p, gy = nel * p;
-  const int c0 = blockIdx.x * C;
-  double2* S = bsm;                // [C][p][nel]
-  double2* T = bsm + C * p * nel;  // [C][p][nel]
-  double2* tw = T + C * p * nel;   // [nel/2]
-  for (int t = threadIdx.x; t < nel / 2; t += blockDim.x) tw[t] = by.tw[t];
-  for (int t = threadIdx.x; t < C * gy; t += blockDim.x) {
-    const int q = t / gy, u = t - q * gy, e = u / p, i = u - e * p;
-    S[(q * p + i) * nel + bitrev(e, by.logn)] =
-        c0 + q < cols ? xh[(size_t)(c0 + q) * gy + u] : make_double2(0.0, 0.0);
+  const int nel = by.nel, logn = by.logn, gy = nel * P;
+  const int c = blockIdx.x;
+  double2* S = bsm;            // [P][nel]
+  double2* T = bsm + P * nel;  // [P][nel]
+  double2* tw = T + P * nel;   // [nel/2]
+  load_twiddles(tw, by.tw, nel >> 1);
+  double2* col = xh + (size_t)c * gy;
+  for (int t = threadIdx.x; t < gy; t += blockDim.x) {
+    const int e = t / P, i = t - e * P;
+    S[i * nel + bitrev(e, logn)] = col[t];
   }
   __syncthreads();
-  fft_seqs(S, C * p, nel, by.logn, tw, false);
-  double mux[C];
+  fft_seqs<P>(S, nel, logn, tw, false);
+  const double mux = bx.mu[c];  // mu is [m][k]: the x mode's index is c
+  // T[k][m] = (sum_i conj(V_m[i][k]) S[i][m]) / (alpha + cx mu_x + cy mu_y(m, k))
+  for (int o = threadIdx.x; o < nel * P; o += blockDim.x) {
+    const int m = o / P, k = o - m * P;
+    const double2* V = by.V + (size_t)m * P * P + k;
+    double2 vv[P];
 #pragma unroll
-  for (int q = 0; q < C; q++) {
-    const int c = min(c0 + q, cols - 1), kx = c % bx.p, mxi = c / bx.p;
-    mux[q] = bx.mu[mxi * bx.p + kx];
-  }
-  // T[q][k][m] = (sum_i conj(V_m[i][k]) S[q][i][m]) / (alpha + cx mu_x + cy mu_y(m, k))
-  for (int o = threadIdx.x; o < nel * p * C; o += blockDim.x) {
-    const int mk = o / C, q = o - mk * C, m = mk / p, k = mk - m * p;
-    const double2* V = by.V + (size_t)m * p * p + k;
-    const double2* Sq = S + (q * p) * nel + m;
+    for (int i = 0; i < P; i++) vv[i] = V[i * P];
     double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-    for (int i = 0; i < kBlochMaxP; i++) {
-      if (i < p) {
-        const double2 t = cmulc(V[i * p], Sq[i * nel]);
-        acc.x += t.x;
-        acc.y += t.y;
-      }
+    for (int i = 0; i < P; i++) {
+      const double2 t = cmulc(vv[i], S[i * nel + m]);
+      acc.x += t.x;
+      acc.y += t.y;
     }
-    const double d = alpha + cx * mux[q] + cy * by.mu[m * p + k];
+    const double d = alpha + cx * mux + cy * by.mu[o];
     const double f = fabs(d) <= null_tol ? 0.0 : scale / d;
-    T[(q * p + k) * nel + m] = make_double2(acc.x * f, acc.y * f);
+    T[k * nel + m] = make_double2(acc.x * f, acc.y * f);
   }
   __syncthreads();
-  // S[q][i][rev(m)] = sum_k V_m[i][k] T[q][k][m], then the inverse FFT over m
-  for (int o = threadIdx.x; o < nel * p * C; o += blockDim.x) {
-    const int mi = o / C, q = o - mi * C, m = mi / p, i = mi - m * p;
-    const double2* V = by.V + (size_t)m * p * p + i * p;
-    const double2* Tq = T + (q * p) * nel + m;
+  // S[i][rev(m)] = sum_k V_m[i][k] T[k][m], then the inverse FFT over m
+  for (int o = threadIdx.x; o < nel * P; o += blockDim.x) {
+    const int m = o / P, i = o - m * P;
+    const double2* V = by.V + (size_t)m * P * P + i * P;
+    double2 vv[P];
+#pragma unroll
+    for (int k = 0; k < P; k++) vv[k] = V[k];
     double2 acc = make_double2(0.0, 0.0);
 #pragma unroll
-    for (int k = 0; k < kBlochMaxP; k++) {
-      if (k < p) {
-        const double2 t = cmul(V[k], Tq[k * nel]);
-        acc.x += t.x;
-        acc.y += t.y;
-      }
+    for (int k = 0; k < P; k++) {
+      const double2 t = cmul(vv[k], T[k * nel + m]);
+      acc.x += t.x;
+      acc.y += t.y;
     }
-    S[(q * p + i) * nel + bitrev(m, by.logn)] = acc;
+    S[i * nel + bitrev(m, logn)] = acc;
   }
   __syncthreads();
-  fft_seqs(S, C * p, nel, by.logn, tw, true);
-  for (int t = threadIdx.x; t < C * gy; t += blockDim.x) {
-    const int q = t / gy, u = t - q * gy, e = u / p, i = u - e * p;
-    if (c0 + q < cols) xh[(size_t)(c0 + q) * gy + u] = S[(q * p + i) * nel + e];
+  fft_seqs<P>(S, nel, logn, tw, true);
+  for (int t = threadIdx.x; t < gy; t += blockDim.x) {
+    const int e = t / P, i = t - e * P;
+    col[t] = S[i * nel + e];
   }
 }
 
-// R consecutive rows: T[r][i][m] = sum_k V_m[i][k] xh[(m,k) * gy + y] for
+// Row y = blockIdx.x: T[i][m] = sum_k V_m[i][k] xh[(m,k) * gy + y] for
 // m <= nel/2, the rest by conjugate symmetry, inverse FFT over m, out (+)=
 // the real part.
-template <int R>
+template <int P>
 __global__ void __launch_bounds__(kBlochThreads, 8) bloch_x_backward(BlochDir bx, int gy,
-                                                                  const double2* __restrict__ xh,
-                                                                  double* __restrict__ out,
-                                                                  int accumulate) {
+                                                                     const double2* __restrict__ xh,
+                                                                     double* __restrict__ out,
+                                                                     int accumulate) {
   extern __shared__ double2 bsm[];
-  const int nel = bx.nel, p = bx.p, gx = nel * p, mx = nel / 2 + 1;
-  const int y0 = blockIdx.x * R;
-  double2* S = bsm;  // [R][p][nel]
-  double2* tw = bsm + R * gx;  // [nel/2]
-  for (int t = threadIdx.x; t < nel / 2; t += blockDim.x) tw[t] = bx.tw[t];
-  for (int o = threadIdx.x; o < mx * p * R; o += blockDim.x) {
-    const int mi = o / R, r = o - mi * R, m = mi / p, i = mi - m * p;
-    const double2* V = bx.V + (size_t)m * p * p + i * p;
-    const double2* col = xh + (size_t)(m * p) * gy + y0 + r;
-    double2 acc = make_double2(0.0, 0.0);
-    if (y0 + r < gy) {
+  const int nel = bx.nel, logn = bx.logn, gx = nel * P, mx = nel / 2 + 1;
+  const int y = blockIdx.x;
+  double2* S = bsm;            // [P][nel]
+  double2* tw = bsm + P * nel;  // [nel/2]
+  load_twiddles(tw, bx.tw, nel >> 1);
+  for (int o = threadIdx.x; o < mx * P; o += blockDim.x) {
+    const int m = o / P, i = o - m * P;
+    const double2* V = bx.V + (size_t)m * P * P + i * P;
+    const double2* col = xh + (size_t)(m * P) * gy + y;
+    double2 vv[P], xv[P];
 #pragma unroll
-      for (int k = 0; k < kBlochMaxP; k++) {
-        if (k < p) {
-          const double2 t = cmul(V[k], col[(size_t)k * gy]);
-          acc.x += t.x;
-          acc.y += t.y;
-        }
-      }
+    for (int k = 0; k < P; k++) {
+      vv[k] = V[k];
+      xv[k] = col[(size_t)k * gy];
     }
-    double2* Sr = S + (r * p + i) * nel;
-    Sr[bitrev(m, bx.logn)] = acc;
-    if (m > 0 && m < nel - m) Sr[bitrev(nel - m, bx.logn)] = make_double2(acc.x, -acc.y);
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+      const double2 t = cmul(vv[k], xv[k]);
+      acc.x += t.x;
+      acc.y += t.y;
+    }
+    S[i * nel + bitrev(m, logn)] = acc;
+    if (m > 0 && m < nel - m) S[i * nel + bitrev(nel - m, logn)] = make_double2(acc.x, -acc.y);
   }
   __syncthreads();
-  fft_seqs(S, R * p, nel, bx.logn, tw, true);
-  for (int t = threadIdx.x; t < R * gx; t += blockDim.x) {
-    const int r = t / gx, u = t - r * gx, e = u / p, i = u - e * p;
-    const int y = y0 + r;
-    if (y >= gy) continue;
-    const double v = S[(r * p + i) * nel + e].x;
-    double* dst = out + (size_t)y * gx + u;
+  fft_seqs<P>(S, nel, logn, tw, true);
+  for (int t = threadIdx.x; t < gx; t += blockDim.x) {
+    const int e = t / P, i = t - e * P;
+    const double v = S[i * nel + e].x;
+    double* dst = out + (size_t)y * gx + t;
     *dst = accumulate ? *dst + v : v;
   }
+}
+
+template <int P>
+cudaError_t bloch_run(const BlochDir& bx, const BlochDir& by, double alpha, double cx, double cy,
+                      double null_tol, const double* in, double* out, bool accumulate,
+                      double2* xh, cudaStream_t s) {
+  const int gy = by.nel * P, cols = (bx.nel / 2 + 1) * P;
+  const size_t smx = sizeof(double2) * ((size_t)P * bx.nel + bx.nel / 2 + 1);
+  const size_t smy = sizeof(double2) * (2 * (size_t)P * by.nel + by.nel / 2 + 1);
+  if (smx > 48 * 1024 || smy > 48 * 1024) return cudaErrorInvalidValue;
+  bloch_x_forward<P><<<gy, kBlochThreads, smx, s>>>(bx, gy, in, xh);
+  bloch_y_solve<P><<<cols, kBlochThreads, smy, s>>>(bx, by, alpha, cx, cy, null_tol,
+                                                    1.0 / ((double)bx.nel * by.nel), xh);
+  bloch_x_backward<P><<<gy, kBlochThreads, smx, s>>>(bx, gy, xh, out, accumulate ? 1 : 0);
+  return cudaGetLastError();
 }
 
 }  // namespace
@@ -235,21 +243,22 @@ size_t bloch_spectrum_elems(const BlochDir& bx, const BlochDir& by) {
   return (size_t)(bx.nel / 2 + 1) * bx.p * by.nel * by.p;
 }
 
+// One row (x passes) or one x mode (y pass) per block: the passes are
+// latency-bound, and one block per row keeps every SM's warp slots filled.
 cudaError_t launch_bloch_inverse(const BlochDir& bx, const BlochDir& by, double alpha, double cx,
                                  double cy, double null_tol, const double* in, double* out,
                                  bool accumulate, double2* xh, cudaStream_t s) {
-  const int gy = by.nel * by.p, cols = (bx.nel / 2 + 1) * bx.p;
-  // one row (x passes) or one x mode (y pass) per block: the passes are
-  // latency-bound, and one block per row keeps every SM's warp slots filled
-  const size_t smx = sizeof(double2) * ((size_t)bx.p * bx.nel + bx.nel / 2 + 1);
-  const size_t smy = sizeof(double2) * (2 * (size_t)by.p * by.nel + by.nel / 2 + 1);
-  if (smx > 48 * 1024 || smy > 48 * 1024) return cudaErrorInvalidValue;
-  const double scale = 1.0 / ((double)bx.nel * by.nel);
-  bloch_x_forward<1><<<gy, kBlochThreads, smx, s>>>(bx, gy, in, xh);
-  bloch_y_solve<1><<<cols, kBlochThreads, smy, s>>>(bx, by, cols, alpha, cx, cy, null_tol, scale,
-                                                    xh);
-  bloch_x_backward<1><<<gy, kBlochThreads, smx, s>>>(bx, gy, xh, out, accumulate ? 1 : 0);
-  return cudaGetLastError();
+  if (bx.p != by.p) return cudaErrorInvalidValue;
+#define SE_BLOCH_P(n) \
+  case n:             \
+    return bloch_run<n>(bx, by, alpha, cx, cy, null_tol, in, out, accumulate, xh, s);
+  switch (bx.p) {
+    SE_BLOCH_P(2) SE_BLOCH_P(3) SE_BLOCH_P(4) SE_BLOCH_P(5) SE_BLOCH_P(6) SE_BLOCH_P(7)
+    SE_BLOCH_P(8) SE_BLOCH_P(9) SE_BLOCH_P(10) SE_BLOCH_P(11) SE_BLOCH_P(12)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef SE_BLOCH_P
 }
 
 }  // namespace seg
