@@ -299,10 +299,33 @@ def run_gpu(args, rank, world):
             e1.record(stream)
             torch.cuda.synchronize()
             sl_ms.append(e0.elapsed_time(e1))
-        log("FDM product kernel timing")
-        # the FDM transform x = A^{-1} r of the bench's system alone: four
-        # FP64 tensor-core product launches (fdm_dgemm_kernel, M = N = K = 512),
-        # CUDA events on the library's stream, L2 flushed before each call
+        log("FDM inverse timing")
+        # the dense FDM transform (four fdm_dgemm_kernel launches) on a mesh
+        # whose element count is not a power of two (63 x 64 elements, p = 8:
+        # 504 x 512 unknowns), the path of walled and general meshes, CUDA
+        # events on the library's stream, L2 flushed before each call
+        md = S.Mesh("dense", [NX - 1, NY], "legendre", P, [0.0, 0.0], [1.0, 1.0], [True, True])
+        bcd = S.BCs(False, False, False, False, md)
+        ud, fd = S.Field("ud", md, 1, bcd), S.Field("fd", md, 1, bcd)
+        hd = S.HelmholtzEqn(ud, fd, -LAMBDA, -1.0, 1.0, 0,
+                            S.solver_opts(rtol=RTOL, mode=S.MODE_EXACT, method=S.METHOD_FDM))
+        rd = torch.randn(hd.vecSize, dtype=torch.float64, device="cuda")
+        xd = torch.empty_like(rd)
+        for _ in range(3):
+            hd.fdm_apply(rd.data_ptr(), xd.data_ptr())
+        dense_ms = []
+        for _ in range(max(5, min(args.steps, 20))):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            hd.fdm_apply(rd.data_ptr(), xd.data_ptr())
+            e1.record(stream)
+            torch.cuda.synchronize()
+            dense_ms.append(e0.elapsed_time(e1))
+        dense_gx, dense_gy = (NX - 1) * P, NY * P
+        del hd, rd, xd, ud, fd, bcd, md
+        # the bench system's FP64 inverse x = A^{-1} r alone (doubly periodic,
+        # 64 = 2^6 elements a direction: the Bloch form, three launches)
         helm = S.HelmholtzEqn(u, adv.fieldSL, -LAMBDA, -1.0, 1.0, 0,
                               S.solver_opts(rtol=RTOL, mode=S.MODE_EXACT, method=S.METHOD_FDM))
         ngf = helm.vecSize
@@ -363,6 +386,7 @@ def run_gpu(args, rank, world):
             "nv": m.nVertsTotal, "clocks": clock,
             "variants": results, "sl_ms": float(np.median(sl_ms)), "fp64_tflops": fp64_tflops,
             "fdm_apply_ms": float(np.median(fdm_ms)), "gx": int(round(ng ** 0.5)),
+            "dense_fdm_ms": float(np.median(dense_ms)), "dense_gx": dense_gx, "dense_gy": dense_gy,
             "tc_apply_ms": float(np.median(tc_ms)), "residual_ms": float(np.median(res_ms))}
 
 
@@ -453,30 +477,56 @@ SL_TRAFFIC_BYTES = 6.358016e6
 FDM_GEMM_TRAFFIC_BYTES = 4.211968e6
 
 
-def roofline(r):
-    """Roofline of the step's dominant kernel, the FDM product kernel
-    (fdm_dgemm_kernel, four launches of M = N = K = 512 per refinement step):
-    achieved = algorithmic FLOPs per launch (2 M N K) / mean launch time,
-    the launch time measured live as one FDM transform (exactly four such
-    launches) / 4, against the FP64 DGEMM rate measured in the same run
-    (MEASURED_PEAKS.json holds no FP64 figure). DRAM traffic per launch from
-    one ncu capture of the kernel."""
-    g = r["gx"]
-    flops = 2.0 * g ** 3
-    launch_ms = r["fdm_apply_ms"] / 4
-    achieved = flops / (launch_ms * 1e-3) / 1e12
-    return {"kernel": "fdm_dgemm_kernel (FP64 DMMA, 32x32 tiles, M=N=K=512)", "bound": "tensor",
-            "achieved": achieved, "peak": r["fp64_tflops"], "unit": "TFLOP/s",
+def dense_fdm_roofline(r):
+    """The dense FDM product kernel (fdm_dgemm_kernel, four launches per
+    inverse; the path of meshes whose element counts are not powers of two
+    and of walled directions), timed live as one inverse of a 63 x 64
+    element, p = 8 system (504 x 512 unknowns): achieved = the four
+    products' algorithmic FLOPs (2 M N K each) / the inverse's time, against
+    the FP64 DGEMM rate measured in the same run (MEASURED_PEAKS.json holds
+    no FP64 figure). DRAM traffic per launch from one ncu capture of the
+    512^3 product."""
+    gx, gy = r["dense_gx"], r["dense_gy"]
+    flops = 2 * (2.0 * gy * gx * gx) + 2 * (2.0 * gy * gx * gy)
+    t = r["dense_fdm_ms"] * 1e-3
+    achieved = flops / t / 1e12
+    return {"kernel": "fdm_dgemm_kernel (FP64 DMMA, 32x32 tiles), 4 launches, 504x512 unknowns",
+            "bound": "tensor", "achieved": achieved, "peak": r["fp64_tflops"], "unit": "TFLOP/s",
             "frac": achieved / r["fp64_tflops"],
             "peak_source": "FP64 DGEMM (torch.matmul float64 8192^3) measured in this run",
-            "launch_ms": launch_ms, "algorithmic_flops_per_launch": flops,
-            "algorithmic_bytes_per_launch": 3 * 8 * g * g, "traffic": FDM_GEMM_TRAFFIC_BYTES}
+            "inverse_ms": r["dense_fdm_ms"], "launch_ms": r["dense_fdm_ms"] / 4,
+            "algorithmic_flops_per_inverse": flops, "traffic": FDM_GEMM_TRAFFIC_BYTES}
+
+
+def bloch_roofline(r):
+    """The bench system's FP64 inverse in Bloch form (bloch_x_forward,
+    bloch_y_solve, bloch_x_backward): algorithmic bytes per inverse = the
+    right-hand side read and the solution written (16 B per unknown) plus
+    four passes over the complex half spectrum (written, read and written,
+    read: 16 B per complex entry each), against the measured HBM bandwidth.
+    The passes are latency-bound (one row or mode per block, FFT stages
+    separated by block barriers), not bandwidth-bound."""
+    peaks = read_peaks()
+    g, p = r["gx"], P
+    nel = g // p
+    spec = (nel // 2 + 1) * p * g
+    nbytes = 16.0 * g * g + 4 * 16.0 * spec
+    t = r["fdm_apply_ms"] * 1e-3
+    achieved = nbytes / t / 1e9
+    return {"kernel": "bloch_x_forward + bloch_y_solve + bloch_x_backward (FP64, radix-2 FFT over "
+                      "64 elements, 8 x 8 blocks per wavenumber)", "bound": "hbm",
+            "achieved": achieved, "peak": peaks[0], "unit": "GB/s", "frac": achieved / peaks[0],
+            "peak_source": peaks[1] + " (MEASURED_PEAKS.json hbm_gbs)",
+            "inverse_ms": r["fdm_apply_ms"], "algorithmic_bytes_per_inverse": nbytes}
 
 
 def sl_roofline(r):
-    """The SL advection kernel: algorithmic bytes per launch / measured
-    launch time against the measured HBM copy bandwidth, and its FP64 rate
-    against the measured DGEMM (the kernel is bound by its FP64 gathers)."""
+    """The step's dominant kernel, the SL advection (sl_first_kernel<8>, one
+    launch per step, about a quarter of the step): algorithmic bytes per
+    launch (32 per vertex) / measured launch time against the measured HBM
+    copy bandwidth, and its FP64 rate against the measured DGEMM. The kernel
+    is bound by its L1 gathers of the element blocks (DRAM nearly idle), so
+    both fractions are low."""
     peaks = read_peaks()
     nv = r["nv"]
     t = r["sl_ms"] * 1e-3
@@ -511,8 +561,9 @@ def tc_roofline(r):
                       "TMA, 4-CTA cluster split-K), M=N=K=512", "bound": "tensor",
             "achieved": achieved, "peak": bf16 / 2, "unit": "TFLOP/s", "frac": achieved / (bf16 / 2),
             "peak_source": f"{src} BF16 GEMM rate / 2 (MEASURED_PEAKS.json bf16_tflops)",
-            "inverse_ms": r["tc_apply_ms"], "fp64_inverse_ms": r["fdm_apply_ms"],
-            "speedup_vs_fp64_inverse": r["fdm_apply_ms"] / r["tc_apply_ms"],
+            "inverse_ms": r["tc_apply_ms"], "fp64_bloch_inverse_ms": r["fdm_apply_ms"],
+            "fp64_dense_inverse_ms_504x512": r["dense_fdm_ms"],
+            "speedup_vs_fp64_bloch_inverse": r["fdm_apply_ms"] / r["tc_apply_ms"],
             "tensor_flops_per_inverse": flops, "useful_flops_per_inverse": flops / 3}
 
 
@@ -1180,7 +1231,8 @@ def main():
     line.update({
         "variants": variants, "parity_vs_cpu": parity, "vs_cpu": ratios,
         "tc_roofline": tc_roofline(r), "residual_roofline": residual_roofline(r),
-        "sl_roofline": sl_roofline(r), "roofline": roofline(r), "cpu_baseline": cpu,
+        "dense_fdm_roofline": dense_fdm_roofline(r), "bloch_roofline": bloch_roofline(r),
+        "roofline": sl_roofline(r), "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * r["nv"],
                 "d2h_bytes_per_step": 8 * r["nv"], "ms_per_step": r["e2e_ms"],
                 "mode": "two independent steps in flight on two streams (upload, advection, "
@@ -1191,7 +1243,8 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["step_ms"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": config({"solver": "fast diagonalization, FP64, refined to rtol 1e-10",
+        "config": config({"solver": "fast diagonalization (Bloch form: FFT across elements, 8x8 "
+                                    "blocks per wavenumber), FP64, refined to rtol 1e-10",
                           "parallelism": f"replicas{world}"}),
     })
     print(json.dumps(line), flush=True)
