@@ -110,11 +110,49 @@ __device__ __forceinline__ V2 vfma(double s, V2 v, V2 acc) {
   return {fma(s, v.a, acc.a), fma(s, v.b, acc.b)};
 }
 
-// Sources: the nodal value of a field at vertex k.
+// Sources: the nodal value of a field at vertex k (operator()), the N+1
+// values of a vertex row from vertex r0 (row), and an L2 prefetch of the
+// line holding vertex k.
+//
+// Scalar rows of even orders are read as 16-byte pairs: an element row
+// starts at an even or odd vertex index, the same for every thread of a warp
+// when N is even (the row offsets are multiples of N, the row pitch is odd),
+// so a row of 9 values at p=8 is 5 loads instead of 9. Odd orders (whose
+// rows start at both parities within a warp) read single values.
 struct Scalar {
   typedef V1 T;
   const double* __restrict__ p;
   __device__ __forceinline__ T operator()(int k) const { return {__ldg(p + k)}; }
+  template <int N>
+  __device__ __forceinline__ void row(int r0, T* v) const {
+    const double* q = p + r0;
+    if constexpr (N % 2 == 0) {
+      // 16-byte alignment from the address itself (q is 8-byte aligned)
+      if ((reinterpret_cast<uintptr_t>(q) & 8u) == 0) {
+#pragma unroll
+        for (int k = 0; k < N; k += 2) {
+          const double2 d = __ldg(reinterpret_cast<const double2*>(q + k));
+          v[k].a = d.x;
+          v[k + 1].a = d.y;
+        }
+        v[N].a = __ldg(q + N);
+      } else {
+        v[0].a = __ldg(q);
+#pragma unroll
+        for (int k = 1; k < N; k += 2) {
+          const double2 d = __ldg(reinterpret_cast<const double2*>(q + k));
+          v[k].a = d.x;
+          v[k + 1].a = d.y;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k <= N; k++) v[k].a = __ldg(q + k);
+    }
+  }
+  __device__ __forceinline__ void prefetch(int k) const {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p + k));
+  }
 };
 struct Vec2 {
   typedef V2 T;
@@ -122,6 +160,14 @@ struct Vec2 {
   __device__ __forceinline__ T operator()(int k) const {
     double2 v = __ldg(p + k);
     return {v.x, v.y};
+  }
+  template <int N>
+  __device__ __forceinline__ void row(int r0, T* v) const {
+#pragma unroll
+    for (int k = 0; k <= N; k++) v[k] = (*this)(r0 + k);
+  }
+  __device__ __forceinline__ void prefetch(int k) const {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p + k));
   }
 };
 // c0*v + c1*vm with the reference's rounding (Advector::ExtrapolateVelocities,
@@ -134,6 +180,11 @@ struct Vec2Mix {
   __device__ __forceinline__ T operator()(int k) const {
     double2 a = __ldg(v + k), b = __ldg(vm + k);
     return {xadd(xmul(c0, a.x), xmul(c1, b.x)), xadd(xmul(c0, a.y), xmul(c1, b.y))};
+  }
+  template <int N>
+  __device__ __forceinline__ void row(int r0, T* v) const {
+#pragma unroll
+    for (int k = 0; k <= N; k++) v[k] = (*this)(r0 + k);
   }
 };
 
@@ -155,9 +206,10 @@ __device__ __forceinline__ typename Src::T interp(const MeshDev& m, const Src& s
   T acc = vzero(T());
   if (sy >= 0) {
     cardinal<N>(m, lx, cx);
-    const int row = base + sy * nvx;
+    T rv[N + 1];
+    src.template row<N>(base + sy * nvx, rv);
 #pragma unroll
-    for (int i = 0; i <= N; i++) acc = vfma(cx[i], src(row + i), acc);
+    for (int i = 0; i <= N; i++) acc = vfma(cx[i], rv[i], acc);
     return acc;
   }
   cardinal<N>(m, ly, cy);
@@ -169,10 +221,11 @@ __device__ __forceinline__ typename Src::T interp(const MeshDev& m, const Src& s
   cardinal<N>(m, lx, cx);
 #pragma unroll
   for (int j = 0; j <= N; j++) {
+    T rv[N + 1];
+    src.template row<N>(base + j * nvx, rv);
     T r = vzero(T());
-    const int row = base + j * nvx;
 #pragma unroll
-    for (int i = 0; i <= N; i++) r = vfma(cx[i], src(row + i), r);
+    for (int i = 0; i <= N; i++) r = vfma(cx[i], rv[i], r);
     acc = vfma(cy[j], r, acc);
   }
   return acc;
@@ -202,7 +255,7 @@ __device__ __forceinline__ void store_with_copies(const MeshDev& m, double* out,
 
 // Advector::FirstOrder with IntegrateRK2 (src/base/Advector.cpp:136-148,181-201).
 template <int N, class FSrc>
-__global__ void __launch_bounds__(256) sl_first_kernel(const MeshDev m, FSrc field,
+__global__ void __launch_bounds__(256, 2) sl_first_kernel(const MeshDev m, FSrc field,
                                                        const double2* __restrict__ vel,
                                                        double dt, double half_dt,
                                                        double* __restrict__ out,
@@ -215,6 +268,9 @@ __global__ void __launch_bounds__(256) sl_first_kernel(const MeshDev m, FSrc fie
   const bool owner = i < nvx - m.periodic[0] && j < nvy - m.periodic[1];
   if (i >= nvx || j >= nvy || (!owner && !dep_el)) return;
   Vec2 v{vel};
+  // the tracer near this vertex, where most departure points land: its
+  // lines start their way from HBM while the velocity is interpolated
+  field.prefetch(j * nvx + i);
   const double ox = vertex_coord(m, 0, i), oy = vertex_coord(m, 1, j);
   V2 u = interp<N>(m, v, ox, oy, nullptr, err);
   double xh = wrap(m, 0, xsub(ox, xmul(half_dt, u.a)));
@@ -234,7 +290,7 @@ __global__ void __launch_bounds__(256) sl_first_kernel(const MeshDev m, FSrc fie
 // Advector::SecondOrder (src/base/Advector.cpp:203-246) with the
 // extrapolated velocities formed on the fly at each gathered vertex.
 template <int N, class FSrc>
-__global__ void __launch_bounds__(256) sl_second_kernel(const MeshDev m, FSrc field,
+__global__ void __launch_bounds__(256, 2) sl_second_kernel(const MeshDev m, FSrc field,
                                                         FSrc field_prev,
                                                         const double2* __restrict__ vel,
                                                         const double2* __restrict__ vel_prev,
@@ -294,8 +350,10 @@ template <int N>
 cudaError_t launch_sl_n(const MeshDev& m, int ndofs, const double* field, const double* vel,
                         const double* field_prev, const double* vel_prev, double dt, double* out,
                         int* dep_el, double* dep_xy, unsigned* err, cudaStream_t s) {
-  dim3 block(32, 8);
-  dim3 grid((m.nVerts[0] + 31) / 32, (m.nVerts[1] + 7) / 8);
+  // a warp covers 8 x 4 vertices, about one element: its departure points
+  // fall in fewer element blocks than a row of 32 vertices' do
+  dim3 block(8, 32);
+  dim3 grid((m.nVerts[0] + 7) / 8, (m.nVerts[1] + 31) / 32);
   const double half_dt = 0.5 * dt;
   const double2* v = reinterpret_cast<const double2*>(vel);
   const double2* vm = reinterpret_cast<const double2*>(vel_prev);
