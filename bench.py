@@ -18,9 +18,9 @@ and one elliptic inversion to rtol.
          (CUDA events on the library's stream, L2 flushed between steps)
   e2e    the same through the public C-ABI with host buffers: every step
          uploads the tracer from page-locked host memory and downloads the
-         solution to it; two independent steps in flight on two streams, so
-         that one step's copies overlap the other's kernels (the one-at-a-time
-         figure is reported beside it)
+         solution to it; four independent steps in flight on four streams,
+         so that one step's copies overlap the others' kernels (the
+         one-at-a-time figure is reported beside it)
 
 ``--impl reference`` times the CPU restatement of the reference's path (the
 oracle: reference-identical SL, restated AIJ assembly and PETSc-style
@@ -269,7 +269,7 @@ def run_gpu(args, rank, world):
                 # end to end through the public API with pinned host buffers:
                 # each step one upload, advection, solve and download, one at a
                 # time with the L2 flushed before each (serial), and as a
-                # two-deep pipeline of independent steps on two streams
+                # pipeline of independent steps on E2E_DEPTH streams
                 # (pipelined, the reported e2e)
                 h_in = torch.from_numpy(np.ascontiguousarray(phi0)).pin_memory()
                 h_out = torch.empty(m.nVertsTotal, dtype=torch.float64).pin_memory()
@@ -398,18 +398,22 @@ def run_gpu(args, rank, world):
             "tc_apply_ms": float(np.median(tc_ms)), "residual_ms": float(np.median(res_ms))}
 
 
+E2E_DEPTH = 4
+
+
 def e2e_pipelined(S, lib, m, bc, v, phi0, dt, opts, steps, warmup, stream0):
     """Per-step time of independent steps (upload from page-locked host
     memory, SL advection, FDM solve, download to page-locked host memory)
-    through the public API, two in flight on two streams so that one step's
-    copies overlap the other's kernels. Device time between an event before
-    the first step and one after the last download, over the steps."""
+    through the public API, E2E_DEPTH in flight on as many streams so that
+    one step's copies overlap the others' kernels and the host queues a step
+    while earlier ones run. Device time between an event before the first
+    step and one after the last download, over the steps."""
     import ctypes
 
     import torch
-    streams = [stream0, torch.cuda.Stream()]
+    streams = [stream0] + [torch.cuda.Stream() for _ in range(E2E_DEPTH - 1)]
     pipes = []
-    for j in range(2):
+    for j in range(E2E_DEPTH):
         S.set_stream(streams[j].cuda_stream)
         phi = S.Field(f"phi{j}", m, 1, bc)
         u = S.Field(f"u{j}", m, 1, bc)
@@ -430,7 +434,7 @@ def e2e_pipelined(S, lib, m, bc, v, phi0, dt, opts, steps, warmup, stream0):
 
     def run(n):
         for k in range(n):
-            j = k % 2
+            j = k % E2E_DEPTH
             p = pipes[j]
             S.set_stream(streams[j].cuda_stream)
             if p["pending"]:  # this pipe's previous step: its output buffer is reused
@@ -442,20 +446,22 @@ def e2e_pipelined(S, lib, m, bc, v, phi0, dt, opts, steps, warmup, stream0):
             assert lib.se_field_download_async(p["u"]._h, p["pin_out"]) == 0
             p["pending"] = True
 
-    run(max(warmup, 2))
-    for j in range(2):
+    run(max(warmup, E2E_DEPTH))
+    for j in range(E2E_DEPTH):
         finish(pipes[j])
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(streams[0])
-    streams[1].wait_event(e0)
+    for st in streams[1:]:
+        st.wait_event(e0)
     run(steps)
-    for j in range(2):
+    for j in range(E2E_DEPTH):
         finish(pipes[j])
-    streams[0].wait_stream(streams[1])
+    for st in streams[1:]:
+        streams[0].wait_stream(st)
     e1.record(streams[0])
     torch.cuda.synchronize()
-    out = pipes[(steps - 1) % 2]["h_out"].numpy()
+    out = pipes[(steps - 1) % E2E_DEPTH]["h_out"].numpy()
     if not np.all(np.isfinite(out)):
         raise RuntimeError("pipelined end-to-end step produced a non-finite field")
     return e0.elapsed_time(e1) / steps
@@ -1244,8 +1250,9 @@ def main():
         "roofline": sl_roofline(r), "cpu_baseline": cpu,
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * r["nv"],
                 "d2h_bytes_per_step": 8 * r["nv"], "ms_per_step": r["e2e_ms"],
-                "mode": "two independent steps in flight on two streams (upload, advection, "
-                        "solve, download each), no L2 flush (inputs arrive from host memory)",
+                "mode": f"{E2E_DEPTH} independent steps in flight on {E2E_DEPTH} streams (upload, "
+                        "advection, solve, download each), no L2 flush (inputs arrive from host "
+                        "memory)",
                 "serial_ms_per_step": r["e2e_serial_ms"]},
         "gpu_launches": int(round((GPU_LAUNCHES_FIXED + GPU_LAUNCHES_PER_REFINEMENT
                                    * r["variants"][HEADLINE]["its"]) * args.steps)),

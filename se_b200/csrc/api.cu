@@ -297,6 +297,8 @@ struct se_linsys {
   unsigned* d_rescount;  // arrival counter of the fused residual + test (zero between launches)
   FdmParams* h_fparams;  // pinned host copies for asynchronous transfers
   FdmState* h_fstate;
+  FdmParams fparams_last;    // the parameters in d_fparams
+  bool fparams_sent;         // d_fparams holds fparams_last
   int async_pending;       // 1: FDM solve queued; 2: synchronous result held
   int async_rc;
   se_solve_stats async_stats;
@@ -1277,7 +1279,7 @@ int fdm_setup(se_linsys* ls, int prec) {
   ls->SxT_lo = prec ? ex->lowT[prec] : nullptr;
   ls->SyT_lo = prec ? ey->lowT[prec] : nullptr;
   if (!ls->X1) {
-    ls->fpart_n = std::max(kFdmPartials, residual_blocks(op));
+    ls->fpart_n = std::max(kFdmPartials, std::max(residual_blocks(op), residual_partial_blocks(op)));
     if ((rc = dalloc(&ls->X1, n)) || (rc = dalloc(&ls->X2, n)) || (rc = dalloc(&ls->ax, n)) ||
         (rc = dalloc(&ls->zlow, 64)) || (rc = dalloc(&ls->fpart, 2 * (size_t)ls->fpart_n + 16)))
       return rc;
@@ -1538,22 +1540,31 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
               cudaGraphConditionalHandleCreate(&hc, cg, 0, hybrid ? cudaGraphCondAssignDefault : 0) ==
                   cudaSuccess;
     if (hybrid) ok = ok && cudaGraphConditionalHandleCreate(&hf, cg, 0, 0) == cudaSuccess;
-    // prologue
-    ok = ok && launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, cs) == cudaSuccess;
-    // a right-hand side off the range of a singular operator: solve for the
-    // one Jacobi CG with the null space removed converges to
-    if (remove_null)
-      ok = ok && launch_project_null(ls->f, ls->dinv, n, ls->fpart, kFdmPartials,
-                                     ls->fpart + 2 * ls->fpart_n + 4, cs) == cudaSuccess;
-    ok = ok && cudaMemcpyAsync(ls->r, ls->f, sizeof(double) * n, cudaMemcpyDeviceToDevice, cs) == cudaSuccess;
-    // the tensor-core inverse reads r as TF32 hi/lo pairs: the first from f,
-    // the others from the residual kernel
-    if (prec == 1)
-      ok = ok && launch_tc_split(ls->f, op_gy(ls), op_gx(ls), op_gx(ls), ls->tcY[0], ls->tcY[1],
-                                 ls->tc_px, cs) == cudaSuccess;
-    ok = ok && cudaMemsetAsync(ls->x, 0, sizeof(double) * n, cs) == cudaSuccess;
-    ok = ok && launch_norms(ls->f, wv, n, nt == SE_NORM_NATURAL, ls->fpart, kFdmPartials, res, cs) == cudaSuccess;
-    ok = ok && launch_fdm_init(ls->d_fparams, ls->d_fstate, res, hybrid ? hf : hc, cs) == cudaSuccess;
+    // prologue: without a null space to remove and with an FP64 first
+    // inverse, one launch (f, r = f, x = 0, the initial norm and test);
+    // otherwise the pieces one by one
+    if (!remove_null && prec != 1) {
+      ok = ok && launch_fdm_prologue(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f,
+                                     ls->r, ls->x, wv, nt == SE_NORM_NATURAL, ls->fpart,
+                                     kFdmPartials, res, ls->d_rescount, ls->d_fparams,
+                                     ls->d_fstate, hybrid ? hf : hc, cs) == cudaSuccess;
+    } else {
+      ok = ok && launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, cs) == cudaSuccess;
+      // a right-hand side off the range of a singular operator: solve for the
+      // one Jacobi CG with the null space removed converges to
+      if (remove_null)
+        ok = ok && launch_project_null(ls->f, ls->dinv, n, ls->fpart, kFdmPartials,
+                                       ls->fpart + 2 * ls->fpart_n + 4, cs) == cudaSuccess;
+      ok = ok && cudaMemcpyAsync(ls->r, ls->f, sizeof(double) * n, cudaMemcpyDeviceToDevice, cs) == cudaSuccess;
+      // the tensor-core inverse reads r as TF32 hi/lo pairs: the first from f,
+      // the others from the residual kernel
+      if (prec == 1)
+        ok = ok && launch_tc_split(ls->f, op_gy(ls), op_gx(ls), op_gx(ls), ls->tcY[0], ls->tcY[1],
+                                   ls->tc_px, cs) == cudaSuccess;
+      ok = ok && cudaMemsetAsync(ls->x, 0, sizeof(double) * n, cs) == cudaSuccess;
+      ok = ok && launch_norms(ls->f, wv, n, nt == SE_NORM_NATURAL, ls->fpart, kFdmPartials, res, cs) == cudaSuccess;
+      ok = ok && launch_fdm_init(ls->d_fparams, ls->d_fstate, res, hybrid ? hf : hc, cs) == cudaSuccess;
+    }
     // a conditional node after what was captured so far, its body captured on
     // stream bs by `fill`
     std::vector<cudaGraph_t> bodies;
@@ -1650,13 +1661,19 @@ int fdm_launch(se_linsys* ls, int remove_null) {
     for (cudaEvent_t& e : ls->ev)
       if (!e) CK(cudaEventCreate(&e));
   }
-  FdmParams& p = *ls->h_fparams;
+  // the loop's parameters go up only when they differ from the last upload
+  FdmParams p;
+  std::memset(&p, 0, sizeof(p));
   p.rtol = ls->opts.rtol;
   p.atol = ls->opts.atol;
   p.dtol = ls->opts.dtol;
   p.max_it = ls->opts.max_it;
-  p.pad = 0;
-  CK(cudaMemcpyAsync(ls->d_fparams, ls->h_fparams, sizeof(FdmParams), cudaMemcpyHostToDevice, g_stream));
+  if (!ls->fparams_sent || std::memcmp(&p, &ls->fparams_last, sizeof(p)) != 0) {
+    *ls->h_fparams = p;
+    CK(cudaMemcpyAsync(ls->d_fparams, ls->h_fparams, sizeof(FdmParams), cudaMemcpyHostToDevice, g_stream));
+    ls->fparams_last = p;
+    ls->fparams_sent = true;
+  }
   CK(cudaEventRecord(ls->ev[0], g_stream));
   CK(cudaGraphLaunch(ls->fdm_exec, g_stream));
   CK(cudaEventRecord(ls->ev[1], g_stream));
@@ -2420,7 +2437,9 @@ int se_advector_destroy(se_advector* adv) {
 int se_advect(se_advector* adv, double dt) {
   if (!adv) return fail(SE_ERR_ARG, "null advector");
   const se_mesh* me = adv->field->mesh;
-  CK(cudaMemsetAsync(adv->err, 0, sizeof(unsigned), g_stream));
+  // the error word is read back only with the recorded departures: cleared
+  // for the advections that record them
+  if (adv->record) CK(cudaMemsetAsync(adv->err, 0, sizeof(unsigned), g_stream));
   CK(launch_sl(me->dev, adv->field->ndofs, adv->field->vals, adv->vel->vals,
                adv->field_prev ? adv->field_prev->vals : nullptr,
                adv->vel_prev ? adv->vel_prev->vals : nullptr, dt, adv->sl->vals,
@@ -2841,7 +2860,7 @@ int se_linsys_residual(se_linsys* ls, const double* x_dev, const double* b_dev, 
   if (!ls || !x_dev || !b_dev || !r_dev) return fail(SE_ERR_ARG, "null argument");
   if (r_dev == x_dev || r_dev == b_dev) return fail(SE_ERR_ARG, "r must not alias x or b");
   if (!ls->fpart) {
-    ls->fpart_n = std::max(kFdmPartials, residual_blocks(ls->op));
+    ls->fpart_n = std::max(kFdmPartials, std::max(residual_blocks(ls->op), residual_partial_blocks(ls->op)));
     if (int rc = dalloc(&ls->fpart, 2 * (size_t)ls->fpart_n + 16)) return rc;
   }
   CK(launch_residual(ls->op, x_dev, b_dev, r_dev, nullptr, 0, ls->fpart, g_stream));

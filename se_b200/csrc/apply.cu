@@ -647,11 +647,11 @@ constexpr int kEfThreads = 256, kEfWarps = kEfThreads / 32;
 // Stage the tile's vertices and its N-vertex halo to the left and below into
 // X (zero where a vertex is no unknown): warp w takes rows w, w + 8, ...;
 // lane l columns l, l + 32, l + 64; all copies issued before the wait.
-template <int N>
+template <int N, int H = EfTile<N>::H>
 __device__ __forceinline__ void ef_stage(const OpDev& op, const double* __restrict__ x, double* X,
                                          int gx0, int gy0) {
   typedef EfTile<N> T;
-  constexpr int SW = T::SW, W = T::W, H = T::H;
+  constexpr int SW = T::SW, W = T::W;
   const Dir& dx = op.d[0];
   const Dir& dy = op.d[1];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -806,21 +806,136 @@ cudaError_t launch_ef(const OpDev& op, const double* x, double* y, cudaStream_t 
 }
 
 // ------------------------------- refinement residual, orders 4 to 8 ----
-// r = b - A x on apply_ef_kernel's tile: the stiffness sums of both passes,
-// the combination and the subtraction in double-double (the stiffness rows
-// sum to zero, so the taps cancel and a plain FP64 sum loses the digits a
-// 1e-10 residual needs), rounded once. Per-block partial sums of (w r)^2 (or
-// r w r when natural) and r^2; the block that finishes last sums the
-// partials in block order and runs the FDM loop's convergence test (ResTail).
-// Optionally also writes r's TF32 hi/lo split for the tensor-core inverse.
+// r = b - A x on apply_ef_kernel's tile with TY / kResSplit output rows: the
+// stiffness sums of both passes, the combination and the subtraction in
+// double-double (the stiffness rows sum to zero, so the taps cancel and a
+// plain FP64 sum loses the digits a 1e-10 residual needs), rounded once.
+// Each element row (x pass) and column (y pass) is shared by kResSplit
+// thread groups, warp-uniform, each forming a contiguous share of its N
+// outputs in the same order as one thread would: twice the blocks of half
+// the depth for this latency-bound kernel, and the same bits. Per-block
+// partial sums of (w r)^2 (or r w r when natural) and r^2; the block that
+// finishes last sums the partials in block order and runs the FDM loop's
+// convergence test (ResTail). Optionally also writes r's TF32 hi/lo split
+// for the tensor-core inverse.
+constexpr int kResSplit = 2;
+template <int N>
+struct ResTile {
+  typedef EfTile<N> E;
+  static constexpr int EX = E::EX, TX = E::TX, W = E::W, OXP = E::OXP;
+  static constexpr int TY = E::TY / kResSplit;   // output rows: 16, 14, 12, 10, 8
+  static constexpr int H = TY + N + 1;           // staged rows
+  static constexpr int ITEMS = EX * TY;          // rows (x pass) = columns (y pass)
+  static constexpr int GROUP = kEfThreads / kResSplit;  // threads of one share
+  static constexpr int CH = (N + kResSplit - 1) / kResSplit;  // outputs of a share
+  static_assert(TY % N == 0 && ITEMS <= GROUP && GROUP % 32 == 0, "residual tile shape");
+};
+
+// x pass of outputs [A0, A1) of one element row: v = the row's 2N+1 staged
+// values (left element, shared node, own element).
+template <int N, int A0, int A1>
+__device__ __forceinline__ void res_xpass(const OpDev& op, const double* row, bool own, bool left,
+                                          double* OXH, double* OXL) {
+  constexpr int n = N + 1;
+  double v[2 * N + 1];
+#pragma unroll
+  for (int k = (A0 == 0 ? 0 : N); k <= 2 * N; k++) v[k] = row[k];
+#pragma unroll
+  for (int a = A0; a < A1; a++) {
+    double hi = 0.0, lo = 0.0;
+    if (own) {
+#pragma unroll
+      for (int q = 0; q < n; q++) dd_fma(hi, lo, op.Kh[a * n + q], v[N + q]);
+    }
+    if (A0 == 0 && a == 0 && left) {
+      double h2 = 0.0, l2 = 0.0;
+#pragma unroll
+      for (int q = 0; q < n; q++) dd_fma(h2, l2, op.Kh[N * n + q], v[q]);
+      dd_add(hi, lo, h2);
+      lo += l2;
+    }
+    OXH[a] = hi;
+    OXL[a] = lo;
+  }
+}
+
+// y pass, combination and residual of outputs [A0, A1) of one element
+// column; accumulates the norm partials.
+template <int N, int A0, int A1>
+__device__ __forceinline__ void res_ypass(const OpDev& op, const double* col, const double* OXH,
+                                          const double* OXL, const double* sw, int c, int e,
+                                          int gx, int gy0, bool own, bool left,
+                                          const double* __restrict__ b, double* __restrict__ rout,
+                                          const double* __restrict__ wv, int natural,
+                                          double& acc0, double& acc1, float* __restrict__ sp_hi,
+                                          float* __restrict__ sp_lo, int sp_pitch) {
+  typedef ResTile<N> T;
+  constexpr int n = N + 1, W = T::W, OXP = T::OXP;
+  const Dir& dx = op.d[0];
+  const Dir& dy = op.d[1];
+  double v[2 * N + 1];
+#pragma unroll
+  for (int k = (A0 == 0 ? 0 : N); k <= 2 * N; k++) v[k] = col[k * W];
+  double yh[A1 - A0], yl[A1 - A0];
+#pragma unroll
+  for (int a = A0; a < A1; a++) {
+    double hi = 0.0, lo = 0.0;
+    if (own) {
+#pragma unroll
+      for (int q = 0; q < n; q++) dd_fma(hi, lo, op.Kh[a * n + q], v[N + q]);
+    }
+    if (A0 == 0 && a == 0 && left) {
+      double h2 = 0.0, l2 = 0.0;
+#pragma unroll
+      for (int q = 0; q < n; q++) dd_fma(h2, l2, op.Kh[N * n + q], v[q]);
+      dd_add(hi, lo, h2);
+      lo += l2;
+    }
+    yh[a - A0] = hi;
+    yl[a - A0] = lo;
+  }
+  if (gx < dx.lo || gx >= dx.hi) return;
+  const double wx = wsum<N>(dx, sw, gx / N, gx % N);
+  const double w0 = (own ? op.w[0] : 0.0) + (left ? op.w[N] : 0.0);
+  const int gyb = gy0 + e * N;
+  const size_t ux = (size_t)(gx - dx.lo);
+#pragma unroll
+  for (int a = A0; a < A1; a++) {
+    const int gy = gyb + a;
+    if (gy < dy.lo || gy >= dy.hi) continue;
+    const double wy = a == 0 ? w0 : op.w[a];
+    const size_t k = (size_t)(gy - dy.lo) * op.G[0] + ux;
+    const double cm = -op.alpha * wx * wy, cx = -op.beta[0] * wy, cy = -op.beta[1] * wx;
+    double hi = b[k], lo = 0.0;
+    dd_fma(hi, lo, cm, v[N + a]);
+    dd_fma(hi, lo, cx, OXH[(e * N + a) * OXP + c]);
+    lo = fma(cx, OXL[(e * N + a) * OXP + c], lo);
+    dd_fma(hi, lo, cy, yh[a - A0]);
+    lo = fma(cy, yl[a - A0], lo);
+    const double rv = hi + lo;
+    rout[k] = rv;
+    const double z = wv ? rv * wv[k] : rv;
+    acc0 += natural ? z * rv : z * z;
+    acc1 += rv * rv;
+    if (sp_hi) {
+      uint32_t h;
+      asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"((float)rv));
+      const float fh = __uint_as_float(h);
+      const size_t o = (size_t)(gy - dy.lo) * sp_pitch + ux;
+      sp_hi[o] = fh;
+      sp_lo[o] = (float)(rv - (double)fh);
+    }
+  }
+}
+
 template <int N>
 __global__ void __launch_bounds__(kEfThreads, 2)
     residual_ef_kernel(const OpDev op, const double* __restrict__ x, const double* __restrict__ b,
                        double* __restrict__ rout, const double* __restrict__ wv, int natural,
                        double* __restrict__ partial, const ResTail tail, float* __restrict__ sp_hi,
                        float* __restrict__ sp_lo, int sp_pitch) {
-  typedef EfTile<N> T;
-  constexpr int W = T::W, OXP = T::OXP, TX = T::TX, TY = T::TY, H = T::H;
+  typedef ResTile<N> T;
+  constexpr int W = T::W, OXP = T::OXP, TX = T::TX, TY = T::TY, H = T::H, CH = T::CH;
   extern __shared__ __align__(16) double efsm[];
   double* X = efsm;              // staged vertices
   double* OXH = X + H * W;       // x-pass stiffness sums, high parts
@@ -832,104 +947,36 @@ __global__ void __launch_bounds__(kEfThreads, 2)
   const Dir& dy = op.d[1];
   const int gx0 = blockIdx.x * TX, gy0 = blockIdx.y * TY;
   const int tid = threadIdx.x;
+  // share of the outputs (warp-uniform) and item of this thread
+  const int sub = tid / T::GROUP, item = tid - sub * T::GROUP;
   if (tid <= N) sw[tid] = op.w[tid];
-  ef_stage<N>(op, x, X, gx0, gy0);
+  ef_stage<N, H>(op, x, X, gx0, gy0);
   __syncthreads();
-  constexpr int n = N + 1;
-  if (tid < T::ITEMS) {  // x pass
-    const int r = tid % TY, e = tid / TY;
+  if (item < T::ITEMS) {  // x pass
+    const int r = item % TY, e = item / TY;
     const int ex = gx0 / N + e;
     const double* row = X + (r + N) * W + e * N;
-    double v[2 * N + 1];
-#pragma unroll
-    for (int k = 0; k <= 2 * N; k++) v[k] = row[k];
     const bool own = ex < dx.nE, left = ex > 0 || dx.periodic;
-    double oh[N], ol[N];
-#pragma unroll
-    for (int a = 0; a < N; a++) {
-      double hi = 0.0, lo = 0.0;
-      if (own) {
-#pragma unroll
-        for (int q = 0; q < n; q++) dd_fma(hi, lo, op.Kh[a * n + q], v[N + q]);
-      }
-      oh[a] = hi;
-      ol[a] = lo;
-    }
-    if (left) {
-      double hi = 0.0, lo = 0.0;
-#pragma unroll
-      for (int q = 0; q < n; q++) dd_fma(hi, lo, op.Kh[N * n + q], v[q]);
-      dd_add(oh[0], ol[0], hi);
-      ol[0] += lo;
-    }
-#pragma unroll
-    for (int a = 0; a < N; a++) {
-      OXH[r * OXP + e * N + a] = oh[a];
-      OXL[r * OXP + e * N + a] = ol[a];
-    }
+    double* oh = OXH + r * OXP + e * N;
+    double* ol = OXL + r * OXP + e * N;
+    if (kResSplit == 1 || sub == 0)
+      res_xpass<N, 0, CH>(op, row, own, left, oh, ol);
+    else
+      res_xpass<N, CH, N>(op, row, own, left, oh, ol);
   }
   __syncthreads();
   double acc0 = 0.0, acc1 = 0.0;
-  if (tid < T::ITEMS) {  // y pass, the combination and the residual
-    const int c = tid % TX, e = tid / TX;
+  if (item < T::ITEMS) {  // y pass, the combination and the residual
+    const int c = item % TX, e = item / TX;
     const int ey = gy0 / N + e;
-    const int gx = gx0 + c;
     const double* col = X + (e * N) * W + c + N;
-    double v[2 * N + 1];
-#pragma unroll
-    for (int k = 0; k <= 2 * N; k++) v[k] = col[k * W];
     const bool own = ey < dy.nE, left = ey > 0 || dy.periodic;
-    double yh[N], yl[N];
-#pragma unroll
-    for (int a = 0; a < N; a++) {
-      double hi = 0.0, lo = 0.0;
-      if (own) {
-#pragma unroll
-        for (int q = 0; q < n; q++) dd_fma(hi, lo, op.Kh[a * n + q], v[N + q]);
-      }
-      yh[a] = hi;
-      yl[a] = lo;
-    }
-    if (left) {
-      double hi = 0.0, lo = 0.0;
-#pragma unroll
-      for (int q = 0; q < n; q++) dd_fma(hi, lo, op.Kh[N * n + q], v[q]);
-      dd_add(yh[0], yl[0], hi);
-      yl[0] += lo;
-    }
-    if (gx >= dx.lo && gx < dx.hi) {
-      const double wx = wsum<N>(dx, sw, gx / N, gx % N);
-      const double w0 = (own ? op.w[0] : 0.0) + (left ? op.w[N] : 0.0);
-      const int gyb = gy0 + e * N;
-      const size_t ux = (size_t)(gx - dx.lo);
-#pragma unroll
-      for (int a = 0; a < N; a++) {
-        const int gy = gyb + a;
-        if (gy < dy.lo || gy >= dy.hi) continue;
-        const double wy = a == 0 ? w0 : op.w[a];
-        const size_t k = (size_t)(gy - dy.lo) * op.G[0] + ux;
-        const double cm = -op.alpha * wx * wy, cx = -op.beta[0] * wy, cy = -op.beta[1] * wx;
-        double hi = b[k], lo = 0.0;
-        dd_fma(hi, lo, cm, v[N + a]);
-        dd_fma(hi, lo, cx, OXH[(e * N + a) * OXP + c]);
-        lo = fma(cx, OXL[(e * N + a) * OXP + c], lo);
-        dd_fma(hi, lo, cy, yh[a]);
-        lo = fma(cy, yl[a], lo);
-        const double rv = hi + lo;
-        rout[k] = rv;
-        const double z = wv ? rv * wv[k] : rv;
-        acc0 += natural ? z * rv : z * z;
-        acc1 += rv * rv;
-        if (sp_hi) {
-          uint32_t h;
-          asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"((float)rv));
-          const float fh = __uint_as_float(h);
-          const size_t o = (size_t)(gy - dy.lo) * sp_pitch + ux;
-          sp_hi[o] = fh;
-          sp_lo[o] = (float)(rv - (double)fh);
-        }
-      }
-    }
+    if (kResSplit == 1 || sub == 0)
+      res_ypass<N, 0, CH>(op, col, OXH, OXL, sw, c, e, gx0 + c, gy0, own, left, b, rout, wv,
+                          natural, acc0, acc1, sp_hi, sp_lo, sp_pitch);
+    else
+      res_ypass<N, CH, N>(op, col, OXH, OXL, sw, c, e, gx0 + c, gy0, own, left, b, rout, wv,
+                          natural, acc0, acc1, sp_hi, sp_lo, sp_pitch);
   }
   // block sums in a fixed order
   const int lane = tid & 31, warp = tid >> 5;
@@ -997,7 +1044,7 @@ template <int N>
 cudaError_t launch_res_ef(const OpDev& op, const double* x, const double* b, double* r,
                           const double* w, int natural, double* partial, const ResTail& tail,
                           float* sh, float* sl, int sp, cudaStream_t s) {
-  typedef EfTile<N> T;
+  typedef ResTile<N> T;
   constexpr size_t smem = sizeof(double) * ((size_t)T::H * T::W + 2 * (size_t)T::TY * T::OXP + 16);
   if (smem > 48 * 1024) {
     static bool attr[64] = {};
@@ -1027,7 +1074,7 @@ bool residual_ef_supported(const OpDev& op) {
 namespace {
 template <int N>
 int res_ef_blocks(const OpDev& op) {
-  typedef EfTile<N> T;
+  typedef ResTile<N> T;
   return ((op.d[0].hi + T::TX - 1) / T::TX) * ((op.d[1].hi + T::TY - 1) / T::TY);
 }
 }  // namespace

@@ -272,6 +272,15 @@ struct FdmState {
 // iteration-0 test; sets the while-condition (1 = iterate).
 cudaError_t launch_fdm_init(const FdmParams* p, FdmState* st, const double* res,
                             cudaGraphConditionalHandle h, cudaStream_t s);
+// The prologue of an FDM solve in one launch (linsys.cu): f as
+// launch_rhs_assemble, r = f, x = 0, res = {norm^2 of f (weights w, natural
+// or not), |f|^2} and the loop's set-up as launch_fdm_init. partial holds at
+// least 2 * npart doubles; count is zero on entry and on return.
+cudaError_t launch_fdm_prologue(const OpDev& op, const MeshDev& m, const double* rhs_vals,
+                                const double* lift, double* f, double* r, double* x,
+                                const double* w, int natural, double* partial, int npart,
+                                double* res, unsigned* count, const FdmParams* p, FdmState* st,
+                                cudaGraphConditionalHandle h, cudaStream_t s);
 // After a refinement step: iteration count, the residual tests (RTOL, ATOL,
 // DTOL, NANORINF, ITS, and stagnation at the rounding floor) and the
 // while-condition.

@@ -65,20 +65,7 @@ __global__ void add_low_kernel(double* __restrict__ x, const T* __restrict__ y, 
 // ------------------------------------------------- refinement loop control --
 __global__ void fdm_init_kernel(const FdmParams* __restrict__ p, FdmState* __restrict__ st,
                                 const double* __restrict__ res, cudaGraphConditionalHandle h) {
-  const double dp = sqrt(fabs(res[0]));
-  st->rnorm0 = dp;
-  st->ttol = fmax(p->rtol * dp, p->atol);
-  st->dp = dp;
-  st->best = dp;
-  st->its = 0;
-  st->stalled = 0;
-  st->kerr = 0;
-  int reason = 0;
-  if (!(dp == dp) || isinf(dp)) reason = -9;
-  else if (dp <= st->ttol) reason = dp < p->atol ? 3 : 2;
-  else if (p->max_it <= 0) reason = -3;
-  st->reason = reason;
-  cudaGraphSetConditional(h, reason == 0 ? 1u : 0u);
+  fdm_init_state(p, st, res[0], h);
 }
 
 __global__ void fdm_check_kernel(const FdmParams* __restrict__ p, FdmState* __restrict__ st,

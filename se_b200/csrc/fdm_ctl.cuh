@@ -9,6 +9,28 @@
 
 namespace seg {
 
+// The loop's set-up from res0, the squared norm of the right-hand side:
+// rnorm0, the tolerance, the iteration-0 test; sets the while-condition
+// (1 = iterate).
+__device__ __forceinline__ void fdm_init_state(const FdmParams* __restrict__ p,
+                                               FdmState* __restrict__ st, double res0,
+                                               cudaGraphConditionalHandle h) {
+  const double dp = sqrt(fabs(res0));
+  st->rnorm0 = dp;
+  st->ttol = fmax(p->rtol * dp, p->atol);
+  st->dp = dp;
+  st->best = dp;
+  st->its = 0;
+  st->stalled = 0;
+  st->kerr = 0;
+  int reason = 0;
+  if (!(dp == dp) || isinf(dp)) reason = -9;
+  else if (dp <= st->ttol) reason = dp < p->atol ? 3 : 2;
+  else if (p->max_it <= 0) reason = -3;
+  st->reason = reason;
+  cudaGraphSetConditional(h, reason == 0 ? 1u : 0u);
+}
+
 __device__ __forceinline__ void fdm_check_state(const FdmParams* __restrict__ p,
                                                 FdmState* __restrict__ st, double res0,
                                                 cudaGraphConditionalHandle h) {

@@ -17,7 +17,10 @@
 // so the result is deterministic and needs no atomics.
 //
 // The persistent CG that drives this operator is in cg.cu.
+#include <algorithm>
+
 #include "common.cuh"
+#include "fdm_ctl.cuh"
 
 namespace seg {
 namespace {
@@ -123,11 +126,10 @@ __device__ __forceinline__ int contribs(const Dir& d, int g, int* v, int* side) 
   }
   return k;
 }
-__global__ void rhs_assemble_kernel(const OpDev op, const MeshDev m, const double* __restrict__ rhs,
-                                    const double* __restrict__ lift, double* __restrict__ f) {
-  const int ux = blockIdx.x * blockDim.x + threadIdx.x;
-  const int uy = blockIdx.y * blockDim.y + threadIdx.y;
-  if (ux >= op.G[0] || uy >= op.G[1]) return;
+// FieldRHS + Vector::Assemble at unknown (ux, uy), plus the lifting.
+__device__ __forceinline__ double rhs_value(const OpDev& op, const MeshDev& m,
+                                           const double* __restrict__ rhs,
+                                           const double* __restrict__ lift, int ux, int uy) {
   const Dir &dx = op.d[0], &dy = op.d[1];
   const int gx = ux + dx.lo, gy = uy + dy.lo;
   int vx[2], sx[2], vy[2], sy[2];
@@ -143,7 +145,92 @@ __global__ void rhs_assemble_kernel(const OpDev op, const MeshDev m, const doubl
     }
   }
   const size_t k = (size_t)uy * op.G[0] + ux;
-  f[k] = s + (lift ? lift[k] : 0.0);
+  return s + (lift ? lift[k] : 0.0);
+}
+__global__ void rhs_assemble_kernel(const OpDev op, const MeshDev m, const double* __restrict__ rhs,
+                                    const double* __restrict__ lift, double* __restrict__ f) {
+  const int ux = blockIdx.x * blockDim.x + threadIdx.x;
+  const int uy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ux >= op.G[0] || uy >= op.G[1]) return;
+  f[(size_t)uy * op.G[0] + ux] = rhs_value(op, m, rhs, lift, ux, uy);
+}
+
+// Fixed-order sum of two values over a 256-thread block; result in thread 0.
+__device__ __forceinline__ void block_sum2_256(double& a, double& b, double (*red)[2]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_down_sync(0xffffffffu, a, o);
+    b += __shfl_down_sync(0xffffffffu, b, o);
+  }
+  if (lane == 0) {
+    red[warp][0] = a;
+    red[warp][1] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = b = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      a += red[q][0];
+      b += red[q][1];
+    }
+  }
+}
+
+// The FDM solve's prologue in one launch: the right-hand side f (as
+// rhs_assemble_kernel), r = f, x = 0 and per-block partial sums of the
+// initial norms (of (w f)^2, or f w f when natural, and of f^2; w == nullptr
+// means w = 1); the block that arrives last sums the partials in block order
+// and runs the refinement loop's initial test, which sets its condition.
+// No block waits for another.
+__global__ void __launch_bounds__(256)
+    fdm_prologue_kernel(const OpDev op, const MeshDev m, const double* __restrict__ rhs,
+                        const double* __restrict__ lift, double* __restrict__ f,
+                        double* __restrict__ r, double* __restrict__ x,
+                        const double* __restrict__ w, int natural, double* __restrict__ partial,
+                        double* __restrict__ res, unsigned* __restrict__ count,
+                        const FdmParams* __restrict__ p, FdmState* __restrict__ st,
+                        cudaGraphConditionalHandle h) {
+  __shared__ double red[8][2];
+  __shared__ unsigned last;
+  const size_t n = (size_t)op.G[0] * op.G[1];
+  double s0 = 0.0, s1 = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const int uy = (int)(k / op.G[0]), ux = (int)(k - (size_t)uy * op.G[0]);
+    const double v = rhs_value(op, m, rhs, lift, ux, uy);
+    f[k] = v;
+    r[k] = v;
+    x[k] = 0.0;
+    const double z = w ? v * w[k] : v;
+    s0 = fma(z, natural ? v : z, s0);
+    s1 = fma(v, v, s1);
+  }
+  block_sum2_256(s0, s1, red);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = s0;
+    partial[2 * blockIdx.x + 1] = s1;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(count, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  s0 = s1 = 0.0;
+  for (unsigned k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+    s0 += __ldcg(partial + 2 * k);
+    s1 += __ldcg(partial + 2 * k + 1);
+  }
+  __syncthreads();
+  block_sum2_256(s0, s1, red);
+  if (threadIdx.x == 0) {
+    res[0] = s0;
+    res[1] = s1;
+    *count = 0u;
+    fdm_init_state(p, st, s0, h);
+  }
 }
 
 // Matrix::Assemble's Dirichlet lifting (src/base/Matrix.cpp:117-140):
@@ -215,6 +302,18 @@ cudaError_t launch_rhs_assemble(const OpDev& op, const MeshDev& m, const double*
                                 const double* lift, double* f, cudaStream_t s) {
   dim3 block(32, 8), grid((op.G[0] + 31) / 32, (op.G[1] + 7) / 8);
   rhs_assemble_kernel<<<grid, block, 0, s>>>(op, m, rhs_vals, lift, f);
+  return cudaGetLastError();
+}
+cudaError_t launch_fdm_prologue(const OpDev& op, const MeshDev& m, const double* rhs_vals,
+                                const double* lift, double* f, double* r, double* x,
+                                const double* w, int natural, double* partial, int npart,
+                                double* res, unsigned* count, const FdmParams* p, FdmState* st,
+                                cudaGraphConditionalHandle h, cudaStream_t s) {
+  const size_t n = (size_t)op.G[0] * op.G[1];
+  if (n == 0 || npart <= 0 || !count) return cudaErrorInvalidValue;
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)npart);
+  fdm_prologue_kernel<<<blocks, 256, 0, s>>>(op, m, rhs_vals, lift, f, r, x, w, natural, partial,
+                                             res, count, p, st, h);
   return cudaGetLastError();
 }
 cudaError_t launch_lift(const OpDev& op, const MeshDev& m, const double* sol_vals, double* lift,
