@@ -18,7 +18,7 @@ and one elliptic inversion to rtol.
          (CUDA events on the library's stream, L2 flushed between steps)
   e2e    the same through the public C-ABI with host buffers: every step
          uploads the tracer from page-locked host memory and downloads the
-         solution to it; four independent steps in flight on four streams,
+         solution to it; eight independent steps in flight on eight streams,
          so that one step's copies overlap the others' kernels (the
          one-at-a-time figure is reported beside it)
 
@@ -398,7 +398,7 @@ def run_gpu(args, rank, world):
             "tc_apply_ms": float(np.median(tc_ms)), "residual_ms": float(np.median(res_ms))}
 
 
-E2E_DEPTH = 4
+E2E_DEPTH = 8
 
 
 def e2e_pipelined(S, lib, m, bc, v, phi0, dt, opts, steps, warmup, stream0):
