@@ -959,7 +959,9 @@ __global__ void __launch_bounds__(kEfThreads, 2)
     const bool own = ex < dx.nE, left = ex > 0 || dx.periodic;
     double* oh = OXH + r * OXP + e * N;
     double* ol = OXL + r * OXP + e * N;
-    if (kResSplit == 1 || sub == 0)
+    if constexpr (kResSplit == 1)
+      res_xpass<N, 0, N>(op, row, own, left, oh, ol);
+    else if (sub == 0)
       res_xpass<N, 0, CH>(op, row, own, left, oh, ol);
     else
       res_xpass<N, CH, N>(op, row, own, left, oh, ol);
@@ -971,7 +973,10 @@ __global__ void __launch_bounds__(kEfThreads, 2)
     const int ey = gy0 / N + e;
     const double* col = X + (e * N) * W + c + N;
     const bool own = ey < dy.nE, left = ey > 0 || dy.periodic;
-    if (kResSplit == 1 || sub == 0)
+    if constexpr (kResSplit == 1)
+      res_ypass<N, 0, N>(op, col, OXH, OXL, sw, c, e, gx0 + c, gy0, own, left, b, rout, wv,
+                         natural, acc0, acc1, sp_hi, sp_lo, sp_pitch);
+    else if (sub == 0)
       res_ypass<N, 0, CH>(op, col, OXH, OXL, sw, c, e, gx0 + c, gy0, own, left, b, rout, wv,
                           natural, acc0, acc1, sp_hi, sp_lo, sp_pitch);
     else
