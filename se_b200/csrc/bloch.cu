@@ -79,20 +79,24 @@ __device__ __forceinline__ void load_twiddles(double2* tw, const double2* g, int
 
 // Row y = blockIdx.x of the real G_y x G_x array F: S[i][m] =
 // sum_e F(e, i) e^{-i th_m e}, then xh[(m, k) * gy + y] =
-// sum_i conj(V_m[i][k]) S[i][m] for m = 0..nel/2.
+// sum_i conj(V_m[i][k]) S[i][m] for m = 0..nel/2. With a gate whose reason
+// is already set (a refinement loop whose initial test decided), F is read
+// as zero, so that the inverse adds nothing.
 template <int P>
 __global__ void __launch_bounds__(kBlochThreads, 8) bloch_x_forward(BlochDir bx, int gy,
                                                                     const double* __restrict__ F,
-                                                                    double2* __restrict__ xh) {
+                                                                    double2* __restrict__ xh,
+                                                                    const FdmState* gate) {
   extern __shared__ double2 bsm[];
   const int nel = bx.nel, logn = bx.logn, gx = nel * P, mx = nel / 2 + 1;
   const int y = blockIdx.x;
   double2* S = bsm;            // [P][nel]
   double2* tw = bsm + P * nel;  // [nel/2]
   load_twiddles(tw, bx.tw, nel >> 1);
+  const bool closed = gate && *(volatile const int*)&gate->reason != 0;
   for (int t = threadIdx.x; t < gx; t += blockDim.x) {
     const int e = t / P, i = t - e * P;
-    S[i * nel + bitrev(e, logn)] = make_double2(F[(size_t)y * gx + t], 0.0);
+    S[i * nel + bitrev(e, logn)] = make_double2(closed ? 0.0 : F[(size_t)y * gx + t], 0.0);
   }
   __syncthreads();
   fft_seqs<P>(S, nel, logn, tw, false);
@@ -225,12 +229,12 @@ __global__ void __launch_bounds__(kBlochThreads, 8) bloch_x_backward(BlochDir bx
 template <int P>
 cudaError_t bloch_run(const BlochDir& bx, const BlochDir& by, double alpha, double cx, double cy,
                       double null_tol, const double* in, double* out, bool accumulate,
-                      double2* xh, cudaStream_t s) {
+                      double2* xh, const FdmState* gate, cudaStream_t s) {
   const int gy = by.nel * P, cols = (bx.nel / 2 + 1) * P;
   const size_t smx = sizeof(double2) * ((size_t)P * bx.nel + bx.nel / 2 + 1);
   const size_t smy = sizeof(double2) * (2 * (size_t)P * by.nel + by.nel / 2 + 1);
   if (smx > 48 * 1024 || smy > 48 * 1024) return cudaErrorInvalidValue;
-  bloch_x_forward<P><<<gy, kBlochThreads, smx, s>>>(bx, gy, in, xh);
+  bloch_x_forward<P><<<gy, kBlochThreads, smx, s>>>(bx, gy, in, xh, gate);
   bloch_y_solve<P><<<cols, kBlochThreads, smy, s>>>(bx, by, alpha, cx, cy, null_tol,
                                                     1.0 / ((double)bx.nel * by.nel), xh);
   bloch_x_backward<P><<<gy, kBlochThreads, smx, s>>>(bx, gy, xh, out, accumulate ? 1 : 0);
@@ -247,11 +251,12 @@ size_t bloch_spectrum_elems(const BlochDir& bx, const BlochDir& by) {
 // latency-bound, and one block per row keeps every SM's warp slots filled.
 cudaError_t launch_bloch_inverse(const BlochDir& bx, const BlochDir& by, double alpha, double cx,
                                  double cy, double null_tol, const double* in, double* out,
-                                 bool accumulate, double2* xh, cudaStream_t s) {
+                                 bool accumulate, double2* xh, const FdmState* gate,
+                                 cudaStream_t s) {
   if (bx.p != by.p) return cudaErrorInvalidValue;
 #define SE_BLOCH_P(n) \
   case n:             \
-    return bloch_run<n>(bx, by, alpha, cx, cy, null_tol, in, out, accumulate, xh, s);
+    return bloch_run<n>(bx, by, alpha, cx, cy, null_tol, in, out, accumulate, xh, gate, s);
   switch (bx.p) {
     SE_BLOCH_P(2) SE_BLOCH_P(3) SE_BLOCH_P(4) SE_BLOCH_P(5) SE_BLOCH_P(6) SE_BLOCH_P(7)
     SE_BLOCH_P(8) SE_BLOCH_P(9) SE_BLOCH_P(10) SE_BLOCH_P(11) SE_BLOCH_P(12)

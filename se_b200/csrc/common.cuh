@@ -347,9 +347,12 @@ struct BlochDir {
 // x (= or +=) A^{-1} in for a doubly periodic system by Bloch waves (three
 // launches); xh: bloch_spectrum_elems complex work. Shared memory limits:
 // 16 p nel bytes (x direction) and 32 p nel bytes (y) each at most 48 KB.
+// gate (nullable): a refinement loop's state; when its reason is set on
+// the device, in is read as zero (the step adds nothing).
 cudaError_t launch_bloch_inverse(const BlochDir& bx, const BlochDir& by, double alpha, double cx,
                                  double cy, double null_tol, const double* in, double* out,
-                                 bool accumulate, double2* xh, cudaStream_t s);
+                                 bool accumulate, double2* xh, const FdmState* gate,
+                                 cudaStream_t s);
 size_t bloch_spectrum_elems(const BlochDir& bx, const BlochDir& by);
 
 struct FdmLow {

@@ -34,6 +34,12 @@ __device__ __forceinline__ void fdm_init_state(const FdmParams* __restrict__ p,
 __device__ __forceinline__ void fdm_check_state(const FdmParams* __restrict__ p,
                                                 FdmState* __restrict__ st, double res0,
                                                 cudaGraphConditionalHandle h) {
+  // a loop already decided (the initial test, before a first step that the
+  // solve graph runs unconditionally): the decision and count stand
+  if (st->reason != 0) {
+    cudaGraphSetConditional(h, 0u);
+    return;
+  }
   const double dp = sqrt(fabs(res0));
   const int its = st->its + 1;
   st->its = its;
