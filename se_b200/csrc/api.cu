@@ -1368,7 +1368,8 @@ int fdm_apply64(se_linsys* ls, const double* in, double* out, bool accumulate,
   }
   const FdmLow low{ls->zlow, ls->SxT, gx, ls->lowk};
   CK(launch_fdm_gemm(0, 0, in, 1, ls->SxT, ls->X1, 1, gy, gx, gx, gx, gx, gx, nullptr, nullptr,
-                     nullptr, nullptr, 0, 0, 0, 0, g_stream));
+                     nullptr, nullptr, 0, 0, 0, 0, g_stream, nullptr,
+                     gate ? &gate->reason : nullptr));
   CK(launch_fdm_gemm(0, 1, ls->Sy, 1, ls->X1, ls->X2, 1, gy, gx, gy, gy, gx, gx, nullptr, nullptr,
                      ls->lx, ls->ly, op.alpha, op.beta[0], op.beta[1], nt, g_stream, &low));
   CK(launch_fdm_gemm(0, 0, ls->X2, 1, ls->Sx, ls->X1, 1, gy, gx, gx, gx, gx, gx, nullptr, nullptr,
@@ -1531,16 +1532,11 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
     cudaGraph_t cg = nullptr;
     const cudaGraphNode_t* deps = nullptr;
     size_t ndeps = 0;
-    // prec 3 (FP64 first step, tensor-core steps after): an IF node for the
-    // first step (condition hf, set by the initial test) and the while loop
-    // (condition hc, reset to 0 at every launch, set by each step's test);
-    // otherwise the while loop alone, its condition set by the initial test
-    const bool hybrid = prec == 3;
-    cudaGraphConditionalHandle hc, hf = 0;
+    // the while loop's condition hc: set by the initial test and by each
+    // step's test (prec 3: FP64 first step, tensor-core steps after)
+    cudaGraphConditionalHandle hc;
     bool ok = cudaStreamGetCaptureInfo(cs, &status, nullptr, &cg, &deps, &ndeps) == cudaSuccess &&
-              cudaGraphConditionalHandleCreate(&hc, cg, 0, hybrid ? cudaGraphCondAssignDefault : 0) ==
-                  cudaSuccess;
-    if (hybrid) ok = ok && cudaGraphConditionalHandleCreate(&hf, cg, 0, 0) == cudaSuccess;
+              cudaGraphConditionalHandleCreate(&hc, cg, 0, 0) == cudaSuccess;
     // prologue: without a null space to remove and with an FP64 first
     // inverse, one launch (f, r = f, x = 0, the initial norm and test);
     // otherwise the pieces one by one
@@ -1548,7 +1544,7 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
       ok = ok && launch_fdm_prologue(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f,
                                      ls->r, ls->x, wv, nt == SE_NORM_NATURAL, ls->fpart,
                                      kFdmPartials, res, ls->d_rescount, ls->d_fparams,
-                                     ls->d_fstate, hybrid ? hf : hc, cs) == cudaSuccess;
+                                     ls->d_fstate, hc, cs) == cudaSuccess;
     } else {
       ok = ok && launch_rhs_assemble(ls->op, m, ls->rhs ? ls->rhs->vals : nullptr, ls->lift, ls->f, cs) == cudaSuccess;
       // a right-hand side off the range of a singular operator: solve for the
@@ -1564,7 +1560,7 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
                                    ls->tc_px, cs) == cudaSuccess;
       ok = ok && cudaMemsetAsync(ls->x, 0, sizeof(double) * n, cs) == cudaSuccess;
       ok = ok && launch_norms(ls->f, wv, n, nt == SE_NORM_NATURAL, ls->fpart, kFdmPartials, res, cs) == cudaSuccess;
-      ok = ok && launch_fdm_init(ls->d_fparams, ls->d_fstate, res, hybrid ? hf : hc, cs) == cudaSuccess;
+      ok = ok && launch_fdm_init(ls->d_fparams, ls->d_fstate, res, hc, cs) == cudaSuccess;
     }
     // a conditional node after what was captured so far, its body captured on
     // stream bs by `fill`
@@ -1615,18 +1611,18 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
                   : SE_ERR_CUDA;
       return brc;
     };
-    // FP64 steps of a Bloch-form system: the first step as plain nodes of
-    // the graph (most solves need only it), the loop for the rest. A step
-    // whose initial test has decided adds nothing: the x pass reads the
-    // residual as zero and the test keeps the decision. The conditional
-    // node cost about 4 us a solve at 64x64 elements, p = 8.
-    if (prec == 0 && ls->bloch && ok) {
+    // An FP64 first step (prec 0 and 3) as plain nodes of the graph (most
+    // solves need only it), the loop for the rest: the conditional node
+    // cost about 4 us a solve at 64x64 elements, p = 8. A step whose
+    // initial test has decided adds nothing: its first pass (the Bloch x
+    // pass, or the first dense product) takes the residual as zero, and its
+    // test keeps the decision and the count.
+    if ((prec == 0 || prec == 3) && ok) {
       const cudaStream_t body_stream = bs;
       bs = cs;
       ok = step(0, ls->d_fstate) == SE_OK;
       bs = body_stream;
     }
-    if (hybrid) add_cond(hf, cudaGraphCondTypeIf, [&]() { return step(0, nullptr); });
     add_cond(hc, cudaGraphCondTypeWhile, [&]() { return step(prec == 3 ? 1 : prec, nullptr); });
     cudaGraph_t body = bodies.empty() ? nullptr : bodies.back();
     // epilogue

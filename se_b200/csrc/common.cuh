@@ -364,7 +364,8 @@ cudaError_t launch_fdm_gemm(int prec, int epi, const void* A, int a_fp64, const 
                             int c_fp64, int M, int N, int K, int lda, int ldb, int ldc,
                             const double* amax, const double* cmax, const double* lx,
                             const double* ly, double alpha, double bx, double by, double null_tol,
-                            cudaStream_t s, const FdmLow* low = nullptr);
+                            cudaStream_t s, const FdmLow* low = nullptr,
+                            const int* gate = nullptr);
 
 // Fast-diagonalization pieces (fdm.cu). prec: 0 FP64, 1 FP32, 2 BF16.
 cudaError_t launch_spectral_divide(int prec, void* v, int gx, int gy, const double* lx,

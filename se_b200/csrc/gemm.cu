@@ -127,6 +127,9 @@ struct GemmArgs {
   double* zlow;
   const double* ex;
   int ldex, lowk;
+  // FP64 plain stores: when *gate != 0 (a refinement loop that has already
+  // decided) the product is stored as zero; nullptr: no gate
+  const int* gate;
 };
 
 enum { EPI_STORE = 0, EPI_DIVIDE = 1, EPI_ACCUM = 2 };
@@ -412,6 +415,7 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_kernel(const GemmArgs<do
   extern __shared__ __align__(16) double dsm[];
   double* As = dsm;
   double* Bs = dsm + C::ST * C::A_ELEMS;
+  const bool closed = EPI == EPI_STORE && g.gate && *g.gate != 0;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   const int wm = (warp / C::WN) * (C::BM / C::WM), wn = (warp % C::WN) * (C::BN / C::WN);
@@ -524,7 +528,7 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_kernel(const GemmArgs<do
           if constexpr (EPI == EPI_ACCUM)
             *dst += v;
           else
-            *dst = v;
+            *dst = closed ? 0.0 : v;
         }
       }
 }
@@ -574,6 +578,7 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_ksplit_kernel(
   extern __shared__ __align__(16) double dsm[];
   double* As = dsm;
   double* Bs = dsm + C::ST * C::A_ELEMS;
+  const bool closed = EPI == EPI_STORE && g.gate && *g.gate != 0;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   const int m0 = blockIdx.y * C::BM, n0 = blockIdx.x * C::BN;
@@ -690,7 +695,7 @@ __global__ void __launch_bounds__(C::THREADS) fdm_dgemm_ksplit_kernel(
     if constexpr (EPI == EPI_ACCUM)
       *dst += v;
     else
-      *dst = v;
+      *dst = closed ? 0.0 : v;
   }
 }
 
@@ -747,12 +752,13 @@ cudaError_t launch_fdm_gemm(int prec, int epi, const void* A, int a_fp64, const 
                             int c_fp64, int M, int N, int K, int lda, int ldb, int ldc,
                             const double* amax, const double* cmax, const double* lx,
                             const double* ly, double alpha, double bx, double by, double null_tol,
-                            cudaStream_t s, const FdmLow* low) {
+                            cudaStream_t s, const FdmLow* low, const int* gate) {
 #define SE_GEMM_ARGS(TA, TB, TC)                                                              \
   GemmArgs<TA, TB, TC> g{(const TA*)A, (const TB*)B, (TC*)C, M, N, K, lda, ldb, ldc, amax, cmax, \
-                         lx, ly, alpha, bx, by, null_tol, nullptr, nullptr, 0, 0}
+                         lx, ly, alpha, bx, by, null_tol, nullptr, nullptr, 0, 0, nullptr}
   if (prec == 0) {
     SE_GEMM_ARGS(double, double, double);
+    g.gate = gate;
     if (low && low->k > 0) {
       if (low->k > kLowMax || !low->zlow || (epi != EPI_DIVIDE && !low->ex))
         return cudaErrorInvalidValue;

@@ -362,32 +362,42 @@ def test_poisson_null_space(segpu, oracle):
     assert segpu.load_library().se_linsys_solve(ls._h, 3, None) == segpu.SE_ERR_ARG
 
 
-def test_fdm_bloch_first_step_keeps_initial_decision(segpu, oracle):
-    """The FP64 Bloch-form solve runs its first refinement step outside the
-    refinement loop. When the initial test has already decided, that step
-    adds nothing. With max_it = 0 the FDM solve ends as the CG drop-in does:
-    reason -3 (ITS) at iteration 0 with the zero initial guess. A zero
-    right-hand side converges at iteration 0 with a zero solution, and the
-    next solve of the same system converges as before."""
-    om, m, fs, fr, ls, *_ = build(segpu, oracle, CASES_BLOCH[0], -3.0, -1.0, 1.0, False, seed=5)
-    for method in (segpu.METHOD_FDM, segpu.METHOD_CG):
-        fs.vals = 1.0  # doubly periodic: every vertex is overwritten by the solve
-        ls.set_opts(segpu.solver_opts(rtol=1e-10, max_it=0, method=method,
-                                      mode=segpu.MODE_EXACT))
+@pytest.mark.parametrize("case", [CASES_BLOCH[0], CASES[1]], ids=["bloch", "dense-channel"])
+@pytest.mark.parametrize("prec", ["PREC_FP64", "PREC_FP64_TC"])
+def test_fdm_first_step_keeps_initial_decision(segpu, oracle, case, prec):
+    """FP64 first refinement steps run outside the refinement loop (the
+    Bloch form and the dense inverse; FP64 and FP64-then-tensor-core). When
+    the initial test has already decided, that step adds nothing. With
+    max_it = 0 the FDM solve ends as the CG drop-in does: reason -3 (ITS) at
+    iteration 0, the same field (zero initial guess, Dirichlet values kept).
+    A zero right-hand side with zero boundary values converges at iteration
+    0 with a zero solution. The next solve of the same system converges to
+    the oracle's solution as before."""
+    om, m, fs, fr, ls, *_ = build(segpu, oracle, case, -3.0, -1.0, 1.0, False, seed=5)
+    sol0, rhs = fs.vals.copy(), fr.vals.copy()
+    fdm = dict(rtol=1e-10, method=segpu.METHOD_FDM, precision=getattr(segpu, prec),
+               mode=segpu.MODE_EXACT)
+    fields = []
+    for opts in (dict(fdm, max_it=0), dict(rtol=1e-10, max_it=0, mode=segpu.MODE_EXACT)):
+        fs.vals = sol0
+        ls.set_opts(segpu.solver_opts(**opts))
+        ls.Assemble()
         st = ls.Solve("helm_")
-        assert st["reason"] == -3 and st["its"] == 0, (method, st)
-        assert np.abs(fs.vals).max() == 0.0
-    rhs = fr.vals.copy()
-    fr.vals = 0.0
-    ls.set_opts(segpu.solver_opts(rtol=1e-10, method=segpu.METHOD_FDM, mode=segpu.MODE_EXACT))
+        assert st["reason"] == -3 and st["its"] == 0, (opts, st)
+        fields.append(fs.vals.copy())
+    assert np.array_equal(fields[0], fields[1])
+    fs.vals, fr.vals = 0.0, 0.0
+    ls.set_opts(segpu.solver_opts(**fdm))
+    ls.Assemble()
     st = ls.Solve("helm_")
     assert st["its"] == 0 and st["reason"] in (2, 3), st
     assert np.abs(fs.vals).max() == 0.0
-    fr.vals = rhs
+    fs.vals, fr.vals = sol0, rhs
+    ls.Assemble()
     st = ls.Solve("helm_")
-    assert st["reason"] == 2 and st["its"] <= 2, st
-    ref_sol, _ = oracle.helmholtz_solve(om, np.zeros(om.nv), rhs, -3.0, -1.0, 1.0,
-                                        bcs=CASES_BLOCH[0][6], quirk=False, rtol=1e-14)
+    assert st["reason"] == 2 and st["its"] <= 4, st
+    ref_sol, _ = oracle.helmholtz_solve(om, sol0, rhs, -3.0, -1.0, 1.0, bcs=case[6], quirk=False,
+                                        rtol=1e-14)
     assert np.abs(fs.vals - ref_sol).max() <= 1e-8 * np.abs(ref_sol).max()
 
 
