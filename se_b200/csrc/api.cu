@@ -297,6 +297,10 @@ struct se_linsys {
   unsigned* d_rescount;  // arrival counter of the fused residual + test (zero between launches)
   FdmParams* h_fparams;  // pinned host copies for asynchronous transfers
   FdmState* h_fstate;
+  // device address of h_fstate when the pinned buffer is mapped (the solve
+  // graph's last kernel then writes the state there), else null
+  FdmState* h_fstate_dev;
+  bool fdm_state_mapped;  // the current solve graph writes h_fstate_dev
   FdmParams fparams_last;    // the parameters in d_fparams
   bool fparams_sent;         // d_fparams holds fparams_last
   int async_pending;       // 1: FDM solve queued; 2: synchronous result held
@@ -1626,7 +1630,9 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
     add_cond(hc, cudaGraphCondTypeWhile, [&]() { return step(prec == 3 ? 1 : prec, nullptr); });
     cudaGraph_t body = bodies.empty() ? nullptr : bodies.back();
     // epilogue
-    ok = ok && launch_update_field(ls->op, m, ls->x, ls->sol->vals, cs) == cudaSuccess;
+    // (and the loop state to the mapped host buffer, when there is one)
+    ok = ok && launch_update_field(ls->op, m, ls->x, ls->sol->vals, cs, ls->d_fstate,
+                                   ls->h_fstate_dev) == cudaSuccess;
     const bool ended = cudaStreamEndCapture(cs, &graph) == cudaSuccess;
     if (!ok || !ended) {
       cudaGetLastError();
@@ -1642,6 +1648,7 @@ int fdm_build_graph(se_linsys* ls, int prec, int remove_null) {
       break;
     }
     ls->fdm_key = prec | (remove_null << 2) | (nt << 3) | (ls->opts.mode << 6);
+    ls->fdm_state_mapped = ls->h_fstate_dev != nullptr;
   } while (0);
   if (graph) cudaGraphDestroy(graph);
   cleanup();
@@ -1664,14 +1671,22 @@ int fdm_launch(se_linsys* ls, int remove_null, bool upload_params) {
   const int prec = pr == SE_PREC_FP64 ? 0 : pr == SE_PREC_MIXED ? 1 : pr == SE_PREC_FP64_TC ? 3 : 2;
   if (int rc = fdm_setup(ls, prec == 3 ? 1 : prec)) return rc;
   const int key = prec | ((remove_null != 0) << 2) | (ls->opts.norm_type << 3) | (ls->opts.mode << 6);
-  if (!ls->fdm_exec || ls->fdm_key != key)
-    if (int rc = fdm_build_graph(ls, prec, remove_null != 0)) return rc;
   if (!ls->h_fparams) {
+    // page-locked and mapped: the state comes back through the graph's last
+    // kernel instead of a copy; a buffer that cannot be mapped falls back to
+    // the copy
     void* p = nullptr;
-    CK(cudaMallocHost(&p, sizeof(FdmParams) + sizeof(FdmState)));
+    CK(cudaHostAlloc(&p, sizeof(FdmParams) + sizeof(FdmState), cudaHostAllocMapped));
     ls->h_fparams = static_cast<FdmParams*>(p);
     ls->h_fstate = reinterpret_cast<FdmState*>(ls->h_fparams + 1);
+    void* dp = nullptr;
+    if (cudaHostGetDevicePointer(&dp, p, 0) == cudaSuccess && dp)
+      ls->h_fstate_dev = reinterpret_cast<FdmState*>(static_cast<FdmParams*>(dp) + 1);
+    else
+      cudaGetLastError();
   }
+  if (!ls->fdm_exec || ls->fdm_key != key)
+    if (int rc = fdm_build_graph(ls, prec, remove_null != 0)) return rc;
   if (!ls->ev[2]) {
     for (cudaEvent_t& e : ls->ev)
       if (!e) CK(cudaEventCreate(&e));
@@ -1691,7 +1706,8 @@ int fdm_launch(se_linsys* ls, int remove_null, bool upload_params) {
   CK(cudaEventRecord(ls->ev[0], g_stream));
   CK(cudaGraphLaunch(ls->fdm_exec, g_stream));
   CK(cudaEventRecord(ls->ev[1], g_stream));
-  CK(cudaMemcpyAsync(ls->h_fstate, ls->d_fstate, sizeof(FdmState), cudaMemcpyDeviceToHost, g_stream));
+  if (!ls->fdm_state_mapped)
+    CK(cudaMemcpyAsync(ls->h_fstate, ls->d_fstate, sizeof(FdmState), cudaMemcpyDeviceToHost, g_stream));
   CK(cudaEventRecord(ls->ev[2], g_stream));
   return SE_OK;
 }

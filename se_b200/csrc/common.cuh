@@ -201,9 +201,12 @@ cudaError_t launch_rhs_assemble(const OpDev& op, const MeshDev& m, const double*
 // lift = -A[unknowns, Dirichlet] * sol_vals[Dirichlet].
 cudaError_t launch_lift(const OpDev& op, const MeshDev& m, const double* sol_vals, double* lift,
                         cudaStream_t s);
-// sol_vals[unknown vertices and their periodic copies] = x.
+// sol_vals[unknown vertices and their periodic copies] = x; with st and
+// st_host (the device address of a mapped page-locked buffer) also
+// *st_host = *st.
 cudaError_t launch_update_field(const OpDev& op, const MeshDev& m, const double* x,
-                                double* sol_vals, cudaStream_t s);
+                                double* sol_vals, cudaStream_t s, const FdmState* st = nullptr,
+                                FdmState* st_host = nullptr);
 
 // Persistent CG over a batch of solves.
 struct CgSolve {

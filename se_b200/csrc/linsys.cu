@@ -272,10 +272,18 @@ __global__ void lift_kernel(const OpDev op, const MeshDev m, const double* __res
 }
 
 // Vector::UpdateField (src/base/Vector.cpp:40-61) with the periodic copies.
+// Also copies a refinement loop's final state st to st_host (a mapped
+// page-locked buffer) when both are given: the solve graph's last kernel
+// returns the state without a separate copy.
 __global__ void update_field_kernel(const OpDev op, const MeshDev m, const double* __restrict__ x,
-                                    double* __restrict__ sol) {
+                                    double* __restrict__ sol, const FdmState* __restrict__ st,
+                                    FdmState* st_host) {
   const int ux = blockIdx.x * blockDim.x + threadIdx.x;
   const int uy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (st && st_host && ux == 0 && uy == 0) {
+    *st_host = *st;
+    __threadfence_system();
+  }
   if (ux >= op.G[0] || uy >= op.G[1]) return;
   const int gx = ux + op.d[0].lo, gy = uy + op.d[1].lo;
   const int nvx = m.nVerts[0], nvy = m.nVerts[1];
@@ -323,9 +331,10 @@ cudaError_t launch_lift(const OpDev& op, const MeshDev& m, const double* sol_val
   return cudaGetLastError();
 }
 cudaError_t launch_update_field(const OpDev& op, const MeshDev& m, const double* x,
-                                double* sol_vals, cudaStream_t s) {
+                                double* sol_vals, cudaStream_t s, const FdmState* st,
+                                FdmState* st_host) {
   dim3 block(32, 8), grid((op.G[0] + 31) / 32, (op.G[1] + 7) / 8);
-  update_field_kernel<<<grid, block, 0, s>>>(op, m, x, sol_vals);
+  update_field_kernel<<<grid, block, 0, s>>>(op, m, x, sol_vals, st, st_host);
   return cudaGetLastError();
 }
 
