@@ -468,11 +468,11 @@ def e2e_pipelined(S, lib, m, bc, v, phi0, dt, opts, steps, warmup, stream0):
 
 
 # Kernels of the library launched per headline step: SL advection; in the
-# FDM solve graph the right-hand side assembly, the initial norm (partials and
-# final) and test, per refinement step (one here) the three Bloch-form inverse
-# kernels and one residual kernel that also forms the norm and runs the
-# convergence test, then the field update.
-GPU_LAUNCHES_FIXED = 1 + (1 + 2 + 1) + 1
+# FDM solve graph the prologue (right-hand side, r = f, x = 0, the initial
+# norm and test in one kernel), per refinement step (one here) the three
+# Bloch-form inverse kernels and one residual kernel that also forms the
+# norm and runs the convergence test, then the field update.
+GPU_LAUNCHES_FIXED = 1 + 1 + 1
 GPU_LAUNCHES_PER_REFINEMENT = 3 + 1
 
 
