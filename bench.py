@@ -471,8 +471,9 @@ def e2e_pipelined(S, lib, m, bc, v, phi0, dt, opts, steps, warmup, stream0):
 # FDM solve graph the prologue (right-hand side, r = f, x = 0, the initial
 # norm and test in one kernel), per refinement step (one here) the three
 # Bloch-form inverse kernels and one residual kernel that also forms the
-# norm and runs the convergence test, then the field update.
-GPU_LAUNCHES_FIXED = 1 + 1 + 1
+# norm and runs the convergence test, then the field update; the copy of the
+# advected field back into the tracer (se_field_copy's copy kernel).
+GPU_LAUNCHES_FIXED = 1 + 1 + 1 + 1
 GPU_LAUNCHES_PER_REFINEMENT = 3 + 1
 
 

@@ -2111,8 +2111,8 @@ int se_field_copy(se_field* dst, const se_field* src) {
   if (int rc = check_field(src)) return rc;
   if (dst->mesh->nVertsTotal != src->mesh->nVertsTotal || dst->ndofs != src->ndofs)
     return fail(SE_ERR_ARG, "field shapes differ");
-  CK(cudaMemcpyAsync(dst->vals, src->vals, sizeof(double) * dst->mesh->nVertsTotal * dst->ndofs,
-                     cudaMemcpyDeviceToDevice, g_stream));
+  if (dst == src) return SE_OK;
+  CK(launch_copy(dst->vals, src->vals, (size_t)dst->mesh->nVertsTotal * dst->ndofs, g_stream));
   return SE_OK;
 }
 int se_field_periodic_update(se_field* field) {

@@ -201,6 +201,8 @@ cudaError_t launch_rhs_assemble(const OpDev& op, const MeshDev& m, const double*
 // lift = -A[unknowns, Dirichlet] * sol_vals[Dirichlet].
 cudaError_t launch_lift(const OpDev& op, const MeshDev& m, const double* sol_vals, double* lift,
                         cudaStream_t s);
+// dst[0, n) = src[0, n) on the stream (device arrays that do not overlap).
+cudaError_t launch_copy(double* dst, const double* src, size_t n, cudaStream_t s);
 // sol_vals[unknown vertices and their periodic copies] = x; with st and
 // st_host (the device address of a mapped page-locked buffer) also
 // *st_host = *st.

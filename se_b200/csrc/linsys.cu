@@ -272,6 +272,17 @@ __global__ void lift_kernel(const OpDev op, const MeshDev m, const double* __res
 }
 
 // Vector::UpdateField (src/base/Vector.cpp:40-61) with the periodic copies.
+// dst = src over n2 16-byte pairs and, with an odd count, the last value.
+__global__ void __launch_bounds__(256) copy_pairs_kernel(double2* __restrict__ dst,
+                                                         const double2* __restrict__ src,
+                                                         size_t n2, double* __restrict__ dlast,
+                                                         const double* __restrict__ slast) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n2;
+       k += (size_t)gridDim.x * blockDim.x)
+    dst[k] = src[k];
+  if (dlast && blockIdx.x == 0 && threadIdx.x == 0) *dlast = *slast;
+}
+
 // Also copies a refinement loop's final state st to st_host (a mapped
 // page-locked buffer) when both are given: the solve graph's last kernel
 // returns the state without a separate copy.
@@ -322,6 +333,20 @@ cudaError_t launch_fdm_prologue(const OpDev& op, const MeshDev& m, const double*
   const int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)npart);
   fdm_prologue_kernel<<<blocks, 256, 0, s>>>(op, m, rhs_vals, lift, f, r, x, w, natural, partial,
                                              res, count, p, st, h);
+  return cudaGetLastError();
+}
+cudaError_t launch_copy(double* dst, const double* src, size_t n, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  // a copy kernel over 16-byte pairs when both ends are 16-byte aligned
+  // (its launch waits less than the driver's device-to-device copy)
+  if (((reinterpret_cast<uintptr_t>(dst) | reinterpret_cast<uintptr_t>(src)) & 15u) != 0)
+    return cudaMemcpyAsync(dst, src, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+  const size_t n2 = n / 2;
+  const int blocks = (int)std::min<size_t>(std::max<size_t>((n2 + 255) / 256, 1), 148 * 8);
+  copy_pairs_kernel<<<blocks, 256, 0, s>>>(reinterpret_cast<double2*>(dst),
+                                           reinterpret_cast<const double2*>(src), n2,
+                                           (n & 1) ? dst + n - 1 : nullptr,
+                                           (n & 1) ? src + n - 1 : nullptr);
   return cudaGetLastError();
 }
 cudaError_t launch_lift(const OpDev& op, const MeshDev& m, const double* sol_vals, double* lift,
